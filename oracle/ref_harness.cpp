@@ -1,0 +1,248 @@
+// Harness that drives the reference Bridge++ corelib CPU path (compiled from
+// its own sources by oracle/Makefile.ref) so that its outputs can serve as
+// golden vectors for the oracle and as the timed CPU baseline.
+//
+// This file is test infrastructure: nothing in the product links it.
+//
+// Usage:  ref_harness <command> <params.txt> <in_dir> <out_dir>
+//
+// params.txt holds "key value [value...]" lines:
+//   lattice Nx Ny Nz Nt      Ls n      mq x      M0 x      b x     c x
+//   alpha x                  bc bx by bz bt      threads n
+//   tol x (squared)          maxiter n           sigma s0 s1 ...
+//   reps n                   modes Deo Doe ...
+// Inputs (raw little-endian float64):
+//   in_dir/gauge.bin  lexical links, Field_G(Nvol, 4) layout
+//                     re/im + 2*(col + 3*row) + 18*(site + Nvol*mu)
+//   in_dir/src.bin    5D half-lattice spinor, Field(24, Nvol/2, Ls) layout
+//                     re/im + 2*(color + 3*spin) + 24*(site + Nvol2*s)
+// Commands:
+//   modes   : applies AFopr_Domainwall_eo<Field>::mult / mult_dag for every
+//             listed mode (reference src/lib/Fopr/afopr_Domainwall_eo-tmpl.h)
+//             and writes out_dir/<mode>.bin ("dag_<mode>" for mult_dag).
+//   cg      : Solver_CG on mode DdagD (src/lib/Solver/solver_CG.cpp), writes
+//             out_dir/cg_x.bin and out_dir/cg_info.txt.
+//   shiftcg : Shiftsolver_CG on DdagD + sigma_i (src/lib/Solver/
+//             shiftsolver_CG.cpp), writes out_dir/shift_<i>.bin.
+//   time    : times `reps` applications of mode(s) inside an OpenMP parallel
+//             region, prints "mode seconds_per_call".
+
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <string>
+#include <sstream>
+#include <fstream>
+#include <vector>
+#include <chrono>
+
+#include "bridge_setup.h"
+#include "Parameters/parameters.h"
+#include "Parameters/commonParameters.h"
+#include "ResourceManager/threadManager.h"
+#include "Field/field.h"
+#include "Field/field_G.h"
+#include "Field/field_F.h"
+#include "Fopr/fopr_Domainwall_eo.h"
+#include "Solver/solver_CG.h"
+#include "Solver/shiftsolver_CG.h"
+#include "IO/bridgeIO.h"
+
+using Bridge::vout;
+
+namespace {
+
+typedef std::map<std::string, std::vector<std::string> > Kv;
+
+Kv read_params(const char *path)
+{
+  Kv kv;
+  std::ifstream f(path);
+  std::string line;
+  while (std::getline(f, line)) {
+    std::istringstream is(line);
+    std::string key;
+    if (!(is >> key) || key[0] == '#') continue;
+    std::vector<std::string> vals;
+    std::string v;
+    while (is >> v) vals.push_back(v);
+    kv[key] = vals;
+  }
+  return kv;
+}
+
+double getd(const Kv& kv, const char *k, double def)
+{
+  Kv::const_iterator it = kv.find(k);
+  return (it == kv.end() || it->second.empty()) ? def : atof(it->second[0].c_str());
+}
+
+int geti(const Kv& kv, const char *k, int def)
+{
+  Kv::const_iterator it = kv.find(k);
+  return (it == kv.end() || it->second.empty()) ? def : atoi(it->second[0].c_str());
+}
+
+std::vector<int> getiv(const Kv& kv, const char *k)
+{
+  std::vector<int> r;
+  Kv::const_iterator it = kv.find(k);
+  if (it != kv.end())
+    for (size_t i = 0; i < it->second.size(); ++i) r.push_back(atoi(it->second[i].c_str()));
+  return r;
+}
+
+void read_bin(const std::string& path, double *p, size_t n)
+{
+  FILE *f = fopen(path.c_str(), "rb");
+  if (!f) { fprintf(stderr, "cannot open %s\n", path.c_str()); exit(2); }
+  size_t got = fread(p, sizeof(double), n, f);
+  fclose(f);
+  if (got != n) { fprintf(stderr, "short read %s: %zu of %zu\n", path.c_str(), got, n); exit(2); }
+}
+
+void write_bin(const std::string& path, const double *p, size_t n)
+{
+  FILE *f = fopen(path.c_str(), "wb");
+  if (!f) { fprintf(stderr, "cannot write %s\n", path.c_str()); exit(2); }
+  fwrite(p, sizeof(double), n, f);
+  fclose(f);
+}
+
+Parameters dwf_params(const Kv& kv)
+{
+  Parameters p;
+  p.set_string("kernel_type", "Wilson");
+  p.set_string("gamma_matrix_type", "Dirac");
+  p.set_double("quark_mass", getd(kv, "mq", 0.01));
+  p.set_double("domain_wall_height", getd(kv, "M0", 1.8));
+  p.set_int("extent_of_5th_dimension", geti(kv, "Ls", 8));
+  std::vector<int> bc = getiv(kv, "bc");
+  if (bc.size() != 4) { bc.assign(4, 1); bc[3] = -1; }
+  p.set_int_vector("boundary_condition", bc);
+  p.set_double("coefficient_b", getd(kv, "b", 1.0));
+  p.set_double("coefficient_c", getd(kv, "c", 0.0));
+  p.set_double("parameter_alpha", getd(kv, "alpha", 1.0));
+  p.set_string("verbose_level", "Crucial");
+  return p;
+}
+
+}  // namespace
+
+int main(int argc, char **argv)
+{
+  if (argc < 5) {
+    fprintf(stderr, "usage: %s <modes|cg|shiftcg|time> params.txt in_dir out_dir\n", argv[0]);
+    return 2;
+  }
+  const std::string cmd = argv[1];
+  Kv kv = read_params(argv[2]);
+  const std::string in_dir = argv[3], out_dir = argv[4];
+
+  std::vector<int> lat = getiv(kv, "lattice");
+  if (lat.size() != 4) { fprintf(stderr, "lattice missing\n"); return 2; }
+  std::vector<int> grid(4, 1);
+  const int nthreads = geti(kv, "threads", 1);
+
+  int one = 1;
+  char *fake_argv0 = argv[0];
+  char **fake_argv = &fake_argv0;
+  bridge_initialize(&one, &fake_argv);
+  bridge_setup(lat, grid, nthreads, 3, "stdout", "Crucial");
+
+  const int Nvol = CommonParameters::Nvol();
+  const int Nvol2 = Nvol / 2;
+  const int Ls = geti(kv, "Ls", 8);
+
+  Field_G U(Nvol, 4);
+  read_bin(in_dir + "/gauge.bin", U.ptr(0), size_t(18) * Nvol * 4);
+
+  Parameters pf = dwf_params(kv);
+  Fopr_Domainwall_eo fopr(pf);
+  fopr.set_config(&U);
+
+  const size_t nsp = size_t(24) * Nvol2 * Ls;
+  Field src(24, Nvol2, Ls), out(24, Nvol2, Ls);
+  read_bin(in_dir + "/src.bin", src.ptr(0), nsp);
+
+  Kv::const_iterator mit = kv.find("modes");
+  std::vector<std::string> modes;
+  if (mit != kv.end()) modes = mit->second;
+
+  if (cmd == "modes") {
+    for (size_t i = 0; i < modes.size(); ++i) {
+      std::string m = modes[i];
+      bool dag = false;
+      if (m.compare(0, 4, "dag_") == 0) { dag = true; m = m.substr(4); }
+      out.set(0.0);
+      if (m == "Deo" || m == "Doe" || m == "Dee" || m == "Doo" ||
+          m == "Dee_inv" || m == "Doo_inv") {
+        if (dag) fopr.mult_dag(out, src, m); else fopr.mult(out, src, m);
+      } else if (m == "gm5R") {
+        fopr.mult_gm5R(out, src);
+      } else if (m == "R") {
+        fopr.mult_R(out, src);
+      } else {
+        fopr.set_mode(m);
+        if (dag) fopr.mult_dag(out, src); else fopr.mult(out, src);
+      }
+      write_bin(out_dir + "/" + modes[i] + ".bin", out.ptr(0), nsp);
+    }
+  } else if (cmd == "cg") {
+    fopr.set_mode("DdagD");
+    Solver_CG solver(&fopr);
+    solver.set_parameters(geti(kv, "maxiter", 10000), 1, getd(kv, "tol", 1e-20), false);
+    int nconv = 0;
+    double diff = 0.0;
+    solver.solve(out, src, nconv, diff);
+    write_bin(out_dir + "/cg_x.bin", out.ptr(0), nsp);
+    FILE *f = fopen((out_dir + "/cg_info.txt").c_str(), "w");
+    fprintf(f, "nconv %d\ndiff %.17e\n", nconv, diff);
+    fclose(f);
+  } else if (cmd == "shiftcg") {
+    fopr.set_mode("DdagD");
+    Kv::const_iterator sit = kv.find("sigma");
+    std::vector<double> sigma;
+    for (size_t i = 0; i < sit->second.size(); ++i) sigma.push_back(atof(sit->second[i].c_str()));
+    Shiftsolver_CG solver(&fopr, geti(kv, "maxiter", 10000), getd(kv, "tol", 1e-20));
+    std::vector<Field> xs(sigma.size(), Field(24, Nvol2, Ls));
+    int nconv = 0;
+    double diff = 0.0;
+    solver.solve(xs, sigma, src, nconv, diff);
+    for (size_t i = 0; i < sigma.size(); ++i) {
+      char name[64];
+      snprintf(name, sizeof(name), "/shift_%zu.bin", i);
+      write_bin(out_dir + name, xs[i].ptr(0), nsp);
+    }
+    FILE *f = fopen((out_dir + "/shift_info.txt").c_str(), "w");
+    fprintf(f, "nconv %d\ndiff %.17e\n", nconv, diff);
+    fclose(f);
+  } else if (cmd == "time") {
+    const int reps = geti(kv, "reps", 10);
+    for (size_t i = 0; i < modes.size(); ++i) {
+      const std::string m = modes[i];
+      fopr.set_mode(m == "Deo" || m == "Doe" ? std::string("D") : m);
+      // one untimed call to touch memory
+#pragma omp parallel
+      {
+        if (m == "Deo" || m == "Doe") fopr.mult(out, src, m); else fopr.mult(out, src);
+      }
+      std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+#pragma omp parallel
+      {
+        for (int r = 0; r < reps; ++r) {
+          if (m == "Deo" || m == "Doe") fopr.mult(out, src, m); else fopr.mult(out, src);
+        }
+      }
+      std::chrono::steady_clock::time_point t1 = std::chrono::steady_clock::now();
+      double sec = std::chrono::duration<double>(t1 - t0).count() / reps;
+      printf("%s %.9e\n", m.c_str(), sec);
+    }
+  } else {
+    fprintf(stderr, "unknown command %s\n", cmd.c_str());
+    return 2;
+  }
+  fflush(stdout);
+  return 0;
+}

@@ -1,0 +1,104 @@
+"""Generate the golden fixtures in this directory from the reference itself.
+
+Runs ``oracle/_ref/ref_harness`` (the reference Bridge++ corelib CPU path,
+built from the reference sources by ``make -f oracle/Makefile.ref``) on seeded
+synthetic inputs and stores its outputs.  Inputs are not stored: they are
+regenerated bit-for-bit from the recorded seeds by ``b200dwf.synth``.
+
+    python tests/golden/make_golden.py
+
+Needs the reference tree (to build the harness); the committed .npz files are
+what the tests read, so the tests themselves run without it.
+"""
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(REPO, "lqcd-dwf-hmc_b200"))
+from b200dwf import synth  # noqa: E402
+
+HARNESS = os.path.join(REPO, "oracle", "_ref", "ref_harness")
+
+# Operator cases.  Ls=4 keeps every fixture small while exercising the s=0
+# wall, the bulk and the s=Ls-1 wall of M5 and of the LU factors.
+CASES = {
+    "shamir": dict(lattice=[4, 4, 4, 4], Ls=4, mq=0.01, M0=1.8, b=1.0, c=0.0,
+                   alpha=1.0, bc=[1, 1, 1, -1], gauge=("hot", 11), src=12,
+                   modes=["Deo", "Doe", "dag_Deo", "dag_Doe", "Dee", "dag_Dee",
+                          "Dee_inv", "dag_Dee_inv", "D", "dag_D", "DdagD",
+                          "H", "dag_H", "gm5R", "R"]),
+    "mobius_alpha": dict(lattice=[4, 4, 4, 4], Ls=4, mq=0.02, M0=1.0, b=1.5,
+                         c=0.5, alpha=1.3, bc=[1, -1, 1, -1],
+                         gauge=("near", 21), src=22,
+                         modes=["Deo", "dag_Deo", "Dee", "dag_Dee", "Dee_inv",
+                                "dag_Dee_inv", "DdagD", "H"]),
+}
+SOLVE = dict(case="shamir", tol=1e-24, sigma=[0.05, 0.2, 1.0], maxiter=5000)
+
+
+def write_params(path, case, extra=None):
+    with open(path, "w") as f:
+        f.write("lattice %s\n" % " ".join(map(str, case["lattice"])))
+        for k in ("Ls", "mq", "M0", "b", "c", "alpha"):
+            f.write("%s %r\n" % (k, case[k]))
+        f.write("bc %s\n" % " ".join(map(str, case["bc"])))
+        for k, v in (extra or {}).items():
+            if isinstance(v, (list, tuple)):
+                f.write("%s %s\n" % (k, " ".join(map(repr, v))))
+            else:
+                f.write("%s %s\n" % (k, v))
+
+
+def inputs(case):
+    kind, gseed = case["gauge"]
+    u = synth.gauge_field(case["lattice"], gseed, kind)
+    src = synth.spinor_field(case["lattice"], case["Ls"], case["src"])
+    return u, src
+
+
+def run(cmd, case, extra, tmp):
+    u, src = inputs(case)
+    u.tofile(os.path.join(tmp, "gauge.bin"))
+    src.tofile(os.path.join(tmp, "src.bin"))
+    write_params(os.path.join(tmp, "params.txt"), case, extra)
+    subprocess.run([HARNESS, cmd, os.path.join(tmp, "params.txt"), tmp, tmp],
+                   check=True, stdout=subprocess.DEVNULL)
+
+
+def main():
+    for name, case in CASES.items():
+        with tempfile.TemporaryDirectory() as tmp:
+            run("modes", case, {"modes": " ".join(case["modes"])}, tmp)
+            out = {m: np.fromfile(os.path.join(tmp, m + ".bin")) for m in case["modes"]}
+        meta = {k: v for k, v in case.items() if k != "modes"}
+        meta["modes"] = case["modes"]
+        np.savez_compressed(os.path.join(HERE, "dwf_%s.npz" % name),
+                            meta=json.dumps(meta), **out)
+        print("wrote dwf_%s.npz" % name)
+
+    case = CASES[SOLVE["case"]]
+    with tempfile.TemporaryDirectory() as tmp:
+        run("cg", case, {"tol": SOLVE["tol"], "maxiter": SOLVE["maxiter"]}, tmp)
+        x = np.fromfile(os.path.join(tmp, "cg_x.bin"))
+        info = open(os.path.join(tmp, "cg_info.txt")).read()
+        run("shiftcg", case, {"tol": SOLVE["tol"], "maxiter": SOLVE["maxiter"],
+                              "sigma": SOLVE["sigma"]}, tmp)
+        xs = [np.fromfile(os.path.join(tmp, "shift_%d.bin" % i))
+              for i in range(len(SOLVE["sigma"]))]
+        sinfo = open(os.path.join(tmp, "shift_info.txt")).read()
+    meta = dict(SOLVE, cg_info=info, shift_info=sinfo)
+    np.savez_compressed(os.path.join(HERE, "solve_shamir.npz"),
+                        meta=json.dumps(meta), cg_x=x,
+                        **{"shift_%d" % i: v for i, v in enumerate(xs)})
+    print("wrote solve_shamir.npz", info.strip().replace("\n", " "),
+          sinfo.strip().replace("\n", " "))
+
+
+if __name__ == "__main__":
+    main()
