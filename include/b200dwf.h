@@ -1,0 +1,121 @@
+/*
+ * b200dwf -- C ABI of the B200-native even/odd 5D domain-wall fermion hot
+ * path (operator, solvers) that stands in for the reference's flat device
+ * kernel layer `namespace BridgeACC` and the classes built on it.
+ *
+ * Conventions shared by every entry point
+ *   - Return value: 0 on success, a negative B200_E* code on failure; the
+ *     message of the last failure on the calling thread is b200_last_error().
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *   - Fields are device buffers of b200_dwf_field_bytes(op, prec) bytes holding
+ *     one even/odd 5D half-lattice spinor (Nvol/2 sites x Ls) in the library's
+ *     HBM layout; convert()/reverse() move data to and from the reference's
+ *     host layout Field(24, Nvol/2, Ls):
+ *         ri + 2*(color + 3*spin) + 24*(site_eo + Nvol2*s).
+ *   - prec: B200_F64, B200_F32, B200_F16 (per-(site,s) scaled fp16 storage,
+ *     fp32 arithmetic) or B200_BF16 (same with bf16 storage).
+ *
+ * Reference interfaces each group replaces (paths relative to the reference
+ * tree; the reference's own header is src/lib_alt_Accel/BridgeOpenACC/
+ * bridgeACC_Domainwall.h:14-495 for the kernels):
+ */
+#ifndef B200DWF_H
+#define B200DWF_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  B200_F64 = 0,
+  B200_F32 = 1,
+  B200_F16 = 2,
+  B200_BF16 = 3
+};
+
+enum {
+  B200_OK = 0,
+  B200_EINVAL = -1,     /* invalid argument / unsupported size */
+  B200_ECUDA = -2,      /* CUDA runtime error */
+  B200_ENOMEM = -3,     /* device allocation failed */
+  B200_ENOCONV = -4     /* solver did not converge within its iteration cap */
+};
+
+typedef struct b200_dwf b200_dwf_t;
+
+/* Message of the last error on this thread (never NULL). */
+const char *b200_last_error(void);
+
+/* Select the CUDA device of this process: device = rank % ndev + offset.
+ * Replaces DeviceManager_OpenACC::init
+ * (src/lib_alt_Accel/ResourceManager/deviceManager_OpenACC.cpp:31-50). */
+int b200_init(int rank, int device_offset);
+
+/* ---------------------------------------------------------------- operator
+ * AFopr_Domainwall_5din_eo construction and parameters
+ * (src/lib_alt_Accel/Fopr/afopr_Domainwall_5din_eo-tmpl.h:31-147 init,
+ *  :330-405 set_parameters, :410-477 set_precond_parameters).
+ * lattice = {Nx, Ny, Nz, Nt} (Nx even), Ls in {4, 6, 8, 12, 16},
+ * b, c: Ls Moebius coefficients (NULL = Shamir b=1, c=0), alpha: Neff alpha,
+ * bc: boundary phases {bx, by, bz, bt} (1 periodic, -1 antiperiodic, 0 open). */
+int b200_dwf_create(b200_dwf_t **op, const int lattice[4], int Ls, double mq,
+                    double M0, const double *b, const double *c, double alpha,
+                    const int bc[4]);
+int b200_dwf_destroy(b200_dwf_t *op);
+
+/* set_config(Field *U) + convert_gauge: lexical links in the reference
+ * Field_G(Nvol, 4) host layout ri + 2*(col + 3*row) + 18*(site + Nvol*mu)
+ * (afopr_Domainwall_5din_eo-tmpl.h:514-551).  Builds the links for every
+ * precision the operator is applied in. */
+int b200_dwf_set_config(b200_dwf_t *op, const double *u_lex_host, void *stream);
+/* Same, from a device buffer of the same layout. */
+int b200_dwf_set_config_device(b200_dwf_t *op, const double *u_lex_dev, void *stream);
+
+/* Bytes of one field of this operator in precision prec. */
+size_t b200_dwf_field_bytes(const b200_dwf_t *op, int prec);
+/* Number of reals in the reference host layout (24 * Nvol/2 * Ls). */
+size_t b200_dwf_field_nreal(const b200_dwf_t *op);
+
+/* convert(AFIELD&, const Field&) / reverse(Field&, const AFIELD&)
+ * (afopr_Domainwall_5din_eo-tmpl.h:555-620): host double array in the
+ * reference layout <-> device field.  Synchronous on `stream`. */
+int b200_field_convert(b200_dwf_t *op, int prec, void *v_dev, const double *w_host,
+                       void *stream);
+int b200_field_reverse(b200_dwf_t *op, int prec, double *v_host, const void *w_dev,
+                       void *stream);
+
+/* mult / mult_dag (afopr_Domainwall_5din_eo-tmpl.h:634-767).  mode is one of
+ *   "D" "Ddag" "DdagD" "H" "Hdag" "Deo" "Doe" "Dee" "Doo" "Dee_inv" "Doo_inv"
+ *   "gm5R" "R"
+ * dag != 0 selects mult_dag.  v and w are distinct fields of precision prec. */
+int b200_dwf_mult(b200_dwf_t *op, int prec, void *v, const void *w,
+                  const char *mode, int dag, void *stream);
+
+/* ---------------------------------------------------------------- fields
+ * AField<REAL, ACCEL> BLAS (src/lib_alt_Accel/Field/afield-tmpl.h:637-720 ->
+ * BridgeOpenACC/src/afield_openacc-inc.h:130-355).  norm2/dot accumulate in
+ * double and return synchronously. */
+int b200_field_axpby(b200_dwf_t *op, int prec, void *y, double a, const void *x,
+                     double b, void *stream);                  /* y = a x + b y */
+int b200_field_norm2(b200_dwf_t *op, int prec, const void *x, double *result,
+                     void *stream);
+int b200_field_dot(b200_dwf_t *op, int prec, const void *x, const void *y,
+                   double *result, void *stream);              /* Re <x, y> */
+int b200_field_copy_convert(b200_dwf_t *op, int prec_out, void *out, int prec_in,
+                            const void *in, void *stream);     /* convert_h */
+
+/* ---------------------------------------------------------------- solvers
+ * ASolver_CG on DdagD, zero initial guess (src/lib_alt/Solver/
+ * asolver_CG-tmpl.h:118-234): stops when |r|^2/|b|^2 < tol2; returns the
+ * iteration count and diff = sqrt(|DdagD x - b|^2 / |b|^2) from a true
+ * residual.  Returns B200_ENOCONV (x still written) if maxiter is reached. */
+int b200_cg_solve(b200_dwf_t *op, int prec, void *x, const void *b, int maxiter,
+                  double tol2, int *nconv, double *diff, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

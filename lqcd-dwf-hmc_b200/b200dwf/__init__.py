@@ -1,0 +1,182 @@
+"""Python binding of the B200 domain-wall library (libb200dwf.so, C ABI in
+include/b200dwf.h).
+
+The host-side mirror of the reference operator interface
+``AFopr_Domainwall_5din_eo`` (src/lib_alt_Accel/Fopr/afopr_Domainwall_5din_eo.h):
+``set_config``, ``set_mode``, ``mult``/``mult_dag`` (with and without an
+explicit mode), ``convert``/``reverse``, ``field_nin/nvol/nex``.  Device fields
+are ``torch`` uint8 buffers on the current CUDA device; PyTorch is only the
+allocator here, every operation runs in the library's own sm_100a kernels.
+
+The library is loaded from this package directory; importing the operator on a
+machine without the built library raises instead of falling back to anything.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from . import synth  # noqa: F401
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(os.path.dirname(HERE), "libb200dwf.so")
+
+F64, F32, F16, BF16 = 0, 1, 2, 3
+PREC_NAMES = {"f64": F64, "f32": F32, "f16": F16, "bf16": BF16}
+
+_lib = None
+
+
+class B200Error(RuntimeError):
+    pass
+
+
+def lib():
+    """Load libb200dwf.so (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIBPATH):
+        raise B200Error("libb200dwf.so not built (run `make -C lqcd-dwf-hmc_b200`)")
+    L = ctypes.CDLL(LIBPATH)
+    vp = ctypes.c_void_p
+    dp = ctypes.POINTER(ctypes.c_double)
+    ip = ctypes.POINTER(ctypes.c_int)
+    L.b200_last_error.restype = ctypes.c_char_p
+    L.b200_init.argtypes = [ctypes.c_int, ctypes.c_int]
+    L.b200_dwf_create.argtypes = [ctypes.POINTER(vp), ip, ctypes.c_int, ctypes.c_double,
+                                  ctypes.c_double, dp, dp, ctypes.c_double, ip]
+    L.b200_dwf_destroy.argtypes = [vp]
+    L.b200_dwf_set_config.argtypes = [vp, dp, vp]
+    L.b200_dwf_set_config_device.argtypes = [vp, vp, vp]
+    L.b200_dwf_field_bytes.argtypes = [vp, ctypes.c_int]
+    L.b200_dwf_field_bytes.restype = ctypes.c_size_t
+    L.b200_dwf_field_nreal.argtypes = [vp]
+    L.b200_dwf_field_nreal.restype = ctypes.c_size_t
+    L.b200_field_convert.argtypes = [vp, ctypes.c_int, vp, dp, vp]
+    L.b200_field_reverse.argtypes = [vp, ctypes.c_int, dp, vp, vp]
+    L.b200_dwf_mult.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_char_p, ctypes.c_int, vp]
+    L.b200_field_axpby.argtypes = [vp, ctypes.c_int, vp, ctypes.c_double, vp, ctypes.c_double, vp]
+    L.b200_field_norm2.argtypes = [vp, ctypes.c_int, vp, dp, vp]
+    L.b200_field_dot.argtypes = [vp, ctypes.c_int, vp, vp, dp, vp]
+    L.b200_field_copy_convert.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, vp, vp]
+    L.b200_cg_solve.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_double,
+                                ip, dp, vp]
+    _lib = L
+    return L
+
+
+def check(rc):
+    if rc != 0:
+        raise B200Error("b200 error %d: %s" % (rc, lib().b200_last_error().decode()))
+    return rc
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Field:
+    """One device 5D half-lattice spinor of a DomainWall operator."""
+
+    def __init__(self, op, prec=F64):
+        import torch
+        self.op = op
+        self.prec = prec
+        nbytes = lib().b200_dwf_field_bytes(op.handle, prec)
+        self.buf = torch.zeros(nbytes, dtype=torch.uint8, device="cuda")
+
+    @property
+    def ptr(self):
+        return ctypes.c_void_p(self.buf.data_ptr())
+
+
+class DomainWall:
+    """Mirror of AFopr_Domainwall_5din_eo<AField<REAL, B200>> over the C ABI."""
+
+    def __init__(self, lattice, Ls, mq, M0, b=1.0, c=0.0, alpha=1.0, bc=(1, 1, 1, -1)):
+        L = lib()
+        self.lattice = list(lattice)
+        self.Ls = Ls
+        bb = np.full(Ls, b, np.float64) if np.isscalar(b) else np.ascontiguousarray(b, np.float64)
+        cc = np.full(Ls, c, np.float64) if np.isscalar(c) else np.ascontiguousarray(c, np.float64)
+        h = ctypes.c_void_p()
+        check(L.b200_dwf_create(ctypes.byref(h), (ctypes.c_int * 4)(*lattice), Ls, mq, M0,
+                                _dp(bb), _dp(cc), alpha, (ctypes.c_int * 4)(*bc)))
+        self.handle = h
+        self.mode = "D"
+        self.nvol = int(np.prod(lattice)) // 2
+        self.nreal = 24 * self.nvol * Ls
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and _lib is not None:
+            _lib.b200_dwf_destroy(h)
+            self.handle = None
+
+    # AFopr interface ---------------------------------------------------
+    def field_nin(self):
+        return 24 * self.Ls
+
+    def field_nvol(self):
+        return self.nvol
+
+    def field_nex(self):
+        return 1
+
+    def needs_convert(self):
+        return True
+
+    def set_config(self, u_lex):
+        u = np.ascontiguousarray(u_lex, np.float64)
+        check(lib().b200_dwf_set_config(self.handle, _dp(u), None))
+
+    def set_mode(self, mode):
+        self.mode = mode
+
+    def new_field(self, prec=F64):
+        return Field(self, prec)
+
+    def convert(self, v, w_host):
+        w = np.ascontiguousarray(w_host, np.float64)
+        check(lib().b200_field_convert(self.handle, v.prec, v.ptr, _dp(w), None))
+
+    def reverse(self, w):
+        out = np.empty(self.nreal)
+        check(lib().b200_field_reverse(self.handle, w.prec, _dp(out), w.ptr, None))
+        return out
+
+    def mult(self, v, w, mode=None):
+        check(lib().b200_dwf_mult(self.handle, w.prec, v.ptr, w.ptr,
+                                  (mode or self.mode).encode(), 0, None))
+
+    def mult_dag(self, v, w, mode=None):
+        check(lib().b200_dwf_mult(self.handle, w.prec, v.ptr, w.ptr,
+                                  (mode or self.mode).encode(), 1, None))
+
+    # AField BLAS -------------------------------------------------------
+    def axpby(self, y, a, x, b):
+        check(lib().b200_field_axpby(self.handle, y.prec, y.ptr, a, x.ptr if x else None, b, None))
+
+    def norm2(self, x):
+        r = ctypes.c_double()
+        check(lib().b200_field_norm2(self.handle, x.prec, x.ptr, ctypes.byref(r), None))
+        return r.value
+
+    def dot(self, x, y):
+        r = ctypes.c_double()
+        check(lib().b200_field_dot(self.handle, x.prec, x.ptr, y.ptr, ctypes.byref(r), None))
+        return r.value
+
+    def copy_convert(self, out, inp):
+        check(lib().b200_field_copy_convert(self.handle, out.prec, out.ptr, inp.prec, inp.ptr, None))
+
+    # solvers -----------------------------------------------------------
+    def cg(self, x, b, tol2, maxiter=10000):
+        n = ctypes.c_int()
+        d = ctypes.c_double()
+        rc = lib().b200_cg_solve(self.handle, b.prec, x.ptr, b.ptr, maxiter, tol2,
+                                 ctypes.byref(n), ctypes.byref(d), None)
+        if rc not in (0, -4):
+            check(rc)
+        return n.value, d.value, rc

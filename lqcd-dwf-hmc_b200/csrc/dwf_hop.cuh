@@ -1,0 +1,397 @@
+// Fused even/odd 5D domain-wall hopping kernel for sm_100a.
+//
+// One thread per (4D site, s).  A warp holds G = 32/Ls complete 4D sites, so
+// every SU(3) link is fetched by one broadcast transaction per site and reused
+// by all Ls lanes of that site from registers.  The fifth-dimension operators
+// that surround the hop in the reference (the M5 pre-factor of D_eo, M5^+ after
+// the dagger hop, M_ee^-1 = U^-1 L^-1 and its dagger, gamma5 R) are all linear
+// maps along s that are block-diagonal in chirality, so any chain of them is a
+// pair of dense Ls x Ls real matrices (E+, E-).  The kernel applies that pair in
+// its epilogue on a shared-memory tile of the site's whole fifth-dimension
+// column, then optionally forms o1 = c*X + E(acc), o2 = F(o1), stores o1/o2 and
+// reduces |o1|^2 -- the fusions used by the CG iteration.
+//
+// Reference behaviour (file:line relative to the reference tree):
+//   hop with Dirac projections, no -kappa: src/lib_alt_Accel/BridgeOpenACC/src/
+//     mult_Domainwall_5din_eo_openacc-inc.h:450-550 (+ inc/ files); jgm5=1
+//     gives the gamma5-sandwiched dagger hop.
+//   boundary phase applied at the lattice edge in-kernel (inc/*_xyz, bc2).
+#pragma once
+
+#include "dwf_common.cuh"
+
+namespace b200 {
+
+enum LinkFmt { LINK_F64_18 = 0, LINK_F64_12 = 1, LINK_F32_12 = 2, LINK_F16_12 = 3 };
+
+template <int LF> struct LinkLoad;
+
+template <> struct LinkLoad<LINK_F64_18> {
+  using R = double;
+  static constexpr int kChunks = 9;
+  __device__ static void load(const void* base, size_t idx, double* u) {
+    const double2* p = reinterpret_cast<const double2*>(base) + idx * 9;
+#pragma unroll
+    for (int j = 0; j < 9; ++j) { double2 c = __ldg(p + j); u[2 * j] = c.x; u[2 * j + 1] = c.y; }
+  }
+};
+template <> struct LinkLoad<LINK_F64_12> {
+  using R = double;
+  static constexpr int kChunks = 6;
+  __device__ static void load(const void* base, size_t idx, double* u) {
+    const double2* p = reinterpret_cast<const double2*>(base) + idx * 6;
+#pragma unroll
+    for (int j = 0; j < 6; ++j) { double2 c = __ldg(p + j); u[2 * j] = c.x; u[2 * j + 1] = c.y; }
+    su3_reconstruct(u);
+  }
+};
+template <> struct LinkLoad<LINK_F32_12> {
+  using R = float;
+  static constexpr int kChunks = 3;
+  __device__ static void load(const void* base, size_t idx, float* u) {
+    const float4* p = reinterpret_cast<const float4*>(base) + idx * 3;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      float4 c = __ldg(p + j);
+      u[4 * j] = c.x; u[4 * j + 1] = c.y; u[4 * j + 2] = c.z; u[4 * j + 3] = c.w;
+    }
+    su3_reconstruct(u);
+  }
+};
+template <> struct LinkLoad<LINK_F16_12> {
+  using R = float;
+  static constexpr int kChunks = 2;
+  __device__ static void load(const void* base, size_t idx, float* u) {
+    const uint4* p = reinterpret_cast<const uint4*>(base) + idx * 2;
+    uint4 a = __ldg(p), b = __ldg(p + 1);
+    unsigned int w[6] = {a.x, a.y, a.z, a.w, b.x, b.y};
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+      float2 f = HalfOps<__half>::to2(w[j]);
+      u[2 * j] = f.x; u[2 * j + 1] = f.y;
+    }
+    su3_reconstruct(u);
+  }
+};
+
+// ------------------------------------------------------------ complex helpers
+template <typename R>
+__device__ __forceinline__ void cmul_acc(R& ore, R& oim, R ar, R ai, R br, R bi) {
+  ore = fma(ar, br, ore); ore = fma(-ai, bi, ore);
+  oim = fma(ar, bi, oim); oim = fma(ai, br, oim);
+}
+
+// out[2] (half spinor, 3 colors each, 12 reals) = U * h  or U^+ * h
+template <typename R, bool kDag>
+__device__ __forceinline__ void su3_mult_half(const R* u, const R* h, R* o) {
+#pragma unroll
+  for (int a = 0; a < 2; ++a) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      R re = 0, im = 0;
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const R ur = kDag ? u[2 * (i + 3 * j)] : u[2 * (j + 3 * i)];
+        const R ui = kDag ? -u[2 * (i + 3 * j) + 1] : u[2 * (j + 3 * i) + 1];
+        cmul_acc(re, im, ur, ui, h[6 * a + 2 * j], h[6 * a + 2 * j + 1]);
+      }
+      o[6 * a + 2 * i] = re;
+      o[6 * a + 2 * i + 1] = im;
+    }
+  }
+}
+
+// Spin projection (1 - sign*gamma_mu) w -> half spinor h (2 spins x 3 colors)
+// and reconstruction acc += ph * (1 - sign*gamma_mu)-shaped result from uh.
+// Dirac basis (reference src/lib/Tools/gammaMatrixSet_Dirac.cpp:31-60).
+// w index: ri + 2*(c + 3*sp).  sign = +1 forward (1-g), -1 backward (1+g).
+template <typename R, int MU, int SIGN>
+__device__ __forceinline__ void project(const R* w, R* h) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const R w0r = w[2 * c], w0i = w[2 * c + 1];
+    const R w1r = w[2 * (c + 3)], w1i = w[2 * (c + 3) + 1];
+    const R w2r = w[2 * (c + 6)], w2i = w[2 * (c + 6) + 1];
+    const R w3r = w[2 * (c + 9)], w3i = w[2 * (c + 9) + 1];
+    R h0r, h0i, h1r, h1i;
+    if (MU == 0) {        // (1 -+ g1): h0 = w0 +- i w3, h1 = w1 +- i w2
+      h0r = w0r - SIGN * w3i; h0i = w0i + SIGN * w3r;
+      h1r = w1r - SIGN * w2i; h1i = w1i + SIGN * w2r;
+    } else if (MU == 1) { // (1 -+ g2): h0 = w0 +- w3, h1 = w1 -+ w2
+      h0r = w0r + SIGN * w3r; h0i = w0i + SIGN * w3i;
+      h1r = w1r - SIGN * w2r; h1i = w1i - SIGN * w2i;
+    } else if (MU == 2) { // (1 -+ g3): h0 = w0 +- i w2, h1 = w1 -+ i w3
+      h0r = w0r - SIGN * w2i; h0i = w0i + SIGN * w2r;
+      h1r = w1r + SIGN * w3i; h1i = w1i - SIGN * w3r;
+    } else {              // (1 - g4) keeps lower spins, (1 + g4) upper, x2
+      if (SIGN > 0) { h0r = 2 * w2r; h0i = 2 * w2i; h1r = 2 * w3r; h1i = 2 * w3i; }
+      else          { h0r = 2 * w0r; h0i = 2 * w0i; h1r = 2 * w1r; h1i = 2 * w1i; }
+    }
+    h[2 * c] = h0r; h[2 * c + 1] = h0i;
+    h[6 + 2 * c] = h1r; h[6 + 2 * c + 1] = h1i;
+  }
+}
+
+template <typename R, int MU, int SIGN>
+__device__ __forceinline__ void reconstruct_acc(R* acc, const R* o, R ph) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const R a0r = ph * o[2 * c], a0i = ph * o[2 * c + 1];
+    const R a1r = ph * o[6 + 2 * c], a1i = ph * o[6 + 2 * c + 1];
+    R* r0 = acc + 2 * c;
+    R* r1 = acc + 2 * (c + 3);
+    R* r2 = acc + 2 * (c + 6);
+    R* r3 = acc + 2 * (c + 9);
+    if (MU == 3) {
+      if (SIGN > 0) { r2[0] += a0r; r2[1] += a0i; r3[0] += a1r; r3[1] += a1i; }
+      else          { r0[0] += a0r; r0[1] += a0i; r1[0] += a1r; r1[1] += a1i; }
+      continue;
+    }
+    r0[0] += a0r; r0[1] += a0i;
+    r1[0] += a1r; r1[1] += a1i;
+    if (MU == 0) {        // rows 2,3 = -+ i h1, -+ i h0
+      r2[0] += SIGN * a1i; r2[1] -= SIGN * a1r;
+      r3[0] += SIGN * a0i; r3[1] -= SIGN * a0r;
+    } else if (MU == 1) { // rows 2,3 = -+ h1, +- h0
+      r2[0] -= SIGN * a1r; r2[1] -= SIGN * a1i;
+      r3[0] += SIGN * a0r; r3[1] += SIGN * a0i;
+    } else {              // MU==2: rows 2,3 = -+ i h0, +- i h1
+      r2[0] += SIGN * a0i; r2[1] -= SIGN * a0r;
+      r3[0] -= SIGN * a1i; r3[1] += SIGN * a1r;
+    }
+  }
+}
+
+// ------------------------------------------------------------ parameters
+struct HopParams {
+  const void* in;        // input field (parity 1-ieo)
+  const void* links;     // plan links (layout per LinkFmt)
+  void* out1;            // o1 store target (nullable)
+  void* out2;            // o2 store target (nullable)
+  const void* x1;        // axpy operand X (nullable)
+  const double* E;       // [2][Ls][Ls] chiral matrices applied to acc
+  const double* F;       // optional [2][Ls][Ls] second map, o2 = F o1
+  const void* x2;        // second axpy operand (nullable)
+  // o1 = ce * E(acc) + c_x1 * X1 + c_x2 * X2; each scalar is multiplied by
+  // the device value behind its _dev pointer when that pointer is non-null
+  double ce, c_x1, c_x2;
+  const double* ce_dev;
+  const double* c_x1_dev;
+  const double* c_x2_dev;
+  double* red;           // per-block partials of |o1|^2 (nullable)
+  int vh, nx2, ny, nz, nt, ls;
+  int ieo;               // output parity (0 even, 1 odd)
+  double bc[4];
+};
+
+// Epilogue tile helpers.  Tile layout per warp: [site g][s][24 reals].
+// unit u = (g, color, ri, pair): 12 per site; the unit's fifth-dimension
+// column is moved to the chiral basis x+- = v_pair +- v_(pair+2), multiplied by
+// the dense E+ / E- (uniform smem reads, broadcast to the warp) and moved back.
+template <typename R, int LS, int G>
+__device__ __forceinline__ void apply_chiral(const R* __restrict__ tile_in, R* __restrict__ tile_out,
+                                             const R* __restrict__ Em, int lane) {
+#pragma unroll 1
+  for (int u = lane; u < 12 * G; u += 32) {
+    const int g = u / 12;
+    const int r = u - 12 * g;
+    const int pair = r / 6;
+    const int cr = r - 6 * pair;
+    const R* ti = tile_in + g * LS * 24 + 6 * pair + cr;
+    R* to = tile_out + g * LS * 24 + 6 * pair + cr;
+    R xp[LS], xm[LS];
+#pragma unroll
+    for (int s = 0; s < LS; ++s) {
+      const R a = ti[s * 24];
+      const R b = ti[s * 24 + 12];
+      xp[s] = a + b;
+      xm[s] = a - b;
+    }
+#pragma unroll
+    for (int s = 0; s < LS; ++s) {
+      R yp = 0, ym = 0;
+#pragma unroll
+      for (int t = 0; t < LS; ++t) {
+        yp = fma(Em[s * LS + t], xp[t], yp);
+        ym = fma(Em[LS * LS + s * LS + t], xm[t], ym);
+      }
+      to[s * 24] = R(0.5) * (yp + ym);
+      to[s * 24 + 12] = R(0.5) * (yp - ym);
+    }
+  }
+}
+
+template <int LS, int P, int LF, bool kDagHop>
+__global__ void __launch_bounds__(128) dwf_hop_kernel(HopParams p) {
+  using St = Store<P>;
+  using R = typename St::R;
+  constexpr int G = 32 / LS;              // sites per warp
+  constexpr int WARPS = 4;
+  constexpr int TILE = WARPS * G * LS * 24;
+
+  extern __shared__ unsigned char smem_raw[];
+  R* sE = reinterpret_cast<R*>(smem_raw);              // 2*LS*LS
+  R* sF = sE + 2 * LS * LS;                             // 2*LS*LS
+  R* tileA = sF + 2 * LS * LS;                          // TILE
+  R* tileB = tileA + TILE;                              // TILE
+  __shared__ double red_warp[WARPS];
+
+  const int tid = threadIdx.x;
+  for (int i = tid; i < 2 * LS * LS; i += blockDim.x) {
+    sE[i] = (R)p.E[i];
+    sF[i] = p.F ? (R)p.F[i] : R(0);
+  }
+
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const int g = lane / LS;
+  const int s = lane - g * LS;
+  const int site = (blockIdx.x * WARPS + warp) * G + g;
+  const bool active = (g < G) && (site < p.vh);
+  const size_t vh = p.vh;
+
+  R acc[24];
+#pragma unroll
+  for (int i = 0; i < 24; ++i) acc[i] = 0;
+
+  if (active) {
+    const int ix2 = site % p.nx2;
+    const int iyzt = site / p.nx2;
+    const int y = iyzt % p.ny;
+    const int izt = iyzt / p.ny;
+    const int z = izt % p.nz;
+    const int t = izt / p.nz;
+    const int keo = (p.ieo + y + z + t) & 1;
+    const int x = 2 * ix2 + keo;
+    const int nx = 2 * p.nx2;
+    const int ieo = p.ieo;
+    const size_t strideMu = vh;          // links: ((parity*4+mu)*Vh + site)
+
+#define B200_HOP_DIR(MU, COORD, EXT, NBP, NBM)                                       \
+    {                                                                                \
+      R w[24], h[12], o[12], u[18];                                                  \
+      /* forward: (1 - g_mu) U_mu(x) w(x+mu) */                                      \
+      {                                                                              \
+        const bool edge = (COORD == EXT - 1);                                        \
+        const R ph = edge ? (R)p.bc[MU] : R(1);                                      \
+        const int nb = NBP;                                                          \
+        St::load(p.in, vh, LS, nb, s, w);                                            \
+        if (kDagHop) {                                                               \
+          _Pragma("unroll") for (int q = 0; q < 12; ++q) {                           \
+            R tmp = w[q]; w[q] = w[q + 12]; w[q + 12] = tmp; }                       \
+        }                                                                            \
+        project<R, MU, 1>(w, h);                                                     \
+        LinkLoad<LF>::load(p.links, (size_t)(ieo + 2 * MU) * strideMu + site, u);    \
+        su3_mult_half<R, false>(u, h, o);                                            \
+        reconstruct_acc<R, MU, 1>(acc, o, ph);                                       \
+      }                                                                              \
+      /* backward: (1 + g_mu) U_mu(x-mu)^+ w(x-mu) */                                \
+      {                                                                              \
+        const bool edge = (COORD == 0);                                              \
+        const R ph = edge ? (R)p.bc[MU] : R(1);                                      \
+        const int nb = NBM;                                                          \
+        St::load(p.in, vh, LS, nb, s, w);                                            \
+        if (kDagHop) {                                                               \
+          _Pragma("unroll") for (int q = 0; q < 12; ++q) {                           \
+            R tmp = w[q]; w[q] = w[q + 12]; w[q + 12] = tmp; }                       \
+        }                                                                            \
+        project<R, MU, -1>(w, h);                                                    \
+        LinkLoad<LF>::load(p.links, (size_t)(1 - ieo + 2 * MU) * strideMu + nb, u);  \
+        su3_mult_half<R, true>(u, h, o);                                             \
+        reconstruct_acc<R, MU, -1>(acc, o, ph);                                      \
+      }                                                                              \
+    }
+
+    const int row = p.nx2 * iyzt;
+    // x: neighbour x+1 has ix2 + keo (wrapping inside the row), x-1 has ix2 - (1-keo)
+    B200_HOP_DIR(0, x, nx,
+                 row + ((ix2 + keo == p.nx2) ? 0 : ix2 + keo),
+                 row + ((ix2 - 1 + keo < 0) ? p.nx2 - 1 : ix2 - 1 + keo));
+    const int sy = p.nx2;
+    B200_HOP_DIR(1, y, p.ny,
+                 (y == p.ny - 1) ? site - (p.ny - 1) * sy : site + sy,
+                 (y == 0) ? site + (p.ny - 1) * sy : site - sy);
+    const int sz = p.nx2 * p.ny;
+    B200_HOP_DIR(2, z, p.nz,
+                 (z == p.nz - 1) ? site - (p.nz - 1) * sz : site + sz,
+                 (z == 0) ? site + (p.nz - 1) * sz : site - sz);
+    const int st = p.nx2 * p.ny * p.nz;
+    B200_HOP_DIR(3, t, p.nt,
+                 (t == p.nt - 1) ? site - (p.nt - 1) * st : site + st,
+                 (t == 0) ? site + (p.nt - 1) * st : site - st);
+#undef B200_HOP_DIR
+  }
+
+  // ---------------- epilogue: chiral fifth-dimension map on the site tile
+  R* myA = tileA + (size_t)warp * G * LS * 24;
+  R* myB = tileB + (size_t)warp * G * LS * 24;
+  if (g < G) {
+#pragma unroll
+    for (int i = 0; i < 24; ++i) myA[(g * LS + s) * 24 + i] = acc[i];
+  }
+  __syncthreads();   // also covers the sE/sF fill
+  apply_chiral<R, LS, G>(myA, myB, sE, lane);
+  __syncwarp();
+
+  double nrm = 0.0;
+  if (active) {
+    R o1[24];
+    const R ce = (R)(p.ce * (p.ce_dev ? *p.ce_dev : 1.0));
+#pragma unroll
+    for (int i = 0; i < 24; ++i) o1[i] = ce * myB[(g * LS + s) * 24 + i];
+    if (p.x1) {
+      R xv[24];
+      St::load(p.x1, vh, LS, site, s, xv);
+      const R c = (R)(p.c_x1 * (p.c_x1_dev ? *p.c_x1_dev : 1.0));
+#pragma unroll
+      for (int i = 0; i < 24; ++i) o1[i] = fma(c, xv[i], o1[i]);
+    }
+    if (p.x2) {
+      R xv[24];
+      St::load(p.x2, vh, LS, site, s, xv);
+      const R c = (R)(p.c_x2 * (p.c_x2_dev ? *p.c_x2_dev : 1.0));
+#pragma unroll
+      for (int i = 0; i < 24; ++i) o1[i] = fma(c, xv[i], o1[i]);
+    }
+    if (p.out1) St::store(p.out1, vh, LS, site, s, o1);
+    if (p.red) {
+#pragma unroll
+      for (int i = 0; i < 24; ++i) nrm += (double)o1[i] * (double)o1[i];
+    }
+    if (p.F) {
+#pragma unroll
+      for (int i = 0; i < 24; ++i) myA[(g * LS + s) * 24 + i] = o1[i];
+    }
+  }
+  if (p.F) {
+    __syncwarp();
+    apply_chiral<R, LS, G>(myA, myB, sF, lane);
+    __syncwarp();
+    if (active) {
+      R o2[24];
+#pragma unroll
+      for (int i = 0; i < 24; ++i) o2[i] = myB[(g * LS + s) * 24 + i];
+      St::store(p.out2, vh, LS, site, s, o2);
+    }
+  }
+  if (p.red) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) nrm += __shfl_xor_sync(0xffffffffu, nrm, off);
+    if (lane == 0) red_warp[warp] = nrm;
+    __syncthreads();
+    if (tid == 0) {
+      double b = 0.0;
+#pragma unroll
+      for (int w = 0; w < WARPS; ++w) b += red_warp[w];
+      p.red[blockIdx.x] = b;
+    }
+  }
+}
+
+template <int LS, int P>
+constexpr size_t hop_smem_bytes() {
+  using R = typename Store<P>::R;
+  return sizeof(R) * (4 * LS * LS + 2 * 4 * (32 / LS) * LS * 24);
+}
+
+}  // namespace b200

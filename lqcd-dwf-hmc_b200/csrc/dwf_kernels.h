@@ -1,0 +1,89 @@
+// Host-side launch interface of the B200 domain-wall kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+#include "dwf_common.cuh"
+
+namespace b200 {
+
+struct HopParams;
+
+// Geometry of one even/odd half lattice with Ls fifth-dimension slices.
+struct Geom {
+  int nx2, ny, nz, nt, ls;
+  int vh;
+};
+
+// Parameters of the site-local fifth-dimension kernel:
+//   o1 = cx1*X1 + cx2*X2 + ce * E(in)     (E: chiral pair of Ls x Ls maps)
+//   o2 = F(o1)
+// Scalars with a _dev pointer are multiplied by that device value at run time.
+struct SopParams {
+  const void* in;
+  const void* x1;
+  const void* x2;
+  void* out1;
+  void* out2;
+  const double* E;
+  const double* F;
+  double cx1, cx2, ce;
+  const double* cx1_dev;
+  const double* cx2_dev;
+  const double* ce_dev;
+  double* red;        // per-block partials of |o1|^2
+  Geom g;
+};
+
+// CG vector update fused with the M5 pre-factor of the next hop:
+//   x += alpha*p;  p = r + beta*p;  y = E(p)   (alpha, beta device scalars)
+struct CgUpdParams {
+  void* x;
+  void* p;
+  const void* r;
+  void* y;
+  const double* E;
+  const double* alpha;
+  const double* beta;
+  Geom g;
+};
+
+// number of blocks the reductions of each launcher produce
+int hop_grid(int ls, int vh);
+int site_s_grid(int ls, int vh);
+constexpr int kSiteSBlock = 128;
+
+// Hop kernel dispatch (prec = storage precision of in/out fields).
+cudaError_t launch_hop(int prec, bool dag, const HopParams& p, cudaStream_t st);
+cudaError_t launch_sop(int prec, const SopParams& p, cudaStream_t st);
+cudaError_t launch_cg_update(int prec, const CgUpdParams& p, cudaStream_t st);
+
+// y = a*x + b*y over the whole field (a, b optionally scaled by device values)
+cudaError_t launch_axpby(int prec, const Geom& g, void* y, const void* x, double a,
+                         const double* a_dev, double b, const double* b_dev, cudaStream_t st);
+// partial sums of <x,y> (real part, double accumulation) into red[grid]
+cudaError_t launch_dot(int prec, const Geom& g, const void* x, const void* y, double* red,
+                       cudaStream_t st);
+cudaError_t launch_convert(int pout, void* out, int pin, const void* in, const Geom& g,
+                           cudaStream_t st);
+cudaError_t launch_from_corelib(int prec, void* out, const double* in_dev, const Geom& g,
+                                cudaStream_t st);
+cudaError_t launch_to_corelib(int prec, double* out_dev, const void* in, const Geom& g,
+                              cudaStream_t st);
+// lexical links (corelib Field_G layout) -> even/odd links in link format lf
+cudaError_t launch_links_from_lex(int lf, void* out, const double* u_lex_dev, const Geom& g,
+                                  cudaStream_t st);
+
+// out[0] = sum(partials[0..n)); op selects a solver scalar update afterwards:
+enum FinalizeOp {
+  FIN_SUM = 0,          // out[0] = s
+  FIN_CG_ALPHA = 1,     // sc[PQ] = s; sc[ALPHA] = sc[RR] / s
+  FIN_CG_BETA = 2,      // sc[BETA] = s / sc[RR]; sc[RR] = s
+};
+enum CgScalar { SC_RR = 0, SC_PQ = 1, SC_ALPHA = 2, SC_BETA = 3, SC_RR_NEW = 4, SC_N = 8 };
+cudaError_t launch_finalize(const double* partials, int n, double* out, int op, cudaStream_t st);
+
+size_t link_bytes(int lf, size_t vh);
+
+}  // namespace b200

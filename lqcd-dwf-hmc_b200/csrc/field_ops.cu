@@ -1,0 +1,514 @@
+// Site-local fifth-dimension kernel, field BLAS, reductions, layout and
+// precision conversions of the B200 domain-wall library.
+#include "dwf_hop.cuh"
+#include "dwf_kernels.h"
+
+namespace b200 {
+
+cudaError_t launch_hop_p0(bool dag, const HopParams& p, cudaStream_t st);
+cudaError_t launch_hop_p1(bool dag, const HopParams& p, cudaStream_t st);
+cudaError_t launch_hop_p2(bool dag, const HopParams& p, cudaStream_t st);
+cudaError_t launch_hop_p3(bool dag, const HopParams& p, cudaStream_t st);
+
+int hop_grid(int ls, int vh) {
+  const int g = 32 / ls;
+  const int per_block = 4 * g;
+  return (vh + per_block - 1) / per_block;
+}
+
+int site_s_grid(int ls, int vh) {
+  const long n = (long)vh * ls;
+  return (int)((n + kSiteSBlock - 1) / kSiteSBlock);
+}
+
+cudaError_t launch_hop(int prec, bool dag, const HopParams& p, cudaStream_t st) {
+  switch (prec) {
+    case PREC_F64: return launch_hop_p0(dag, p, st);
+    case PREC_F32: return launch_hop_p1(dag, p, st);
+    case PREC_F16: return launch_hop_p2(dag, p, st);
+    case PREC_BF16: return launch_hop_p3(dag, p, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+// ------------------------------------------------------------ block reduce
+__device__ __forceinline__ void block_reduce_store(double v, double* red) {
+  __shared__ double ws[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  if (lane == 0) ws[warp] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double b = 0.0;
+    const int nw = (blockDim.x + 31) >> 5;
+    for (int w = 0; w < nw; ++w) b += ws[w];
+    red[blockIdx.x] = b;
+  }
+}
+
+__device__ __forceinline__ double dev_scale(double c, const double* dev) {
+  return dev ? c * (*dev) : c;
+}
+
+// ------------------------------------------------------------ sop kernel
+template <int LS, int P>
+__global__ void __launch_bounds__(128) sop_kernel(SopParams p) {
+  using St = Store<P>;
+  using R = typename St::R;
+  constexpr int G = 32 / LS;
+  constexpr int WARPS = 4;
+  constexpr int TILE = WARPS * G * LS * 24;
+  extern __shared__ unsigned char smem_raw[];
+  R* sE = reinterpret_cast<R*>(smem_raw);
+  R* sF = sE + 2 * LS * LS;
+  R* tileA = sF + 2 * LS * LS;
+  R* tileB = tileA + TILE;
+
+  const int tid = threadIdx.x;
+  for (int i = tid; i < 2 * LS * LS; i += blockDim.x) {
+    sE[i] = p.E ? (R)p.E[i] : R(0);
+    sF[i] = p.F ? (R)p.F[i] : R(0);
+  }
+  const int lane = tid & 31, warp = tid >> 5;
+  const int g = lane / LS;
+  const int s = lane - g * LS;
+  const int site = (blockIdx.x * WARPS + warp) * G + g;
+  const bool active = (g < G) && (site < p.g.vh);
+  const size_t vh = p.g.vh;
+  R* myA = tileA + warp * G * LS * 24;
+  R* myB = tileB + warp * G * LS * 24;
+
+  R v[24];
+#pragma unroll
+  for (int i = 0; i < 24; ++i) v[i] = 0;
+  if (active && p.in) St::load(p.in, vh, LS, site, s, v);
+  if (g < G) {
+#pragma unroll
+    for (int i = 0; i < 24; ++i) myA[(g * LS + s) * 24 + i] = v[i];
+  }
+  __syncthreads();
+  if (p.E) {
+    apply_chiral<R, LS, G>(myA, myB, sE, lane);
+    __syncwarp();
+  }
+  const R* src = p.E ? myB : myA;
+  double nrm = 0.0;
+  R o1[24];
+#pragma unroll
+  for (int i = 0; i < 24; ++i) o1[i] = 0;
+  if (active) {
+    const R ce = (R)dev_scale(p.ce, p.ce_dev);
+#pragma unroll
+    for (int i = 0; i < 24; ++i) o1[i] = ce * src[(g * LS + s) * 24 + i];
+    if (p.x1) {
+      R xv[24];
+      St::load(p.x1, vh, LS, site, s, xv);
+      const R c = (R)dev_scale(p.cx1, p.cx1_dev);
+#pragma unroll
+      for (int i = 0; i < 24; ++i) o1[i] = fma(c, xv[i], o1[i]);
+    }
+    if (p.x2) {
+      R xv[24];
+      St::load(p.x2, vh, LS, site, s, xv);
+      const R c = (R)dev_scale(p.cx2, p.cx2_dev);
+#pragma unroll
+      for (int i = 0; i < 24; ++i) o1[i] = fma(c, xv[i], o1[i]);
+    }
+    if (p.out1) St::store(p.out1, vh, LS, site, s, o1);
+    if (p.red) {
+#pragma unroll
+      for (int i = 0; i < 24; ++i) nrm += (double)o1[i] * (double)o1[i];
+    }
+  }
+  if (p.F) {
+    __syncwarp();
+    if (g < G) {
+#pragma unroll
+      for (int i = 0; i < 24; ++i) myA[(g * LS + s) * 24 + i] = o1[i];
+    }
+    __syncwarp();
+    apply_chiral<R, LS, G>(myA, myB, sF, lane);
+    __syncwarp();
+    if (active) {
+      R o2[24];
+#pragma unroll
+      for (int i = 0; i < 24; ++i) o2[i] = myB[(g * LS + s) * 24 + i];
+      St::store(p.out2, vh, LS, site, s, o2);
+    }
+  }
+  if (p.red) block_reduce_store(nrm, p.red);
+}
+
+template <int LS, int P>
+cudaError_t run_sop(const SopParams& p, cudaStream_t st) {
+  using R = typename Store<P>::R;
+  constexpr size_t smem = sizeof(R) * (4 * LS * LS + 2 * 4 * (32 / LS) * LS * 24);
+  auto k = sop_kernel<LS, P>;
+  static bool attr_done = false;
+  if (!attr_done) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr_done = true;
+  }
+  k<<<hop_grid(LS, p.g.vh), 128, smem, st>>>(p);
+  return cudaGetLastError();
+}
+
+template <int P>
+cudaError_t sop_ls(const SopParams& p, cudaStream_t st) {
+  switch (p.g.ls) {
+    case 4: return run_sop<4, P>(p, st);
+    case 6: return run_sop<6, P>(p, st);
+    case 8: return run_sop<8, P>(p, st);
+    case 12: return run_sop<12, P>(p, st);
+    case 16: return run_sop<16, P>(p, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_sop(int prec, const SopParams& p, cudaStream_t st) {
+  switch (prec) {
+    case PREC_F64: return sop_ls<PREC_F64>(p, st);
+    case PREC_F32: return sop_ls<PREC_F32>(p, st);
+    case PREC_F16: return sop_ls<PREC_F16>(p, st);
+    case PREC_BF16: return sop_ls<PREC_BF16>(p, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+// ------------------------------------------------------------ CG update
+template <int LS, int P>
+__global__ void __launch_bounds__(128) cg_update_kernel(CgUpdParams p) {
+  using St = Store<P>;
+  using R = typename St::R;
+  constexpr int G = 32 / LS;
+  constexpr int WARPS = 4;
+  constexpr int TILE = WARPS * G * LS * 24;
+  extern __shared__ unsigned char smem_raw[];
+  R* sE = reinterpret_cast<R*>(smem_raw);
+  R* tileA = sE + 2 * LS * LS;
+  R* tileB = tileA + TILE;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < 2 * LS * LS; i += blockDim.x) sE[i] = (R)p.E[i];
+  const int lane = tid & 31, warp = tid >> 5;
+  const int g = lane / LS;
+  const int s = lane - g * LS;
+  const int site = (blockIdx.x * WARPS + warp) * G + g;
+  const bool active = (g < G) && (site < p.g.vh);
+  const size_t vh = p.g.vh;
+  R* myA = tileA + warp * G * LS * 24;
+  R* myB = tileB + warp * G * LS * 24;
+  R pv[24];
+#pragma unroll
+  for (int i = 0; i < 24; ++i) pv[i] = 0;
+  if (active) {
+    const R alpha = (R)(*p.alpha), beta = (R)(*p.beta);
+    R xv[24], rv[24];
+    St::load(p.x, vh, LS, site, s, xv);
+    St::load(p.p, vh, LS, site, s, pv);
+    St::load(p.r, vh, LS, site, s, rv);
+#pragma unroll
+    for (int i = 0; i < 24; ++i) {
+      xv[i] = fma(alpha, pv[i], xv[i]);
+      pv[i] = fma(beta, pv[i], rv[i]);
+    }
+    St::store(p.x, vh, LS, site, s, xv);
+    St::store(p.p, vh, LS, site, s, pv);
+  }
+  if (g < G) {
+#pragma unroll
+    for (int i = 0; i < 24; ++i) myA[(g * LS + s) * 24 + i] = pv[i];
+  }
+  __syncthreads();
+  apply_chiral<R, LS, G>(myA, myB, sE, lane);
+  __syncwarp();
+  if (active) {
+    R o[24];
+#pragma unroll
+    for (int i = 0; i < 24; ++i) o[i] = myB[(g * LS + s) * 24 + i];
+    St::store(p.y, vh, LS, site, s, o);
+  }
+}
+
+template <int LS, int P>
+cudaError_t run_cgu(const CgUpdParams& p, cudaStream_t st) {
+  using R = typename Store<P>::R;
+  constexpr size_t smem = sizeof(R) * (2 * LS * LS + 2 * 4 * (32 / LS) * LS * 24);
+  auto k = cg_update_kernel<LS, P>;
+  static bool attr_done = false;
+  if (!attr_done) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr_done = true;
+  }
+  k<<<hop_grid(LS, p.g.vh), 128, smem, st>>>(p);
+  return cudaGetLastError();
+}
+
+template <int P>
+cudaError_t cgu_ls(const CgUpdParams& p, cudaStream_t st) {
+  switch (p.g.ls) {
+    case 4: return run_cgu<4, P>(p, st);
+    case 6: return run_cgu<6, P>(p, st);
+    case 8: return run_cgu<8, P>(p, st);
+    case 12: return run_cgu<12, P>(p, st);
+    case 16: return run_cgu<16, P>(p, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_cg_update(int prec, const CgUpdParams& p, cudaStream_t st) {
+  switch (prec) {
+    case PREC_F64: return cgu_ls<PREC_F64>(p, st);
+    case PREC_F32: return cgu_ls<PREC_F32>(p, st);
+    case PREC_F16: return cgu_ls<PREC_F16>(p, st);
+    case PREC_BF16: return cgu_ls<PREC_BF16>(p, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+// ------------------------------------------------------------ BLAS
+template <int P>
+__global__ void axpby_kernel(Geom g, void* y, const void* x, double a, const double* a_dev,
+                             double b, const double* b_dev) {
+  using St = Store<P>;
+  using R = typename St::R;
+  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long)g.vh * g.ls) return;
+  const int site = (int)(idx / g.ls), s = (int)(idx % g.ls);
+  const R av = (R)dev_scale(a, a_dev), bv = (R)dev_scale(b, b_dev);
+  R yv[24], xv[24];
+  if (bv != R(0)) St::load(y, g.vh, g.ls, site, s, yv);
+  else {
+#pragma unroll
+    for (int i = 0; i < 24; ++i) yv[i] = 0;
+  }
+  if (x && av != R(0)) {
+    St::load(x, g.vh, g.ls, site, s, xv);
+#pragma unroll
+    for (int i = 0; i < 24; ++i) yv[i] = fma(av, xv[i], bv * yv[i]);
+  } else {
+#pragma unroll
+    for (int i = 0; i < 24; ++i) yv[i] = bv * yv[i];
+  }
+  St::store(y, g.vh, g.ls, site, s, yv);
+}
+
+template <int P>
+__global__ void dot_kernel(Geom g, const void* x, const void* y, double* red) {
+  using St = Store<P>;
+  using R = typename St::R;
+  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  double acc = 0.0;
+  if (idx < (long)g.vh * g.ls) {
+    const int site = (int)(idx / g.ls), s = (int)(idx % g.ls);
+    R xv[24], yv[24];
+    St::load(x, g.vh, g.ls, site, s, xv);
+    if (y == x) {
+#pragma unroll
+      for (int i = 0; i < 24; ++i) acc += (double)xv[i] * (double)xv[i];
+    } else {
+      St::load(y, g.vh, g.ls, site, s, yv);
+#pragma unroll
+      for (int i = 0; i < 24; ++i) acc += (double)xv[i] * (double)yv[i];
+    }
+  }
+  block_reduce_store(acc, red);
+}
+
+template <int PO, int PI>
+__global__ void convert_kernel(Geom g, void* out, const void* in) {
+  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long)g.vh * g.ls) return;
+  const int site = (int)(idx / g.ls), s = (int)(idx % g.ls);
+  typename Store<PI>::R v[24];
+  typename Store<PO>::R w[24];
+  Store<PI>::load(in, g.vh, g.ls, site, s, v);
+#pragma unroll
+  for (int i = 0; i < 24; ++i) w[i] = (typename Store<PO>::R)v[i];
+  Store<PO>::store(out, g.vh, g.ls, site, s, w);
+}
+
+// corelib Field(24, Vh, Ls): ri + 2*(c + 3*sp) + 24*(site + Vh*s)
+template <int P>
+__global__ void from_corelib_kernel(Geom g, void* out, const double* in) {
+  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long)g.vh * g.ls) return;
+  const int site = (int)(idx / g.ls), s = (int)(idx % g.ls);
+  const double* src = in + 24 * ((size_t)site + (size_t)g.vh * s);
+  typename Store<P>::R v[24];
+#pragma unroll
+  for (int i = 0; i < 24; ++i) v[i] = (typename Store<P>::R)src[i];
+  Store<P>::store(out, g.vh, g.ls, site, s, v);
+}
+
+template <int P>
+__global__ void to_corelib_kernel(Geom g, double* out, const void* in) {
+  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long)g.vh * g.ls) return;
+  const int site = (int)(idx / g.ls), s = (int)(idx % g.ls);
+  typename Store<P>::R v[24];
+  Store<P>::load(in, g.vh, g.ls, site, s, v);
+  double* dst = out + 24 * ((size_t)site + (size_t)g.vh * s);
+#pragma unroll
+  for (int i = 0; i < 24; ++i) dst[i] = (double)v[i];
+}
+
+// links: out index (ieo + 2*mu)*Vh + site_eo  (reference m_Ueo ordering,
+// src/lib_alt_Accel/Fopr/afopr_Domainwall_5din_eo-tmpl.h:140-141)
+template <int LF>
+__global__ void links_kernel(Geom g, void* out, const double* u) {
+  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long)8 * g.vh) return;
+  const int site = (int)(idx % g.vh);
+  const int pm = (int)(idx / g.vh);       // ieo + 2*mu
+  const int ieo = pm & 1, mu = pm >> 1;
+  const int ix2 = site % g.nx2;
+  const int iyzt = site / g.nx2;
+  const int y = iyzt % g.ny;
+  const int z = (iyzt / g.ny) % g.nz;
+  const int t = iyzt / (g.ny * g.nz);
+  const int x = 2 * ix2 + ((ieo + y + z + t) & 1);
+  const int nx = 2 * g.nx2;
+  const size_t lex = x + (size_t)nx * (y + (size_t)g.ny * (z + (size_t)g.nz * t));
+  const size_t vol = (size_t)2 * g.vh;
+  const double* m = u + 18 * (lex + vol * mu);
+  if (LF == LINK_F64_18) {
+    double2* o = reinterpret_cast<double2*>(out) + idx * 9;
+    for (int j = 0; j < 9; ++j) o[j] = make_double2(m[2 * j], m[2 * j + 1]);
+  } else if (LF == LINK_F64_12) {
+    double2* o = reinterpret_cast<double2*>(out) + idx * 6;
+    for (int j = 0; j < 6; ++j) o[j] = make_double2(m[2 * j], m[2 * j + 1]);
+  } else if (LF == LINK_F32_12) {
+    float4* o = reinterpret_cast<float4*>(out) + idx * 3;
+    for (int j = 0; j < 3; ++j)
+      o[j] = make_float4((float)m[4 * j], (float)m[4 * j + 1], (float)m[4 * j + 2], (float)m[4 * j + 3]);
+  } else {
+    uint4* o = reinterpret_cast<uint4*>(out) + idx * 2;
+    unsigned int w[8];
+    for (int j = 0; j < 6; ++j) w[j] = HalfOps<__half>::from2((float)m[2 * j], (float)m[2 * j + 1]);
+    w[6] = 0u; w[7] = 0u;
+    o[0] = make_uint4(w[0], w[1], w[2], w[3]);
+    o[1] = make_uint4(w[4], w[5], w[6], w[7]);
+  }
+}
+
+size_t link_bytes(int lf, size_t vh) {
+  const size_t n = 8 * vh;
+  switch (lf) {
+    case LINK_F64_18: return n * 9 * 16;
+    case LINK_F64_12: return n * 6 * 16;
+    case LINK_F32_12: return n * 3 * 16;
+    default: return n * 2 * 16;
+  }
+}
+
+__global__ void finalize_kernel(const double* partials, int n, double* out, int op) {
+  __shared__ double ws[32];
+  double v = 0.0;
+  // fixed assignment of partials to threads -> deterministic result
+  for (int i = threadIdx.x; i < n; i += blockDim.x) v += partials[i];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += ws[w];
+    if (op == FIN_SUM) {
+      out[0] = s;
+    } else if (op == FIN_CG_ALPHA) {
+      out[SC_PQ] = s;
+      out[SC_ALPHA] = out[SC_RR] / s;
+    } else if (op == FIN_CG_BETA) {
+      out[SC_BETA] = s / out[SC_RR];
+      out[SC_RR] = s;
+    }
+  }
+}
+
+// ------------------------------------------------------------ launchers
+#define B200_PREC_SWITCH(prec, FN)                          \
+  switch (prec) {                                           \
+    case PREC_F64: FN(PREC_F64); break;                     \
+    case PREC_F32: FN(PREC_F32); break;                     \
+    case PREC_F16: FN(PREC_F16); break;                     \
+    case PREC_BF16: FN(PREC_BF16); break;                   \
+    default: return cudaErrorInvalidValue;                  \
+  }
+
+cudaError_t launch_axpby(int prec, const Geom& g, void* y, const void* x, double a,
+                         const double* a_dev, double b, const double* b_dev, cudaStream_t st) {
+  const int grid = site_s_grid(g.ls, g.vh);
+#define L(PP) axpby_kernel<PP><<<grid, kSiteSBlock, 0, st>>>(g, y, x, a, a_dev, b, b_dev)
+  B200_PREC_SWITCH(prec, L)
+#undef L
+  return cudaGetLastError();
+}
+
+cudaError_t launch_dot(int prec, const Geom& g, const void* x, const void* y, double* red,
+                       cudaStream_t st) {
+  const int grid = site_s_grid(g.ls, g.vh);
+#define L(PP) dot_kernel<PP><<<grid, kSiteSBlock, 0, st>>>(g, x, y, red)
+  B200_PREC_SWITCH(prec, L)
+#undef L
+  return cudaGetLastError();
+}
+
+cudaError_t launch_convert(int pout, void* out, int pin, const void* in, const Geom& g,
+                           cudaStream_t st) {
+  const int grid = site_s_grid(g.ls, g.vh);
+#define L2(PO, PI) convert_kernel<PO, PI><<<grid, kSiteSBlock, 0, st>>>(g, out, in)
+#define LIN(PO)                                             \
+  switch (pin) {                                            \
+    case PREC_F64: L2(PO, PREC_F64); break;                 \
+    case PREC_F32: L2(PO, PREC_F32); break;                 \
+    case PREC_F16: L2(PO, PREC_F16); break;                 \
+    case PREC_BF16: L2(PO, PREC_BF16); break;               \
+    default: return cudaErrorInvalidValue;                  \
+  }
+  B200_PREC_SWITCH(pout, LIN)
+#undef LIN
+#undef L2
+  return cudaGetLastError();
+}
+
+cudaError_t launch_from_corelib(int prec, void* out, const double* in_dev, const Geom& g,
+                                cudaStream_t st) {
+  const int grid = site_s_grid(g.ls, g.vh);
+#define L(PP) from_corelib_kernel<PP><<<grid, kSiteSBlock, 0, st>>>(g, out, in_dev)
+  B200_PREC_SWITCH(prec, L)
+#undef L
+  return cudaGetLastError();
+}
+
+cudaError_t launch_to_corelib(int prec, double* out_dev, const void* in, const Geom& g,
+                              cudaStream_t st) {
+  const int grid = site_s_grid(g.ls, g.vh);
+#define L(PP) to_corelib_kernel<PP><<<grid, kSiteSBlock, 0, st>>>(g, out_dev, in)
+  B200_PREC_SWITCH(prec, L)
+#undef L
+  return cudaGetLastError();
+}
+
+cudaError_t launch_links_from_lex(int lf, void* out, const double* u_lex_dev, const Geom& g,
+                                  cudaStream_t st) {
+  const long n = 8L * g.vh;
+  const int grid = (int)((n + 127) / 128);
+  switch (lf) {
+    case LINK_F64_18: links_kernel<LINK_F64_18><<<grid, 128, 0, st>>>(g, out, u_lex_dev); break;
+    case LINK_F64_12: links_kernel<LINK_F64_12><<<grid, 128, 0, st>>>(g, out, u_lex_dev); break;
+    case LINK_F32_12: links_kernel<LINK_F32_12><<<grid, 128, 0, st>>>(g, out, u_lex_dev); break;
+    case LINK_F16_12: links_kernel<LINK_F16_12><<<grid, 128, 0, st>>>(g, out, u_lex_dev); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_finalize(const double* partials, int n, double* out, int op, cudaStream_t st) {
+  finalize_kernel<<<1, 1024, 0, st>>>(partials, n, out, op);
+  return cudaGetLastError();
+}
+
+}  // namespace b200
