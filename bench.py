@@ -1,0 +1,369 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 even/odd domain-wall hot path.
+
+Workload (the operator/solver configuration the Dslash GB/s metric is quoted
+on): 16^3x32 lattice, Ls=16, Shamir DWF M0=1.8, m=0.01, seeded near-unit SU(3)
+links exp(i*0.3*H) followed by 2 stout steps rho=0.1, Gaussian RHS, FP64.
+
+A step is one even/odd Dslash apply and its dagger through the reference
+operator interface: mult(v, w, "Deo") then mult_dag(v', w, "Deo").  Its
+algorithmic traffic is the fused D_eo byte count per 4D half-site
+    B = Ls*24*(8 + 8) + 8*18*8 = 7296 bytes  (Ls=16, FP64, 18-real links)
+counted once per apply (two applies per step).
+
+The JSON line also carries the dominant kernel's roofline (the fused hop
+kernel timed alone with CUDA events), an end-to-end number through the C ABI
+with host buffers, the FP64 CG time-to-solution at |r|/|b| < 1e-10 and the
+reference corelib CPU path timed on this host as the CPU baseline.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "lqcd-dwf-hmc_b200"))
+
+LATTICE = [16, 16, 16, 32]
+LS = 16
+MQ, M0 = 0.01, 1.8
+SEED_U, SEED_B = 1234567, 7654321
+BYTES_PER_HALF_SITE = LS * 24 * (8 + 8) + 8 * 18 * 8
+REF_HARNESS = os.path.join(REPO, "oracle", "_ref", "ref_harness")
+WORKLOAD = "dwf_eo_dslash_16x16x16x32_Ls16_f64"
+METRIC = "Dslash HBM GB/s (D_eo + D_eo^dag, 16^3x32 Ls=16 FP64)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cg", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--lattice", type=int, nargs=4, default=LATTICE)
+    return ap.parse_args()
+
+
+def workload_inputs(lattice, ls):
+    from b200dwf import synth
+    u = synth.gauge_field(lattice, SEED_U, "near", eps=0.3)
+    u = synth.stout_smear(u, lattice, 0.1, 2)
+    b = synth.spinor_field(lattice, ls, SEED_B)
+    return u, b
+
+
+def vh_of(lattice):
+    return int(np.prod(lattice)) // 2
+
+
+def read_peaks():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def read_traffic():
+    """DRAM bytes per launch of the hop kernel from the committed ncu summary."""
+    path = os.path.join(REPO, "profiles", "hop_kernel_f64_16x16x16x32_Ls16.md")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        cmd = ["nvidia-smi", "-i", str(self.device),
+               "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+               "clocks_event_reasons.sw_power_cap",
+               "--format=csv,noheader,nounits", "-lms", "100"]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thr = threading.Thread(target=self._read, daemon=True)
+            self.thr.start()
+        except OSError:
+            self.proc = None
+        time.sleep(0.25)
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        time.sleep(0.15)
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 6:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[2:6]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ reference (CPU) arm
+def run_reference_cpu(lattice, ls, steps, warmup, budget_s=60.0, threads=None):
+    """Time the reference corelib Fopr_Domainwall_eo (oracle/_ref, built from
+    the reference sources) on this host: one step = mult(v,w,"Deo") +
+    mult_dag(v,w,"Deo") on the same workload.  Returns (GB/s, seconds/step,
+    reps, threads)."""
+    if not os.path.exists(REF_HARNESS):
+        raise RuntimeError("oracle/_ref/ref_harness not built")
+    threads = threads or os.cpu_count() or 1
+    u, b = workload_inputs(lattice, ls)
+    vh = vh_of(lattice)
+    with tempfile.TemporaryDirectory() as d:
+        u.tofile(os.path.join(d, "gauge.bin"))
+        b.tofile(os.path.join(d, "src.bin"))
+
+        def timed(reps):
+            with open(os.path.join(d, "params.txt"), "w") as f:
+                f.write("lattice %s\nLs %d\nmq %r\nM0 %r\nthreads %d\nreps %d\nmodes Deo dag_Deo\n"
+                        % (" ".join(map(str, lattice)), ls, MQ, M0, threads, reps))
+            r = subprocess.run([REF_HARNESS, "time", os.path.join(d, "params.txt"), d, d],
+                               capture_output=True, text=True, check=True)
+            t = {}
+            for line in r.stdout.splitlines():
+                p = line.split()
+                if len(p) == 2 and p[0] in ("Deo", "dag_Deo"):
+                    t[p[0]] = float(p[1])
+            return t["Deo"] + t["dag_Deo"]
+
+        probe = timed(1)
+        reps = int(max(1, min(steps, budget_s / max(probe, 1e-6))))
+        t_step = timed(reps)
+    gbs = 2 * BYTES_PER_HALF_SITE * vh / t_step / 1e9
+    return gbs, t_step, reps, threads
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    try:
+        gbs, t_step, reps, threads = run_reference_cpu(args.lattice, LS, args.steps, args.warmup)
+    except Exception as e:  # noqa: BLE001
+        print(json.dumps({"impl": "reference", "unavailable": "reference corelib harness failed: %s" % e}))
+        return
+    line = {
+        "impl": "reference", "metric": METRIC, "value": gbs, "unit": "GB/s", "n_gpus": args.gpus,
+        "steps": reps, "warmup": 1, "ms_per_step": t_step * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "lattice": args.lattice, "Ls": LS, "M0": M0, "mq": MQ,
+                   "links": "near-unit exp(i*0.3*H) + 2 stout rho=0.1", "parallelism": "replicas"},
+        "cpu_baseline": {"value": gbs, "unit": "GB/s", "cores": threads, "kind": "reference",
+                         "sample": "%d steps of corelib Fopr_Domainwall_eo mult Deo + mult_dag Deo on "
+                                   "the full workload lattice (bounded to ~60 s)" % reps},
+        "e2e": {"value": gbs, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+# ------------------------------------------------------------------ B200 arm
+def b200_arm(args, rank, world, local_rank):
+    import torch
+    import b200dwf
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    torch.cuda.set_device(local_rank)
+    b200dwf.check(b200dwf.lib().b200_init(local_rank, 0))
+    lattice = args.lattice
+    vh = vh_of(lattice)
+    u, b = workload_inputs(lattice, LS)
+    op = b200dwf.DomainWall(lattice, LS, MQ, M0, 1.0, 0.0, 1.0, (1, 1, 1, -1))
+    op.set_config(u)
+    w = op.new_field(0)
+    v1 = op.new_field(0)
+    v2 = op.new_field(0)
+    op.convert(w, b)
+    step_bytes = 2 * BYTES_PER_HALF_SITE * vh
+
+    def step():
+        op.mult(v1, w, "Deo")
+        op.mult_dag(v2, w, "Deo")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        e0.record()
+        for _ in range(args.steps):
+            step()
+        e1.record()
+        torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    t_total = e0.elapsed_time(e1) / 1e3
+    if dist is not None:
+        tt = torch.tensor([t_total], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_total = float(tt.item())
+    value = world * step_bytes * args.steps / t_total / 1e9
+
+    # dominant kernel: mult_dag("Deo") is exactly one launch of the fused hop kernel
+    nk = max(50, min(args.steps, 500))
+    for _ in range(10):
+        op.mult_dag(v2, w, "Deo")
+    torch.cuda.synchronize()
+    k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    k0.record()
+    for _ in range(nk):
+        op.mult_dag(v2, w, "Deo")
+    k1.record()
+    torch.cuda.synchronize()
+    t_hop = k0.elapsed_time(k1) / 1e3 / nk
+    peak, peak_kind = read_peaks()
+    achieved = BYTES_PER_HALF_SITE * vh / t_hop / 1e9
+    traffic = read_traffic()
+
+    # end to end through the C ABI with pinned host buffers
+    nbytes = 24 * vh * LS * 8
+    h_in = torch.from_numpy(b).pin_memory()
+    h_out1 = torch.empty(24 * vh * LS, dtype=torch.float64).pin_memory()
+    h_out2 = torch.empty(24 * vh * LS, dtype=torch.float64).pin_memory()
+    ne = max(3, min(args.steps, 20))
+
+    def e2e_step():
+        op.convert(w, h_in.numpy())
+        step()
+        op.reverse(v1, out=h_out1.numpy())
+        op.reverse(v2, out=h_out2.numpy())
+
+    e2e_step()
+    torch.cuda.synchronize()
+    barrier()
+    q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    q0.record()
+    for _ in range(ne):
+        e2e_step()
+    q1.record()
+    torch.cuda.synchronize()
+    t_e2e = q0.elapsed_time(q1) / 1e3
+    if dist is not None:
+        tt = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_e2e = float(tt.item())
+    e2e_value = world * step_bytes * ne / t_e2e / 1e9
+
+    # FP64 CG time to solution, |r|/|b| < 1e-10
+    cg = None
+    if not args.no_cg:
+        x = op.new_field(0)
+        torch.cuda.synchronize()
+        c0 = time.perf_counter()
+        n, diff, rc = op.cg(x, w, 1e-20, 20000)
+        torch.cuda.synchronize()
+        c1 = time.perf_counter()
+        cg = {"tol_rel_residual": 1e-10, "iterations": n, "true_rel_residual": diff,
+              "seconds": c1 - c0, "converged": rc == 0,
+              "ms_per_iteration": (c1 - c0) * 1e3 / max(n, 1)}
+
+    if rank != 0:
+        return
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        try:
+            gbs, t_step, reps, threads = run_reference_cpu(lattice, LS, 100, 1, budget_s=20.0)
+            cpu = {"value": gbs, "unit": "GB/s", "cores": threads, "kind": "reference",
+                   "sample": "%d steps (Deo + Ddag_eo) of the reference corelib Fopr_Domainwall_eo "
+                             "on the full workload lattice, bounded to ~20 s" % reps}
+        except Exception as e:  # noqa: BLE001
+            cpu = {"value": None, "unit": "GB/s", "cores": 0, "kind": "reference",
+                   "sample": "unavailable: %s" % e}
+    line = {
+        "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_total * 1e3 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "lattice": lattice, "Ls": LS, "M0": M0, "mq": MQ,
+                   "links": "near-unit exp(i*0.3*H) + 2 stout rho=0.1", "parallelism": "replicas",
+                   "l2": "inputs larger than L2 (%.0f MB per field)" % (nbytes / 1e6)},
+        "clocks": clk.summary(),
+        "gpu_launches": 3 * args.steps,
+        "roofline": {"kernel": "dwf_hop_kernel<16,f64,dag> (mult_dag Deo)", "bound": "hbm",
+                     "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": BYTES_PER_HALF_SITE * vh,
+                     "launch_us": t_hop * 1e6},
+        "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": nbytes,
+                "d2h_bytes_per_step": 2 * nbytes},
+        "cg_f64": cg,
+        "autotune": b200dwf.tuning_table().strip().splitlines(),
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        b200_arm(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -114,6 +114,14 @@ int b200_field_copy_convert(b200_dwf_t *op, int prec_out, void *out, int prec_in
 int b200_cg_solve(b200_dwf_t *op, int prec, void *x, const void *b, int maxiter,
                   double tol2, int *nconv, double *diff, void *stream);
 
+/* ---------------------------------------------------------------- tuning
+ * Text table of the autotuner's choices (one line per geometry, precision and
+ * kernel epilogue: chosen occupancy variant and its time per launch).  The
+ * reference picks its kernel shape at compile time (NUM_WORKERS /
+ * VECTOR_LENGTH, src/lib_alt_Accel/inline/define_params.h:35-36); here the
+ * choice is measured on the first launch (disable with B200_AUTOTUNE=0). */
+int b200_tuning_table(char *buf, size_t n);
+
 #ifdef __cplusplus
 }
 #endif

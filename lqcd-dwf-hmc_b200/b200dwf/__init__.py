@@ -60,6 +60,7 @@ def lib():
     L.b200_field_norm2.argtypes = [vp, ctypes.c_int, vp, dp, vp]
     L.b200_field_dot.argtypes = [vp, ctypes.c_int, vp, vp, dp, vp]
     L.b200_field_copy_convert.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, vp, vp]
+    L.b200_tuning_table.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
     L.b200_cg_solve.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_double,
                                 ip, dp, vp]
     _lib = L
@@ -70,6 +71,13 @@ def check(rc):
     if rc != 0:
         raise B200Error("b200 error %d: %s" % (rc, lib().b200_last_error().decode()))
     return rc
+
+
+def tuning_table():
+    """The autotuner's choices so far, one text line per kernel configuration."""
+    buf = ctypes.create_string_buffer(16384)
+    check(lib().b200_tuning_table(buf, len(buf)))
+    return buf.value.decode()
 
 
 def _dp(a):
@@ -141,8 +149,9 @@ class DomainWall:
         w = np.ascontiguousarray(w_host, np.float64)
         check(lib().b200_field_convert(self.handle, v.prec, v.ptr, _dp(w), None))
 
-    def reverse(self, w):
-        out = np.empty(self.nreal)
+    def reverse(self, w, out=None):
+        if out is None:
+            out = np.empty(self.nreal)
         check(lib().b200_field_reverse(self.handle, w.prec, _dp(out), w.ptr, None))
         return out
 

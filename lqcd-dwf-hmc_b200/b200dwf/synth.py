@@ -104,3 +104,60 @@ def plaquette(links, lattice):
                           np.conj(umu_xnu), np.conj(unu))
             tot += np.trace(p, axis1=-2, axis2=-1).real.sum()
     return tot / (6 * 3 * nvol)
+
+
+def _as_complex(links, lattice):
+    nx, ny, nz, nt = lattice
+    r = links.reshape(4, nt, nz, ny, nx, 3, 3, 2)
+    return r[..., 0] + 1j * r[..., 1]
+
+
+def _as_real(u):
+    out = np.empty(u.shape + (2,))
+    out[..., 0] = u.real
+    out[..., 1] = u.imag
+    return out.reshape(-1)
+
+
+def _dag(m):
+    return np.conj(np.swapaxes(m, -1, -2))
+
+
+def staples(u):
+    """Sum over nu != mu of the two plaquette staples attached to U_mu(x):
+    U_nu(x) U_mu(x+nu) U_nu(x+mu)^+ + U_nu(x-nu)^+ U_mu(x-nu) U_nu(x-nu+mu).
+    u: complex [4, t, z, y, x, 3, 3]; array axis of direction mu is 3-mu."""
+    c = np.zeros_like(u)
+    for mu in range(4):
+        amu = 4 - mu
+        for nu in range(4):
+            if nu == mu:
+                continue
+            anu = 4 - nu
+            unu = u[nu]
+            umu_xnu = np.roll(u[mu], -1, axis=anu - 1)
+            unu_xmu = np.roll(unu, -1, axis=amu - 1)
+            c[mu] += unu @ umu_xnu @ _dag(unu_xmu)
+            unu_xmnu = np.roll(unu, 1, axis=anu - 1)
+            umu_xmnu = np.roll(u[mu], 1, axis=anu - 1)
+            unu_xmnu_pmu = np.roll(unu_xmnu, -1, axis=amu - 1)
+            c[mu] += _dag(unu_xmnu) @ umu_xmnu @ unu_xmnu_pmu
+    return c
+
+
+def stout_smear(links, lattice, rho, nsteps):
+    """Stout smearing U -> exp(iQ) U with Q = (i/2)(W^+ - W) - (i/6) tr(W^+ - W),
+    W = rho C U^+ (Morningstar-Peardon), applied nsteps times to all four
+    directions at once (the APE-type uniform-rho stout used by the reference
+    Smear_APE + Projection_Stout_SU3).  Returns links in the same layout."""
+    u = _as_complex(links, lattice).copy()
+    for _ in range(nsteps):
+        c = staples(u)
+        w = rho * c @ _dag(u)
+        a = _dag(w) - w
+        tr = np.trace(a, axis1=-2, axis2=-1)[..., None, None] / 3.0
+        q = 0.5j * (a - tr * np.eye(3))
+        ev, vec = np.linalg.eigh(q)
+        expq = vec @ (np.exp(1j * ev)[..., None] * _dag(vec))
+        u = expq @ u
+    return _as_real(u)

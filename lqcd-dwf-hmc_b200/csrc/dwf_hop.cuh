@@ -19,6 +19,7 @@
 #pragma once
 
 #include "dwf_common.cuh"
+#include "dwf_chain.cuh"
 
 namespace b200 {
 
@@ -169,8 +170,9 @@ struct HopParams {
   void* out1;            // o1 store target (nullable)
   void* out2;            // o2 store target (nullable)
   const void* x1;        // axpy operand X (nullable)
-  const double* E;       // [2][Ls][Ls] chiral matrices applied to acc
-  const double* F;       // optional [2][Ls][Ls] second map, o2 = F o1
+  int epi;               // EpiKind applied to the hop result
+  int fk;                // FKind second map, o2 = F o1 (F_NONE: no o2)
+  int variant;           // occupancy variant (0/1), chosen by the autotuner
   const void* x2;        // second axpy operand (nullable)
   // o1 = ce * E(acc) + c_x1 * X1 + c_x2 * X2; each scalar is multiplied by
   // the device value behind its _dev pointer when that pointer is non-null
@@ -184,64 +186,28 @@ struct HopParams {
   double bc[4];
 };
 
-// Epilogue tile helpers.  Tile layout per warp: [site g][s][24 reals].
-// unit u = (g, color, ri, pair): 12 per site; the unit's fifth-dimension
-// column is moved to the chiral basis x+- = v_pair +- v_(pair+2), multiplied by
-// the dense E+ / E- (uniform smem reads, broadcast to the warp) and moved back.
-template <typename R, int LS, int G>
-__device__ __forceinline__ void apply_chiral(const R* __restrict__ tile_in, R* __restrict__ tile_out,
-                                             const R* __restrict__ Em, int lane) {
-#pragma unroll 1
-  for (int u = lane; u < 12 * G; u += 32) {
-    const int g = u / 12;
-    const int r = u - 12 * g;
-    const int pair = r / 6;
-    const int cr = r - 6 * pair;
-    const R* ti = tile_in + g * LS * 24 + 6 * pair + cr;
-    R* to = tile_out + g * LS * 24 + 6 * pair + cr;
-    R xp[LS], xm[LS];
-#pragma unroll
-    for (int s = 0; s < LS; ++s) {
-      const R a = ti[s * 24];
-      const R b = ti[s * 24 + 12];
-      xp[s] = a + b;
-      xm[s] = a - b;
-    }
-#pragma unroll
-    for (int s = 0; s < LS; ++s) {
-      R yp = 0, ym = 0;
-#pragma unroll
-      for (int t = 0; t < LS; ++t) {
-        yp = fma(Em[s * LS + t], xp[t], yp);
-        ym = fma(Em[LS * LS + s * LS + t], xm[t], ym);
-      }
-      to[s * 24] = R(0.5) * (yp + ym);
-      to[s * 24 + 12] = R(0.5) * (yp - ym);
-    }
-  }
-}
+// Occupancy variants (minimum resident 128-thread blocks per SM requested from
+// the register allocator); the plan's autotuner times both and keeps the faster.
+template <int P> struct HopMinBlocks { static constexpr int v0 = 3, v1 = 4; };
+template <> struct HopMinBlocks<PREC_F32> { static constexpr int v0 = 4, v1 = 6; };
+template <> struct HopMinBlocks<PREC_F16> { static constexpr int v0 = 4, v1 = 6; };
+template <> struct HopMinBlocks<PREC_BF16> { static constexpr int v0 = 4, v1 = 6; };
 
-template <int LS, int P, int LF, bool kDagHop>
-__global__ void __launch_bounds__(128) dwf_hop_kernel(HopParams p) {
+template <int LS, int P, int LF, int EPI, int FK, int MB>
+__global__ void __launch_bounds__(128, MB)
+dwf_hop_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename Store<P>::R> k) {
   using St = Store<P>;
   using R = typename St::R;
+  constexpr bool kDagHop = EpiIsDag<EPI>::v;
   constexpr int G = 32 / LS;              // sites per warp
   constexpr int WARPS = 4;
-  constexpr int TILE = WARPS * G * LS * 24;
+  constexpr bool kTile = (EPI != EPI_HALF) || (FK != F_NONE);
 
   extern __shared__ unsigned char smem_raw[];
-  R* sE = reinterpret_cast<R*>(smem_raw);              // 2*LS*LS
-  R* sF = sE + 2 * LS * LS;                             // 2*LS*LS
-  R* tileA = sF + 2 * LS * LS;                          // TILE
-  R* tileB = tileA + TILE;                              // TILE
+  R* tile_all = reinterpret_cast<R*>(smem_raw);        // WARPS * G * LS * 24
   __shared__ double red_warp[WARPS];
 
   const int tid = threadIdx.x;
-  for (int i = tid; i < 2 * LS * LS; i += blockDim.x) {
-    sE[i] = (R)p.E[i];
-    sF[i] = p.F ? (R)p.F[i] : R(0);
-  }
-
   const int lane = tid & 31;
   const int warp = tid >> 5;
   const int g = lane / LS;
@@ -265,15 +231,13 @@ __global__ void __launch_bounds__(128) dwf_hop_kernel(HopParams p) {
     const int x = 2 * ix2 + keo;
     const int nx = 2 * p.nx2;
     const int ieo = p.ieo;
-    const size_t strideMu = vh;          // links: ((parity*4+mu)*Vh + site)
+    const size_t strideMu = vh;          // links: ((ieo + 2*mu)*Vh + site)
 
 #define B200_HOP_DIR(MU, COORD, EXT, NBP, NBM)                                       \
     {                                                                                \
       R w[24], h[12], o[12], u[18];                                                  \
-      /* forward: (1 - g_mu) U_mu(x) w(x+mu) */                                      \
       {                                                                              \
-        const bool edge = (COORD == EXT - 1);                                        \
-        const R ph = edge ? (R)p.bc[MU] : R(1);                                      \
+        const R ph = (COORD == EXT - 1) ? (R)p.bc[MU] : R(1);                        \
         const int nb = NBP;                                                          \
         St::load(p.in, vh, LS, nb, s, w);                                            \
         if (kDagHop) {                                                               \
@@ -285,10 +249,8 @@ __global__ void __launch_bounds__(128) dwf_hop_kernel(HopParams p) {
         su3_mult_half<R, false>(u, h, o);                                            \
         reconstruct_acc<R, MU, 1>(acc, o, ph);                                       \
       }                                                                              \
-      /* backward: (1 + g_mu) U_mu(x-mu)^+ w(x-mu) */                                \
       {                                                                              \
-        const bool edge = (COORD == 0);                                              \
-        const R ph = edge ? (R)p.bc[MU] : R(1);                                      \
+        const R ph = (COORD == 0) ? (R)p.bc[MU] : R(1);                              \
         const int nb = NBM;                                                          \
         St::load(p.in, vh, LS, nb, s, w);                                            \
         if (kDagHop) {                                                               \
@@ -303,7 +265,6 @@ __global__ void __launch_bounds__(128) dwf_hop_kernel(HopParams p) {
     }
 
     const int row = p.nx2 * iyzt;
-    // x: neighbour x+1 has ix2 + keo (wrapping inside the row), x-1 has ix2 - (1-keo)
     B200_HOP_DIR(0, x, nx,
                  row + ((ix2 + keo == p.nx2) ? 0 : ix2 + keo),
                  row + ((ix2 - 1 + keo < 0) ? p.nx2 - 1 : ix2 - 1 + keo));
@@ -322,23 +283,34 @@ __global__ void __launch_bounds__(128) dwf_hop_kernel(HopParams p) {
 #undef B200_HOP_DIR
   }
 
-  // ---------------- epilogue: chiral fifth-dimension map on the site tile
-  R* myA = tileA + (size_t)warp * G * LS * 24;
-  R* myB = tileB + (size_t)warp * G * LS * 24;
-  if (g < G) {
+  // ---------------- epilogue: fifth-dimension chain on the site column
+  R* tile = tile_all + (size_t)warp * G * LS * 24;
+  R o1[24];
+  if (!kTile || EPI == EPI_HALF) {
 #pragma unroll
-    for (int i = 0; i < 24; ++i) myA[(g * LS + s) * 24 + i] = acc[i];
+    for (int i = 0; i < 24; ++i) o1[i] = R(-0.5) * acc[i];
+  } else {
+    if (g < G) {
+#pragma unroll
+      for (int i = 0; i < 24; ++i) tile[(g * LS + s) * 24 + i] = acc[i];
+    }
+    __syncwarp();
+    tile_chiral<R, LS, G>(tile, lane, [&](R* xp, R* xm) {
+      apply_epi<R, LS, 0, EPI>(k, xp);
+      apply_epi<R, LS, 1, EPI>(k, xm);
+    });
+    __syncwarp();
+    if (g < G) {
+#pragma unroll
+      for (int i = 0; i < 24; ++i) o1[i] = tile[(g * LS + s) * 24 + i];
+    }
   }
-  __syncthreads();   // also covers the sE/sF fill
-  apply_chiral<R, LS, G>(myA, myB, sE, lane);
-  __syncwarp();
 
   double nrm = 0.0;
   if (active) {
-    R o1[24];
     const R ce = (R)(p.ce * (p.ce_dev ? *p.ce_dev : 1.0));
 #pragma unroll
-    for (int i = 0; i < 24; ++i) o1[i] = ce * myB[(g * LS + s) * 24 + i];
+    for (int i = 0; i < 24; ++i) o1[i] *= ce;
     if (p.x1) {
       R xv[24];
       St::load(p.x1, vh, LS, site, s, xv);
@@ -358,19 +330,23 @@ __global__ void __launch_bounds__(128) dwf_hop_kernel(HopParams p) {
 #pragma unroll
       for (int i = 0; i < 24; ++i) nrm += (double)o1[i] * (double)o1[i];
     }
-    if (p.F) {
-#pragma unroll
-      for (int i = 0; i < 24; ++i) myA[(g * LS + s) * 24 + i] = o1[i];
-    }
   }
-  if (p.F) {
+  if (FK != F_NONE) {
     __syncwarp();
-    apply_chiral<R, LS, G>(myA, myB, sF, lane);
+    if (g < G) {
+#pragma unroll
+      for (int i = 0; i < 24; ++i) tile[(g * LS + s) * 24 + i] = o1[i];
+    }
+    __syncwarp();
+    tile_chiral<R, LS, G>(tile, lane, [&](R* xp, R* xm) {
+      apply_f<R, LS, 0, FK>(k, xp);
+      apply_f<R, LS, 1, FK>(k, xm);
+    });
     __syncwarp();
     if (active) {
       R o2[24];
 #pragma unroll
-      for (int i = 0; i < 24; ++i) o2[i] = myB[(g * LS + s) * 24 + i];
+      for (int i = 0; i < 24; ++i) o2[i] = tile[(g * LS + s) * 24 + i];
       St::store(p.out2, vh, LS, site, s, o2);
     }
   }
@@ -391,7 +367,7 @@ __global__ void __launch_bounds__(128) dwf_hop_kernel(HopParams p) {
 template <int LS, int P>
 constexpr size_t hop_smem_bytes() {
   using R = typename Store<P>::R;
-  return sizeof(R) * (4 * LS * LS + 2 * 4 * (32 / LS) * LS * 24);
+  return sizeof(R) * (4 * (32 / LS) * LS * 24);
 }
 
 }  // namespace b200

@@ -5,6 +5,7 @@
 #include <stddef.h>
 
 #include "dwf_common.cuh"
+#include "dwf_chain.cuh"
 
 namespace b200 {
 
@@ -16,9 +17,13 @@ struct Geom {
   int vh;
 };
 
+// Site-local fifth-dimension maps (chiral-basis chains of dwf_chain.cuh).
+enum SopKind {
+  SOP_ID = 0, SOP_M5PRE, SOP_M5DAG, SOP_DEE, SOP_DEE_T, SOP_LU, SOP_LUDAG, SOP_G5R, SOP_R
+};
+
 // Parameters of the site-local fifth-dimension kernel:
-//   o1 = cx1*X1 + cx2*X2 + ce * E(in)     (E: chiral pair of Ls x Ls maps)
-//   o2 = F(o1)
+//   o1 = ce * A(in) + cx1*X1 + cx2*X2,   o2 = B(o1)   (A = opa, B = opb)
 // Scalars with a _dev pointer are multiplied by that device value at run time.
 struct SopParams {
   const void* in;
@@ -26,8 +31,7 @@ struct SopParams {
   const void* x2;
   void* out1;
   void* out2;
-  const double* E;
-  const double* F;
+  int opa, opb;
   double cx1, cx2, ce;
   const double* cx1_dev;
   const double* cx2_dev;
@@ -37,13 +41,12 @@ struct SopParams {
 };
 
 // CG vector update fused with the M5 pre-factor of the next hop:
-//   x += alpha*p;  p = r + beta*p;  y = E(p)   (alpha, beta device scalars)
+//   x += alpha*p;  p = r + beta*p;  y = M5pre(p)   (alpha, beta device scalars)
 struct CgUpdParams {
   void* x;
   void* p;
   const void* r;
   void* y;
-  const double* E;
   const double* alpha;
   const double* beta;
   Geom g;
@@ -54,10 +57,20 @@ int hop_grid(int ls, int vh);
 int site_s_grid(int ls, int vh);
 constexpr int kSiteSBlock = 128;
 
-// Hop kernel dispatch (prec = storage precision of in/out fields).
-cudaError_t launch_hop(int prec, bool dag, const HopParams& p, cudaStream_t st);
-cudaError_t launch_sop(int prec, const SopParams& p, cudaStream_t st);
-cudaError_t launch_cg_update(int prec, const CgUpdParams& p, cudaStream_t st);
+// Fifth-dimension chain coefficients of one operator in both arithmetic types.
+struct ChainCoefs {
+  ChainCoef<double> d;
+  ChainCoef<float> f;
+  ChainCoef<double> dee_d;   // D_ee: b -> b(4-M0)+1, c -> c(4-M0)-1
+  ChainCoef<float> dee_f;
+};
+
+// Hop kernel dispatch (prec = storage precision of in/out fields; the hop
+// direction (plain or gamma5-sandwiched dagger) follows from p.epi).
+cudaError_t launch_hop(int prec, const HopParams& p, const ChainCoefs& c, cudaStream_t st);
+cudaError_t launch_cg_update(int prec, const CgUpdParams& p, const ChainCoefs& c, cudaStream_t st);
+cudaError_t launch_sop(int prec, const SopParams& p, const ChainCoefs& c, cudaStream_t st);
+
 
 // y = a*x + b*y over the whole field (a, b optionally scaled by device values)
 cudaError_t launch_axpby(int prec, const Geom& g, void* y, const void* x, double a,

@@ -5,8 +5,12 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/b200dwf.h"
@@ -40,68 +44,8 @@ int fail(int code, const char* fmt, ...) {
 bool ls_supported(int ls) { return ls == 4 || ls == 6 || ls == 8 || ls == 12 || ls == 16; }
 }  // namespace
 
-// ------------------------------------------------------------ chiral maps
-// Every fifth-dimension operator of the even/odd DWF matrix is block-diagonal
-// in chirality x+- = v_p +- v_(p+2) (Dirac basis, gamma5 swaps spins p, p+2)
-// and acts identically on every site, color, re/im and spin pair.  A map is
-// stored as two dense Ls x Ls real matrices: m[chi*Ls*Ls + s*Ls + t].
+// ------------------------------------------------------------ coefficients
 namespace {
-
-struct Chiral {
-  int ls = 0;
-  std::vector<double> m;
-  Chiral() {}
-  explicit Chiral(int n) : ls(n), m(2 * n * n, 0.0) {}
-  double& at(int chi, int s, int t) { return m[(size_t)chi * ls * ls + s * ls + t]; }
-  double at(int chi, int s, int t) const { return m[(size_t)chi * ls * ls + s * ls + t]; }
-  static Chiral identity(int n, double sp = 1.0, double sm = 1.0) {
-    Chiral r(n);
-    for (int s = 0; s < n; ++s) { r.at(0, s, s) = sp; r.at(1, s, s) = sm; }
-    return r;
-  }
-};
-
-// C = A * B  (B applied first)
-Chiral mul(const Chiral& A, const Chiral& B) {
-  Chiral C(A.ls);
-  for (int chi = 0; chi < 2; ++chi)
-    for (int s = 0; s < A.ls; ++s)
-      for (int t = 0; t < A.ls; ++t) {
-        double v = 0;
-        for (int k = 0; k < A.ls; ++k) v += A.at(chi, s, k) * B.at(chi, k, t);
-        C.at(chi, s, t) = v;
-      }
-  return C;
-}
-
-Chiral transpose(const Chiral& A) {
-  Chiral C(A.ls);
-  for (int chi = 0; chi < 2; ++chi)
-    for (int s = 0; s < A.ls; ++s)
-      for (int t = 0; t < A.ls; ++t) C.at(chi, s, t) = A.at(chi, t, s);
-  return C;
-}
-
-Chiral scaled(const Chiral& A, double a) {
-  Chiral C = A;
-  for (auto& v : C.m) v *= a;
-  return C;
-}
-
-// Build a chiral map from a function that applies it to one chirality column.
-template <typename Fn>
-Chiral from_fn(int ls, Fn fn) {
-  Chiral C(ls);
-  std::vector<double> x(ls), y(ls);
-  for (int chi = 0; chi < 2; ++chi)
-    for (int t = 0; t < ls; ++t) {
-      std::fill(x.begin(), x.end(), 0.0);
-      x[t] = 1.0;
-      fn(chi, x.data(), y.data());
-      for (int s = 0; s < ls; ++s) C.at(chi, s, t) = y[s];
-    }
-  return C;
-}
 
 struct DwfCoef {
   int ls;
@@ -129,108 +73,6 @@ void set_precond(DwfCoef& k) {
   k.g = k.e[n - 2] * k.dm[n - 2];
 }
 
-// M5-type map y = cw*Wf(x) + cv*(Fup (1-g5) x(s+1) + Fdn (1+g5) x(s-1)) in the
-// chiral basis.  Wf = (alpha P+ + P-) at s=0, (P+ + alpha P-) at s=Ls-1, alpha
-// in the bulk; Fup = alpha/2 except -mq/2 at s=Ls-1, Fdn = alpha/2 except
-// -mq/2 at s=0 (walls wrap in s).  Reference: D_eo pre-factor
-// mult_Domainwall_5din_eo_openacc-inc.h:122-227, D_ee :14-119.
-Chiral m5_map(const DwfCoef& k, const std::vector<double>& cw, const std::vector<double>& cv) {
-  const int n = k.ls;
-  return from_fn(n, [&](int chi, const double* x, double* y) {
-    for (int s = 0; s < n; ++s) {
-      double wf;
-      if (chi == 0) wf = (s == n - 1) ? 1.0 : k.alpha;
-      else wf = (s == 0) ? 1.0 : k.alpha;
-      const double fup = (s == n - 1) ? -0.5 * k.mq : 0.5 * k.alpha;
-      const double fdn = (s == 0) ? -0.5 * k.mq : 0.5 * k.alpha;
-      double v = cw[s] * wf * x[s];
-      if (chi == 0) v += 2.0 * cv[s] * fdn * x[(s - 1 + n) % n];
-      else v += 2.0 * cv[s] * fup * x[(s + 1) % n];
-      y[s] = v;
-    }
-  });
-}
-
-// M_ee^-1 = U^-1 L^-1 (corelib afopr_Domainwall_eo-tmpl.h:1022-1119; Accel
-// mult_Domainwall_5din_LUinv_openacc-inc.h:14-200), chiral form.
-Chiral lu_inv_map(const DwfCoef& k) {
-  const int n = k.ls;
-  return from_fn(n, [&](int chi, const double* w, double* out) {
-    std::vector<double> v(n);
-    // L^-1
-    if (chi == 0) {
-      v[0] = w[0];
-      for (int s = 1; s < n; ++s) v[s] = w[s] + k.dm[s] / k.dp[s - 1] * v[s - 1];
-    } else {
-      double y = 0;
-      for (int s = 0; s < n - 1; ++s) { v[s] = w[s]; y += k.e[s] * w[s]; }
-      v[n - 1] = w[n - 1] - y;
-    }
-    // U^-1
-    if (chi == 0) {
-      out[n - 1] = k.alpha * v[n - 1] / (k.dp[n - 1] + k.g);
-      const double Y = out[n - 1];
-      for (int s = n - 2; s >= 0; --s) out[s] = (v[s] - k.f[s] * Y) / k.dp[s];
-    } else {
-      out[n - 1] = v[n - 1] / (k.dp[n - 1] + k.g);
-      for (int s = n - 2; s >= 0; --s) out[s] = (v[s] + k.dm[s] * out[s + 1]) / k.dp[s];
-      out[0] *= k.alpha;
-    }
-  });
-}
-
-// (M_ee^-1)^+ = L^-+ U^-+ (corelib afopr_Domainwall_eo-tmpl.h:1124-1240; Accel
-// mult_Domainwall_5din_LUinv_openacc-inc.h:204-398), chiral form.
-Chiral lu_dag_inv_map(const DwfCoef& k) {
-  const int n = k.ls;
-  return from_fn(n, [&](int chi, const double* w, double* out) {
-    std::vector<double> v(n);
-    // U^-+
-    if (chi == 0) {
-      double Y = 0;
-      for (int s = 0; s < n - 1; ++s) { v[s] = w[s] / k.dp[s]; Y += k.f[s] * v[s]; }
-      v[n - 1] = k.alpha * (w[n - 1] - Y) / (k.dp[n - 1] + k.g);
-    } else {
-      v[0] = k.alpha * w[0] / k.dp[0];
-      for (int s = 1; s < n - 1; ++s) v[s] = (w[s] + k.dm[s - 1] * v[s - 1]) / k.dp[s];
-      v[n - 1] = (w[n - 1] + k.dm[n - 2] * v[n - 2]) / (k.dp[n - 1] + k.g);
-    }
-    // L^-+
-    if (chi == 0) {
-      out[n - 1] = v[n - 1];
-      for (int s = n - 2; s >= 0; --s) out[s] = v[s] + k.dm[s + 1] / k.dp[s] * out[s + 1];
-    } else {
-      const double Y = v[n - 1];
-      out[n - 1] = v[n - 1];
-      for (int s = n - 2; s >= 0; --s) out[s] = v[s] - k.e[s] * Y;
-    }
-  });
-}
-
-Chiral reflect_map(int n, double sm) {
-  Chiral C(n);
-  for (int s = 0; s < n; ++s) { C.at(0, n - 1 - s, s) = 1.0; C.at(1, n - 1 - s, s) = sm; }
-  return C;
-}
-
-enum MatId {
-  MAT_M5PRE = 0,   // D_eo pre-factor (alone, before a hop)
-  MAT_HALF,        // -1/2 (hop of D_eo)
-  MAT_DDAGEO,      // M5^+ (-1/2 g5)            : Ddag_eo epilogue
-  MAT_DEE,
-  MAT_DEE_T,
-  MAT_LU,
-  MAT_LUDAG,
-  MAT_G5R,
-  MAT_R,
-  MAT_K1,          // M5pre LU (-1/2)           : D chain, first hop
-  MAT_K2N,         // -LU (-1/2)                : D chain, second hop (o = w - ...)
-  MAT_K3,          // LUdag M5^+ (-1/2 g5)      : Ddag chain, first hop
-  MAT_K4N,         // -M5^+ (-1/2 g5)           : Ddag chain, second hop
-  MAT_ID,
-  MAT_COUNT
-};
-
 }  // namespace
 
 // ------------------------------------------------------------ plan
@@ -239,7 +81,6 @@ struct b200_dwf {
   DwfCoef k;
   int bc[4];
   Geom g;
-  double* mats = nullptr;       // device [MAT_COUNT][2][Ls][Ls]
   void* links[4] = {nullptr, nullptr, nullptr, nullptr};
   double* u_lex = nullptr;      // device copy of the lexical links
   bool have_links = false;
@@ -249,7 +90,8 @@ struct b200_dwf {
   double* sc_host = nullptr;    // pinned mirror
   double* stage = nullptr;      // device f64 staging for convert/reverse
   void* work[8][4] = {};        // work fields per precision
-  const double* mat(int id) const { return mats + (size_t)id * 2 * k.ls * k.ls; }
+  void* tune_out[2][4] = {};    // autotuner scratch outputs per precision
+  ChainCoefs coefs;             // fifth-dimension chain coefficients
 };
 
 namespace {
@@ -278,9 +120,11 @@ int ensure_links(b200_dwf* op, int prec, cudaStream_t st) {
   return 0;
 }
 
-HopParams hop_base(const b200_dwf* op, int prec, int ieo) {
+HopParams hop_base(const b200_dwf* op, int prec, int ieo, int epi, int fk = F_NONE) {
   HopParams p;
   memset(&p, 0, sizeof(p));
+  p.epi = epi;
+  p.fk = fk;
   p.links = op->links[link_format_for(prec)];
   p.vh = op->g.vh; p.nx2 = op->g.nx2; p.ny = op->g.ny; p.nz = op->g.nz; p.nt = op->g.nt;
   p.ls = op->g.ls;
@@ -298,41 +142,105 @@ SopParams sop_base(const b200_dwf* op) {
   return p;
 }
 
-int run_hop(b200_dwf* op, int prec, bool dag, HopParams& p, cudaStream_t st) {
-  B200_CHECK_CUDA(launch_hop(prec, dag, p, st));
+// ------------------------------------------------------------ autotuner
+// The hop kernel comes in occupancy variants (register budget per thread).
+// On the first launch of a (geometry, precision, epilogue) combination the
+// variants are timed with CUDA events on the caller's stream, writing to
+// scratch outputs, and the fastest is kept for the rest of the process.
+// B200_AUTOTUNE=0 disables tuning (variant 0).  The first call of a
+// combination must not be inside a CUDA graph capture.
+typedef std::tuple<int, int, int, int, int> TuneKey;   // vh, ls, prec, epi, fk
+std::map<TuneKey, std::pair<int, float> > g_tune;
+std::mutex g_tune_mu;
+
+bool tuning_enabled() {
+  const char* e = getenv("B200_AUTOTUNE");
+  return !(e && e[0] == '0');
+}
+
+int tune_hop(b200_dwf* op, int prec, const HopParams& p0, cudaStream_t st, int* best) {
+  for (int i = 0; i < 2; ++i)
+    if (!op->tune_out[i][prec]) {
+      const size_t bytes = field_bytes(prec, op->g.vh, op->g.ls);
+      if (cudaMalloc(&op->tune_out[i][prec], bytes) != cudaSuccess)
+        return fail(B200_ENOMEM, "cudaMalloc for autotuner scratch failed");
+    }
+  HopParams p = p0;
+  if (p.out1) p.out1 = op->tune_out[0][prec];
+  if (p.out2) p.out2 = op->tune_out[1][prec];
+  cudaEvent_t a, b;
+  B200_CHECK_CUDA(cudaEventCreate(&a));
+  B200_CHECK_CUDA(cudaEventCreate(&b));
+  float best_ms = 1e30f;
+  *best = 0;
+  for (int v = 0; v < 2; ++v) {
+    p.variant = v;
+    B200_CHECK_CUDA(launch_hop(prec, p, op->coefs, st));
+    B200_CHECK_CUDA(cudaEventRecord(a, st));
+    for (int r = 0; r < 3; ++r) B200_CHECK_CUDA(launch_hop(prec, p, op->coefs, st));
+    B200_CHECK_CUDA(cudaEventRecord(b, st));
+    B200_CHECK_CUDA(cudaEventSynchronize(b));
+    float ms = 0.f;
+    B200_CHECK_CUDA(cudaEventElapsedTime(&ms, a, b));
+    if (ms < best_ms) { best_ms = ms; *best = v; }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[TuneKey(op->g.vh, op->g.ls, prec, p0.epi, p0.fk)] = std::make_pair(*best, best_ms / 3.f);
   return 0;
 }
 
-int run_sop(int prec, SopParams& p, cudaStream_t st) {
-  B200_CHECK_CUDA(launch_sop(prec, p, st));
+int run_hop(b200_dwf* op, int prec, HopParams& p, cudaStream_t st) {
+  int variant = 0;
+  if (tuning_enabled()) {
+    const TuneKey key(op->g.vh, op->g.ls, prec, p.epi, p.fk);
+    bool found = false;
+    {
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      auto it = g_tune.find(key);
+      if (it != g_tune.end()) { variant = it->second.first; found = true; }
+    }
+    if (!found) {
+      int rc = tune_hop(op, prec, p, st, &variant);
+      if (rc) return rc;
+    }
+  }
+  p.variant = variant;
+  B200_CHECK_CUDA(launch_hop(prec, p, op->coefs, st));
   return 0;
 }
 
-// v = E(w) with a site-local map
-int apply_sop(b200_dwf* op, int prec, void* v, const void* w, int mat, cudaStream_t st) {
+int run_sop(b200_dwf* op, int prec, SopParams& p, cudaStream_t st) {
+  B200_CHECK_CUDA(launch_sop(prec, p, op->coefs, st));
+  return 0;
+}
+
+// v = A(w) with a site-local fifth-dimension map A (SopKind)
+int apply_sop(b200_dwf* op, int prec, void* v, const void* w, int opa, cudaStream_t st) {
   SopParams p = sop_base(op);
-  p.in = w; p.out1 = v; p.E = op->mat(mat);
-  return run_sop(prec, p, st);
+  p.in = w; p.out1 = v; p.opa = opa;
+  return run_sop(op, prec, p, st);
 }
 
 // D = 1 - M_ee^-1 D_eo M_oo^-1 D_oe on w; v = w - ...;  optional F(v) -> v2,
 // optional |v|^2 partials.  With F the first output may be skipped (v = null).
-int apply_D(b200_dwf* op, int prec, void* v, const void* w, int fmat, void* v2, double* red,
+int apply_D(b200_dwf* op, int prec, void* v, const void* w, int fk, void* v2, double* red,
             cudaStream_t st) {
   int rc;
   if ((rc = ensure_work(op, prec, 0)) || (rc = ensure_work(op, prec, 1))) return rc;
   void* t0 = op->work[0][prec];
   void* y1 = op->work[1][prec];
-  if ((rc = apply_sop(op, prec, t0, w, MAT_M5PRE, st))) return rc;
-  HopParams p1 = hop_base(op, prec, 1);
-  p1.in = t0; p1.out1 = y1; p1.E = op->mat(MAT_K1);
-  if ((rc = run_hop(op, prec, false, p1, st))) return rc;
-  HopParams p2 = hop_base(op, prec, 0);
-  p2.in = y1; p2.out1 = v; p2.E = op->mat(MAT_K2N);
+  if ((rc = apply_sop(op, prec, t0, w, SOP_M5PRE, st))) return rc;
+  HopParams p1 = hop_base(op, prec, 1, EPI_K1);
+  p1.in = t0; p1.out1 = y1;
+  if ((rc = run_hop(op, prec, p1, st))) return rc;
+  HopParams p2 = hop_base(op, prec, 0, EPI_K2N, fk);
+  p2.in = y1; p2.out1 = v;
   p2.x1 = w; p2.c_x1 = 1.0;
-  if (fmat >= 0) { p2.F = op->mat(fmat); p2.out2 = v2; }
+  p2.out2 = v2;
   p2.red = red;
-  return run_hop(op, prec, false, p2, st);
+  return run_hop(op, prec, p2, st);
 }
 
 // Ddag = 1 - D_eo^+ M_oo^-+ D_oe^+ M_ee^-+ on u = LUdag(x);  v = xw - ...
@@ -341,20 +249,20 @@ int apply_Ddag_from_u(b200_dwf* op, int prec, void* v, const void* xw, const voi
   int rc;
   if ((rc = ensure_work(op, prec, 3))) return rc;
   void* t3 = op->work[3][prec];
-  HopParams p3 = hop_base(op, prec, 1);
-  p3.in = u; p3.out1 = t3; p3.E = op->mat(MAT_K3);
-  if ((rc = run_hop(op, prec, true, p3, st))) return rc;
-  HopParams p4 = hop_base(op, prec, 0);
-  p4.in = t3; p4.out1 = v; p4.E = op->mat(MAT_K4N);
+  HopParams p3 = hop_base(op, prec, 1, EPI_K3);
+  p3.in = u; p3.out1 = t3;
+  if ((rc = run_hop(op, prec, p3, st))) return rc;
+  HopParams p4 = hop_base(op, prec, 0, EPI_K4N);
+  p4.in = t3; p4.out1 = v;
   p4.x1 = xw; p4.c_x1 = 1.0;
-  return run_hop(op, prec, true, p4, st);
+  return run_hop(op, prec, p4, st);
 }
 
 int apply_Ddag(b200_dwf* op, int prec, void* v, const void* w, cudaStream_t st) {
   int rc;
   if ((rc = ensure_work(op, prec, 2))) return rc;
   void* u = op->work[2][prec];
-  if ((rc = apply_sop(op, prec, u, w, MAT_LUDAG, st))) return rc;
+  if ((rc = apply_sop(op, prec, u, w, SOP_LUDAG, st))) return rc;
   return apply_Ddag_from_u(op, prec, v, w, u, st);
 }
 
@@ -363,7 +271,7 @@ int apply_DdagD(b200_dwf* op, int prec, void* v, const void* w, cudaStream_t st)
   if ((rc = ensure_work(op, prec, 2)) || (rc = ensure_work(op, prec, 4))) return rc;
   void* t2 = op->work[4][prec];
   void* u = op->work[2][prec];
-  if ((rc = apply_D(op, prec, t2, w, MAT_LUDAG, u, nullptr, st))) return rc;
+  if ((rc = apply_D(op, prec, t2, w, F_LUDAG, u, nullptr, st))) return rc;
   return apply_Ddag_from_u(op, prec, v, t2, u, st);
 }
 
@@ -373,8 +281,8 @@ int apply_Hdag(b200_dwf* op, int prec, void* v, const void* w, cudaStream_t st) 
   void* gw = op->work[4][prec];
   void* u = op->work[2][prec];
   SopParams p = sop_base(op);
-  p.in = w; p.out1 = gw; p.E = op->mat(MAT_G5R); p.F = op->mat(MAT_LUDAG); p.out2 = u;
-  if ((rc = run_sop(prec, p, st))) return rc;
+  p.in = w; p.out1 = gw; p.opa = SOP_G5R; p.opb = SOP_LUDAG; p.out2 = u;
+  if ((rc = run_sop(op, prec, p, st))) return rc;
   return apply_Ddag_from_u(op, prec, v, gw, u, st);
 }
 
@@ -394,23 +302,23 @@ int apply_mode(b200_dwf* op, int prec, void* v, const void* w, const std::string
   if (mode == "Deo" || mode == "Doe") {
     const int out_par = (mode == "Deo") ? (dag ? 1 : 0) : (dag ? 0 : 1);
     if (dag) {
-      HopParams p = hop_base(op, prec, out_par);
-      p.in = w; p.out1 = v; p.E = op->mat(MAT_DDAGEO);
-      return run_hop(op, prec, true, p, st);
+      HopParams p = hop_base(op, prec, out_par, EPI_DDAGEO);
+      p.in = w; p.out1 = v;
+      return run_hop(op, prec, p, st);
     }
     if ((rc = ensure_work(op, prec, 0))) return rc;
     void* t0 = op->work[0][prec];
-    if ((rc = apply_sop(op, prec, t0, w, MAT_M5PRE, st))) return rc;
-    HopParams p = hop_base(op, prec, out_par);
-    p.in = t0; p.out1 = v; p.E = op->mat(MAT_HALF);
-    return run_hop(op, prec, false, p, st);
+    if ((rc = apply_sop(op, prec, t0, w, SOP_M5PRE, st))) return rc;
+    HopParams p = hop_base(op, prec, out_par, EPI_HALF);
+    p.in = t0; p.out1 = v;
+    return run_hop(op, prec, p, st);
   }
-  if (mode == "Dee" || mode == "Doo") return apply_sop(op, prec, v, w, dag ? MAT_DEE_T : MAT_DEE, st);
-  if (mode == "Dee_inv" || mode == "Doo_inv") return apply_sop(op, prec, v, w, dag ? MAT_LUDAG : MAT_LU, st);
-  if (mode == "gm5R") return apply_sop(op, prec, v, w, MAT_G5R, st);
-  if (mode == "R") return apply_sop(op, prec, v, w, MAT_R, st);
-  if (mode == "D") return apply_D(op, prec, v, w, -1, nullptr, nullptr, st);
-  if (mode == "H") return apply_D(op, prec, nullptr, w, MAT_G5R, v, nullptr, st);
+  if (mode == "Dee" || mode == "Doo") return apply_sop(op, prec, v, w, dag ? SOP_DEE_T : SOP_DEE, st);
+  if (mode == "Dee_inv" || mode == "Doo_inv") return apply_sop(op, prec, v, w, dag ? SOP_LUDAG : SOP_LU, st);
+  if (mode == "gm5R") return apply_sop(op, prec, v, w, SOP_G5R, st);
+  if (mode == "R") return apply_sop(op, prec, v, w, SOP_R, st);
+  if (mode == "D") return apply_D(op, prec, v, w, F_NONE, nullptr, nullptr, st);
+  if (mode == "H") return apply_D(op, prec, nullptr, w, F_G5R, v, nullptr, st);
   if (mode == "Ddag") return apply_Ddag(op, prec, v, w, st);
   if (mode == "Hdag") return apply_Hdag(op, prec, v, w, st);
   if (mode == "DdagD") return apply_DdagD(op, prec, v, w, st);
@@ -475,50 +383,53 @@ int b200_dwf_create(b200_dwf_t** out, const int lattice[4], int Ls, double mq, d
   op->g.nx2 = lattice[0] / 2; op->g.ny = lattice[1]; op->g.nz = lattice[2]; op->g.nt = lattice[3];
   op->g.ls = Ls; op->g.vh = (int)(vol / 2);
 
-  // fifth-dimension maps
-  const DwfCoef& k = op->k;
-  std::vector<double> F1(Ls), F2(Ls);
-  for (int s = 0; s < Ls; ++s) {
-    F1[s] = k.b[s] * (4.0 - k.M0) + 1.0;
-    F2[s] = k.c[s] * (4.0 - k.M0) - 1.0;
+  // fifth-dimension chain coefficients (both arithmetic types)
+  {
+    const DwfCoef& kk = op->k;
+    ChainCoef<double>& cd = op->coefs.d;
+    memset(&cd, 0, sizeof(cd));
+    for (int s = 0; s < Ls; ++s) {
+      cd.wb[s] = kk.b[s];
+      cd.wc2[s] = 2.0 * kk.c[s];
+      cd.dm[s] = kk.dm[s];
+      cd.dpinv[s] = 1.0 / kk.dp[s];
+      cd.e[s] = kk.e[s];
+      cd.f[s] = kk.f[s];
+      cd.rl[s] = (s >= 1) ? kk.dm[s] / kk.dp[s - 1] : 0.0;
+      cd.rld[s] = (s <= Ls - 2) ? kk.dm[s + 1] / kk.dp[s] : 0.0;
+    }
+    cd.alpha = kk.alpha;
+    cd.half_alpha = 0.5 * kk.alpha;
+    cd.mhalf_mq = -0.5 * kk.mq;
+    cd.dpg_inv = 1.0 / (kk.dp[Ls - 1] + kk.g);
+    ChainCoef<float>& cf = op->coefs.f;
+    for (int s = 0; s < kMaxLs; ++s) {
+      cf.wb[s] = (float)cd.wb[s]; cf.wc2[s] = (float)cd.wc2[s]; cf.rl[s] = (float)cd.rl[s];
+      cf.rld[s] = (float)cd.rld[s]; cf.dm[s] = (float)cd.dm[s]; cf.dpinv[s] = (float)cd.dpinv[s];
+      cf.e[s] = (float)cd.e[s]; cf.f[s] = (float)cd.f[s];
+    }
+    cf.alpha = (float)cd.alpha; cf.half_alpha = (float)cd.half_alpha;
+    cf.mhalf_mq = (float)cd.mhalf_mq; cf.dpg_inv = (float)cd.dpg_inv;
+    // D_ee is the M5-type map with b -> b(4-M0)+1, c -> c(4-M0)-1
+    // (reference src/lib_alt_Accel/BridgeOpenACC/src/mult_Domainwall_5din_eo_openacc-inc.h:14-119)
+    op->coefs.dee_d = cd;
+    for (int s = 0; s < Ls; ++s) {
+      op->coefs.dee_d.wb[s] = kk.b[s] * (4.0 - kk.M0) + 1.0;
+      op->coefs.dee_d.wc2[s] = 2.0 * (kk.c[s] * (4.0 - kk.M0) - 1.0);
+    }
+    op->coefs.dee_f = cf;
+    for (int s = 0; s < kMaxLs; ++s) {
+      op->coefs.dee_f.wb[s] = (float)op->coefs.dee_d.wb[s];
+      op->coefs.dee_f.wc2[s] = (float)op->coefs.dee_d.wc2[s];
+    }
   }
-  std::vector<Chiral> M(MAT_COUNT);
-  const Chiral m5pre = m5_map(k, k.b, k.c);
-  const Chiral half = Chiral::identity(Ls, -0.5, -0.5);
-  const Chiral halfg5 = Chiral::identity(Ls, -0.5, 0.5);
-  const Chiral lu = lu_inv_map(k);
-  const Chiral ludag = lu_dag_inv_map(k);
-  const Chiral m5dag = transpose(m5pre);
-  M[MAT_M5PRE] = m5pre;
-  M[MAT_HALF] = half;
-  M[MAT_DDAGEO] = mul(m5dag, halfg5);
-  M[MAT_DEE] = m5_map(k, F1, F2);
-  M[MAT_DEE_T] = transpose(M[MAT_DEE]);
-  M[MAT_LU] = lu;
-  M[MAT_LUDAG] = ludag;
-  M[MAT_G5R] = reflect_map(Ls, -1.0);
-  M[MAT_R] = reflect_map(Ls, 1.0);
-  M[MAT_K1] = mul(m5pre, mul(lu, half));
-  M[MAT_K2N] = scaled(mul(lu, half), -1.0);
-  M[MAT_K3] = mul(ludag, M[MAT_DDAGEO]);
-  M[MAT_K4N] = scaled(M[MAT_DDAGEO], -1.0);
-  M[MAT_ID] = Chiral::identity(Ls);
-  std::vector<double> flat;
-  for (int i = 0; i < MAT_COUNT; ++i) flat.insert(flat.end(), M[i].m.begin(), M[i].m.end());
-
   const int red_n = site_s_grid(Ls, op->g.vh) + hop_grid(Ls, op->g.vh);
   op->red_n = red_n;
-  if (cudaMalloc(&op->mats, flat.size() * sizeof(double)) != cudaSuccess ||
-      cudaMalloc(&op->red, (size_t)red_n * sizeof(double)) != cudaSuccess ||
+  if (cudaMalloc(&op->red, (size_t)red_n * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&op->sc, SC_N * sizeof(double)) != cudaSuccess ||
       cudaMallocHost(&op->sc_host, SC_N * sizeof(double)) != cudaSuccess) {
     b200_dwf_destroy(op);
     return fail(B200_ENOMEM, "device allocation for the operator plan failed");
-  }
-  cudaError_t e = cudaMemcpy(op->mats, flat.data(), flat.size() * sizeof(double), cudaMemcpyHostToDevice);
-  if (e != cudaSuccess) {
-    b200_dwf_destroy(op);
-    return fail(B200_ECUDA, "upload of fifth-dimension maps failed: %s", cudaGetErrorString(e));
   }
   *out = op;
   return 0;
@@ -526,7 +437,6 @@ int b200_dwf_create(b200_dwf_t** out, const int lattice[4], int Ls, double mq, d
 
 int b200_dwf_destroy(b200_dwf_t* op) {
   if (!op) return 0;
-  cudaFree(op->mats);
   for (int i = 0; i < 4; ++i) cudaFree(op->links[i]);
   cudaFree(op->u_lex);
   cudaFree(op->red);
@@ -535,6 +445,8 @@ int b200_dwf_destroy(b200_dwf_t* op) {
   cudaFree(op->stage);
   for (int i = 0; i < 8; ++i)
     for (int p = 0; p < 4; ++p) cudaFree(op->work[i][p]);
+  for (int i = 0; i < 2; ++i)
+    for (int p = 0; p < 4; ++p) cudaFree(op->tune_out[i][p]);
   delete op;
   return 0;
 }
@@ -669,40 +581,40 @@ int b200_cg_solve(b200_dwf_t* op, int prec, void* x, const void* b, int maxiter,
     if (diff) *diff = 0.0;
     return 0;
   }
-  if ((rc = apply_sop(op, prec, yp, p, MAT_M5PRE, st))) return rc;
+  if ((rc = apply_sop(op, prec, yp, p, SOP_M5PRE, st))) return rc;
 
   int it_conv = -1;
   double rr = bnorm2;
   for (int it = 0; it < maxiter; ++it) {
-    HopParams p1 = hop_base(op, prec, 1);
-    p1.in = yp; p1.out1 = y1; p1.E = op->mat(MAT_K1);
-    if ((rc = run_hop(op, prec, false, p1, st))) return rc;
+    HopParams p1 = hop_base(op, prec, 1, EPI_K1);
+    p1.in = yp; p1.out1 = y1;
+    if ((rc = run_hop(op, prec, p1, st))) return rc;
 
-    HopParams p2 = hop_base(op, prec, 0);
-    p2.in = y1; p2.out1 = t2; p2.E = op->mat(MAT_K2N);
+    HopParams p2 = hop_base(op, prec, 0, EPI_K2N, F_LUDAG);
+    p2.in = y1; p2.out1 = t2;
     p2.x1 = p; p2.c_x1 = 1.0;
-    p2.F = op->mat(MAT_LUDAG); p2.out2 = u;
+    p2.out2 = u;
     p2.red = op->red;
-    if ((rc = run_hop(op, prec, false, p2, st))) return rc;
+    if ((rc = run_hop(op, prec, p2, st))) return rc;
     if ((rc = reduce_to(op, nb_hop, op->sc, FIN_CG_ALPHA, st))) return rc;
 
-    HopParams p3 = hop_base(op, prec, 1);
-    p3.in = u; p3.out1 = t3; p3.E = op->mat(MAT_K3);
-    if ((rc = run_hop(op, prec, true, p3, st))) return rc;
+    HopParams p3 = hop_base(op, prec, 1, EPI_K3);
+    p3.in = u; p3.out1 = t3;
+    if ((rc = run_hop(op, prec, p3, st))) return rc;
 
-    HopParams p4 = hop_base(op, prec, 0);
-    p4.in = t3; p4.out1 = r; p4.E = op->mat(MAT_K4N);
+    HopParams p4 = hop_base(op, prec, 0, EPI_K4N);
+    p4.in = t3; p4.out1 = r;
     p4.ce = -1.0; p4.ce_dev = op->sc + SC_ALPHA;
     p4.x1 = r; p4.c_x1 = 1.0;
     p4.x2 = t2; p4.c_x2 = -1.0; p4.c_x2_dev = op->sc + SC_ALPHA;
     p4.red = op->red;
-    if ((rc = run_hop(op, prec, true, p4, st))) return rc;
+    if ((rc = run_hop(op, prec, p4, st))) return rc;
     if ((rc = reduce_to(op, nb_hop, op->sc, FIN_CG_BETA, st))) return rc;
 
     CgUpdParams pu;
-    pu.x = x; pu.p = p; pu.r = r; pu.y = yp; pu.E = op->mat(MAT_M5PRE);
+    pu.x = x; pu.p = p; pu.r = r; pu.y = yp;
     pu.alpha = op->sc + SC_ALPHA; pu.beta = op->sc + SC_BETA; pu.g = g;
-    B200_CHECK_CUDA(launch_cg_update(prec, pu, st));
+    B200_CHECK_CUDA(launch_cg_update(prec, pu, op->coefs, st));
 
     if ((rc = host_scalar(op, SC_RR, &rr, st))) return rc;
     if (!(rr == rr)) return fail(B200_ENOCONV, "CG breakdown: residual is NaN at iteration %d", it + 1);
@@ -719,6 +631,22 @@ int b200_cg_solve(b200_dwf_t* op, int prec, void* x, const void* b, int maxiter,
   if (nconv) *nconv = it_conv < 0 ? maxiter : it_conv;
   if (it_conv < 0) return fail(B200_ENOCONV, "CG not converged in %d iterations: |r|^2/|b|^2 = %.3e",
                                maxiter, rr / bnorm2);
+  return 0;
+}
+
+int b200_tuning_table(char* buf, size_t n) {
+  if (!buf || n == 0) return fail(B200_EINVAL, "invalid buffer");
+  std::string out;
+  static const char* pn[4] = {"f64", "f32", "f16", "bf16"};
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  for (const auto& kv : g_tune) {
+    char line[160];
+    snprintf(line, sizeof(line), "vh=%d ls=%d prec=%s epi=%d fk=%d variant=%d us=%.2f\n",
+             std::get<0>(kv.first), std::get<1>(kv.first), pn[std::get<2>(kv.first) & 3],
+             std::get<3>(kv.first), std::get<4>(kv.first), kv.second.first, kv.second.second * 1e3f);
+    out += line;
+  }
+  snprintf(buf, n, "%s", out.c_str());
   return 0;
 }
 

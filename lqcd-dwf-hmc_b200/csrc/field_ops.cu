@@ -3,12 +3,14 @@
 #include "dwf_hop.cuh"
 #include "dwf_kernels.h"
 
+#include <type_traits>
+
 namespace b200 {
 
-cudaError_t launch_hop_p0(bool dag, const HopParams& p, cudaStream_t st);
-cudaError_t launch_hop_p1(bool dag, const HopParams& p, cudaStream_t st);
-cudaError_t launch_hop_p2(bool dag, const HopParams& p, cudaStream_t st);
-cudaError_t launch_hop_p3(bool dag, const HopParams& p, cudaStream_t st);
+cudaError_t launch_hop_p0(const HopParams& p, const ChainCoefs& c, cudaStream_t st);
+cudaError_t launch_hop_p1(const HopParams& p, const ChainCoefs& c, cudaStream_t st);
+cudaError_t launch_hop_p2(const HopParams& p, const ChainCoefs& c, cudaStream_t st);
+cudaError_t launch_hop_p3(const HopParams& p, const ChainCoefs& c, cudaStream_t st);
 
 int hop_grid(int ls, int vh) {
   const int g = 32 / ls;
@@ -21,12 +23,12 @@ int site_s_grid(int ls, int vh) {
   return (int)((n + kSiteSBlock - 1) / kSiteSBlock);
 }
 
-cudaError_t launch_hop(int prec, bool dag, const HopParams& p, cudaStream_t st) {
+cudaError_t launch_hop(int prec, const HopParams& p, const ChainCoefs& c, cudaStream_t st) {
   switch (prec) {
-    case PREC_F64: return launch_hop_p0(dag, p, st);
-    case PREC_F32: return launch_hop_p1(dag, p, st);
-    case PREC_F16: return launch_hop_p2(dag, p, st);
-    case PREC_BF16: return launch_hop_p3(dag, p, st);
+    case PREC_F64: return launch_hop_p0(p, c, st);
+    case PREC_F32: return launch_hop_p1(p, c, st);
+    case PREC_F16: return launch_hop_p2(p, c, st);
+    case PREC_BF16: return launch_hop_p3(p, c, st);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -52,153 +54,193 @@ __device__ __forceinline__ double dev_scale(double c, const double* dev) {
 }
 
 // ------------------------------------------------------------ sop kernel
-template <int LS, int P>
-__global__ void __launch_bounds__(128) sop_kernel(SopParams p) {
+// Site-local fifth-dimension map: o1 = ce*A(in) + cx1*X1 + cx2*X2, o2 = B(o1).
+template <typename R, int LS, int CHI, int OP>
+__device__ __forceinline__ void sop_apply(const ChainCoef<R>& k, const ChainCoef<R>& kee, R* x) {
+  switch (OP) {
+    case SOP_ID: break;
+    case SOP_M5PRE: chain_m5pre<R, LS, CHI>(k, x); break;
+    case SOP_M5DAG: chain_m5dag<R, LS, CHI>(k, x); break;
+    case SOP_DEE: chain_m5pre<R, LS, CHI>(kee, x); break;
+    case SOP_DEE_T: chain_m5dag<R, LS, CHI>(kee, x); break;
+    case SOP_LU: chain_lu_inv<R, LS, CHI>(k, x); break;
+    case SOP_LUDAG: chain_ludag<R, LS, CHI>(k, x); break;
+    case SOP_G5R: chain_g5r<R, LS, CHI>(x); break;
+    case SOP_R: {
+      R y[LS];
+#pragma unroll
+      for (int s = 0; s < LS; ++s) y[s] = x[LS - 1 - s];
+#pragma unroll
+      for (int s = 0; s < LS; ++s) x[s] = y[s];
+    } break;
+  }
+}
+
+template <int LS, int P, int OPA, int OPB>
+__global__ void __launch_bounds__(128)
+sop_kernel(SopParams p, const __grid_constant__ ChainCoef<typename Store<P>::R> k,
+           const __grid_constant__ ChainCoef<typename Store<P>::R> kee) {
   using St = Store<P>;
   using R = typename St::R;
   constexpr int G = 32 / LS;
   constexpr int WARPS = 4;
-  constexpr int TILE = WARPS * G * LS * 24;
   extern __shared__ unsigned char smem_raw[];
-  R* sE = reinterpret_cast<R*>(smem_raw);
-  R* sF = sE + 2 * LS * LS;
-  R* tileA = sF + 2 * LS * LS;
-  R* tileB = tileA + TILE;
-
+  R* tile_all = reinterpret_cast<R*>(smem_raw);
   const int tid = threadIdx.x;
-  for (int i = tid; i < 2 * LS * LS; i += blockDim.x) {
-    sE[i] = p.E ? (R)p.E[i] : R(0);
-    sF[i] = p.F ? (R)p.F[i] : R(0);
-  }
   const int lane = tid & 31, warp = tid >> 5;
   const int g = lane / LS;
   const int s = lane - g * LS;
   const int site = (blockIdx.x * WARPS + warp) * G + g;
   const bool active = (g < G) && (site < p.g.vh);
   const size_t vh = p.g.vh;
-  R* myA = tileA + warp * G * LS * 24;
-  R* myB = tileB + warp * G * LS * 24;
+  R* tile = tile_all + warp * G * LS * 24;
 
   R v[24];
 #pragma unroll
   for (int i = 0; i < 24; ++i) v[i] = 0;
   if (active && p.in) St::load(p.in, vh, LS, site, s, v);
-  if (g < G) {
+  if (OPA != SOP_ID) {
+    if (g < G) {
 #pragma unroll
-    for (int i = 0; i < 24; ++i) myA[(g * LS + s) * 24 + i] = v[i];
-  }
-  __syncthreads();
-  if (p.E) {
-    apply_chiral<R, LS, G>(myA, myB, sE, lane);
+      for (int i = 0; i < 24; ++i) tile[(g * LS + s) * 24 + i] = v[i];
+    }
     __syncwarp();
-  }
-  const R* src = p.E ? myB : myA;
-  double nrm = 0.0;
-  R o1[24];
+    tile_chiral<R, LS, G>(tile, lane, [&](R* xp, R* xm) {
+      sop_apply<R, LS, 0, OPA>(k, kee, xp);
+      sop_apply<R, LS, 1, OPA>(k, kee, xm);
+    });
+    __syncwarp();
+    if (g < G) {
 #pragma unroll
-  for (int i = 0; i < 24; ++i) o1[i] = 0;
+      for (int i = 0; i < 24; ++i) v[i] = tile[(g * LS + s) * 24 + i];
+    }
+  }
+  double nrm = 0.0;
   if (active) {
     const R ce = (R)dev_scale(p.ce, p.ce_dev);
 #pragma unroll
-    for (int i = 0; i < 24; ++i) o1[i] = ce * src[(g * LS + s) * 24 + i];
+    for (int i = 0; i < 24; ++i) v[i] *= ce;
     if (p.x1) {
       R xv[24];
       St::load(p.x1, vh, LS, site, s, xv);
       const R c = (R)dev_scale(p.cx1, p.cx1_dev);
 #pragma unroll
-      for (int i = 0; i < 24; ++i) o1[i] = fma(c, xv[i], o1[i]);
+      for (int i = 0; i < 24; ++i) v[i] = fma(c, xv[i], v[i]);
     }
     if (p.x2) {
       R xv[24];
       St::load(p.x2, vh, LS, site, s, xv);
       const R c = (R)dev_scale(p.cx2, p.cx2_dev);
 #pragma unroll
-      for (int i = 0; i < 24; ++i) o1[i] = fma(c, xv[i], o1[i]);
+      for (int i = 0; i < 24; ++i) v[i] = fma(c, xv[i], v[i]);
     }
-    if (p.out1) St::store(p.out1, vh, LS, site, s, o1);
+    if (p.out1) St::store(p.out1, vh, LS, site, s, v);
     if (p.red) {
 #pragma unroll
-      for (int i = 0; i < 24; ++i) nrm += (double)o1[i] * (double)o1[i];
+      for (int i = 0; i < 24; ++i) nrm += (double)v[i] * (double)v[i];
     }
   }
-  if (p.F) {
+  if (OPB != SOP_ID) {
     __syncwarp();
     if (g < G) {
 #pragma unroll
-      for (int i = 0; i < 24; ++i) myA[(g * LS + s) * 24 + i] = o1[i];
+      for (int i = 0; i < 24; ++i) tile[(g * LS + s) * 24 + i] = v[i];
     }
     __syncwarp();
-    apply_chiral<R, LS, G>(myA, myB, sF, lane);
+    tile_chiral<R, LS, G>(tile, lane, [&](R* xp, R* xm) {
+      sop_apply<R, LS, 0, OPB>(k, kee, xp);
+      sop_apply<R, LS, 1, OPB>(k, kee, xm);
+    });
     __syncwarp();
     if (active) {
       R o2[24];
 #pragma unroll
-      for (int i = 0; i < 24; ++i) o2[i] = myB[(g * LS + s) * 24 + i];
+      for (int i = 0; i < 24; ++i) o2[i] = tile[(g * LS + s) * 24 + i];
       St::store(p.out2, vh, LS, site, s, o2);
     }
   }
   if (p.red) block_reduce_store(nrm, p.red);
 }
 
-template <int LS, int P>
-cudaError_t run_sop(const SopParams& p, cudaStream_t st) {
+template <int LS, int P, int OPA, int OPB>
+cudaError_t run_sop(const SopParams& p, const ChainCoefs& c, cudaStream_t st) {
   using R = typename Store<P>::R;
-  constexpr size_t smem = sizeof(R) * (4 * LS * LS + 2 * 4 * (32 / LS) * LS * 24);
-  auto k = sop_kernel<LS, P>;
+  constexpr size_t smem = sizeof(R) * (4 * (32 / LS) * LS * 24);
+  auto k = sop_kernel<LS, P, OPA, OPB>;
   static bool attr_done = false;
   if (!attr_done) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     attr_done = true;
   }
-  k<<<hop_grid(LS, p.g.vh), 128, smem, st>>>(p);
+  const bool dbl = std::is_same<R, double>::value;
+  const ChainCoef<R>& kc = *reinterpret_cast<const ChainCoef<R>*>(dbl ? (const void*)&c.d : (const void*)&c.f);
+  const ChainCoef<R>& ke = *reinterpret_cast<const ChainCoef<R>*>(dbl ? (const void*)&c.dee_d : (const void*)&c.dee_f);
+  k<<<hop_grid(LS, p.g.vh), 128, smem, st>>>(p, kc, ke);
   return cudaGetLastError();
 }
 
-template <int P>
-cudaError_t sop_ls(const SopParams& p, cudaStream_t st) {
-  switch (p.g.ls) {
-    case 4: return run_sop<4, P>(p, st);
-    case 6: return run_sop<6, P>(p, st);
-    case 8: return run_sop<8, P>(p, st);
-    case 12: return run_sop<12, P>(p, st);
-    case 16: return run_sop<16, P>(p, st);
+template <int LS, int P>
+cudaError_t sop_ops(const SopParams& p, const ChainCoefs& c, cudaStream_t st) {
+  if (p.opb == SOP_LUDAG) {
+    if (p.opa == SOP_G5R) return run_sop<LS, P, SOP_G5R, SOP_LUDAG>(p, c, st);
+    return cudaErrorInvalidValue;
+  }
+  if (p.opb != SOP_ID) return cudaErrorInvalidValue;
+  switch (p.opa) {
+    case SOP_ID: return run_sop<LS, P, SOP_ID, SOP_ID>(p, c, st);
+    case SOP_M5PRE: return run_sop<LS, P, SOP_M5PRE, SOP_ID>(p, c, st);
+    case SOP_M5DAG: return run_sop<LS, P, SOP_M5DAG, SOP_ID>(p, c, st);
+    case SOP_DEE: return run_sop<LS, P, SOP_DEE, SOP_ID>(p, c, st);
+    case SOP_DEE_T: return run_sop<LS, P, SOP_DEE_T, SOP_ID>(p, c, st);
+    case SOP_LU: return run_sop<LS, P, SOP_LU, SOP_ID>(p, c, st);
+    case SOP_LUDAG: return run_sop<LS, P, SOP_LUDAG, SOP_ID>(p, c, st);
+    case SOP_G5R: return run_sop<LS, P, SOP_G5R, SOP_ID>(p, c, st);
+    case SOP_R: return run_sop<LS, P, SOP_R, SOP_ID>(p, c, st);
     default: return cudaErrorInvalidValue;
   }
 }
 
-cudaError_t launch_sop(int prec, const SopParams& p, cudaStream_t st) {
+template <int P>
+cudaError_t sop_ls(const SopParams& p, const ChainCoefs& c, cudaStream_t st) {
+  switch (p.g.ls) {
+    case 4: return sop_ops<4, P>(p, c, st);
+    case 6: return sop_ops<6, P>(p, c, st);
+    case 8: return sop_ops<8, P>(p, c, st);
+    case 12: return sop_ops<12, P>(p, c, st);
+    case 16: return sop_ops<16, P>(p, c, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_sop(int prec, const SopParams& p, const ChainCoefs& c, cudaStream_t st) {
   switch (prec) {
-    case PREC_F64: return sop_ls<PREC_F64>(p, st);
-    case PREC_F32: return sop_ls<PREC_F32>(p, st);
-    case PREC_F16: return sop_ls<PREC_F16>(p, st);
-    case PREC_BF16: return sop_ls<PREC_BF16>(p, st);
+    case PREC_F64: return sop_ls<PREC_F64>(p, c, st);
+    case PREC_F32: return sop_ls<PREC_F32>(p, c, st);
+    case PREC_F16: return sop_ls<PREC_F16>(p, c, st);
+    case PREC_BF16: return sop_ls<PREC_BF16>(p, c, st);
     default: return cudaErrorInvalidValue;
   }
 }
 
 // ------------------------------------------------------------ CG update
 template <int LS, int P>
-__global__ void __launch_bounds__(128) cg_update_kernel(CgUpdParams p) {
+__global__ void __launch_bounds__(128)
+cg_update_kernel(CgUpdParams p, const __grid_constant__ ChainCoef<typename Store<P>::R> k) {
   using St = Store<P>;
   using R = typename St::R;
   constexpr int G = 32 / LS;
   constexpr int WARPS = 4;
-  constexpr int TILE = WARPS * G * LS * 24;
   extern __shared__ unsigned char smem_raw[];
-  R* sE = reinterpret_cast<R*>(smem_raw);
-  R* tileA = sE + 2 * LS * LS;
-  R* tileB = tileA + TILE;
+  R* tile_all = reinterpret_cast<R*>(smem_raw);
   const int tid = threadIdx.x;
-  for (int i = tid; i < 2 * LS * LS; i += blockDim.x) sE[i] = (R)p.E[i];
   const int lane = tid & 31, warp = tid >> 5;
   const int g = lane / LS;
   const int s = lane - g * LS;
   const int site = (blockIdx.x * WARPS + warp) * G + g;
   const bool active = (g < G) && (site < p.g.vh);
   const size_t vh = p.g.vh;
-  R* myA = tileA + warp * G * LS * 24;
-  R* myB = tileB + warp * G * LS * 24;
+  R* tile = tile_all + warp * G * LS * 24;
   R pv[24];
 #pragma unroll
   for (int i = 0; i < 24; ++i) pv[i] = 0;
@@ -218,23 +260,26 @@ __global__ void __launch_bounds__(128) cg_update_kernel(CgUpdParams p) {
   }
   if (g < G) {
 #pragma unroll
-    for (int i = 0; i < 24; ++i) myA[(g * LS + s) * 24 + i] = pv[i];
+    for (int i = 0; i < 24; ++i) tile[(g * LS + s) * 24 + i] = pv[i];
   }
-  __syncthreads();
-  apply_chiral<R, LS, G>(myA, myB, sE, lane);
+  __syncwarp();
+  tile_chiral<R, LS, G>(tile, lane, [&](R* xp, R* xm) {
+    chain_m5pre<R, LS, 0>(k, xp);
+    chain_m5pre<R, LS, 1>(k, xm);
+  });
   __syncwarp();
   if (active) {
     R o[24];
 #pragma unroll
-    for (int i = 0; i < 24; ++i) o[i] = myB[(g * LS + s) * 24 + i];
+    for (int i = 0; i < 24; ++i) o[i] = tile[(g * LS + s) * 24 + i];
     St::store(p.y, vh, LS, site, s, o);
   }
 }
 
 template <int LS, int P>
-cudaError_t run_cgu(const CgUpdParams& p, cudaStream_t st) {
+cudaError_t run_cgu(const CgUpdParams& p, const ChainCoefs& c, cudaStream_t st) {
   using R = typename Store<P>::R;
-  constexpr size_t smem = sizeof(R) * (2 * LS * LS + 2 * 4 * (32 / LS) * LS * 24);
+  constexpr size_t smem = sizeof(R) * (4 * (32 / LS) * LS * 24);
   auto k = cg_update_kernel<LS, P>;
   static bool attr_done = false;
   if (!attr_done) {
@@ -242,28 +287,30 @@ cudaError_t run_cgu(const CgUpdParams& p, cudaStream_t st) {
     if (e != cudaSuccess) return e;
     attr_done = true;
   }
-  k<<<hop_grid(LS, p.g.vh), 128, smem, st>>>(p);
+  const ChainCoef<R>& kc = *reinterpret_cast<const ChainCoef<R>*>(
+      std::is_same<R, double>::value ? (const void*)&c.d : (const void*)&c.f);
+  k<<<hop_grid(LS, p.g.vh), 128, smem, st>>>(p, kc);
   return cudaGetLastError();
 }
 
 template <int P>
-cudaError_t cgu_ls(const CgUpdParams& p, cudaStream_t st) {
+cudaError_t cgu_ls(const CgUpdParams& p, const ChainCoefs& c, cudaStream_t st) {
   switch (p.g.ls) {
-    case 4: return run_cgu<4, P>(p, st);
-    case 6: return run_cgu<6, P>(p, st);
-    case 8: return run_cgu<8, P>(p, st);
-    case 12: return run_cgu<12, P>(p, st);
-    case 16: return run_cgu<16, P>(p, st);
+    case 4: return run_cgu<4, P>(p, c, st);
+    case 6: return run_cgu<6, P>(p, c, st);
+    case 8: return run_cgu<8, P>(p, c, st);
+    case 12: return run_cgu<12, P>(p, c, st);
+    case 16: return run_cgu<16, P>(p, c, st);
     default: return cudaErrorInvalidValue;
   }
 }
 
-cudaError_t launch_cg_update(int prec, const CgUpdParams& p, cudaStream_t st) {
+cudaError_t launch_cg_update(int prec, const CgUpdParams& p, const ChainCoefs& c, cudaStream_t st) {
   switch (prec) {
-    case PREC_F64: return cgu_ls<PREC_F64>(p, st);
-    case PREC_F32: return cgu_ls<PREC_F32>(p, st);
-    case PREC_F16: return cgu_ls<PREC_F16>(p, st);
-    case PREC_BF16: return cgu_ls<PREC_BF16>(p, st);
+    case PREC_F64: return cgu_ls<PREC_F64>(p, c, st);
+    case PREC_F32: return cgu_ls<PREC_F32>(p, c, st);
+    case PREC_F16: return cgu_ls<PREC_F16>(p, c, st);
+    case PREC_BF16: return cgu_ls<PREC_BF16>(p, c, st);
     default: return cudaErrorInvalidValue;
   }
 }

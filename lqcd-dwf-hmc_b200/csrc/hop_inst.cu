@@ -17,30 +17,43 @@ template <> struct DefaultLink<PREC_BF16> { static constexpr int v = LINK_F16_12
 
 namespace {
 
-template <int LS, int P, bool DAG>
-cudaError_t run(const HopParams& p, cudaStream_t st) {
+template <int LS, int P, int EPI, int FK, int MB>
+cudaError_t run_mb(const HopParams& p, const ChainCoefs& c, cudaStream_t st) {
+  using R = typename Store<P>::R;
   constexpr int LF = DefaultLink<P>::v;
   constexpr size_t smem = hop_smem_bytes<LS, P>();
-  auto k = dwf_hop_kernel<LS, P, LF, DAG>;
+  auto k = dwf_hop_kernel<LS, P, LF, EPI, FK, MB>;
   static bool attr_done = false;
   if (!attr_done) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     attr_done = true;
   }
-  const int grid = hop_grid(LS, p.vh);
-  k<<<grid, 128, smem, st>>>(p);
+  const ChainCoef<R>& kc = *reinterpret_cast<const ChainCoef<R>*>(
+      std::is_same<R, double>::value ? (const void*)&c.d : (const void*)&c.f);
+  k<<<hop_grid(LS, p.vh), 128, smem, st>>>(p, kc);
   return cudaGetLastError();
 }
 
-template <bool DAG>
-cudaError_t dispatch_ls(const HopParams& p, cudaStream_t st) {
-  switch (p.ls) {
-    case 4: return run<4, B200_PREC, DAG>(p, st);
-    case 6: return run<6, B200_PREC, DAG>(p, st);
-    case 8: return run<8, B200_PREC, DAG>(p, st);
-    case 12: return run<12, B200_PREC, DAG>(p, st);
-    case 16: return run<16, B200_PREC, DAG>(p, st);
+template <int LS, int P, int EPI, int FK>
+cudaError_t run(const HopParams& p, const ChainCoefs& c, cudaStream_t st) {
+  if (p.variant == 1) return run_mb<LS, P, EPI, FK, HopMinBlocks<P>::v1>(p, c, st);
+  return run_mb<LS, P, EPI, FK, HopMinBlocks<P>::v0>(p, c, st);
+}
+
+template <int LS>
+cudaError_t dispatch_epi(const HopParams& p, const ChainCoefs& c, cudaStream_t st) {
+  constexpr int P = B200_PREC;
+  switch (p.epi) {
+    case EPI_HALF: return run<LS, P, EPI_HALF, F_NONE>(p, c, st);
+    case EPI_DDAGEO: return run<LS, P, EPI_DDAGEO, F_NONE>(p, c, st);
+    case EPI_K1: return run<LS, P, EPI_K1, F_NONE>(p, c, st);
+    case EPI_K2N:
+      if (p.fk == F_LUDAG) return run<LS, P, EPI_K2N, F_LUDAG>(p, c, st);
+      if (p.fk == F_G5R) return run<LS, P, EPI_K2N, F_G5R>(p, c, st);
+      return run<LS, P, EPI_K2N, F_NONE>(p, c, st);
+    case EPI_K3: return run<LS, P, EPI_K3, F_NONE>(p, c, st);
+    case EPI_K4N: return run<LS, P, EPI_K4N, F_NONE>(p, c, st);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -48,8 +61,16 @@ cudaError_t dispatch_ls(const HopParams& p, cudaStream_t st) {
 
 #define B200_CAT2(a, b) a##b
 #define B200_CAT(a, b) B200_CAT2(a, b)
-cudaError_t B200_CAT(launch_hop_p, B200_PREC)(bool dag, const HopParams& p, cudaStream_t st) {
-  return dag ? dispatch_ls<true>(p, st) : dispatch_ls<false>(p, st);
+cudaError_t B200_CAT(launch_hop_p, B200_PREC)(const HopParams& p, const ChainCoefs& c,
+                                             cudaStream_t st) {
+  switch (p.ls) {
+    case 4: return dispatch_epi<4>(p, c, st);
+    case 6: return dispatch_epi<6>(p, c, st);
+    case 8: return dispatch_epi<8>(p, c, st);
+    case 12: return dispatch_epi<12>(p, c, st);
+    case 16: return dispatch_epi<16>(p, c, st);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 }  // namespace b200

@@ -219,25 +219,32 @@ int main(int argc, char **argv)
     fprintf(f, "nconv %d\ndiff %.17e\n", nconv, diff);
     fclose(f);
   } else if (cmd == "time") {
+    // "Deo"/"Doe"/... use mult(v, w, mode); "dag_<mode>" uses mult_dag;
+    // composite modes (D, DdagD, ...) use set_mode + mult.
     const int reps = geti(kv, "reps", 10);
     for (size_t i = 0; i < modes.size(); ++i) {
-      const std::string m = modes[i];
-      fopr.set_mode(m == "Deo" || m == "Doe" ? std::string("D") : m);
-      // one untimed call to touch memory
-#pragma omp parallel
-      {
-        if (m == "Deo" || m == "Doe") fopr.mult(out, src, m); else fopr.mult(out, src);
-      }
+      std::string m = modes[i];
+      bool dag = false;
+      if (m.compare(0, 4, "dag_") == 0) { dag = true; m = m.substr(4); }
+      const bool explicit_mode = (m == "Deo" || m == "Doe" || m == "Dee" || m == "Doo" ||
+                                  m == "Dee_inv" || m == "Doo_inv");
+      if (!explicit_mode) fopr.set_mode(m);
+      // r = -1 is one untimed call that touches all memory first
       std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+      for (int r = -1; r < reps; ++r) {
+        if (r == 0) t0 = std::chrono::steady_clock::now();
 #pragma omp parallel
-      {
-        for (int r = 0; r < reps; ++r) {
-          if (m == "Deo" || m == "Doe") fopr.mult(out, src, m); else fopr.mult(out, src);
+        {
+          if (explicit_mode) {
+            if (dag) fopr.mult_dag(out, src, m); else fopr.mult(out, src, m);
+          } else {
+            if (dag) fopr.mult_dag(out, src); else fopr.mult(out, src);
+          }
         }
       }
       std::chrono::steady_clock::time_point t1 = std::chrono::steady_clock::now();
       double sec = std::chrono::duration<double>(t1 - t0).count() / reps;
-      printf("%s %.9e\n", m.c_str(), sec);
+      printf("%s %.9e\n", modes[i].c_str(), sec);
     }
   } else {
     fprintf(stderr, "unknown command %s\n", cmd.c_str());
