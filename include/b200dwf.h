@@ -114,6 +114,24 @@ int b200_field_copy_convert(b200_dwf_t *op, int prec_out, void *out, int prec_in
 int b200_cg_solve(b200_dwf_t *op, int prec, void *x, const void *b, int maxiter,
                   double tol2, int *nconv, double *diff, void *stream);
 
+/* Allocation-free |x|^2 for callers that cannot allocate device memory: code
+ * inside a CUDA graph capture, code running under a host framework that owns
+ * all device memory through its own pool, or a caller on a GPU whose memory is
+ * already committed.  It needs no operator plan (a plan owns its reduction
+ * scratch): pass the field x (precision prec, nsite 4D half-lattice sites,
+ * Ls = ls) and a host pointer for the result.  No counterpart in the
+ * reference (its norm2 always runs on fields that an operator allocated).
+ *   - Scratch is a fixed 512 KiB device array inside the library, held by
+ *     every GPU that loads it until the process exits; fields larger than
+ *     8,388,608 (site, s) pairs are rejected with B200_EINVAL.
+ *   - The first call on each device looks the array up (once per device);
+ *     make that first call before any stream capture.
+ *   - All calls on a device share the array: calls that overlap on the GPU
+ *     (different streams, no ordering between them) race and give wrong sums.
+ *   - Calls no cudaMalloc/cudaFree; synchronous on `stream`. */
+int b200_field_norm2_noalloc(int prec, const void *x, long nsite, int ls,
+                             double *result, void *stream);
+
 /* ---------------------------------------------------------------- tuning
  * Text table of the autotuner's choices (one line per geometry, precision and
  * kernel epilogue: chosen occupancy variant and its time per launch).  The

@@ -60,6 +60,7 @@ def lib():
     L.b200_field_norm2.argtypes = [vp, ctypes.c_int, vp, dp, vp]
     L.b200_field_dot.argtypes = [vp, ctypes.c_int, vp, vp, dp, vp]
     L.b200_field_copy_convert.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, vp, vp]
+    L.b200_field_norm2_noalloc.argtypes = [ctypes.c_int, vp, ctypes.c_long, ctypes.c_int, dp, vp]
     L.b200_tuning_table.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
     L.b200_cg_solve.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_double,
                                 ip, dp, vp]

@@ -44,6 +44,19 @@ int fail(int code, const char* fmt, ...) {
 bool ls_supported(int ls) { return ls == 4 || ls == 6 || ls == 8 || ls == 12 || ls == 16; }
 }  // namespace
 
+namespace b200 {
+// Error reporting for the library's other translation units.
+void set_last_error(int code, const char* fmt, ...) {
+  (void)code;
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+}
+}  // namespace b200
+
 // ------------------------------------------------------------ coefficients
 namespace {
 
