@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cg", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-solvers", action="store_true",
+                    help="skip the mixed-precision Richardson and multishift timings")
     ap.add_argument("--lattice", type=int, nargs=4, default=LATTICE)
     return ap.parse_args()
 
@@ -308,6 +310,34 @@ def b200_arm(args, rank, world, local_rank):
               "seconds": c1 - c0, "converged": rc == 0,
               "ms_per_iteration": (c1 - c0) * 1e3 / max(n, 1)}
 
+    # mixed-precision Richardson (FP64 outer, inner CG in f32/f16/bf16) and the
+    # 16-pole multishift CG (shifts log-spaced 1e-4..64), same lattice and RHS
+    solvers = None
+    if not args.no_solvers:
+        solvers = {"richardson": {}, "multishift": None}
+        for name, prec, tin in (("f32", 1, 1e-8), ("f16", 2, 1e-4), ("bf16", 3, 1e-4)):
+            x = op.new_field(0)
+            torch.cuda.synchronize()
+            c0 = time.perf_counter()
+            nout, nin, diff, rc = op.richardson(x, w, prec, 1e-20, 100, tin, 20000)
+            torch.cuda.synchronize()
+            c1 = time.perf_counter()
+            solvers["richardson"][name] = {"outer_iterations": nout, "inner_iterations": nin,
+                                           "inner_tol2": tin, "true_rel_residual": diff,
+                                           "seconds": c1 - c0, "converged": rc == 0}
+            del x
+        sigma = list(np.logspace(-4, np.log10(64.0), 16))
+        xs = [op.new_field(0) for _ in sigma]
+        torch.cuda.synchronize()
+        c0 = time.perf_counter()
+        n, diff, rc = op.shiftcg(xs, sigma, w, 1e-20, 20000)
+        torch.cuda.synchronize()
+        c1 = time.perf_counter()
+        solvers["multishift"] = {"shifts": len(sigma), "iterations": n, "max_true_rel_residual": diff,
+                                 "seconds": c1 - c0, "ms_per_iteration": (c1 - c0) * 1e3 / max(n, 1),
+                                 "converged": rc == 0}
+        del xs
+
     if rank != 0:
         return
     cpu = None
@@ -337,6 +367,7 @@ def b200_arm(args, rank, world, local_rank):
         "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": nbytes,
                 "d2h_bytes_per_step": 2 * nbytes},
         "cg_f64": cg,
+        "solvers": solvers,
         "autotune": b200dwf.tuning_table().strip().splitlines(),
         "cpu_baseline": cpu,
     }

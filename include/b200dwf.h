@@ -114,6 +114,30 @@ int b200_field_copy_convert(b200_dwf_t *op, int prec_out, void *out, int prec_in
 int b200_cg_solve(b200_dwf_t *op, int prec, void *x, const void *b, int maxiter,
                   double tol2, int *nconv, double *diff, void *stream);
 
+/* AShiftsolver_CG on DdagD + sigma_i, FP64 (src/lib/Solver/
+ * ashiftsolver_CG-tmpl.h:89-329, used by AFopr_Rational::mult src/lib/Fopr/
+ * afopr_Rational-tmpl.h:181-219 and AForce_F_Rational_Ratio::force_udiv_impl
+ * src/lib_alt/Force/Fermion/aforce_F_Rational_Ratio-tmpl.h:345-460).
+ * x: nshift (<= 32) device fields; converged shifts are dropped as in the
+ * reference.  nconv = iterations (the reference logs iterations - 1);
+ * diff = max_i sqrt(|(DdagD + sigma_i) x_i - b|^2 / |b|^2). */
+int b200_shiftcg_solve(b200_dwf_t *op, void *const *x, const double *sigma, int nshift,
+                       const void *b, int maxiter, double tol2, int *nconv, double *diff,
+                       void *stream);
+
+/* Fprop_alt_Standard_eo_Richardson::invert_DdagD_even
+ * (src/lib_alt/Measurements/Fermion/fprop_alt_Standard_eo_Richardson-tmpl.h:
+ * 27-102, 460-481): ASolver_Richardson<double> (asolver_Richardson-tmpl.h:
+ * 131-213) preconditioned by APrecond_Mixedprec (aprecond_Mixedprec-tmpl.h:
+ * 55-108) around a zero-start inner CG on DdagD in inner_prec (B200_F32, or
+ * B200_F16/B200_BF16 scaled storage with fp32 arithmetic); x, b are FP64
+ * fields.  The reference's inner stop is tol2_inner = 1e-8.  Returns outer and
+ * total inner iteration counts and diff = sqrt(|r|^2/|b|^2) of the FP64
+ * residual. */
+int b200_richardson_solve(b200_dwf_t *op, int inner_prec, void *x, const void *b,
+                          int maxiter, double tol2, int maxiter_inner, double tol2_inner,
+                          int *nconv, int *nconv_inner, double *diff, void *stream);
+
 /* Allocation-free |x|^2 for callers that cannot allocate device memory: code
  * inside a CUDA graph capture, code running under a host framework that owns
  * all device memory through its own pool, or a caller on a GPU whose memory is

@@ -60,6 +60,10 @@ def lib():
     L.b200_field_norm2.argtypes = [vp, ctypes.c_int, vp, dp, vp]
     L.b200_field_dot.argtypes = [vp, ctypes.c_int, vp, vp, dp, vp]
     L.b200_field_copy_convert.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, vp, vp]
+    L.b200_shiftcg_solve.argtypes = [vp, ctypes.POINTER(vp), dp, ctypes.c_int, vp, ctypes.c_int,
+                                     ctypes.c_double, ip, dp, vp]
+    L.b200_richardson_solve.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_double,
+                                        ctypes.c_int, ctypes.c_double, ip, ip, dp, vp]
     L.b200_field_norm2_noalloc.argtypes = [ctypes.c_int, vp, ctypes.c_long, ctypes.c_int, dp, vp]
     L.b200_tuning_table.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
     L.b200_cg_solve.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_double,
@@ -182,6 +186,30 @@ class DomainWall:
         check(lib().b200_field_copy_convert(self.handle, out.prec, out.ptr, inp.prec, inp.ptr, None))
 
     # solvers -----------------------------------------------------------
+    def shiftcg(self, xs, sigma, b, tol2, maxiter=10000):
+        """Multishift CG on DdagD + sigma_i (FP64 fields)."""
+        arr = (ctypes.c_void_p * len(xs))(*[f.buf.data_ptr() for f in xs])
+        sig = np.ascontiguousarray(sigma, np.float64)
+        n = ctypes.c_int()
+        d = ctypes.c_double()
+        rc = lib().b200_shiftcg_solve(self.handle, arr, _dp(sig), len(xs), b.ptr, maxiter, tol2,
+                                      ctypes.byref(n), ctypes.byref(d), None)
+        if rc not in (0, -4):
+            check(rc)
+        return n.value, d.value, rc
+
+    def richardson(self, x, b, inner_prec, tol2, maxiter=100, tol2_inner=1e-8, maxiter_inner=10000):
+        """Mixed-precision Richardson (FP64 outer, inner CG in inner_prec)."""
+        n = ctypes.c_int()
+        ni = ctypes.c_int()
+        d = ctypes.c_double()
+        rc = lib().b200_richardson_solve(self.handle, inner_prec, x.ptr, b.ptr, maxiter, tol2,
+                                         maxiter_inner, tol2_inner, ctypes.byref(n),
+                                         ctypes.byref(ni), ctypes.byref(d), None)
+        if rc not in (0, -4):
+            check(rc)
+        return n.value, ni.value, d.value, rc
+
     def cg(self, x, b, tol2, maxiter=10000):
         n = ctypes.c_int()
         d = ctypes.c_double()

@@ -174,12 +174,14 @@ struct HopParams {
   int fk;                // FKind second map, o2 = F o1 (F_NONE: no o2)
   int variant;           // occupancy variant (0/1), chosen by the autotuner
   const void* x2;        // second axpy operand (nullable)
-  // o1 = ce * E(acc) + c_x1 * X1 + c_x2 * X2; each scalar is multiplied by
-  // the device value behind its _dev pointer when that pointer is non-null
-  double ce, c_x1, c_x2;
+  const void* x3;        // third axpy operand (nullable)
+  // o1 = ce * E(acc) + c_x1 * X1 + c_x2 * X2 + c_x3 * X3; each scalar is
+  // multiplied by the device value behind its _dev pointer when non-null
+  double ce, c_x1, c_x2, c_x3;
   const double* ce_dev;
   const double* c_x1_dev;
   const double* c_x2_dev;
+  const double* c_x3_dev;
   double* red;           // per-block partials of |o1|^2 (nullable)
   int vh, nx2, ny, nz, nt, ls;
   int ieo;               // output parity (0 even, 1 odd)
@@ -322,6 +324,13 @@ dwf_hop_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename Sto
       R xv[24];
       St::load(p.x2, vh, LS, site, s, xv);
       const R c = (R)(p.c_x2 * (p.c_x2_dev ? *p.c_x2_dev : 1.0));
+#pragma unroll
+      for (int i = 0; i < 24; ++i) o1[i] = fma(c, xv[i], o1[i]);
+    }
+    if (p.x3) {
+      R xv[24];
+      St::load(p.x3, vh, LS, site, s, xv);
+      const R c = (R)(p.c_x3 * (p.c_x3_dev ? *p.c_x3_dev : 1.0));
 #pragma unroll
       for (int i = 0; i < 24; ++i) o1[i] = fma(c, xv[i], o1[i]);
     }

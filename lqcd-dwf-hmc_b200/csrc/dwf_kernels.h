@@ -52,11 +52,6 @@ struct CgUpdParams {
   Geom g;
 };
 
-// number of blocks the reductions of each launcher produce
-int hop_grid(int ls, int vh);
-int site_s_grid(int ls, int vh);
-constexpr int kSiteSBlock = 128;
-
 // Fifth-dimension chain coefficients of one operator in both arithmetic types.
 struct ChainCoefs {
   ChainCoef<double> d;
@@ -64,6 +59,41 @@ struct ChainCoefs {
   ChainCoef<double> dee_d;   // D_ee: b -> b(4-M0)+1, c -> c(4-M0)-1
   ChainCoef<float> dee_f;
 };
+
+// Multishift CG (reference src/lib/Solver/ashiftsolver_CG-tmpl.h:216-286).
+// Device state: scalars MS_* and per-shift arrays of kMaxShift entries.
+constexpr int kMaxShift = 32;
+enum MsScalar {
+  MS_RR = 0, MS_RR_NEW, MS_PQ, MS_BETA, MS_ALPHA, MS_ALPHA_P, MS_BETA_P, MS_PP0,
+  MS_SNORM, MS_SIGMA0, MS_TOL2, MS_NACT, MS_N = 16
+};
+// per-shift arrays follow the scalars: [MS_N + a*kMaxShift + i]
+enum MsArray { MSA_ZETA1 = 0, MSA_ZETA2, MSA_CSH2, MSA_BETAS, MSA_ALPHAS, MSA_ZETA, MSA_PP, MSA_COUNT };
+constexpr int kMsStateSize = MS_N + MSA_COUNT * kMaxShift;
+
+struct MsUpdParams {
+  void* const* xs;       // device array [nshift] of solution fields
+  void* const* ps;       // device array [nshift] of search directions
+  const void* r;
+  void* y0;              // M5pre(p_0) for the next hop
+  const double* st;      // multishift state (MS_*, MSA_*)
+  double* red;           // partials [kMaxShift][nblocks] of |p_i|^2
+  int nblocks;
+  Geom g;
+};
+cudaError_t launch_ms_update(int prec, const MsUpdParams& p, const ChainCoefs& c, cudaStream_t st);
+enum MsStep { MSS_BETA = 0, MSS_ALPHA = 1, MSS_PRUNE = 2 };
+// scalar steps: MSS_BETA sums the K2 partials (pq) -> beta; MSS_ALPHA sums
+// the K4 partials (rr_new) -> alpha and the per-shift zeta recurrence;
+// MSS_PRUNE sums per-shift |p_i|^2 and drops converged shifts.
+cudaError_t launch_ms_scalar(int step, const double* partials, int n, double* st, int nshift,
+                             cudaStream_t stream);
+
+// number of blocks the reductions of each launcher produce
+int hop_grid(int ls, int vh);
+int site_s_grid(int ls, int vh);
+constexpr int kSiteSBlock = 128;
+
 
 // Hop kernel dispatch (prec = storage precision of in/out fields; the hop
 // direction (plain or gamma5-sandwiched dagger) follows from p.epi).

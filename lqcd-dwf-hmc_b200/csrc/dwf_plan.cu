@@ -102,9 +102,13 @@ struct b200_dwf {
   double* sc = nullptr;         // solver scalars (device)
   double* sc_host = nullptr;    // pinned mirror
   double* stage = nullptr;      // device f64 staging for convert/reverse
-  void* work[8][4] = {};        // work fields per precision
+  void* work[12][4] = {};       // work fields per precision
   void* tune_out[2][4] = {};    // autotuner scratch outputs per precision
   ChainCoefs coefs;             // fifth-dimension chain coefficients
+  double* ms_state = nullptr;   // multishift scalar state (device)
+  double* ms_red = nullptr;     // multishift per-shift partials
+  void** ms_ptrs = nullptr;     // device arrays of x_i and p_i pointers
+  std::vector<void*> ms_p;      // multishift search directions p_1..p_(n-1)
 };
 
 namespace {
@@ -456,8 +460,12 @@ int b200_dwf_destroy(b200_dwf_t* op) {
   cudaFree(op->sc);
   if (op->sc_host) cudaFreeHost(op->sc_host);
   cudaFree(op->stage);
-  for (int i = 0; i < 8; ++i)
+  for (int i = 0; i < 12; ++i)
     for (int p = 0; p < 4; ++p) cudaFree(op->work[i][p]);
+  cudaFree(op->ms_state);
+  cudaFree(op->ms_red);
+  cudaFree(op->ms_ptrs);
+  for (void* q : op->ms_p) cudaFree(q);
   for (int i = 0; i < 2; ++i)
     for (int p = 0; p < 4; ++p) cudaFree(op->tune_out[i][p]);
   delete op;
@@ -563,10 +571,11 @@ int b200_field_copy_convert(b200_dwf_t* op, int prec_out, void* out, int prec_in
 //   K3 t3 = LUdag M5^+ (-1/2 g5) hop^+(u)
 //   K4 r  = r - alpha*(t2 - M5^+(-1/2 g5) hop^+(t3)) = r - alpha DdagD p ; rr
 //   K5 x += alpha p ; p = r + beta p ; yp = M5pre p
-int b200_cg_solve(b200_dwf_t* op, int prec, void* x, const void* b, int maxiter, double tol2,
-                  int* nconv, double* diff, void* stream) {
-  if (!op || !x || !b || prec < 0 || prec > 3 || maxiter < 0) return fail(B200_EINVAL, "invalid argument");
-  cudaStream_t st = (cudaStream_t)stream;
+// Scalars stay on the device; the host reads |r|^2 once per iteration for the
+// stopping test.  Returns the iteration count in *nconv and |r|^2/|b|^2 of the
+// recursive residual in *rel2.
+static int cg_core(b200_dwf_t* op, int prec, void* x, const void* b, int maxiter, double tol2,
+                   int* nconv, double* rel2, cudaStream_t st) {
   int rc;
   if ((rc = ensure_links(op, prec, st))) return rc;
   for (int i = 0; i < 8; ++i)
@@ -578,25 +587,20 @@ int b200_cg_solve(b200_dwf_t* op, int prec, void* x, const void* b, int maxiter,
   void* t2 = op->work[4][prec];
   void* r = op->work[5][prec];
   void* p = op->work[6][prec];
-  void* s = op->work[7][prec];
   const Geom& g = op->g;
   const int nb_hop = hop_grid(g.ls, g.vh);
 
-  // r = b, p = b, x = 0, rr = |r|^2, yp = M5pre p
   B200_CHECK_CUDA(launch_axpby(prec, g, r, b, 1.0, nullptr, 0.0, nullptr, st));
   B200_CHECK_CUDA(launch_axpby(prec, g, p, b, 1.0, nullptr, 0.0, nullptr, st));
   B200_CHECK_CUDA(launch_axpby(prec, g, x, nullptr, 0.0, nullptr, 0.0, nullptr, st));
   if ((rc = field_norm2_dev(op, prec, r, op->sc + SC_RR, st))) return rc;
   double bnorm2 = 0.0;
   if ((rc = host_scalar(op, SC_RR, &bnorm2, st))) return rc;
-  if (!(bnorm2 > 0.0)) {
-    if (nconv) *nconv = 0;
-    if (diff) *diff = 0.0;
-    return 0;
-  }
+  *nconv = 0;
+  *rel2 = 0.0;
+  if (!(bnorm2 > 0.0)) return 0;
   if ((rc = apply_sop(op, prec, yp, p, SOP_M5PRE, st))) return rc;
 
-  int it_conv = -1;
   double rr = bnorm2;
   for (int it = 0; it < maxiter; ++it) {
     HopParams p1 = hop_base(op, prec, 1, EPI_K1);
@@ -630,20 +634,237 @@ int b200_cg_solve(b200_dwf_t* op, int prec, void* x, const void* b, int maxiter,
     B200_CHECK_CUDA(launch_cg_update(prec, pu, op->coefs, st));
 
     if ((rc = host_scalar(op, SC_RR, &rr, st))) return rc;
+    *nconv = it + 1;
     if (!(rr == rr)) return fail(B200_ENOCONV, "CG breakdown: residual is NaN at iteration %d", it + 1);
+    if (rr / bnorm2 < tol2) break;
+  }
+  *rel2 = rr / bnorm2;
+  if (!(rr / bnorm2 < tol2))
+    return fail(B200_ENOCONV, "CG not converged in %d iterations: |r|^2/|b|^2 = %.3e", maxiter,
+                rr / bnorm2);
+  return 0;
+}
+
+// sqrt(|DdagD x + sigma x - b|^2 / |b|^2) in precision prec
+static int true_residual(b200_dwf_t* op, int prec, const void* x, const void* b, double sigma,
+                         double* out, cudaStream_t st) {
+  int rc;
+  if ((rc = ensure_work(op, prec, 7))) return rc;
+  void* s = op->work[7][prec];
+  if ((rc = apply_DdagD(op, prec, s, x, st))) return rc;
+  if (sigma != 0.0) B200_CHECK_CUDA(launch_axpby(prec, op->g, s, x, sigma, nullptr, 1.0, nullptr, st));
+  B200_CHECK_CUDA(launch_axpby(prec, op->g, s, b, -1.0, nullptr, 1.0, nullptr, st));
+  if ((rc = field_norm2_dev(op, prec, s, op->sc + SC_RR_NEW, st))) return rc;
+  double d2 = 0.0, b2 = 0.0;
+  if ((rc = host_scalar(op, SC_RR_NEW, &d2, st))) return rc;
+  if ((rc = field_norm2_dev(op, prec, b, op->sc + SC_RR_NEW, st))) return rc;
+  if ((rc = host_scalar(op, SC_RR_NEW, &b2, st))) return rc;
+  *out = b2 > 0.0 ? std::sqrt(d2 / b2) : 0.0;
+  return 0;
+}
+
+int b200_cg_solve(b200_dwf_t* op, int prec, void* x, const void* b, int maxiter, double tol2,
+                  int* nconv, double* diff, void* stream) {
+  if (!op || !x || !b || prec < 0 || prec > 3 || maxiter < 0) return fail(B200_EINVAL, "invalid argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  int n = 0;
+  double rel2 = 0.0;
+  const int rc = cg_core(op, prec, x, b, maxiter, tol2, &n, &rel2, st);
+  if (rc && rc != B200_ENOCONV) return rc;
+  const std::string msg = g_err;
+  double d = 0.0;
+  const int rc2 = true_residual(op, prec, x, b, 0.0, &d, st);
+  if (rc2) return rc2;
+  if (nconv) *nconv = n;
+  if (diff) *diff = d;
+  if (rc) g_err = msg;
+  return rc;
+}
+
+// AShiftsolver_CG (src/lib/Solver/ashiftsolver_CG-tmpl.h:89-329) on
+// DdagD + sigma_i, FP64.  One iteration = the four fused DdagD hops, one fused
+// update of every active shift, and three single-block scalar steps; the host
+// reads |r|^2 once per iteration.
+int b200_shiftcg_solve(b200_dwf_t* op, void* const* x, const double* sigma, int nshift,
+                       const void* b, int maxiter, double tol2, int* nconv, double* diff,
+                       void* stream) {
+  const int prec = PREC_F64;
+  if (!op || !x || !sigma || !b || nshift < 1 || maxiter < 0)
+    return fail(B200_EINVAL, "invalid argument");
+  if (nshift > kMaxShift) return fail(B200_EINVAL, "at most %d shifts (got %d)", kMaxShift, nshift);
+  for (int i = 0; i < nshift; ++i)
+    if (!x[i]) return fail(B200_EINVAL, "null solution field %d", i);
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc;
+  if ((rc = ensure_links(op, prec, st))) return rc;
+  for (int i = 0; i < 8; ++i)
+    if ((rc = ensure_work(op, prec, i))) return rc;
+  const Geom& g = op->g;
+  const int nb_hop = hop_grid(g.ls, g.vh);
+  if (!op->ms_state && cudaMalloc(&op->ms_state, kMsStateSize * sizeof(double)) != cudaSuccess)
+    return fail(B200_ENOMEM, "cudaMalloc for multishift state failed");
+  if (!op->ms_red && cudaMalloc(&op->ms_red, (size_t)kMaxShift * nb_hop * sizeof(double)) != cudaSuccess)
+    return fail(B200_ENOMEM, "cudaMalloc for multishift partials failed");
+  if (!op->ms_ptrs && cudaMalloc(&op->ms_ptrs, 2 * kMaxShift * sizeof(void*)) != cudaSuccess)
+    return fail(B200_ENOMEM, "cudaMalloc for multishift pointers failed");
+  // search directions p_i: work slots 8.. are allocated per shift on demand
+  std::vector<void*> ps(nshift);
+  for (int i = 0; i < nshift; ++i) {
+    if (i == 0) { ps[0] = op->work[6][prec]; continue; }
+    if (op->ms_p.size() < (size_t)i) op->ms_p.resize(i, nullptr);
+    if (!op->ms_p[i - 1] &&
+        cudaMalloc(&op->ms_p[i - 1], field_bytes(prec, g.vh, g.ls)) != cudaSuccess)
+      return fail(B200_ENOMEM, "cudaMalloc for multishift direction %d failed", i);
+    ps[i] = op->ms_p[i - 1];
+  }
+  void* y0 = op->work[0][prec];
+  void* y1 = op->work[1][prec];
+  void* u = op->work[2][prec];
+  void* t3 = op->work[3][prec];
+  void* t2 = op->work[4][prec];
+  void* r = op->work[5][prec];
+  void* p0 = ps[0];
+
+  // init: p_i = b, x_i = 0, r = b, rr = |b|^2 (ashiftsolver_CG-tmpl.h:188-211)
+  for (int i = 0; i < nshift; ++i) {
+    B200_CHECK_CUDA(launch_axpby(prec, g, ps[i], b, 1.0, nullptr, 0.0, nullptr, st));
+    B200_CHECK_CUDA(launch_axpby(prec, g, x[i], nullptr, 0.0, nullptr, 0.0, nullptr, st));
+  }
+  B200_CHECK_CUDA(launch_axpby(prec, g, r, b, 1.0, nullptr, 0.0, nullptr, st));
+  if ((rc = field_norm2_dev(op, prec, r, op->sc + SC_RR, st))) return rc;
+  double bnorm2 = 0.0;
+  if ((rc = host_scalar(op, SC_RR, &bnorm2, st))) return rc;
+  if (!(bnorm2 > 0.0)) {
+    if (nconv) *nconv = 0;
+    if (diff) *diff = 0.0;
+    return 0;
+  }
+  std::vector<double> h(kMsStateSize, 0.0);
+  h[MS_RR] = bnorm2;
+  h[MS_ALPHA_P] = 0.0;
+  h[MS_BETA_P] = 1.0;
+  h[MS_PP0] = bnorm2;
+  h[MS_SNORM] = 1.0 / bnorm2;
+  h[MS_SIGMA0] = sigma[0];
+  h[MS_TOL2] = tol2;
+  h[MS_NACT] = nshift;
+  for (int i = 0; i < nshift; ++i) {
+    h[MS_N + MSA_ZETA1 * kMaxShift + i] = 1.0;
+    h[MS_N + MSA_ZETA2 * kMaxShift + i] = 1.0;
+    h[MS_N + MSA_CSH2 * kMaxShift + i] = sigma[i] - sigma[0];
+  }
+  std::vector<void*> hp(2 * kMaxShift, nullptr);
+  for (int i = 0; i < nshift; ++i) { hp[i] = x[i]; hp[kMaxShift + i] = ps[i]; }
+  B200_CHECK_CUDA(cudaMemcpyAsync(op->ms_state, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+  B200_CHECK_CUDA(cudaMemcpyAsync(op->ms_ptrs, hp.data(), hp.size() * sizeof(void*), cudaMemcpyHostToDevice, st));
+  if ((rc = apply_sop(op, prec, y0, p0, SOP_M5PRE, st))) return rc;
+  double* S = op->ms_state;
+
+  int it_conv = -1;
+  double rr = bnorm2;
+  for (int it = 0; it < maxiter; ++it) {
+    HopParams p1 = hop_base(op, prec, 1, EPI_K1);
+    p1.in = y0; p1.out1 = y1;
+    if ((rc = run_hop(op, prec, p1, st))) return rc;
+    HopParams p2 = hop_base(op, prec, 0, EPI_K2N, F_LUDAG);
+    p2.in = y1; p2.out1 = t2; p2.x1 = p0; p2.c_x1 = 1.0; p2.out2 = u; p2.red = op->red;
+    if ((rc = run_hop(op, prec, p2, st))) return rc;
+    B200_CHECK_CUDA(launch_ms_scalar(MSS_BETA, op->red, nb_hop, S, nshift, st));
+    HopParams p3 = hop_base(op, prec, 1, EPI_K3);
+    p3.in = u; p3.out1 = t3;
+    if ((rc = run_hop(op, prec, p3, st))) return rc;
+    // r += beta (DdagD p0 + sigma0 p0) = r + beta t2 + beta sigma0 p0 + beta K4N(hop)
+    HopParams p4 = hop_base(op, prec, 0, EPI_K4N);
+    p4.in = t3; p4.out1 = r;
+    p4.ce = 1.0; p4.ce_dev = S + MS_BETA;
+    p4.x1 = r; p4.c_x1 = 1.0;
+    p4.x2 = t2; p4.c_x2 = 1.0; p4.c_x2_dev = S + MS_BETA;
+    p4.x3 = p0; p4.c_x3 = sigma[0]; p4.c_x3_dev = S + MS_BETA;
+    p4.red = op->red;
+    if ((rc = run_hop(op, prec, p4, st))) return rc;
+    B200_CHECK_CUDA(launch_ms_scalar(MSS_ALPHA, op->red, nb_hop, S, nshift, st));
+    MsUpdParams mu;
+    mu.xs = op->ms_ptrs; mu.ps = op->ms_ptrs + kMaxShift; mu.r = r; mu.y0 = y0;
+    mu.st = S; mu.red = op->ms_red; mu.nblocks = nb_hop; mu.g = g;
+    B200_CHECK_CUDA(launch_ms_update(prec, mu, op->coefs, st));
+    B200_CHECK_CUDA(launch_ms_scalar(MSS_PRUNE, op->ms_red, nb_hop, S, nshift, st));
+    B200_CHECK_CUDA(cudaMemcpyAsync(op->sc_host, S + MS_RR, sizeof(double), cudaMemcpyDeviceToHost, st));
+    B200_CHECK_CUDA(cudaStreamSynchronize(st));
+    rr = op->sc_host[0];
+    if (!(rr == rr)) return fail(B200_ENOCONV, "multishift CG breakdown: NaN at iteration %d", it + 1);
     if (rr / bnorm2 < tol2) { it_conv = it + 1; break; }
   }
-
-  // true residual |DdagD x - b|^2 / |b|^2
-  if ((rc = apply_DdagD(op, prec, s, x, st))) return rc;
-  B200_CHECK_CUDA(launch_axpby(prec, g, s, b, -1.0, nullptr, 1.0, nullptr, st));
-  if ((rc = field_norm2_dev(op, prec, s, op->sc + SC_RR_NEW, st))) return rc;
-  double d2 = 0.0;
-  if ((rc = host_scalar(op, SC_RR_NEW, &d2, st))) return rc;
-  if (diff) *diff = std::sqrt(d2 / bnorm2);
+  double dmax = 0.0;
+  for (int i = 0; i < nshift; ++i) {
+    double d = 0.0;
+    if ((rc = true_residual(op, prec, x[i], b, sigma[i], &d, st))) return rc;
+    if (d > dmax) dmax = d;
+  }
+  if (diff) *diff = dmax;
   if (nconv) *nconv = it_conv < 0 ? maxiter : it_conv;
-  if (it_conv < 0) return fail(B200_ENOCONV, "CG not converged in %d iterations: |r|^2/|b|^2 = %.3e",
-                               maxiter, rr / bnorm2);
+  if (it_conv < 0) return fail(B200_ENOCONV, "multishift CG not converged in %d iterations", maxiter);
+  return 0;
+}
+
+// ASolver_Richardson (src/lib_alt/Solver/asolver_Richardson-tmpl.h:131-213)
+// with APrecond_Mixedprec (aprecond_Mixedprec-tmpl.h:55-108): FP64 residual
+// and update, inner CG on DdagD in precision inner_prec (fp32 arithmetic over
+// f32/f16/bf16 storage) started from zero on the normalised residual.
+int b200_richardson_solve(b200_dwf_t* op, int inner_prec, void* x, const void* b, int maxiter,
+                          double tol2, int maxiter_inner, double tol2_inner, int* nconv,
+                          int* nconv_inner, double* diff, void* stream) {
+  if (!op || !x || !b || inner_prec < 0 || inner_prec > 3 || maxiter < 0 || maxiter_inner < 1)
+    return fail(B200_EINVAL, "invalid argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  const int P64 = PREC_F64;
+  int rc;
+  if ((rc = ensure_links(op, P64, st)) || (rc = ensure_links(op, inner_prec, st))) return rc;
+  for (int i = 8; i < 12; ++i)
+    if ((rc = ensure_work(op, P64, i)) || (rc = ensure_work(op, inner_prec, i))) return rc;
+  const Geom& g = op->g;
+  void* r = op->work[8][P64];
+  void* s = op->work[9][P64];
+  void* r_in = op->work[10][inner_prec];
+  void* s_in = op->work[11][inner_prec];
+
+  if ((rc = field_norm2_dev(op, P64, b, op->sc + SC_RR_NEW, st))) return rc;
+  double bnorm2 = 0.0;
+  if ((rc = host_scalar(op, SC_RR_NEW, &bnorm2, st))) return rc;
+  B200_CHECK_CUDA(launch_axpby(P64, g, x, nullptr, 0.0, nullptr, 0.0, nullptr, st));
+  int total_inner = 0;
+  if (!(bnorm2 > 0.0)) {
+    if (nconv) *nconv = 0;
+    if (nconv_inner) *nconv_inner = 0;
+    if (diff) *diff = 0.0;
+    return 0;
+  }
+  B200_CHECK_CUDA(launch_axpby(P64, g, r, b, -1.0, nullptr, 0.0, nullptr, st));
+  double r2 = bnorm2;
+  int conv = -1;
+  for (int it = 0; it < maxiter; ++it) {
+    if (r2 < bnorm2 * tol2) { conv = it; break; }
+    const double nrm = std::sqrt(r2);
+    B200_CHECK_CUDA(launch_convert(inner_prec, r_in, P64, r, g, st));
+    B200_CHECK_CUDA(launch_axpby(inner_prec, g, r_in, nullptr, 0.0, nullptr, 1.0 / nrm, nullptr, st));
+    int n_in = 0;
+    double rel_in = 0.0;
+    rc = cg_core(op, inner_prec, s_in, r_in, maxiter_inner, tol2_inner, &n_in, &rel_in, st);
+    if (rc && rc != B200_ENOCONV) return rc;
+    total_inner += n_in;
+    B200_CHECK_CUDA(launch_convert(P64, s, inner_prec, s_in, g, st));
+    B200_CHECK_CUDA(launch_axpby(P64, g, x, s, -nrm, nullptr, 1.0, nullptr, st));
+    if ((rc = apply_DdagD(op, P64, r, x, st))) return rc;
+    B200_CHECK_CUDA(launch_axpby(P64, g, r, b, -1.0, nullptr, 1.0, nullptr, st));
+    if ((rc = field_norm2_dev(op, P64, r, op->sc + SC_RR_NEW, st))) return rc;
+    if ((rc = host_scalar(op, SC_RR_NEW, &r2, st))) return rc;
+    if (!(r2 == r2)) return fail(B200_ENOCONV, "Richardson breakdown: NaN residual at iteration %d", it + 1);
+  }
+  if (conv < 0 && r2 < bnorm2 * tol2) conv = maxiter;
+  if (nconv) *nconv = conv < 0 ? maxiter : conv;
+  if (nconv_inner) *nconv_inner = total_inner;
+  if (diff) *diff = std::sqrt(r2 / bnorm2);
+  if (conv < 0) return fail(B200_ENOCONV, "Richardson not converged in %d iterations: |r|^2/|b|^2 = %.3e",
+                            maxiter, r2 / bnorm2);
   return 0;
 }
 

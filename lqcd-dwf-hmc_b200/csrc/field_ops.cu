@@ -315,6 +315,206 @@ cudaError_t launch_cg_update(int prec, const CgUpdParams& p, const ChainCoefs& c
   }
 }
 
+// ------------------------------------------------------------ multishift
+// x_0 -= beta p_0 ; p_0 = r + alpha p_0 ; y_0 = M5pre(p_0) ; |p_0|^2
+// for active shifts i >= 1: x_i -= beta_i p_i ; p_i = alpha_i p_i + zeta_i r ; |p_i|^2
+// (reference src/lib/Solver/ashiftsolver_CG-tmpl.h:228-262)
+template <int LS, int P>
+__global__ void __launch_bounds__(128)
+ms_update_kernel(MsUpdParams p, const __grid_constant__ ChainCoef<typename Store<P>::R> k) {
+  using St = Store<P>;
+  using R = typename St::R;
+  constexpr int G = 32 / LS;
+  constexpr int WARPS = 4;
+  extern __shared__ unsigned char smem_raw[];
+  R* tile_all = reinterpret_cast<R*>(smem_raw);
+  const int tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
+  const int g = lane / LS;
+  const int s = lane - g * LS;
+  const int site = (blockIdx.x * WARPS + warp) * G + g;
+  const bool active = (g < G) && (site < p.g.vh);
+  const size_t vh = p.g.vh;
+  R* tile = tile_all + warp * G * LS * 24;
+  const int nact = (int)p.st[MS_NACT];
+  const R beta = (R)p.st[MS_BETA], alpha = (R)p.st[MS_ALPHA];
+  R rv[24], pv[24];
+#pragma unroll
+  for (int i = 0; i < 24; ++i) { rv[i] = 0; pv[i] = 0; }
+  double nrm = 0.0;
+  if (active) {
+    R xv[24];
+    St::load(p.r, vh, LS, site, s, rv);
+    St::load(p.xs[0], vh, LS, site, s, xv);
+    St::load(p.ps[0], vh, LS, site, s, pv);
+#pragma unroll
+    for (int i = 0; i < 24; ++i) {
+      xv[i] = fma(-beta, pv[i], xv[i]);
+      pv[i] = fma(alpha, pv[i], rv[i]);
+      nrm += (double)pv[i] * (double)pv[i];
+    }
+    St::store(p.xs[0], vh, LS, site, s, xv);
+    St::store(p.ps[0], vh, LS, site, s, pv);
+  }
+  if (g < G) {
+#pragma unroll
+    for (int i = 0; i < 24; ++i) tile[(g * LS + s) * 24 + i] = pv[i];
+  }
+  __syncwarp();
+  tile_chiral<R, LS, G>(tile, lane, [&](R* xp, R* xm) {
+    chain_m5pre<R, LS, 0>(k, xp);
+    chain_m5pre<R, LS, 1>(k, xm);
+  });
+  __syncwarp();
+  if (active) {
+    R o[24];
+#pragma unroll
+    for (int i = 0; i < 24; ++i) o[i] = tile[(g * LS + s) * 24 + i];
+    St::store(p.y0, vh, LS, site, s, o);
+  }
+  block_reduce_store(nrm, p.red);
+  for (int ish = 1; ish < nact; ++ish) {
+    __syncthreads();
+    const R bs = (R)p.st[MS_N + MSA_BETAS * kMaxShift + ish];
+    const R as = (R)p.st[MS_N + MSA_ALPHAS * kMaxShift + ish];
+    const R zt = (R)p.st[MS_N + MSA_ZETA * kMaxShift + ish];
+    double n2 = 0.0;
+    if (active) {
+      R xv[24], qv[24];
+      St::load(p.xs[ish], vh, LS, site, s, xv);
+      St::load(p.ps[ish], vh, LS, site, s, qv);
+#pragma unroll
+      for (int i = 0; i < 24; ++i) {
+        xv[i] = fma(-bs, qv[i], xv[i]);
+        qv[i] = fma(as, qv[i], zt * rv[i]);
+        n2 += (double)qv[i] * (double)qv[i];
+      }
+      St::store(p.xs[ish], vh, LS, site, s, xv);
+      St::store(p.ps[ish], vh, LS, site, s, qv);
+    }
+    block_reduce_store(n2, p.red + (size_t)ish * p.nblocks);
+  }
+}
+
+template <int LS, int P>
+cudaError_t run_msu(const MsUpdParams& p, const ChainCoefs& c, cudaStream_t st) {
+  using R = typename Store<P>::R;
+  constexpr size_t smem = sizeof(R) * (4 * (32 / LS) * LS * 24);
+  auto k = ms_update_kernel<LS, P>;
+  static bool attr_done = false;
+  if (!attr_done) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr_done = true;
+  }
+  const ChainCoef<R>& kc = *reinterpret_cast<const ChainCoef<R>*>(
+      std::is_same<R, double>::value ? (const void*)&c.d : (const void*)&c.f);
+  k<<<hop_grid(LS, p.g.vh), 128, smem, st>>>(p, kc);
+  return cudaGetLastError();
+}
+
+template <int P>
+cudaError_t msu_ls(const MsUpdParams& p, const ChainCoefs& c, cudaStream_t st) {
+  switch (p.g.ls) {
+    case 4: return run_msu<4, P>(p, c, st);
+    case 6: return run_msu<6, P>(p, c, st);
+    case 8: return run_msu<8, P>(p, c, st);
+    case 12: return run_msu<12, P>(p, c, st);
+    case 16: return run_msu<16, P>(p, c, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_ms_update(int prec, const MsUpdParams& p, const ChainCoefs& c, cudaStream_t st) {
+  switch (prec) {
+    case PREC_F64: return msu_ls<PREC_F64>(p, c, st);
+    case PREC_F32: return msu_ls<PREC_F32>(p, c, st);
+    case PREC_F16: return msu_ls<PREC_F16>(p, c, st);
+    case PREC_BF16: return msu_ls<PREC_BF16>(p, c, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+// deterministic block sum of partials[0..n) into shared memory, returned to thread 0
+__device__ double block_sum_partials(const double* partials, int n) {
+  __shared__ double ws[32];
+  double v = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) v += partials[i];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += ws[w];
+  return s;
+}
+
+__global__ void ms_scalar_kernel(int step, const double* partials, int n, double* st, int nshift) {
+  double* zeta1 = st + MS_N + MSA_ZETA1 * kMaxShift;
+  double* zeta2 = st + MS_N + MSA_ZETA2 * kMaxShift;
+  double* csh2 = st + MS_N + MSA_CSH2 * kMaxShift;
+  double* betas = st + MS_N + MSA_BETAS * kMaxShift;
+  double* alphas = st + MS_N + MSA_ALPHAS * kMaxShift;
+  double* zeta = st + MS_N + MSA_ZETA * kMaxShift;
+  double* pp = st + MS_N + MSA_PP * kMaxShift;
+  if (step == MSS_BETA) {
+    const double pq = block_sum_partials(partials, n);
+    if (threadIdx.x == 0) {
+      st[MS_PQ] = pq;
+      const double pa = pq + st[MS_SIGMA0] * st[MS_PP0];
+      st[MS_BETA] = -st[MS_RR] / pa;
+    }
+  } else if (step == MSS_ALPHA) {
+    const double rr = block_sum_partials(partials, n);
+    if (threadIdx.x == 0) {
+      const double beta = st[MS_BETA];
+      const double alpha = rr / st[MS_RR];
+      st[MS_ALPHA] = alpha;
+      st[MS_RR_NEW] = rr;
+      pp[0] = rr;
+      const double alpha_h = 1.0 + st[MS_ALPHA_P] * beta / st[MS_BETA_P];
+      const int nact = (int)st[MS_NACT];
+      for (int i = 1; i < nact; ++i) {
+        double z = (alpha_h - csh2[i] * beta) / zeta1[i] + (1.0 - alpha_h) / zeta2[i];
+        z = 1.0 / z;
+        const double zr = z / zeta1[i];
+        betas[i] = beta * zr;
+        alphas[i] = alpha * zr * zr;
+        zeta[i] = z;
+        zeta2[i] = zeta1[i];
+        zeta1[i] = z;
+      }
+      st[MS_ALPHA_P] = alpha;
+      st[MS_BETA_P] = beta;
+      st[MS_RR] = rr;
+    }
+  } else {  // MSS_PRUNE
+    const int nact = (int)st[MS_NACT];
+    for (int i = 0; i < nact; ++i) {
+      const double v = block_sum_partials(partials + (size_t)i * n, n);
+      if (threadIdx.x == 0) {
+        if (i == 0) st[MS_PP0] = v;
+        else pp[i] = v * st[MS_SNORM];
+      }
+    }
+    if (threadIdx.x == 0) {
+      int ish1 = nact;
+      for (int i = nact - 1; i >= 0; --i) {
+        if (pp[i] > st[MS_TOL2]) { ish1 = i + 1; break; }
+      }
+      st[MS_NACT] = (double)ish1;
+    }
+  }
+}
+
+cudaError_t launch_ms_scalar(int step, const double* partials, int n, double* st, int nshift,
+                             cudaStream_t stream) {
+  ms_scalar_kernel<<<1, 1024, 0, stream>>>(step, partials, n, st, nshift);
+  return cudaGetLastError();
+}
+
 // ------------------------------------------------------------ BLAS
 template <int P>
 __global__ void axpby_kernel(Geom g, void* y, const void* x, double a, const double* a_dev,
