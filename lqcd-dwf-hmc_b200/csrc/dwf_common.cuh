@@ -1,14 +1,15 @@
 // Shared device-side definitions of the B200 domain-wall library.
 //
-// Field layout in HBM (one even/odd 5D half-lattice spinor):
-//   16-byte chunks indexed (k, site, s) -> (k*Vh + site)*Ls + s,
-//   s (the fifth dimension) fastest, so the Ls lanes that own one 4D site
-//   read/write one contiguous run of Ls*16 bytes per chunk.
+// Field layout in HBM (one even/odd 5D half-lattice spinor), site-major:
+//   every 4D site owns one contiguous "column" of col_bytes(prec, Ls) bytes
+//   holding its whole fifth dimension: 16-byte chunks (k, s) -> k*Ls + s,
+//   s fastest, so the Ls lanes that own the site read one contiguous run of
+//   Ls*16 bytes per chunk and a neighbour's column is one bulk (TMA) copy.
 //   A chunk holds complex components q = color + 3*spin:
 //     f64 : 1 complex  (double2), K = 12 chunks per (site, s)
 //     f32 : 2 complex  (float4),  K = 6
 //     f16/bf16 : 4 complex (8 halves in uint4), K = 3, values scaled by a
-//       per-(site, s) float stored after the chunks at [site*Ls + s].
+//       per-(site, s) float stored after the site's chunks (padded to 16 B).
 // Link layout (one plan, both parities):
 //   f64 : [parity][mu][site] x 9 double2 (full 3x3), or 6 double2 (two rows)
 //   f32 : [parity][mu][site] x 3 float4  (two rows, third reconstructed)
@@ -34,19 +35,30 @@ template <> struct Store<PREC_F64> {
   using Chunk = double2;
   static constexpr int K = 12;
   static constexpr bool kScaled = false;
-  __device__ static void load(const void* base, size_t vh, int ls, int site, int s, R* v) {
-    const double2* p = reinterpret_cast<const double2*>(base);
+  __host__ __device__ static constexpr size_t col_bytes(int ls) { return (size_t)K * ls * 16; }
+  // column already in shared memory (or anywhere): chunk (k, s)
+  __device__ static void load_col(const void* col, int ls, int s, R* v) {
+    const double2* p = reinterpret_cast<const double2*>(col);
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-      double2 c = __ldg(p + ((size_t)k * vh + site) * ls + s);
+      double2 c = p[k * ls + s];
+      v[2 * k] = c.x;
+      v[2 * k + 1] = c.y;
+    }
+  }
+  __device__ static void load(const void* base, size_t vh, int ls, int site, int s, R* v) {
+    const double2* p = reinterpret_cast<const double2*>(base) + (size_t)site * K * ls;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      double2 c = __ldg(p + k * ls + s);
       v[2 * k] = c.x;
       v[2 * k + 1] = c.y;
     }
   }
   __device__ static void store(void* base, size_t vh, int ls, int site, int s, const R* v) {
-    double2* p = reinterpret_cast<double2*>(base);
+    double2* p = reinterpret_cast<double2*>(base) + (size_t)site * K * ls;
 #pragma unroll
-    for (int k = 0; k < K; ++k) p[((size_t)k * vh + site) * ls + s] = make_double2(v[2 * k], v[2 * k + 1]);
+    for (int k = 0; k < K; ++k) p[k * ls + s] = make_double2(v[2 * k], v[2 * k + 1]);
   }
 };
 
@@ -55,19 +67,28 @@ template <> struct Store<PREC_F32> {
   using Chunk = float4;
   static constexpr int K = 6;
   static constexpr bool kScaled = false;
-  __device__ static void load(const void* base, size_t vh, int ls, int site, int s, R* v) {
-    const float4* p = reinterpret_cast<const float4*>(base);
+  __host__ __device__ static constexpr size_t col_bytes(int ls) { return (size_t)K * ls * 16; }
+  __device__ static void load_col(const void* col, int ls, int s, R* v) {
+    const float4* p = reinterpret_cast<const float4*>(col);
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-      float4 c = __ldg(p + ((size_t)k * vh + site) * ls + s);
+      float4 c = p[k * ls + s];
+      v[4 * k] = c.x; v[4 * k + 1] = c.y; v[4 * k + 2] = c.z; v[4 * k + 3] = c.w;
+    }
+  }
+  __device__ static void load(const void* base, size_t vh, int ls, int site, int s, R* v) {
+    const float4* p = reinterpret_cast<const float4*>(base) + (size_t)site * K * ls;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      float4 c = __ldg(p + k * ls + s);
       v[4 * k] = c.x; v[4 * k + 1] = c.y; v[4 * k + 2] = c.z; v[4 * k + 3] = c.w;
     }
   }
   __device__ static void store(void* base, size_t vh, int ls, int site, int s, const R* v) {
-    float4* p = reinterpret_cast<float4*>(base);
+    float4* p = reinterpret_cast<float4*>(base) + (size_t)site * K * ls;
 #pragma unroll
     for (int k = 0; k < K; ++k)
-      p[((size_t)k * vh + site) * ls + s] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+      p[k * ls + s] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
   }
 };
 
@@ -98,15 +119,34 @@ template <typename H> struct StoreHalf {
   using Chunk = uint4;
   static constexpr int K = 3;
   static constexpr bool kScaled = true;
-  __device__ static const float* scales(const void* base, size_t vh, int ls) {
-    return reinterpret_cast<const float*>(reinterpret_cast<const uint4*>(base) + (size_t)K * vh * ls);
+  // column: K*ls chunks, then ls floats of scales padded to 16 bytes
+  __host__ __device__ static constexpr size_t col_bytes(int ls) {
+    return (size_t)K * ls * 16 + (((size_t)ls * 4 + 15) / 16) * 16;
   }
-  __device__ static void load(const void* base, size_t vh, int ls, int site, int s, R* v) {
-    const uint4* p = reinterpret_cast<const uint4*>(base);
-    const float sc = __ldg(scales(base, vh, ls) + (size_t)site * ls + s);
+  __device__ static void decode(const uint4* p, const float sc, int ls, int s, R* v) {
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-      uint4 c = __ldg(p + ((size_t)k * vh + site) * ls + s);
+      uint4 c = p[k * ls + s];
+      float2 a = HalfOps<H>::to2(c.x), b = HalfOps<H>::to2(c.y);
+      float2 d = HalfOps<H>::to2(c.z), e = HalfOps<H>::to2(c.w);
+      v[8 * k + 0] = a.x * sc; v[8 * k + 1] = a.y * sc;
+      v[8 * k + 2] = b.x * sc; v[8 * k + 3] = b.y * sc;
+      v[8 * k + 4] = d.x * sc; v[8 * k + 5] = d.y * sc;
+      v[8 * k + 6] = e.x * sc; v[8 * k + 7] = e.y * sc;
+    }
+  }
+  __device__ static void load_col(const void* col, int ls, int s, R* v) {
+    const uint4* p = reinterpret_cast<const uint4*>(col);
+    const float sc = reinterpret_cast<const float*>(p + K * ls)[s];
+    decode(p, sc, ls, s, v);
+  }
+  __device__ static void load(const void* base, size_t vh, int ls, int site, int s, R* v) {
+    const unsigned char* colp = reinterpret_cast<const unsigned char*>(base) + (size_t)site * col_bytes(ls);
+    const uint4* p = reinterpret_cast<const uint4*>(colp);
+    const float sc = __ldg(reinterpret_cast<const float*>(p + K * ls) + s);
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      uint4 c = __ldg(p + k * ls + s);
       float2 a = HalfOps<H>::to2(c.x), b = HalfOps<H>::to2(c.y);
       float2 d = HalfOps<H>::to2(c.z), e = HalfOps<H>::to2(c.w);
       v[8 * k + 0] = a.x * sc; v[8 * k + 1] = a.y * sc;
@@ -116,14 +156,14 @@ template <typename H> struct StoreHalf {
     }
   }
   __device__ static void store(void* base, size_t vh, int ls, int site, int s, const R* v) {
-    uint4* p = reinterpret_cast<uint4*>(base);
+    unsigned char* colp = reinterpret_cast<unsigned char*>(base) + (size_t)site * col_bytes(ls);
+    uint4* p = reinterpret_cast<uint4*>(colp);
     float m = 0.f;
 #pragma unroll
     for (int i = 0; i < 24; ++i) m = fmaxf(m, fabsf(v[i]));
     const float sc = (m > 0.f) ? m : 1.f;
     const float inv = 1.f / sc;
-    float* sp = const_cast<float*>(scales(base, vh, ls));
-    sp[(size_t)site * ls + s] = sc;
+    reinterpret_cast<float*>(p + K * ls)[s] = sc;
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       uint4 c;
@@ -131,7 +171,7 @@ template <typename H> struct StoreHalf {
       c.y = HalfOps<H>::from2(v[8 * k + 2] * inv, v[8 * k + 3] * inv);
       c.z = HalfOps<H>::from2(v[8 * k + 4] * inv, v[8 * k + 5] * inv);
       c.w = HalfOps<H>::from2(v[8 * k + 6] * inv, v[8 * k + 7] * inv);
-      p[((size_t)k * vh + site) * ls + s] = c;
+      p[k * ls + s] = c;
     }
   }
 };
@@ -141,9 +181,9 @@ template <> struct Store<PREC_BF16> : StoreHalf<__nv_bfloat16> {};
 // Bytes of one field of Vh sites x Ls in precision p.
 inline size_t field_bytes(int p, size_t vh, int ls) {
   switch (p) {
-    case PREC_F64: return vh * ls * 12 * 16;
-    case PREC_F32: return vh * ls * 6 * 16;
-    default: return vh * ls * (3 * 16 + 4);
+    case PREC_F64: return vh * Store<PREC_F64>::col_bytes(ls);
+    case PREC_F32: return vh * Store<PREC_F32>::col_bytes(ls);
+    default: return vh * Store<PREC_F16>::col_bytes(ls);
   }
 }
 

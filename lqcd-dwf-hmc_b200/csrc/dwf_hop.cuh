@@ -20,6 +20,7 @@
 
 #include "dwf_common.cuh"
 #include "dwf_chain.cuh"
+#include "tma_util.cuh"
 
 namespace b200 {
 
@@ -30,6 +31,11 @@ template <int LF> struct LinkLoad;
 template <> struct LinkLoad<LINK_F64_18> {
   using R = double;
   static constexpr int kChunks = 9;
+  __device__ static void load_plain(const void* rec, double* u) {
+    const double2* p = reinterpret_cast<const double2*>(rec);
+#pragma unroll
+    for (int j = 0; j < 9; ++j) { double2 c = p[j]; u[2 * j] = c.x; u[2 * j + 1] = c.y; }
+  }
   __device__ static void load(const void* base, size_t idx, double* u) {
     const double2* p = reinterpret_cast<const double2*>(base) + idx * 9;
 #pragma unroll
@@ -39,6 +45,12 @@ template <> struct LinkLoad<LINK_F64_18> {
 template <> struct LinkLoad<LINK_F64_12> {
   using R = double;
   static constexpr int kChunks = 6;
+  __device__ static void load_plain(const void* rec, double* u) {
+    const double2* p = reinterpret_cast<const double2*>(rec);
+#pragma unroll
+    for (int j = 0; j < 6; ++j) { double2 c = p[j]; u[2 * j] = c.x; u[2 * j + 1] = c.y; }
+    su3_reconstruct(u);
+  }
   __device__ static void load(const void* base, size_t idx, double* u) {
     const double2* p = reinterpret_cast<const double2*>(base) + idx * 6;
 #pragma unroll
@@ -49,6 +61,15 @@ template <> struct LinkLoad<LINK_F64_12> {
 template <> struct LinkLoad<LINK_F32_12> {
   using R = float;
   static constexpr int kChunks = 3;
+  __device__ static void load_plain(const void* rec, float* u) {
+    const float4* p = reinterpret_cast<const float4*>(rec);
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      float4 c = p[j];
+      u[4 * j] = c.x; u[4 * j + 1] = c.y; u[4 * j + 2] = c.z; u[4 * j + 3] = c.w;
+    }
+    su3_reconstruct(u);
+  }
   __device__ static void load(const void* base, size_t idx, float* u) {
     const float4* p = reinterpret_cast<const float4*>(base) + idx * 3;
 #pragma unroll
@@ -62,6 +83,17 @@ template <> struct LinkLoad<LINK_F32_12> {
 template <> struct LinkLoad<LINK_F16_12> {
   using R = float;
   static constexpr int kChunks = 2;
+  __device__ static void load_plain(const void* rec, float* u) {
+    const uint4* p = reinterpret_cast<const uint4*>(rec);
+    uint4 a = p[0], b = p[1];
+    unsigned int w[6] = {a.x, a.y, a.z, a.w, b.x, b.y};
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+      float2 f = HalfOps<__half>::to2(w[j]);
+      u[2 * j] = f.x; u[2 * j + 1] = f.y;
+    }
+    su3_reconstruct(u);
+  }
   __device__ static void load(const void* base, size_t idx, float* u) {
     const uint4* p = reinterpret_cast<const uint4*>(base) + idx * 2;
     uint4 a = __ldg(p), b = __ldg(p + 1);
@@ -183,10 +215,110 @@ struct HopParams {
   const double* c_x2_dev;
   const double* c_x3_dev;
   double* red;           // per-block partials of |o1|^2 (nullable)
+  int* err;              // device error word: set when a bounded wait gives up
   int vh, nx2, ny, nz, nt, ls;
   int ieo;               // output parity (0 even, 1 odd)
   double bc[4];
 };
+
+// Epilogue shared by both hop kernels: chain E on the site column, axpy with
+// up to three fields, store o1, optional F map -> o2, |o1|^2 block partials.
+template <int LS, int P, int EPI, int FK>
+__device__ __forceinline__ void hop_epilogue(const HopParams& p, const ChainCoef<typename Store<P>::R>& k,
+                                             typename Store<P>::R* acc,
+                                             typename Store<P>::R* tile, double* red_warp,
+                                             int tid, int lane, int warp, int g, int s, int site,
+                                             bool active) {
+  using St = Store<P>;
+  using R = typename St::R;
+  constexpr int G = 32 / LS;
+  constexpr int WARPS = 4;
+  const size_t vh = p.vh;
+  R o1[24];
+  if (EPI == EPI_HALF) {
+#pragma unroll
+    for (int i = 0; i < 24; ++i) o1[i] = R(-0.5) * acc[i];
+  } else {
+    if (g < G) {
+#pragma unroll
+      for (int i = 0; i < 24; ++i) tile[(g * LS + s) * 24 + i] = acc[i];
+    }
+    __syncwarp();
+    tile_chiral<R, LS, G>(tile, lane, [&](R* xp, R* xm) {
+      apply_epi<R, LS, 0, EPI>(k, xp);
+      apply_epi<R, LS, 1, EPI>(k, xm);
+    });
+    __syncwarp();
+    if (g < G) {
+#pragma unroll
+      for (int i = 0; i < 24; ++i) o1[i] = tile[(g * LS + s) * 24 + i];
+    }
+  }
+
+  double nrm = 0.0;
+  if (active) {
+    const R ce = (R)(p.ce * (p.ce_dev ? *p.ce_dev : 1.0));
+#pragma unroll
+    for (int i = 0; i < 24; ++i) o1[i] *= ce;
+    if (p.x1) {
+      R xv[24];
+      St::load(p.x1, vh, LS, site, s, xv);
+      const R c = (R)(p.c_x1 * (p.c_x1_dev ? *p.c_x1_dev : 1.0));
+#pragma unroll
+      for (int i = 0; i < 24; ++i) o1[i] = fma(c, xv[i], o1[i]);
+    }
+    if (p.x2) {
+      R xv[24];
+      St::load(p.x2, vh, LS, site, s, xv);
+      const R c = (R)(p.c_x2 * (p.c_x2_dev ? *p.c_x2_dev : 1.0));
+#pragma unroll
+      for (int i = 0; i < 24; ++i) o1[i] = fma(c, xv[i], o1[i]);
+    }
+    if (p.x3) {
+      R xv[24];
+      St::load(p.x3, vh, LS, site, s, xv);
+      const R c = (R)(p.c_x3 * (p.c_x3_dev ? *p.c_x3_dev : 1.0));
+#pragma unroll
+      for (int i = 0; i < 24; ++i) o1[i] = fma(c, xv[i], o1[i]);
+    }
+    if (p.out1) St::store(p.out1, vh, LS, site, s, o1);
+    if (p.red) {
+#pragma unroll
+      for (int i = 0; i < 24; ++i) nrm += (double)o1[i] * (double)o1[i];
+    }
+  }
+  if (FK != F_NONE) {
+    __syncwarp();
+    if (g < G) {
+#pragma unroll
+      for (int i = 0; i < 24; ++i) tile[(g * LS + s) * 24 + i] = o1[i];
+    }
+    __syncwarp();
+    tile_chiral<R, LS, G>(tile, lane, [&](R* xp, R* xm) {
+      apply_f<R, LS, 0, FK>(k, xp);
+      apply_f<R, LS, 1, FK>(k, xm);
+    });
+    __syncwarp();
+    if (active) {
+      R o2[24];
+#pragma unroll
+      for (int i = 0; i < 24; ++i) o2[i] = tile[(g * LS + s) * 24 + i];
+      St::store(p.out2, vh, LS, site, s, o2);
+    }
+  }
+  if (p.red) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) nrm += __shfl_xor_sync(0xffffffffu, nrm, off);
+    if (lane == 0) red_warp[warp] = nrm;
+    __syncthreads();
+    if (tid == 0) {
+      double b = 0.0;
+#pragma unroll
+      for (int w = 0; w < WARPS; ++w) b += red_warp[w];
+      p.red[blockIdx.x] = b;
+    }
+  }
+}
 
 // Occupancy variants (minimum resident 128-thread blocks per SM requested from
 // the register allocator); the plan's autotuner times both and keeps the faster.
@@ -285,92 +417,183 @@ dwf_hop_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename Sto
 #undef B200_HOP_DIR
   }
 
-  // ---------------- epilogue: fifth-dimension chain on the site column
-  R* tile = tile_all + (size_t)warp * G * LS * 24;
-  R o1[24];
-  if (!kTile || EPI == EPI_HALF) {
+  hop_epilogue<LS, P, EPI, FK>(p, k, acc, tile_all + (size_t)warp * G * LS * 24, red_warp, tid, lane,
+                               warp, g, s, site, active);
+}
+
+// ---------------------------------------------------------------------------
+// TMA-staged variant.  Each warp keeps an S-deep pipeline over the 8 hop
+// directions: for every one of its G sites the lane with s == 0 issues two
+// bulk asynchronous copies per direction -- the neighbour site's whole
+// fifth-dimension column (site-major field layout) and the link -- into the
+// warp's shared-memory stage, completing on that stage's mbarrier.  While
+// direction d is computed from shared memory, directions d+1..d+S-1 are in
+// flight, without holding registers.  Stage buffers are reused after the
+// warp's lanes have finished reading them (__syncwarp + proxy fence).
+// All waits are bounded; on timeout the kernel sets p.err and skips its work.
+template <int LS, int P, int LF> struct TmaGeom {
+  static constexpr int G = 32 / LS;
+  static constexpr int COL = (int)Store<P>::col_bytes(LS);
+  static constexpr int LNK = LinkLoad<LF>::kChunks * 16;
+  static constexpr int SLOT = COL + LNK;                       // one site, one direction
+  template <int S> static constexpr int warp_bytes() {
+    // stages, and the epilogue tile (reuses the stage area)
+    return (S * G * SLOT > G * LS * 24 * (int)sizeof(typename Store<P>::R))
+               ? S * G * SLOT
+               : G * LS * 24 * (int)sizeof(typename Store<P>::R);
+  }
+};
+
+template <int LS, int P, int LF, int EPI, int FK, int S>
+__global__ void __launch_bounds__(128)
+dwf_hop_tma_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename Store<P>::R> k) {
+  using St = Store<P>;
+  using R = typename St::R;
+  using TG = TmaGeom<LS, P, LF>;
+  constexpr bool kDagHop = EpiIsDag<EPI>::v;
+  constexpr int G = TG::G;
+  constexpr int WARPS = 4;
+  constexpr int WB = TG::template warp_bytes<S>();
+  constexpr int WBA = (WB + 127) / 128 * 128;
+
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ double red_warp[WARPS];
+  __shared__ __align__(8) uint64_t bars[WARPS][S];
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const int g = lane / LS;
+  const int s = lane - g * LS;
+  const int site = (blockIdx.x * WARPS + warp) * G + g;
+  const bool active = (g < G) && (site < p.vh);
+  const bool issuer = (g < G) && (s == 0);
+  unsigned char* wbase = smem_raw + (size_t)warp * WBA;
+  const size_t vh = p.vh;
+
+  if (lane == 0) {
 #pragma unroll
-    for (int i = 0; i < 24; ++i) o1[i] = R(-0.5) * acc[i];
+    for (int st = 0; st < S; ++st) mbar_init(smem_u32(&bars[warp][st]), G);
+    mbar_fence_init();
+  }
+  __syncwarp();
+
+  // neighbour sites and edge phases of the 8 directions (x+, x-, y+, ..., t-)
+  int nb[8];
+  R ph[8];
+  if (active) {
+    const int ix2 = site % p.nx2;
+    const int iyzt = site / p.nx2;
+    const int y = iyzt % p.ny;
+    const int izt = iyzt / p.ny;
+    const int z = izt % p.nz;
+    const int t = izt / p.nz;
+    const int keo = (p.ieo + y + z + t) & 1;
+    const int x = 2 * ix2 + keo;
+    const int row = p.nx2 * iyzt;
+    nb[0] = row + ((ix2 + keo == p.nx2) ? 0 : ix2 + keo);
+    nb[1] = row + ((ix2 - 1 + keo < 0) ? p.nx2 - 1 : ix2 - 1 + keo);
+    ph[0] = (x == 2 * p.nx2 - 1) ? (R)p.bc[0] : R(1);
+    ph[1] = (x == 0) ? (R)p.bc[0] : R(1);
+    const int sy = p.nx2, sz = p.nx2 * p.ny, st4 = p.nx2 * p.ny * p.nz;
+    nb[2] = (y == p.ny - 1) ? site - (p.ny - 1) * sy : site + sy;
+    nb[3] = (y == 0) ? site + (p.ny - 1) * sy : site - sy;
+    ph[2] = (y == p.ny - 1) ? (R)p.bc[1] : R(1);
+    ph[3] = (y == 0) ? (R)p.bc[1] : R(1);
+    nb[4] = (z == p.nz - 1) ? site - (p.nz - 1) * sz : site + sz;
+    nb[5] = (z == 0) ? site + (p.nz - 1) * sz : site - sz;
+    ph[4] = (z == p.nz - 1) ? (R)p.bc[2] : R(1);
+    ph[5] = (z == 0) ? (R)p.bc[2] : R(1);
+    nb[6] = (t == p.nt - 1) ? site - (p.nt - 1) * st4 : site + st4;
+    nb[7] = (t == 0) ? site + (p.nt - 1) * st4 : site - st4;
+    ph[6] = (t == p.nt - 1) ? (R)p.bc[3] : R(1);
+    ph[7] = (t == 0) ? (R)p.bc[3] : R(1);
   } else {
-    if (g < G) {
 #pragma unroll
-      for (int i = 0; i < 24; ++i) tile[(g * LS + s) * 24 + i] = acc[i];
-    }
-    __syncwarp();
-    tile_chiral<R, LS, G>(tile, lane, [&](R* xp, R* xm) {
-      apply_epi<R, LS, 0, EPI>(k, xp);
-      apply_epi<R, LS, 1, EPI>(k, xm);
-    });
-    __syncwarp();
-    if (g < G) {
-#pragma unroll
-      for (int i = 0; i < 24; ++i) o1[i] = tile[(g * LS + s) * 24 + i];
-    }
+    for (int d = 0; d < 8; ++d) { nb[d] = 0; ph[d] = R(0); }
   }
 
-  double nrm = 0.0;
-  if (active) {
-    const R ce = (R)(p.ce * (p.ce_dev ? *p.ce_dev : 1.0));
+  auto col_ptr = [&](int st) { return wbase + (size_t)(st * G + g) * TG::SLOT; };
+  int nissued = 0;   // directions issued by this warp (uniform across its lanes)
+  auto issue = [&](int d, int st) {
+    ++nissued;
+    if (!issuer) return;
+    const uint32_t bar = smem_u32(&bars[warp][st]);
+    if (!active) { mbar_arrive(bar); return; }
+    const int mu = d >> 1;
+    const bool fwd = (d & 1) == 0;
+    const size_t lidx = fwd ? (size_t)(p.ieo + 2 * mu) * vh + site : (size_t)(1 - p.ieo + 2 * mu) * vh + nb[d];
+    unsigned char* dst = col_ptr(st);
+    mbar_arrive_expect_tx(bar, TG::SLOT);
+    bulk_g2s(smem_u32(dst), reinterpret_cast<const unsigned char*>(p.in) + (size_t)nb[d] * TG::COL,
+             TG::COL, bar);
+    bulk_g2s(smem_u32(dst + TG::COL), reinterpret_cast<const unsigned char*>(p.links) + lidx * TG::LNK,
+             TG::LNK, bar);
+  };
+
 #pragma unroll
-    for (int i = 0; i < 24; ++i) o1[i] *= ce;
-    if (p.x1) {
-      R xv[24];
-      St::load(p.x1, vh, LS, site, s, xv);
-      const R c = (R)(p.c_x1 * (p.c_x1_dev ? *p.c_x1_dev : 1.0));
+  for (int d = 0; d < S; ++d) issue(d, d);
+
+  R acc[24];
 #pragma unroll
-      for (int i = 0; i < 24; ++i) o1[i] = fma(c, xv[i], o1[i]);
-    }
-    if (p.x2) {
-      R xv[24];
-      St::load(p.x2, vh, LS, site, s, xv);
-      const R c = (R)(p.c_x2 * (p.c_x2_dev ? *p.c_x2_dev : 1.0));
-#pragma unroll
-      for (int i = 0; i < 24; ++i) o1[i] = fma(c, xv[i], o1[i]);
-    }
-    if (p.x3) {
-      R xv[24];
-      St::load(p.x3, vh, LS, site, s, xv);
-      const R c = (R)(p.c_x3 * (p.c_x3_dev ? *p.c_x3_dev : 1.0));
-#pragma unroll
-      for (int i = 0; i < 24; ++i) o1[i] = fma(c, xv[i], o1[i]);
-    }
-    if (p.out1) St::store(p.out1, vh, LS, site, s, o1);
-    if (p.red) {
-#pragma unroll
-      for (int i = 0; i < 24; ++i) nrm += (double)o1[i] * (double)o1[i];
-    }
+  for (int i = 0; i < 24; ++i) acc[i] = 0;
+  bool ok = true;
+  int ndone = 0;     // directions whose copies this warp has seen complete
+
+#define B200_TMA_STEP(D, MU, SIGN)                                                   \
+  {                                                                                  \
+    constexpr int st = (D) % S;                                                      \
+    const uint32_t parity = ((D) / S) & 1;                                           \
+    if (ok) {                                                                        \
+      const bool got = mbar_wait_bounded(smem_u32(&bars[warp][st]), parity);         \
+      ok = __all_sync(0xffffffffu, got);                                             \
+      if (ok) ndone = (D) + 1;                                                       \
+      else if (lane == 0 && p.err) atomicExch(p.err, 1);                             \
+    }                                                                                \
+    if (ok && active) {                                                              \
+      R w[24], h[12], o[12], u[18];                                                  \
+      const unsigned char* c = col_ptr(st);                                          \
+      St::load_col(c, LS, s, w);                                                     \
+      if (kDagHop) {                                                                 \
+        _Pragma("unroll") for (int q = 0; q < 12; ++q) {                             \
+          R tmp = w[q]; w[q] = w[q + 12]; w[q + 12] = tmp; }                         \
+      }                                                                              \
+      project<R, MU, SIGN>(w, h);                                                    \
+      LinkLoad<LF>::load_plain(c + TG::COL, u);                                      \
+      su3_mult_half<R, (SIGN < 0)>(u, h, o);                                         \
+      reconstruct_acc<R, MU, SIGN>(acc, o, ph[D]);                                   \
+    }                                                                                \
+    __syncwarp();                                                                    \
+    if ((D) + S < 8 && ok) {                                                         \
+      fence_proxy_async_smem();                                                      \
+      issue((D) + S, st);                                                            \
+    }                                                                                \
   }
-  if (FK != F_NONE) {
-    __syncwarp();
-    if (g < G) {
-#pragma unroll
-      for (int i = 0; i < 24; ++i) tile[(g * LS + s) * 24 + i] = o1[i];
-    }
-    __syncwarp();
-    tile_chiral<R, LS, G>(tile, lane, [&](R* xp, R* xm) {
-      apply_f<R, LS, 0, FK>(k, xp);
-      apply_f<R, LS, 1, FK>(k, xm);
-    });
-    __syncwarp();
-    if (active) {
-      R o2[24];
-#pragma unroll
-      for (int i = 0; i < 24; ++i) o2[i] = tile[(g * LS + s) * 24 + i];
-      St::store(p.out2, vh, LS, site, s, o2);
-    }
+
+  B200_TMA_STEP(0, 0, 1)
+  B200_TMA_STEP(1, 0, -1)
+  B200_TMA_STEP(2, 1, 1)
+  B200_TMA_STEP(3, 1, -1)
+  B200_TMA_STEP(4, 2, 1)
+  B200_TMA_STEP(5, 2, -1)
+  B200_TMA_STEP(6, 3, 1)
+  B200_TMA_STEP(7, 3, -1)
+#undef B200_TMA_STEP
+
+  // A warp that gave up waits (again bounded) for the copies it still has in
+  // flight, then the whole CTA returns without touching its outputs; the host
+  // sees p.err.
+  if (!ok) {
+    for (int d = ndone; d < nissued; ++d) mbar_wait_bounded(smem_u32(&bars[warp][d % S]), (d / S) & 1);
   }
-  if (p.red) {
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) nrm += __shfl_xor_sync(0xffffffffu, nrm, off);
-    if (lane == 0) red_warp[warp] = nrm;
-    __syncthreads();
-    if (tid == 0) {
-      double b = 0.0;
-#pragma unroll
-      for (int w = 0; w < WARPS; ++w) b += red_warp[w];
-      p.red[blockIdx.x] = b;
-    }
-  }
+  if (!__syncthreads_and(ok ? 1 : 0)) return;
+  hop_epilogue<LS, P, EPI, FK>(p, k, acc, reinterpret_cast<R*>(wbase), red_warp, tid, lane, warp, g, s,
+                               site, active);
+}
+
+template <int LS, int P, int LF, int S>
+constexpr size_t hop_tma_smem_bytes() {
+  return (size_t)4 * ((TmaGeom<LS, P, LF>::template warp_bytes<S>() + 127) / 128 * 128);
 }
 
 template <int LS, int P>

@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <cstdint>
 #include <map>
 #include <mutex>
 #include <string>
@@ -42,6 +43,9 @@ int fail(int code, const char* fmt, ...) {
   } while (0)
 
 bool ls_supported(int ls) { return ls == 4 || ls == 6 || ls == 8 || ls == 12 || ls == 16; }
+
+// Field buffers are read by 16-byte vector loads and bulk (TMA) copies.
+bool misaligned(const void* p) { return p && (reinterpret_cast<uintptr_t>(p) & 15u) != 0; }
 }  // namespace
 
 namespace b200 {
@@ -98,9 +102,11 @@ struct b200_dwf {
   double* u_lex = nullptr;      // device copy of the lexical links
   bool have_links = false;
   double* red = nullptr;        // reduction partials
+  int* err = nullptr;           // device error word of the bounded waits
   int red_n = 0;
   double* sc = nullptr;         // solver scalars (device)
   double* sc_host = nullptr;    // pinned mirror
+  int* err_host = nullptr;      // pinned mirror of err
   double* stage = nullptr;      // device f64 staging for convert/reverse
   void* work[12][4] = {};       // work fields per precision
   void* tune_out[2][4] = {};    // autotuner scratch outputs per precision
@@ -147,6 +153,7 @@ HopParams hop_base(const b200_dwf* op, int prec, int ieo, int epi, int fk = F_NO
   p.ls = op->g.ls;
   p.ieo = ieo;
   p.ce = 1.0;
+  p.err = op->err;
   for (int mu = 0; mu < 4; ++mu) p.bc[mu] = op->bc[mu];
   return p;
 }
@@ -167,6 +174,7 @@ SopParams sop_base(const b200_dwf* op) {
 // B200_AUTOTUNE=0 disables tuning (variant 0).  The first call of a
 // combination must not be inside a CUDA graph capture.
 typedef std::tuple<int, int, int, int, int> TuneKey;   // vh, ls, prec, epi, fk
+constexpr int kHopVariants = 3;   // direct loads, TMA 2-stage, TMA 3-stage
 std::map<TuneKey, std::pair<int, float> > g_tune;
 std::mutex g_tune_mu;
 
@@ -190,7 +198,7 @@ int tune_hop(b200_dwf* op, int prec, const HopParams& p0, cudaStream_t st, int* 
   B200_CHECK_CUDA(cudaEventCreate(&b));
   float best_ms = 1e30f;
   *best = 0;
-  for (int v = 0; v < 2; ++v) {
+  for (int v = 0; v < kHopVariants; ++v) {
     p.variant = v;
     B200_CHECK_CUDA(launch_hop(prec, p, op->coefs, st));
     B200_CHECK_CUDA(cudaEventRecord(a, st));
@@ -208,9 +216,20 @@ int tune_hop(b200_dwf* op, int prec, const HopParams& p0, cudaStream_t st, int* 
   return 0;
 }
 
+// B200_HOP_VARIANT=<n> pins the hop variant (no tuning), e.g. to test each.
+int forced_variant() {
+  const char* e = getenv("B200_HOP_VARIANT");
+  if (!e || !e[0]) return -1;
+  const int v = atoi(e);
+  return (v >= 0 && v < kHopVariants) ? v : -1;
+}
+
 int run_hop(b200_dwf* op, int prec, HopParams& p, cudaStream_t st) {
   int variant = 0;
-  if (tuning_enabled()) {
+  const int fv = forced_variant();
+  if (fv >= 0) {
+    variant = fv;
+  } else if (tuning_enabled()) {
     const TuneKey key(op->g.vh, op->g.ls, prec, p.epi, p.fk);
     bool found = false;
     {
@@ -347,10 +366,15 @@ int reduce_to(b200_dwf* op, int nblocks, double* out_dev, int fin_op, cudaStream
   return 0;
 }
 
+// Reads one solver scalar (and the device error word) back to the host.
 int host_scalar(b200_dwf* op, int idx, double* out, cudaStream_t st) {
   B200_CHECK_CUDA(cudaMemcpyAsync(op->sc_host + idx, op->sc + idx, sizeof(double),
                                   cudaMemcpyDeviceToHost, st));
+  B200_CHECK_CUDA(cudaMemcpyAsync(op->err_host, op->err, sizeof(int), cudaMemcpyDeviceToHost, st));
   B200_CHECK_CUDA(cudaStreamSynchronize(st));
+  if (*op->err_host != 0)
+    return fail(B200_ECUDA, "a kernel gave up waiting for its bulk copies (device error word %d)",
+                *op->err_host);
   *out = op->sc_host[idx];
   return 0;
 }
@@ -444,9 +468,15 @@ int b200_dwf_create(b200_dwf_t** out, const int lattice[4], int Ls, double mq, d
   op->red_n = red_n;
   if (cudaMalloc(&op->red, (size_t)red_n * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&op->sc, SC_N * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&op->err, sizeof(int)) != cudaSuccess ||
+      cudaMallocHost(&op->err_host, sizeof(int)) != cudaSuccess ||
       cudaMallocHost(&op->sc_host, SC_N * sizeof(double)) != cudaSuccess) {
     b200_dwf_destroy(op);
     return fail(B200_ENOMEM, "device allocation for the operator plan failed");
+  }
+  if (cudaMemset(op->err, 0, sizeof(int)) != cudaSuccess) {
+    b200_dwf_destroy(op);
+    return fail(B200_ECUDA, "clearing the device error word failed");
   }
   *out = op;
   return 0;
@@ -458,7 +488,9 @@ int b200_dwf_destroy(b200_dwf_t* op) {
   cudaFree(op->u_lex);
   cudaFree(op->red);
   cudaFree(op->sc);
+  cudaFree(op->err);
   if (op->sc_host) cudaFreeHost(op->sc_host);
+  if (op->err_host) cudaFreeHost(op->err_host);
   cudaFree(op->stage);
   for (int i = 0; i < 12; ++i)
     for (int p = 0; p < 4; ++p) cudaFree(op->work[i][p]);
@@ -531,6 +563,7 @@ int b200_dwf_mult(b200_dwf_t* op, int prec, void* v, const void* w, const char* 
                   void* stream) {
   if (!op || !v || !w || !mode || prec < 0 || prec > 3) return fail(B200_EINVAL, "invalid argument");
   if (v == w) return fail(B200_EINVAL, "mult: input and output fields must differ");
+  if (misaligned(v) || misaligned(w)) return fail(B200_EINVAL, "mult: field pointers must be 16-byte aligned");
   return apply_mode(op, prec, v, w, mode, dag, (cudaStream_t)stream);
 }
 
@@ -666,6 +699,7 @@ static int true_residual(b200_dwf_t* op, int prec, const void* x, const void* b,
 int b200_cg_solve(b200_dwf_t* op, int prec, void* x, const void* b, int maxiter, double tol2,
                   int* nconv, double* diff, void* stream) {
   if (!op || !x || !b || prec < 0 || prec > 3 || maxiter < 0) return fail(B200_EINVAL, "invalid argument");
+  if (misaligned(x) || misaligned(b)) return fail(B200_EINVAL, "field pointers must be 16-byte aligned");
   cudaStream_t st = (cudaStream_t)stream;
   int n = 0;
   double rel2 = 0.0;
@@ -693,7 +727,8 @@ int b200_shiftcg_solve(b200_dwf_t* op, void* const* x, const double* sigma, int 
     return fail(B200_EINVAL, "invalid argument");
   if (nshift > kMaxShift) return fail(B200_EINVAL, "at most %d shifts (got %d)", kMaxShift, nshift);
   for (int i = 0; i < nshift; ++i)
-    if (!x[i]) return fail(B200_EINVAL, "null solution field %d", i);
+    if (!x[i] || misaligned(x[i])) return fail(B200_EINVAL, "solution field %d null or not 16-byte aligned", i);
+  if (misaligned(b)) return fail(B200_EINVAL, "field pointers must be 16-byte aligned");
   cudaStream_t st = (cudaStream_t)stream;
   int rc;
   if ((rc = ensure_links(op, prec, st))) return rc;
@@ -815,6 +850,7 @@ int b200_richardson_solve(b200_dwf_t* op, int inner_prec, void* x, const void* b
                           int* nconv_inner, double* diff, void* stream) {
   if (!op || !x || !b || inner_prec < 0 || inner_prec > 3 || maxiter < 0 || maxiter_inner < 1)
     return fail(B200_EINVAL, "invalid argument");
+  if (misaligned(x) || misaligned(b)) return fail(B200_EINVAL, "field pointers must be 16-byte aligned");
   cudaStream_t st = (cudaStream_t)stream;
   const int P64 = PREC_F64;
   int rc;

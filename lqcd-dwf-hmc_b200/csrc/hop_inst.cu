@@ -3,6 +3,8 @@
 #include "dwf_hop.cuh"
 #include "dwf_kernels.h"
 
+#include <type_traits>
+
 #ifndef B200_PREC
 #error "B200_PREC must be defined"
 #endif
@@ -35,9 +37,29 @@ cudaError_t run_mb(const HopParams& p, const ChainCoefs& c, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+template <int LS, int P, int EPI, int FK, int S>
+cudaError_t run_tma(const HopParams& p, const ChainCoefs& c, cudaStream_t st) {
+  using R = typename Store<P>::R;
+  constexpr int LF = DefaultLink<P>::v;
+  constexpr size_t smem = hop_tma_smem_bytes<LS, P, LF, S>();
+  auto k = dwf_hop_tma_kernel<LS, P, LF, EPI, FK, S>;
+  static bool attr_done = false;
+  if (!attr_done) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr_done = true;
+  }
+  const ChainCoef<R>& kc = *reinterpret_cast<const ChainCoef<R>*>(
+      std::is_same<R, double>::value ? (const void*)&c.d : (const void*)&c.f);
+  k<<<hop_grid(LS, p.vh), 128, smem, st>>>(p, kc);
+  return cudaGetLastError();
+}
+
+// variant 0: direct loads; 1: TMA-staged, 2 stages; 2: TMA-staged, 3 stages
 template <int LS, int P, int EPI, int FK>
 cudaError_t run(const HopParams& p, const ChainCoefs& c, cudaStream_t st) {
-  if (p.variant == 1) return run_mb<LS, P, EPI, FK, HopMinBlocks<P>::v1>(p, c, st);
+  if (p.variant == 1) return run_tma<LS, P, EPI, FK, 2>(p, c, st);
+  if (p.variant == 2) return run_tma<LS, P, EPI, FK, 3>(p, c, st);
   return run_mb<LS, P, EPI, FK, HopMinBlocks<P>::v0>(p, c, st);
 }
 
