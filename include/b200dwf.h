@@ -156,6 +156,47 @@ int b200_richardson_solve(b200_dwf_t *op, int inner_prec, void *x, const void *b
 int b200_field_norm2_noalloc(int prec, const void *x, long nsite, int ls,
                              double *result, void *stream);
 
+/* ---------------------------------------------------------------- force
+ * Force_F_Domainwall_eo::force_udiv1 (src/lib/Force/Fermion/
+ * force_F_Domainwall_eo.cpp:170-318; Accel form AForce_F_Domainwall_5din_eo::
+ * force_udiv1_H/Hdag, src/lib_alt_Accel/Force/Fermion/
+ * aforce_F_Domainwall_5din_eo-tmpl.h:342-453) with the reference's argument
+ * order: mode "H": a = zeta (= H eta), b = eta; mode "Hdag": a = eta,
+ * b = zeta.  force: device array in the lexical Field_G(Nvol, 4) layout
+ * (18 reals per (site, mu)), fully overwritten.  FP64 fields; the operator's
+ * parameter_alpha must be 1 (as in the reference). */
+int b200_dwf_force_udiv1(b200_dwf_t *op, const char *mode, double *force, const void *a,
+                         const void *b, void *stream);
+/* force_udiv(force, eta) = force_udiv1_H(H eta, eta) + force_udiv1_Hdag(eta, H eta)
+ * (force_F_Domainwall_eo.cpp:150-167), fused: three hops and two force passes. */
+int b200_dwf_force_udiv(b200_dwf_t *op, double *force, const void *eta, void *stream);
+
+/* ---------------------------------------------------------------- stout
+ * Stout smearing levels and the smeared-force Jacobian, on the device.
+ * Director_Smear + Smear_APE + Projection_Stout_SU3 (src/lib/Smear/
+ * director_Smear.cpp, smear_APE.cpp:108-140, projection_Stout_SU3.cpp:60-500;
+ * alt driver Director_alt_Smear src/lib_alt/Smear/director_alt_Smear-tmpl.h:
+ * 21-286) and ForceSmear_APE::force_udiv (src/lib/Smear/forceSmear_APE.cpp)
+ * chained by AForce_F_Smeared_alt::mult_jacobian (src/lib_alt/Force/Fermion/
+ * aforce_F_Smeared_alt-tmpl.h:170-191).  Links and forces: device arrays in
+ * the lexical Field_G(Nvol, 4) layout. */
+typedef struct b200_smear b200_smear_t;
+int b200_smear_create(b200_smear_t **sm, const int lattice[4], double rho, int nsmear);
+int b200_smear_destroy(b200_smear_t *sm);
+/* set_config + smear: u = thin links (host if on_device == 0, else device). */
+int b200_smear_set_config(b200_smear_t *sm, const double *u, int on_device, void *stream);
+/* Device pointer of smearing level `level` (0 = thin links, nsmear = fully
+ * smeared); NULL if out of range or no config was set. */
+const double *b200_smear_config(b200_smear_t *sm, int level);
+/* Copy of level `level` to host memory (18*4*Nvol doubles). */
+int b200_smear_get_config(b200_smear_t *sm, int level, double *host_out, void *stream);
+/* mult_jacobian: sigma (force w.r.t. the fully smeared links) is replaced in
+ * place by the force w.r.t. the thin links. */
+int b200_smear_jacobian(b200_smear_t *sm, double *sigma, void *stream);
+/* AForce_F::mult_generator (src/lib_alt_Accel/Force/Fermion/aforce_F.cpp:62-75):
+ * force <- -2 * (traceless anti-Hermitian part of U force), per link. */
+int b200_force_mult_generator(const int lattice[4], double *force, const double *u, void *stream);
+
 /* ---------------------------------------------------------------- tuning
  * Text table of the autotuner's choices (one line per geometry, precision and
  * kernel epilogue: chosen occupancy variant and its time per launch).  The

@@ -64,6 +64,16 @@ def lib():
                                      ctypes.c_double, ip, dp, vp]
     L.b200_richardson_solve.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_double,
                                         ctypes.c_int, ctypes.c_double, ip, ip, dp, vp]
+    L.b200_dwf_force_udiv1.argtypes = [vp, ctypes.c_char_p, vp, vp, vp, vp]
+    L.b200_dwf_force_udiv.argtypes = [vp, vp, vp, vp]
+    L.b200_smear_create.argtypes = [ctypes.POINTER(vp), ip, ctypes.c_double, ctypes.c_int]
+    L.b200_smear_destroy.argtypes = [vp]
+    L.b200_smear_set_config.argtypes = [vp, vp, ctypes.c_int, vp]
+    L.b200_smear_config.argtypes = [vp, ctypes.c_int]
+    L.b200_smear_config.restype = ctypes.c_void_p
+    L.b200_smear_jacobian.argtypes = [vp, vp, vp]
+    L.b200_smear_get_config.argtypes = [vp, ctypes.c_int, dp, vp]
+    L.b200_force_mult_generator.argtypes = [ip, vp, vp, vp]
     L.b200_field_norm2_noalloc.argtypes = [ctypes.c_int, vp, ctypes.c_long, ctypes.c_int, dp, vp]
     L.b200_tuning_table.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
     L.b200_cg_solve.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_double,
@@ -185,6 +195,24 @@ class DomainWall:
     def copy_convert(self, out, inp):
         check(lib().b200_field_copy_convert(self.handle, out.prec, out.ptr, inp.prec, inp.ptr, None))
 
+    # force (Force_F_Domainwall_eo) --------------------------------------
+    def _force_buf(self):
+        import torch
+        return torch.empty(18 * 2 * self.nvol * 4, dtype=torch.float64, device="cuda")
+
+    def force_udiv1(self, mode, a, b):
+        """force_udiv1 in mode H (a=zeta, b=eta) or Hdag (a=eta, b=zeta);
+        returns the lexical Field_G(Nvol, 4) force as a numpy array."""
+        f = self._force_buf()
+        check(lib().b200_dwf_force_udiv1(self.handle, mode.encode(), ctypes.c_void_p(f.data_ptr()),
+                                         a.ptr, b.ptr, None))
+        return f.cpu().numpy()
+
+    def force_udiv(self, eta):
+        f = self._force_buf()
+        check(lib().b200_dwf_force_udiv(self.handle, ctypes.c_void_p(f.data_ptr()), eta.ptr, None))
+        return f.cpu().numpy()
+
     # solvers -----------------------------------------------------------
     def shiftcg(self, xs, sigma, b, tol2, maxiter=10000):
         """Multishift CG on DdagD + sigma_i (FP64 fields)."""
@@ -218,3 +246,53 @@ class DomainWall:
         if rc not in (0, -4):
             check(rc)
         return n.value, d.value, rc
+
+
+class StoutSmear:
+    """Mirror of Director_alt_Smear with APE/stout smearing (rho, nsmear) over
+    the C ABI: smearing levels on the device and the smeared-force Jacobian."""
+
+    def __init__(self, lattice, rho, nsmear):
+        self.lattice = list(lattice)
+        self.nsmear = nsmear
+        self.nvol = int(np.prod(lattice))
+        h = ctypes.c_void_p()
+        check(lib().b200_smear_create(ctypes.byref(h), (ctypes.c_int * 4)(*lattice), rho, nsmear))
+        self.handle = h
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and _lib is not None:
+            _lib.b200_smear_destroy(h)
+            self.handle = None
+
+    def set_config(self, u_lex):
+        u = np.ascontiguousarray(u_lex, np.float64)
+        check(lib().b200_smear_set_config(self.handle, u.ctypes.data_as(ctypes.c_void_p), 0, None))
+
+    def config_ptr(self, level):
+        p = lib().b200_smear_config(self.handle, level)
+        if not p:
+            raise B200Error("no smearing level %d" % level)
+        return p
+
+    def config(self, level):
+        out = np.empty(18 * 4 * self.nvol)
+        check(lib().b200_smear_get_config(self.handle, level, _dp(out), None))
+        return out
+
+    def jacobian(self, sigma_lex):
+        import torch
+        t = torch.from_numpy(np.ascontiguousarray(sigma_lex, np.float64)).cuda()
+        check(lib().b200_smear_jacobian(self.handle, ctypes.c_void_p(t.data_ptr()), None))
+        return t.cpu().numpy()
+
+
+def mult_generator(lattice, force_lex, u_lex):
+    """AForce_F::mult_generator on the device: -2 at(U F) per link."""
+    import torch
+    f = torch.from_numpy(np.ascontiguousarray(force_lex, np.float64)).cuda()
+    u = torch.from_numpy(np.ascontiguousarray(u_lex, np.float64)).cuda()
+    check(lib().b200_force_mult_generator((ctypes.c_int * 4)(*lattice), ctypes.c_void_p(f.data_ptr()),
+                                          ctypes.c_void_p(u.data_ptr()), None))
+    return f.cpu().numpy()

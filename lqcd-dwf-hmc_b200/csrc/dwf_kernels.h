@@ -89,6 +89,22 @@ enum MsStep { MSS_BETA = 0, MSS_ALPHA = 1, MSS_PRUNE = 2 };
 cudaError_t launch_ms_scalar(int step, const double* partials, int n, double* st, int nshift,
                              cudaStream_t stream);
 
+// Fermion force terms (force.cu): for the sites x of parity ieo and mu = 0..3,
+//   F_mu(x) = beta F_mu(x) + coef sum_s sum_spin
+//             ( [(1 - g_mu) Y1(x+mu)]_c1 conj(Z1(x))_c2 + [(1 + g_mu) Y2(x+mu)]_c1 conj(Z2(x))_c2 )
+// (either term may be absent), into the lexical Field_G(Nvol, 4) force.
+struct ForceParams {
+  const void* y1;
+  const void* z1;
+  const void* y2;
+  const void* z2;
+  double* force;
+  double coef, beta;
+  int ieo, vh, nx2, ny, nz, nt, ls;
+  double bc[4];
+};
+cudaError_t launch_force(const ForceParams& p, cudaStream_t st);
+
 // number of blocks the reductions of each launcher produce
 int hop_grid(int ls, int vh);
 int site_s_grid(int ls, int vh);

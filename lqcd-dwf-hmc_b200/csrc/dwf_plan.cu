@@ -904,6 +904,102 @@ int b200_richardson_solve(b200_dwf_t* op, int inner_prec, void* x, const void* b
   return 0;
 }
 
+// Force_F_Domainwall_eo (src/lib/Force/Fermion/force_F_Domainwall_eo.cpp:
+// 150-327) on the device.  With y_e = M5pre(eta), y_o = M5pre M_oo^-1 D_oe eta,
+// A_e = M_ee^-+ gm5R zeta and A_o = M_oo^-+ D_oe^+ A_e (both fifth-dimension
+// chains fused into the hops), the reference's terms become
+//   H    : even  +1/2 sum [(1-g) y_o(x+mu)] conj(A_e) ; odd  [(1-g) y_e(x+mu)] conj(A_o)
+//   Hdag : even  +1/2 sum [(1+g) A_o(x+mu)] conj(y_e) ; odd  [(1+g) A_e(x+mu)] conj(y_o)
+// (U^+ U = 1 and the dagger's M5^+ moved onto the conjugated field as M5pre).
+static int force_fields(b200_dwf_t* op, const void* eta, const void* zeta, bool zeta_is_h_eta,
+                        cudaStream_t st) {
+  const int prec = PREC_F64;
+  int rc;
+  if ((rc = ensure_links(op, prec, st))) return rc;
+  for (int i = 0; i < 5; ++i)
+    if ((rc = ensure_work(op, prec, i))) return rc;
+  void* ye = op->work[0][prec];
+  void* yo = op->work[1][prec];
+  void* ae = op->work[2][prec];
+  void* ao = op->work[3][prec];
+  if ((rc = apply_sop(op, prec, ye, eta, SOP_M5PRE, st))) return rc;
+  HopParams p1 = hop_base(op, prec, 1, EPI_K1);
+  p1.in = ye; p1.out1 = yo;
+  if ((rc = run_hop(op, prec, p1, st))) return rc;
+  if (zeta_is_h_eta) {
+    // gm5R (H eta) = D eta, so A_e = LUdag(D eta) comes out of D's second hop
+    HopParams p2 = hop_base(op, prec, 0, EPI_K2N, F_LUDAG);
+    p2.in = yo; p2.out1 = nullptr; p2.x1 = eta; p2.c_x1 = 1.0; p2.out2 = ae;
+    if ((rc = run_hop(op, prec, p2, st))) return rc;
+  } else {
+    SopParams q = sop_base(op);
+    q.in = zeta; q.out1 = op->work[4][prec]; q.opa = SOP_G5R; q.opb = SOP_LUDAG; q.out2 = ae;
+    if ((rc = run_sop(op, prec, q, st))) return rc;
+  }
+  HopParams p3 = hop_base(op, prec, 1, EPI_K3);
+  p3.in = ae; p3.out1 = ao;
+  return run_hop(op, prec, p3, st);
+}
+
+static ForceParams force_base(const b200_dwf_t* op, double* force, int ieo) {
+  ForceParams f;
+  memset(&f, 0, sizeof(f));
+  f.force = force;
+  f.coef = 0.5;
+  f.beta = 0.0;
+  f.ieo = ieo;
+  f.vh = op->g.vh; f.nx2 = op->g.nx2; f.ny = op->g.ny; f.nz = op->g.nz; f.nt = op->g.nt;
+  f.ls = op->g.ls;
+  for (int mu = 0; mu < 4; ++mu) f.bc[mu] = op->bc[mu];
+  return f;
+}
+
+int b200_dwf_force_udiv1(b200_dwf_t* op, const char* mode, double* force, const void* a,
+                         const void* b, void* stream) {
+  if (!op || !mode || !force || !a || !b) return fail(B200_EINVAL, "invalid argument");
+  if (misaligned(a) || misaligned(b)) return fail(B200_EINVAL, "field pointers must be 16-byte aligned");
+  if (op->k.alpha != 1.0)
+    return fail(B200_EINVAL, "force with parameter_alpha != 1 is not available (as in the reference)");
+  const std::string m = mode;
+  if (m != "H" && m != "Hdag") return fail(B200_EINVAL, "%s: unknown mode %s", "Force_F_Domainwall_eo", mode);
+  cudaStream_t st = (cudaStream_t)stream;
+  const bool hdag = (m == "Hdag");
+  const void* eta = hdag ? a : b;     // reference argument order
+  const void* zeta = hdag ? b : a;
+  int rc;
+  if ((rc = force_fields(op, eta, zeta, false, st))) return rc;
+  void* ye = op->work[0][PREC_F64];
+  void* yo = op->work[1][PREC_F64];
+  void* ae = op->work[2][PREC_F64];
+  void* ao = op->work[3][PREC_F64];
+  ForceParams fe = force_base(op, force, 0), fo = force_base(op, force, 1);
+  if (!hdag) { fe.y1 = yo; fe.z1 = ae; fo.y1 = ye; fo.z1 = ao; }
+  else { fe.y2 = ao; fe.z2 = ye; fo.y2 = ae; fo.z2 = yo; }
+  B200_CHECK_CUDA(launch_force(fe, st));
+  B200_CHECK_CUDA(launch_force(fo, st));
+  return 0;
+}
+
+int b200_dwf_force_udiv(b200_dwf_t* op, double* force, const void* eta, void* stream) {
+  if (!op || !force || !eta) return fail(B200_EINVAL, "invalid argument");
+  if (misaligned(eta)) return fail(B200_EINVAL, "field pointers must be 16-byte aligned");
+  if (op->k.alpha != 1.0)
+    return fail(B200_EINVAL, "force with parameter_alpha != 1 is not available (as in the reference)");
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc;
+  if ((rc = force_fields(op, eta, nullptr, true, st))) return rc;
+  void* ye = op->work[0][PREC_F64];
+  void* yo = op->work[1][PREC_F64];
+  void* ae = op->work[2][PREC_F64];
+  void* ao = op->work[3][PREC_F64];
+  ForceParams fe = force_base(op, force, 0), fo = force_base(op, force, 1);
+  fe.y1 = yo; fe.z1 = ae; fe.y2 = ao; fe.z2 = ye;
+  fo.y1 = ye; fo.z1 = ao; fo.y2 = ae; fo.z2 = yo;
+  B200_CHECK_CUDA(launch_force(fe, st));
+  B200_CHECK_CUDA(launch_force(fo, st));
+  return 0;
+}
+
 int b200_tuning_table(char* buf, size_t n) {
   if (!buf || n == 0) return fail(B200_EINVAL, "invalid buffer");
   std::string out;

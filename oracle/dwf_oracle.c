@@ -676,3 +676,164 @@ int oracle_shiftcg(oracle_dwf *op, double *x, const double *sigma, int nshift,
   free(r); free(s); free(tmp); free(p); free(zeta1); free(zeta2); free(csh2); free(pp);
   return conv < 0 ? 1 : 0;
 }
+
+
+/* ---------------- fermion force ---------------- */
+
+/* Forward-mu part of the Wilson hop, output parity ieo:
+ * out(x) = ph * (1 - g_mu) U_mu(x) in(x+mu)   (Fopr_Wilson_eo::mult_up,
+ * src/lib/Fopr/Imp/fopr_Wilson_eo_impl.cpp:656-677) */
+static void hop_up(const oracle_dwf *op, double *out, const double *in, int ieo, int mu)
+{
+  const int *L = op->L;
+  const int Ls = op->Ls;
+  for (int site = 0; site < op->Vh; ++site) {
+    int ix2 = site % op->Nx2;
+    int iyzt = site / op->Nx2;
+    int y = iyzt % L[1];
+    int z = (iyzt / L[1]) % L[2];
+    int t = iyzt / (L[1] * L[2]);
+    int keo = (ieo + y + z + t) % 2;
+    int nc[4] = {2 * ix2 + keo, y, z, t};
+    double ph = 1.0;
+    if (nc[mu] == L[mu] - 1) { nc[mu] = 0; ph = op->bc[mu]; } else nc[mu] += 1;
+    int nb = nc[0] / 2 + op->Nx2 * (nc[1] + L[1] * (nc[2] + L[2] * nc[3]));
+    const double *u = op->ueo + (size_t)NDF * (site + (size_t)op->Vh * (ieo + 2 * mu));
+    for (int s = 0; s < Ls; ++s) {
+      const double *w = cfld(op, in, nb, s);
+      double tmp[NIN], gt[NIN];
+      for (int sp = 0; sp < NSP; ++sp) su3_mult(tmp + 6 * sp, u, w + 6 * sp);
+      gamma_mult(gt, tmp, mu);
+      double *o = fld(op, out, site, s);
+      for (int k = 0; k < NIN; ++k) o[k] = ph * (tmp[k] - gt[k]);
+    }
+  }
+}
+
+/* AFopr_Domainwall_eo::mult_up (afopr_Domainwall_eo-tmpl.h:1262-1316):
+ * the forward-mu part of D_eo, -1/2 hop_up(b w + c V(w)) (alpha = 1) */
+static void mult_up(oracle_dwf *op, double *out, const double *w, int ieo, int mu)
+{
+  size_t n = (size_t)NIN * op->Vh * op->Ls;
+  m5_apply(op, op->w4, w, op->b, op->c);
+  hop_up(op, out, op->w4, ieo, mu);
+  for (size_t i = 0; i < n; ++i) out[i] *= -0.5;
+}
+
+/* AFopr_Domainwall_eo::mult_up_dag (afopr_Domainwall_eo-tmpl.h:1376-1420):
+ * M5^+ applied to -1/2 g5 hop_up(g5 w) */
+static void mult_up_dag(oracle_dwf *op, double *out, const double *w, int ieo, int mu)
+{
+  size_t n = (size_t)NIN * op->Vh * op->Ls;
+  g5_field(op, out, w);
+  hop_up(op, op->w4, out, ieo, mu);
+  g5_field(op, out, op->w4);
+  for (size_t i = 0; i < n; ++i) out[i] *= -0.5;
+  memcpy(op->w4, out, n * sizeof(double));
+  m5_apply_dag(op, out, op->w4, op->b, op->c);
+}
+
+/* force_eo[mu](x) += sum_s sum_spin (U^+ work)(x)_c1 conj(v(x)_c2)
+ * (mult_Field_Gd + tensorProd_Field_F, src/lib/Force/Fermion/Imp/tensorProd.cpp:39-98),
+ * written into the lexical force for the sites of parity ieo */
+static void accumulate_force(const oracle_dwf *op, double *force_lex, const double *v,
+                             const double *work, int ieo, int mu)
+{
+  const int *L = op->L;
+  for (int site = 0; site < op->Vh; ++site) {
+    int ix2 = site % op->Nx2;
+    int iyzt = site / op->Nx2;
+    int y = iyzt % L[1];
+    int z = (iyzt / L[1]) % L[2];
+    int t = iyzt / (L[1] * L[2]);
+    int x = 2 * ix2 + (ieo + y + z + t) % 2;
+    int lex = x + L[0] * (y + L[1] * (z + L[2] * t));
+    const double *u = op->ueo + (size_t)NDF * (site + (size_t)op->Vh * (ieo + 2 * mu));
+    double *F = force_lex + (size_t)NDF * (lex + (size_t)op->V * mu);
+    for (int s = 0; s < op->Ls; ++s) {
+      const double *wk = cfld(op, work, site, s);
+      const double *vv = cfld(op, v, site, s);
+      double w2[NIN];
+      for (int sp = 0; sp < NSP; ++sp) su3_dag_mult(w2 + 6 * sp, u, wk + 6 * sp);
+      for (int c1 = 0; c1 < NC; ++c1)
+        for (int c2 = 0; c2 < NC; ++c2)
+          for (int sp = 0; sp < NSP; ++sp) {
+            double ar = w2[2 * (c1 + 3 * sp)], ai = w2[2 * (c1 + 3 * sp) + 1];
+            double br = vv[2 * (c2 + 3 * sp)], bi = vv[2 * (c2 + 3 * sp) + 1];
+            F[2 * (c2 + 3 * c1)] += ar * br + ai * bi;
+            F[2 * (c2 + 3 * c1) + 1] += ai * br - ar * bi;
+          }
+    }
+  }
+}
+
+int oracle_dwf_force_udiv1(oracle_dwf *op, const char *mode, double *force_lex,
+                           const double *a, const double *b)
+{
+  size_t n = (size_t)NIN * op->Vh * op->Ls;
+  size_t nf = (size_t)NDF * op->V * 4;
+  double *ue = (double *)malloc(n * sizeof(double));
+  double *uo = (double *)malloc(n * sizeof(double));
+  double *ve = (double *)malloc(n * sizeof(double));
+  double *vo = (double *)malloc(n * sizeof(double));
+  double *work = (double *)malloc(n * sizeof(double));
+  double *work2 = (double *)malloc(n * sizeof(double));
+  int hdag;
+  if (!strcmp(mode, "H")) hdag = 0;
+  else if (!strcmp(mode, "Hdag")) hdag = 1;
+  else { free(ue); free(uo); free(ve); free(vo); free(work); free(work2); return -1; }
+  memset(force_lex, 0, nf * sizeof(double));
+  if (!hdag) {
+    /* H: a = zeta_e, b = eta_e  (force_F_Domainwall_eo.cpp:190-247) */
+    memcpy(ue, b, n * sizeof(double));
+    D_eo(op, work, ue, 1);
+    LU_inv(op, uo, work);
+    gm5R(op, work, a);
+    LUdag_inv(op, ve, work);
+    Ddag_eo(op, work, ve, 1);
+    LUdag_inv(op, vo, work);
+    for (int mu = 0; mu < 4; ++mu) {
+      mult_up(op, work2, uo, 0, mu);
+      accumulate_force(op, force_lex, ve, work2, 0, mu);
+    }
+    for (int mu = 0; mu < 4; ++mu) {
+      mult_up(op, work2, ue, 1, mu);
+      accumulate_force(op, force_lex, vo, work2, 1, mu);
+    }
+  } else {
+    /* Hdag: a = eta_e, b = zeta_e  (force_F_Domainwall_eo.cpp:251-318) */
+    memcpy(ve, a, n * sizeof(double));
+    D_eo(op, work, ve, 1);
+    LU_inv(op, vo, work);
+    gm5R(op, work, b);
+    LUdag_inv(op, ue, work);
+    Ddag_eo(op, work, ue, 1);
+    LUdag_inv(op, uo, work);
+    for (int mu = 0; mu < 4; ++mu) {
+      mult_up_dag(op, work2, uo, 0, mu);
+      accumulate_force(op, force_lex, ve, work2, 0, mu);
+    }
+    for (int mu = 0; mu < 4; ++mu) {
+      mult_up_dag(op, work2, ue, 1, mu);
+      accumulate_force(op, force_lex, vo, work2, 1, mu);
+    }
+  }
+  for (size_t i = 0; i < nf; ++i) force_lex[i] = -force_lex[i];
+  free(ue); free(uo); free(ve); free(vo); free(work); free(work2);
+  return 0;
+}
+
+int oracle_dwf_force_udiv(oracle_dwf *op, double *force_lex, const double *eta)
+{
+  size_t n = (size_t)NIN * op->Vh * op->Ls;
+  size_t nf = (size_t)NDF * op->V * 4;
+  double *zeta = (double *)malloc(n * sizeof(double));
+  double *f2 = (double *)malloc(nf * sizeof(double));
+  oracle_dwf_mult(op, "H", 0, zeta, eta);
+  oracle_dwf_force_udiv1(op, "H", force_lex, zeta, eta);
+  oracle_dwf_force_udiv1(op, "Hdag", f2, eta, zeta);
+  for (size_t i = 0; i < nf; ++i) force_lex[i] += f2[i];
+  free(zeta);
+  free(f2);
+  return 0;
+}

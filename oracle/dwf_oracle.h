@@ -46,6 +46,16 @@ int oracle_shiftcg(oracle_dwf *op, double *x, const double *sigma, int nshift,
                    const double *b, double tol2, int maxiter, int *nconv,
                    double *diff);
 
+/* Fermion force of Force_F_Domainwall_eo (reference src/lib/Force/Fermion/
+ * force_F_Domainwall_eo.cpp:150-327): mode "H" computes force_udiv1_H(force,
+ * zeta, eta), mode "Hdag" force_udiv1_Hdag(force, zeta, eta) with the
+ * reference's argument order (eta first for Hdag: pass eta as `zeta_or_eta`).
+ * force_lex: Field_G(Nvol, 4) layout, 18 reals per (site, mu).  alpha must be 1. */
+int oracle_dwf_force_udiv1(oracle_dwf *op, const char *mode, double *force_lex,
+                           const double *a, const double *b);
+/* force_udiv(force, eta) = force_udiv1_H(H eta, eta) + force_udiv1_Hdag(eta, H eta). */
+int oracle_dwf_force_udiv(oracle_dwf *op, double *force_lex, const double *eta);
+
 /* Number of reals in one 5D half-lattice spinor. */
 long oracle_dwf_field_size(const oracle_dwf *op);
 

@@ -34,6 +34,10 @@ def _lib():
         lib.oracle_shiftcg.argtypes = [ctypes.c_void_p, dp, dp, ctypes.c_int, dp,
                                        ctypes.c_double, ctypes.c_int, ip, dp]
         lib.oracle_shiftcg.restype = ctypes.c_int
+        lib.oracle_dwf_force_udiv1.argtypes = [ctypes.c_void_p, ctypes.c_char_p, dp, dp, dp]
+        lib.oracle_dwf_force_udiv1.restype = ctypes.c_int
+        lib.oracle_dwf_force_udiv.argtypes = [ctypes.c_void_p, dp, dp]
+        lib.oracle_dwf_force_udiv.restype = ctypes.c_int
         _LIB = lib
     return _LIB
 
@@ -83,6 +87,23 @@ class OracleDWF:
         rc = _lib().oracle_cg(self._h, _dp(x), _dp(b), tol2, maxiter,
                               ctypes.byref(nconv), ctypes.byref(diff))
         return x, nconv.value, diff.value, rc
+
+    def force_udiv1(self, mode, a, b):
+        """Force_F_Domainwall_eo::force_udiv1 in mode H (a=zeta, b=eta) or
+        Hdag (a=eta, b=zeta); lexical Field_G(Nvol, 4) result."""
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        f = np.empty(18 * int(np.prod(self.lattice)) * 4)
+        rc = _lib().oracle_dwf_force_udiv1(self._h, mode.encode(), _dp(f), _dp(a), _dp(b))
+        if rc != 0:
+            raise ValueError(mode)
+        return f
+
+    def force_udiv(self, eta):
+        eta = np.ascontiguousarray(eta, dtype=np.float64)
+        f = np.empty(18 * int(np.prod(self.lattice)) * 4)
+        _lib().oracle_dwf_force_udiv(self._h, _dp(f), _dp(eta))
+        return f
 
     def shiftcg(self, b, sigma, tol2, maxiter=10000):
         b = np.ascontiguousarray(b, dtype=np.float64)

@@ -26,6 +26,17 @@
 //             shiftsolver_CG.cpp), writes out_dir/shift_<i>.bin.
 //   time    : times `reps` applications of mode(s) inside an OpenMP parallel
 //             region, prints "mode seconds_per_call".
+//   force   : Force_F_Domainwall_eo (src/lib/Force/Fermion/
+//             force_F_Domainwall_eo.cpp:150-327) with eta = src.bin and
+//             zeta = in_dir/src2.bin: writes force_udiv1 in modes "H" and
+//             "Hdag" (force_H.bin, force_Hdag.bin) and force_udiv(eta)
+//             (force_udiv.bin), lexical Field_G(Nvol, 4) layout.
+//   smear   : stout smearing Smear_APE + Projection_Stout_SU3 under
+//             Director_Smear (rho, nsmear): writes smear_<i>.bin for the
+//             levels i = 1..nsmear, and the Jacobian chain of ForceSmear_APE
+//             (src/lib/Smear/forceSmear_APE.cpp, projection_Stout_SU3.cpp
+//             force_recursive) applied to in_dir/sigma.bin from the top
+//             level down to the thin links: jacobian.bin.
 
 #include <cstdio>
 #include <cstdlib>
@@ -47,6 +58,11 @@
 #include "Fopr/fopr_Domainwall_eo.h"
 #include "Solver/solver_CG.h"
 #include "Solver/shiftsolver_CG.h"
+#include "Force/Fermion/force_F_Domainwall_eo.h"
+#include "Smear/projection_Stout_SU3.h"
+#include "Smear/smear_APE.h"
+#include "Smear/forceSmear_APE.h"
+#include "Smear/director_Smear.h"
 #include "IO/bridgeIO.h"
 
 using Bridge::vout;
@@ -218,6 +234,45 @@ int main(int argc, char **argv)
     FILE *f = fopen((out_dir + "/shift_info.txt").c_str(), "w");
     fprintf(f, "nconv %d\ndiff %.17e\n", nconv, diff);
     fclose(f);
+  } else if (cmd == "force") {
+    Field src2(24, Nvol2, Ls);
+    read_bin(in_dir + "/src2.bin", src2.ptr(0), nsp);
+    Force_F_Domainwall_eo force(pf);
+    force.set_config(&U);
+    Field_G F(Nvol, 4);
+    const size_t nf = size_t(18) * Nvol * 4;
+    force.set_mode("H");
+    force.force_udiv1(F, src2, src);
+    write_bin(out_dir + "/force_H.bin", F.ptr(0), nf);
+    force.set_mode("Hdag");
+    force.force_udiv1(F, src, src2);
+    write_bin(out_dir + "/force_Hdag.bin", F.ptr(0), nf);
+    force.force_udiv(F, src);
+    write_bin(out_dir + "/force_udiv.bin", F.ptr(0), nf);
+  } else if (cmd == "smear") {
+    const double rho = getd(kv, "rho", 0.1);
+    const int nsmear = geti(kv, "nsmear", 2);
+    Projection_Stout_SU3 proj;
+    Smear_APE smear(&proj);
+    smear.set_parameters(rho);
+    Director_Smear dr(&smear);
+    dr.set_parameters(nsmear);
+    dr.set_config(&U);
+    const size_t ng = size_t(18) * Nvol * 4;
+    for (int i = 1; i <= nsmear; ++i) {
+      char name[64];
+      snprintf(name, sizeof(name), "/smear_%d.bin", i);
+      write_bin(out_dir + name, dr.get_config(i)->ptr(0), ng);
+    }
+    ForceSmear_APE fsmear(&proj);
+    fsmear.set_parameters(rho);
+    Field_G sigma(Nvol, 4), sigma_p(Nvol, 4);
+    read_bin(in_dir + "/sigma.bin", sigma_p.ptr(0), ng);
+    for (int i = nsmear - 1; i >= 0; --i) {
+      fsmear.force_udiv(sigma, sigma_p, *dr.get_config(i));
+      if (i > 0) copy(sigma_p, sigma);
+    }
+    write_bin(out_dir + "/jacobian.bin", sigma.ptr(0), ng);
   } else if (cmd == "time") {
     // "Deo"/"Doe"/... use mult(v, w, mode); "dag_<mode>" uses mult_dag;
     // composite modes (D, DdagD, ...) use set_mode + mult.

@@ -40,6 +40,12 @@ CASES = {
                                 "dag_Dee_inv", "DdagD", "H"]),
 }
 SOLVE = dict(case="shamir", tol=1e-24, sigma=[0.05, 0.2, 1.0], maxiter=5000)
+# stout smearing (rho, 2 levels) and its Jacobian chain on a random force
+SMEAR = dict(lattice=[4, 4, 4, 4], Ls=4, mq=0.01, M0=1.8, b=1.0, c=0.0, alpha=1.0,
+             bc=[1, 1, 1, -1], gauge=("near", 71), src=72, rho=0.1, nsmear=2, sigma=73)
+# force: Moebius (alpha must be 1 for Force_F_Domainwall_eo), antiperiodic t
+FORCE = dict(lattice=[4, 4, 4, 4], Ls=4, mq=0.02, M0=1.4, b=1.5, c=0.5, alpha=1.0,
+             bc=[1, 1, 1, -1], gauge=("near", 31), src=32, src2=33)
 
 
 def write_params(path, case, extra=None):
@@ -93,6 +99,25 @@ def main():
               for i in range(len(SOLVE["sigma"]))]
         sinfo = open(os.path.join(tmp, "shift_info.txt")).read()
     meta = dict(SOLVE, cg_info=info, shift_info=sinfo)
+    with tempfile.TemporaryDirectory() as tmp:
+        synth.spinor_field(FORCE["lattice"], FORCE["Ls"], FORCE["src2"]).tofile(
+            os.path.join(tmp, "src2.bin"))
+        run("force", FORCE, {}, tmp)
+        forces = {k: np.fromfile(os.path.join(tmp, "force_%s.bin" % k))
+                  for k in ("H", "Hdag", "udiv")}
+    np.savez_compressed(os.path.join(HERE, "force_mobius.npz"), meta=json.dumps(FORCE),
+                        **forces)
+    print("wrote force_mobius.npz")
+    with tempfile.TemporaryDirectory() as tmp:
+        rng = np.random.default_rng(SMEAR["sigma"])
+        rng.standard_normal(18 * 4 * int(np.prod(SMEAR["lattice"]))).tofile(
+            os.path.join(tmp, "sigma.bin"))
+        run("smear", SMEAR, {"rho": SMEAR["rho"], "nsmear": SMEAR["nsmear"]}, tmp)
+        out = {"smear_%d" % i: np.fromfile(os.path.join(tmp, "smear_%d.bin" % i))
+               for i in range(1, SMEAR["nsmear"] + 1)}
+        out["jacobian"] = np.fromfile(os.path.join(tmp, "jacobian.bin"))
+    np.savez_compressed(os.path.join(HERE, "smear_stout.npz"), meta=json.dumps(SMEAR), **out)
+    print("wrote smear_stout.npz")
     np.savez_compressed(os.path.join(HERE, "solve_shamir.npz"),
                         meta=json.dumps(meta), cg_x=x,
                         **{"shift_%d" % i: v for i, v in enumerate(xs)})

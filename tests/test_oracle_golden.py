@@ -57,3 +57,18 @@ def test_plaquette_of_unit_and_random_links():
     assert abs(synth.plaquette(synth.gauge_field(lat, 0, "unit"), lat) - 1.0) < 1e-15
     p = synth.plaquette(synth.gauge_field(lat, 1, "near", eps=0.05), lat)
     assert 0.9 < p < 1.0
+
+
+def test_force_matches_reference():
+    z = np.load(os.path.join(GOLDEN, "force_mobius.npz"))
+    m = json.loads(str(z["meta"]))
+    u = synth.gauge_field(m["lattice"], m["gauge"][1], m["gauge"][0])
+    eta = synth.spinor_field(m["lattice"], m["Ls"], m["src"])
+    zeta = synth.spinor_field(m["lattice"], m["Ls"], m["src2"])
+    op = OracleDWF(m["lattice"], m["Ls"], m["mq"], m["M0"], m["b"], m["c"], m["alpha"], m["bc"])
+    op.set_links(u)
+    for mode, a, b, key in (("H", zeta, eta, "H"), ("Hdag", eta, zeta, "Hdag")):
+        f = op.force_udiv1(mode, a, b)
+        assert np.linalg.norm(f - z[key]) / np.linalg.norm(z[key]) < 1e-14
+    f = op.force_udiv(eta)
+    assert np.linalg.norm(f - z["udiv"]) / np.linalg.norm(z["udiv"]) < 1e-14
