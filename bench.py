@@ -161,10 +161,11 @@ def run_reference_cpu(lattice, ls, steps, warmup, budget_s=60.0, threads=None):
         u.tofile(os.path.join(d, "gauge.bin"))
         b.tofile(os.path.join(d, "src.bin"))
 
-        def timed(reps):
+        def timed(reps, warm):
             with open(os.path.join(d, "params.txt"), "w") as f:
-                f.write("lattice %s\nLs %d\nmq %r\nM0 %r\nthreads %d\nreps %d\nmodes Deo dag_Deo\n"
-                        % (" ".join(map(str, lattice)), ls, MQ, M0, threads, reps))
+                f.write("lattice %s\nLs %d\nmq %r\nM0 %r\nthreads %d\nreps %d\nwarmup %d\n"
+                        "modes Deo dag_Deo\n"
+                        % (" ".join(map(str, lattice)), ls, MQ, M0, threads, reps, warm))
             r = subprocess.run([REF_HARNESS, "time", os.path.join(d, "params.txt"), d, d],
                                capture_output=True, text=True, check=True)
             t = {}
@@ -174,9 +175,9 @@ def run_reference_cpu(lattice, ls, steps, warmup, budget_s=60.0, threads=None):
                     t[p[0]] = float(p[1])
             return t["Deo"] + t["dag_Deo"]
 
-        probe = timed(1)
+        probe = timed(1, 1)
         reps = int(max(1, min(steps, budget_s / max(probe, 1e-6))))
-        t_step = timed(reps)
+        t_step = timed(reps, max(1, warmup))
     gbs = 2 * BYTES_PER_HALF_SITE * vh / t_step / 1e9
     return gbs, t_step, reps, threads
 
@@ -191,7 +192,7 @@ def reference_arm(args, rank, world):
         return
     line = {
         "impl": "reference", "metric": METRIC, "value": gbs, "unit": "GB/s", "n_gpus": args.gpus,
-        "steps": reps, "warmup": 1, "ms_per_step": t_step * 1e3, "higher_is_better": True,
+        "steps": reps, "warmup": max(1, args.warmup), "ms_per_step": t_step * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "lattice": args.lattice, "Ls": LS, "M0": M0, "mq": MQ,
                    "links": "near-unit exp(i*0.3*H) + 2 stout rho=0.1", "parallelism": "replicas"},

@@ -197,6 +197,52 @@ int b200_smear_jacobian(b200_smear_t *sm, double *sigma, void *stream);
  * force <- -2 * (traceless anti-Hermitian part of U force), per link. */
 int b200_force_mult_generator(const int lattice[4], double *force, const double *u, void *stream);
 
+/* ---------------------------------------------------------------- learned preconditioner
+ * No reference counterpart.  A 3-layer linear gauge-covariant 5D convolution
+ * network N ~ (DdagD)^-1 for the even-parity system: channels 4 -> hidden ->
+ * 4 per color (input channels = the 4 spins), 11 paths per layer (identity,
+ * s+1, s-1 with open ends, the 8 link-transported 4D hops with the operator's
+ * boundary phases), complex weights rounded to BF16, FP32 accumulation.  It
+ * takes the place of an APrecond<AFIELD> (src/lib_alt/Solver/aprecond.h:
+ * 28-47) in a flexible solver.  Fields r, z, e: device FP32 fields of the
+ * operator (B200_F32 layout).  Weights: 2*b200_lp_nparams() floats, complex
+ * interleaved, layer-major [layer][path][out][in]. */
+typedef struct b200_lp b200_lp_t;
+int b200_lp_create(b200_lp_t **lp, b200_dwf_t *op, int hidden, unsigned long long seed,
+                   double init_noise);
+int b200_lp_destroy(b200_lp_t *lp);
+int b200_lp_nparams(const b200_lp_t *lp);
+/* FP32 master weights (set resets the optimiser state); get with deployed != 0
+ * returns the BF16-rounded weights the kernels use. */
+int b200_lp_set_weights(b200_lp_t *lp, const float *w, int nfloat);
+int b200_lp_get_weights(b200_lp_t *lp, float *w, int nfloat, int deployed);
+/* z = N(r). */
+int b200_lp_apply(b200_lp_t *lp, void *z, const void *r, void *stream);
+/* loss = |N(r) - e|^2 / |e|^2 and its gradient dL/dRe(w) + i dL/dIm(w),
+ * kept on the device (b200_lp_get_grad copies it out).  Synchronous. */
+int b200_lp_loss_grad(b200_lp_t *lp, const void *r, const void *e, double *loss, void *stream);
+int b200_lp_get_grad(b200_lp_t *lp, float *g, int nfloat);
+/* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on the master weights. */
+int b200_lp_adam_step(b200_lp_t *lp, double lr, void *stream);
+/* `epochs` passes of loss_grad + adam_step over the pairs in a seeded
+ * shuffled order; mean loss of the first and the last epoch. */
+int b200_lp_train(b200_lp_t *lp, int npairs, const void *const *r, const void *const *e,
+                  int epochs, double lr, unsigned long long seed, double *loss_first,
+                  double *loss_last, void *stream);
+/* Plain CG (as b200_cg_solve, without the true residual) copying x after
+ * iteration iters[j] into snaps[j] (fields of precision prec). */
+int b200_cg_snapshots(b200_dwf_t *op, int prec, void *x, const void *b, int maxiter,
+                      double tol2, int nsnap, const int *iters, void *const *snaps,
+                      int *nconv, void *stream);
+/* Flexible CG on DdagD preconditioned by lp: FP64 x, b; the new search
+ * direction is A-orthogonalised against the last mtrunc (1..8) directions.
+ * The FP64 true residual judges the result: if it misses tol2, plain CG on
+ * the residual equation finishes from x (*nconv_fallback iterations, at most
+ * 100000, independent of maxiter).  diff = sqrt(|DdagD x - b|^2 / |b|^2). */
+int b200_fcg_solve(b200_dwf_t *op, b200_lp_t *lp, void *x, const void *b, int maxiter,
+                   double tol2, int mtrunc, int *nconv, int *nconv_fallback, double *diff,
+                   void *stream);
+
 /* ---------------------------------------------------------------- tuning
  * Text table of the autotuner's choices (one line per geometry, precision and
  * kernel epilogue: chosen occupancy variant and its time per launch).  The

@@ -78,6 +78,23 @@ def lib():
     L.b200_tuning_table.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
     L.b200_cg_solve.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_double,
                                 ip, dp, vp]
+    fp = ctypes.POINTER(ctypes.c_float)
+    L.b200_lp_create.argtypes = [ctypes.POINTER(vp), vp, ctypes.c_int, ctypes.c_ulonglong,
+                                 ctypes.c_double]
+    L.b200_lp_destroy.argtypes = [vp]
+    L.b200_lp_nparams.argtypes = [vp]
+    L.b200_lp_set_weights.argtypes = [vp, fp, ctypes.c_int]
+    L.b200_lp_get_weights.argtypes = [vp, fp, ctypes.c_int, ctypes.c_int]
+    L.b200_lp_apply.argtypes = [vp, vp, vp, vp]
+    L.b200_lp_loss_grad.argtypes = [vp, vp, vp, dp, vp]
+    L.b200_lp_get_grad.argtypes = [vp, fp, ctypes.c_int]
+    L.b200_lp_adam_step.argtypes = [vp, ctypes.c_double, vp]
+    L.b200_lp_train.argtypes = [vp, ctypes.c_int, ctypes.POINTER(vp), ctypes.POINTER(vp),
+                                ctypes.c_int, ctypes.c_double, ctypes.c_ulonglong, dp, dp, vp]
+    L.b200_cg_snapshots.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_double,
+                                    ctypes.c_int, ip, ctypes.POINTER(vp), ip, vp]
+    L.b200_fcg_solve.argtypes = [vp, vp, vp, vp, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                 ip, ip, dp, vp]
     _lib = L
     return L
 
@@ -246,6 +263,114 @@ class DomainWall:
         if rc not in (0, -4):
             check(rc)
         return n.value, d.value, rc
+
+    def cg_snapshots(self, x, b, tol2, iters, snaps, maxiter=10000):
+        """Plain CG copying x after each iteration in `iters` into `snaps`."""
+        it = (ctypes.c_int * len(iters))(*iters)
+        arr = (ctypes.c_void_p * len(snaps))(*[f.buf.data_ptr() for f in snaps])
+        n = ctypes.c_int()
+        rc = lib().b200_cg_snapshots(self.handle, b.prec, x.ptr, b.ptr, maxiter, tol2, len(iters),
+                                     it, arr, ctypes.byref(n), None)
+        if rc not in (0, -4):
+            check(rc)
+        return n.value, rc
+
+    def fcg(self, x, b, lp, tol2, maxiter=10000, mtrunc=1):
+        """Flexible CG preconditioned by a LearnedPrecond; returns
+        (iterations, fallback CG iterations, true relative residual, rc)."""
+        n = ctypes.c_int()
+        nf = ctypes.c_int()
+        d = ctypes.c_double()
+        rc = lib().b200_fcg_solve(self.handle, lp.handle, x.ptr, b.ptr, maxiter, tol2, mtrunc,
+                                  ctypes.byref(n), ctypes.byref(nf), ctypes.byref(d), None)
+        if rc not in (0, -4):
+            check(rc)
+        return n.value, nf.value, d.value, rc
+
+
+def _fp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+class LearnedPrecond:
+    """Gauge-covariant 3-layer convolution network N ~ (DdagD)^-1 of a
+    DomainWall operator (the preconditioner slot of APrecond<AFIELD>,
+    src/lib_alt/Solver/aprecond.h).  Fields are FP32 `Field`s of the operator;
+    weights are complex numpy arrays of b200_lp_nparams() entries laid out
+    [layer][path][out][in]."""
+
+    def __init__(self, op, hidden=8, seed=1, init_noise=0.01):
+        self.op = op
+        self.hidden = hidden
+        h = ctypes.c_void_p()
+        check(lib().b200_lp_create(ctypes.byref(h), op.handle, hidden, seed, init_noise))
+        self.handle = h
+        self.nparams = lib().b200_lp_nparams(h)
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and _lib is not None:
+            _lib.b200_lp_destroy(h)
+            self.handle = None
+
+    def weights(self, deployed=True):
+        w = np.empty(2 * self.nparams, np.float32)
+        check(lib().b200_lp_get_weights(self.handle, _fp(w), len(w), 1 if deployed else 0))
+        return w.view(np.complex64).astype(np.complex128)
+
+    def set_weights(self, w):
+        a = np.ascontiguousarray(np.asarray(w, np.complex64)).view(np.float32)
+        check(lib().b200_lp_set_weights(self.handle, _fp(a), len(a)))
+
+    def apply(self, z, r):
+        check(lib().b200_lp_apply(self.handle, z.ptr, r.ptr, None))
+
+    def loss_grad(self, r, e):
+        loss = ctypes.c_double()
+        check(lib().b200_lp_loss_grad(self.handle, r.ptr, e.ptr, ctypes.byref(loss), None))
+        return loss.value
+
+    def grad(self):
+        g = np.empty(2 * self.nparams, np.float32)
+        check(lib().b200_lp_get_grad(self.handle, _fp(g), len(g)))
+        return g.view(np.complex64).astype(np.complex128)
+
+    def adam_step(self, lr):
+        check(lib().b200_lp_adam_step(self.handle, lr, None))
+
+    def train(self, rs, es, epochs, lr, seed=7):
+        ra = (ctypes.c_void_p * len(rs))(*[f.buf.data_ptr() for f in rs])
+        ea = (ctypes.c_void_p * len(es))(*[f.buf.data_ptr() for f in es])
+        l0 = ctypes.c_double()
+        l1 = ctypes.c_double()
+        check(lib().b200_lp_train(self.handle, len(rs), ra, ea, epochs, lr, seed, ctypes.byref(l0),
+                                  ctypes.byref(l1), None))
+        return l0.value, l1.value
+
+
+def cg_training_pairs(op, b, iters, tol2_star=1e-24, maxiter=100000):
+    """(residual, error) pairs of plain CG on DdagD x = b for the learned
+    preconditioner: the iterate x_k after each iteration in `iters`, the error
+    e_k = x* - x_k against a tightly converged x*, and r_k = DdagD e_k (so each
+    pair satisfies DdagD e = r exactly).  Returns FP32 fields (rs, es)."""
+    xs = Field(op, F64)
+    n, _, _ = op.cg(xs, b, tol2_star, maxiter)
+    iters = [k for k in iters if k <= n]
+    snaps = [Field(op, F64) for _ in iters]
+    x = Field(op, F64)
+    op.cg_snapshots(x, b, tol2_star, iters, snaps, maxiter)
+    rs, es = [], []
+    tmp = Field(op, F64)
+    for sf in snaps:
+        op.axpby(sf, 1.0, xs, -1.0)        # e = x* - x_k
+        op.mult(tmp, sf, "DdagD")          # r = DdagD e
+        r32 = Field(op, F32)
+        e32 = Field(op, F32)
+        op.copy_convert(r32, tmp)
+        op.copy_convert(e32, sf)
+        rs.append(r32)
+        es.append(e32)
+    return rs, es
 
 
 class StoutSmear:

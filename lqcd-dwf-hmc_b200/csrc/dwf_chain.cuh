@@ -182,30 +182,62 @@ __device__ __forceinline__ void apply_f(const ChainCoef<R>& k, R* x) {
   else if (FK == F_G5R) chain_g5r<R, LS, CHI>(x);
 }
 
+// A warp's shared-memory tile holds, per (site g, slice s), the 24 reals of
+// one spinor in a row of TileStride<R>::v elements.  The padding (26 doubles,
+// 28 floats) makes both the per-thread 16-byte row accesses and the
+// per-unit column walks of tile_chiral free of bank conflicts.
+template <typename R> struct TileStride { static constexpr int v = 26; };
+template <> struct TileStride<float> { static constexpr int v = 28; };
+
+__device__ __forceinline__ void tile_put(double* row, const double* v) {
+#pragma unroll
+  for (int k = 0; k < 12; ++k) reinterpret_cast<double2*>(row)[k] = make_double2(v[2 * k], v[2 * k + 1]);
+}
+__device__ __forceinline__ void tile_put(float* row, const float* v) {
+#pragma unroll
+  for (int k = 0; k < 6; ++k)
+    reinterpret_cast<float4*>(row)[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+}
+__device__ __forceinline__ void tile_get(const double* row, double* v) {
+#pragma unroll
+  for (int k = 0; k < 12; ++k) {
+    const double2 c = reinterpret_cast<const double2*>(row)[k];
+    v[2 * k] = c.x; v[2 * k + 1] = c.y;
+  }
+}
+__device__ __forceinline__ void tile_get(const float* row, float* v) {
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    const float4 c = reinterpret_cast<const float4*>(row)[k];
+    v[4 * k] = c.x; v[4 * k + 1] = c.y; v[4 * k + 2] = c.z; v[4 * k + 3] = c.w;
+  }
+}
+
 // Run `op` on every unit (site g, color, ri, spin pair) of a warp's tile
-// [g][s][24]: gather the chirality columns, apply, scatter back in place.
+// [g][s][TileStride]: gather the chirality columns, apply, scatter back in place.
 template <typename R, int LS, int G, typename Op>
 __device__ __forceinline__ void tile_chiral(R* tile, int lane, Op op) {
+  constexpr int TS = TileStride<R>::v;
 #pragma unroll 1
   for (int u = lane; u < 12 * G; u += 32) {
     const int g = u / 12;
     const int r = u - 12 * g;
     const int pair = r / 6;
     const int cr = r - 6 * pair;
-    R* t = tile + g * LS * 24 + 6 * pair + cr;
+    R* t = tile + g * LS * TS + 6 * pair + cr;
     R xp[LS], xm[LS];
 #pragma unroll
     for (int s = 0; s < LS; ++s) {
-      const R a = t[s * 24];
-      const R b = t[s * 24 + 12];
+      const R a = t[s * TS];
+      const R b = t[s * TS + 12];
       xp[s] = a + b;
       xm[s] = a - b;
     }
     op(xp, xm);
 #pragma unroll
     for (int s = 0; s < LS; ++s) {
-      t[s * 24] = R(0.5) * (xp[s] + xm[s]);
-      t[s * 24 + 12] = R(0.5) * (xp[s] - xm[s]);
+      t[s * TS] = R(0.5) * (xp[s] + xm[s]);
+      t[s * TS + 12] = R(0.5) * (xp[s] - xm[s]);
     }
   }
 }

@@ -241,7 +241,7 @@ __device__ __forceinline__ void hop_epilogue(const HopParams& p, const ChainCoef
   } else {
     if (g < G) {
 #pragma unroll
-      for (int i = 0; i < 24; ++i) tile[(g * LS + s) * 24 + i] = acc[i];
+      tile_put(tile + (g * LS + s) * TileStride<R>::v, acc);
     }
     __syncwarp();
     tile_chiral<R, LS, G>(tile, lane, [&](R* xp, R* xm) {
@@ -251,7 +251,7 @@ __device__ __forceinline__ void hop_epilogue(const HopParams& p, const ChainCoef
     __syncwarp();
     if (g < G) {
 #pragma unroll
-      for (int i = 0; i < 24; ++i) o1[i] = tile[(g * LS + s) * 24 + i];
+      tile_get(tile + (g * LS + s) * TileStride<R>::v, o1);
     }
   }
 
@@ -291,7 +291,7 @@ __device__ __forceinline__ void hop_epilogue(const HopParams& p, const ChainCoef
     __syncwarp();
     if (g < G) {
 #pragma unroll
-      for (int i = 0; i < 24; ++i) tile[(g * LS + s) * 24 + i] = o1[i];
+      tile_put(tile + (g * LS + s) * TileStride<R>::v, o1);
     }
     __syncwarp();
     tile_chiral<R, LS, G>(tile, lane, [&](R* xp, R* xm) {
@@ -302,7 +302,7 @@ __device__ __forceinline__ void hop_epilogue(const HopParams& p, const ChainCoef
     if (active) {
       R o2[24];
 #pragma unroll
-      for (int i = 0; i < 24; ++i) o2[i] = tile[(g * LS + s) * 24 + i];
+      tile_get(tile + (g * LS + s) * TileStride<R>::v, o2);
       St::store(p.out2, vh, LS, site, s, o2);
     }
   }
@@ -337,8 +337,8 @@ dwf_hop_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename Sto
   constexpr int WARPS = 4;
   constexpr bool kTile = (EPI != EPI_HALF) || (FK != F_NONE);
 
-  extern __shared__ unsigned char smem_raw[];
-  R* tile_all = reinterpret_cast<R*>(smem_raw);        // WARPS * G * LS * 24
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R* tile_all = reinterpret_cast<R*>(smem_raw);        // WARPS * G * LS * TileStride
   __shared__ double red_warp[WARPS];
 
   const int tid = threadIdx.x;
@@ -417,7 +417,7 @@ dwf_hop_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename Sto
 #undef B200_HOP_DIR
   }
 
-  hop_epilogue<LS, P, EPI, FK>(p, k, acc, tile_all + (size_t)warp * G * LS * 24, red_warp, tid, lane,
+  hop_epilogue<LS, P, EPI, FK>(p, k, acc, tile_all + (size_t)warp * G * LS * TileStride<R>::v, red_warp, tid, lane,
                                warp, g, s, site, active);
 }
 
@@ -438,14 +438,15 @@ template <int LS, int P, int LF> struct TmaGeom {
   static constexpr int SLOT = COL + LNK;                       // one site, one direction
   template <int S> static constexpr int warp_bytes() {
     // stages, and the epilogue tile (reuses the stage area)
-    return (S * G * SLOT > G * LS * 24 * (int)sizeof(typename Store<P>::R))
+    using R = typename Store<P>::R;
+    return (S * G * SLOT > G * LS * TileStride<R>::v * (int)sizeof(R))
                ? S * G * SLOT
-               : G * LS * 24 * (int)sizeof(typename Store<P>::R);
+               : G * LS * TileStride<R>::v * (int)sizeof(R);
   }
 };
 
-template <int LS, int P, int LF, int EPI, int FK, int S>
-__global__ void __launch_bounds__(128)
+template <int LS, int P, int LF, int EPI, int FK, int S, int MB>
+__global__ void __launch_bounds__(128, MB)
 dwf_hop_tma_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename Store<P>::R> k) {
   using St = Store<P>;
   using R = typename St::R;
@@ -599,7 +600,7 @@ constexpr size_t hop_tma_smem_bytes() {
 template <int LS, int P>
 constexpr size_t hop_smem_bytes() {
   using R = typename Store<P>::R;
-  return sizeof(R) * (4 * (32 / LS) * LS * 24);
+  return sizeof(R) * (4 * (32 / LS) * LS * TileStride<R>::v);
 }
 
 }  // namespace b200

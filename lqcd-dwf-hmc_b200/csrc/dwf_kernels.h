@@ -145,4 +145,15 @@ cudaError_t launch_finalize(const double* partials, int n, double* out, int op, 
 
 size_t link_bytes(int lf, size_t vh);
 
+// Complex FP64 BLAS on n complex numbers (double2), used by the flexible CG.
+// launch_zdot: out = <x, y> = sum conj(x) y, or sign * <x, y> / Re(den[0])
+// when den is given (partial: zblas_blocks() double2 scratch).
+int zblas_blocks();
+cudaError_t launch_zdot(const void* x, const void* y, size_t n, void* partial, void* out,
+                        const void* den, double sign, cudaStream_t st);
+cudaError_t launch_zaxpy(void* y, const void* x, size_t n, const void* c, cudaStream_t st);
+// x += alpha p ; r -= alpha q ; partial[block] = |r|^2 (zblas_blocks() doubles)
+cudaError_t launch_zcg_update(void* x, void* r, const void* p, const void* q, size_t n,
+                              const void* alpha, double* partial, cudaStream_t st);
+
 }  // namespace b200

@@ -17,6 +17,7 @@
 #include "../../include/b200dwf.h"
 #include "dwf_hop.cuh"
 #include "dwf_kernels.h"
+#include "learned.h"
 
 using namespace b200;
 
@@ -115,6 +116,9 @@ struct b200_dwf {
   double* ms_red = nullptr;     // multishift per-shift partials
   void** ms_ptrs = nullptr;     // device arrays of x_i and p_i pointers
   std::vector<void*> ms_p;      // multishift search directions p_1..p_(n-1)
+  std::vector<void*> fcg_buf;   // flexible-CG fields (FP64 ring of directions)
+  void* fcg_part = nullptr;     // complex reduction partials
+  void* fcg_sc = nullptr;       // complex device scalars
 };
 
 namespace {
@@ -174,7 +178,7 @@ SopParams sop_base(const b200_dwf* op) {
 // B200_AUTOTUNE=0 disables tuning (variant 0).  The first call of a
 // combination must not be inside a CUDA graph capture.
 typedef std::tuple<int, int, int, int, int> TuneKey;   // vh, ls, prec, epi, fk
-constexpr int kHopVariants = 3;   // direct loads, TMA 2-stage, TMA 3-stage
+constexpr int kHopVariants = 5;   // direct, TMA 2-stage, TMA 3-stage, TMA 2-stage + direct at higher occupancy
 std::map<TuneKey, std::pair<int, float> > g_tune;
 std::mutex g_tune_mu;
 
@@ -498,6 +502,9 @@ int b200_dwf_destroy(b200_dwf_t* op) {
   cudaFree(op->ms_red);
   cudaFree(op->ms_ptrs);
   for (void* q : op->ms_p) cudaFree(q);
+  for (void* q : op->fcg_buf) cudaFree(q);
+  cudaFree(op->fcg_part);
+  cudaFree(op->fcg_sc);
   for (int i = 0; i < 2; ++i)
     for (int p = 0; p < 4; ++p) cudaFree(op->tune_out[i][p]);
   delete op;
@@ -607,8 +614,14 @@ int b200_field_copy_convert(b200_dwf_t* op, int prec_out, void* out, int prec_in
 // Scalars stay on the device; the host reads |r|^2 once per iteration for the
 // stopping test.  Returns the iteration count in *nconv and |r|^2/|b|^2 of the
 // recursive residual in *rel2.
+struct CgSnap {
+  int n;                 // number of snapshots
+  const int* iters;      // iteration after which x is copied
+  void* const* dst;      // destination fields (precision of the solve)
+};
+
 static int cg_core(b200_dwf_t* op, int prec, void* x, const void* b, int maxiter, double tol2,
-                   int* nconv, double* rel2, cudaStream_t st) {
+                   int* nconv, double* rel2, cudaStream_t st, const CgSnap* snap = nullptr) {
   int rc;
   if ((rc = ensure_links(op, prec, st))) return rc;
   for (int i = 0; i < 8; ++i)
@@ -665,6 +678,11 @@ static int cg_core(b200_dwf_t* op, int prec, void* x, const void* b, int maxiter
     pu.x = x; pu.p = p; pu.r = r; pu.y = yp;
     pu.alpha = op->sc + SC_ALPHA; pu.beta = op->sc + SC_BETA; pu.g = g;
     B200_CHECK_CUDA(launch_cg_update(prec, pu, op->coefs, st));
+    if (snap)
+      for (int j = 0; j < snap->n; ++j)
+        if (snap->iters[j] == it + 1)
+          B200_CHECK_CUDA(cudaMemcpyAsync(snap->dst[j], x, field_bytes(prec, g.vh, g.ls),
+                                          cudaMemcpyDeviceToDevice, st));
 
     if ((rc = host_scalar(op, SC_RR, &rr, st))) return rc;
     *nconv = it + 1;
@@ -904,6 +922,131 @@ int b200_richardson_solve(b200_dwf_t* op, int inner_prec, void* x, const void* b
   return 0;
 }
 
+// Plain CG (as b200_cg_solve) that copies x after the listed iterations into
+// snapshot fields; the (residual, error) training pairs of the learned
+// preconditioner come from these snapshots and the converged solution.
+int b200_cg_snapshots(b200_dwf_t* op, int prec, void* x, const void* b, int maxiter, double tol2,
+                      int nsnap, const int* iters, void* const* snaps, int* nconv, void* stream) {
+  if (!op || !x || !b || prec < 0 || prec > 3 || maxiter < 0 || nsnap < 0 || (nsnap > 0 && (!iters || !snaps)))
+    return fail(B200_EINVAL, "invalid argument");
+  if (misaligned(x) || misaligned(b)) return fail(B200_EINVAL, "field pointers must be 16-byte aligned");
+  for (int j = 0; j < nsnap; ++j)
+    if (!snaps[j] || misaligned(snaps[j])) return fail(B200_EINVAL, "snapshot %d is not a valid field", j);
+  const CgSnap sn = {nsnap, iters, snaps};
+  int n = 0;
+  double rel2 = 0.0;
+  const int rc = cg_core(op, prec, x, b, maxiter, tol2, &n, &rel2, (cudaStream_t)stream, &sn);
+  if (nconv) *nconv = n;
+  return rc;
+}
+
+// Flexible CG on DdagD (Notay's FCG; the pattern of the reference's flexible
+// solvers, src/lib_alt/Solver/asolver_FBiCGStab-tmpl.h, with the
+// preconditioner slot of APrecond<AFIELD>::mult, src/lib_alt/Solver/
+// aprecond.h:28-47) preconditioned by the learned network: FP64 iterate and
+// residual, z = N(r) in FP32 with BF16 weights, the new direction
+// A-orthogonalised against the last mtrunc directions with complex
+// coefficients (N is not Hermitian).  The FP64 true residual judges the
+// result; if it misses tol2, plain CG on the residual equation finishes the
+// solve from x (its iterations are returned in *nconv_fallback).
+int b200_fcg_solve(b200_dwf_t* op, b200_lp_t* lp, void* x, const void* b, int maxiter, double tol2,
+                   int mtrunc, int* nconv, int* nconv_fallback, double* diff, void* stream) {
+  constexpr int kFallbackMaxiter = 100000;
+  if (!op || !lp || !x || !b || maxiter < 0 || mtrunc < 1 || mtrunc > 8)
+    return fail(B200_EINVAL, "invalid argument");
+  if (misaligned(x) || misaligned(b)) return fail(B200_EINVAL, "field pointers must be 16-byte aligned");
+  cudaStream_t st = (cudaStream_t)stream;
+  const int P64 = PREC_F64, P32 = PREC_F32;
+  int rc;
+  if ((rc = ensure_links(op, P64, st)) || (rc = ensure_links(op, P32, st))) return rc;
+  if ((rc = ensure_work(op, P32, 10)) || (rc = ensure_work(op, P32, 11))) return rc;
+  const Geom& g = op->g;
+  const size_t ncplx = (size_t)g.vh * g.ls * 12;
+  const size_t fb = field_bytes(P64, g.vh, g.ls);
+  const int M = mtrunc;
+  const size_t nbuf = 2 * (size_t)(M + 1) + 3;
+  while (op->fcg_buf.size() < nbuf) {
+    void* q = nullptr;
+    if (cudaMalloc(&q, fb) != cudaSuccess) return fail(B200_ENOMEM, "cudaMalloc for a flexible-CG field failed");
+    op->fcg_buf.push_back(q);
+  }
+  if (!op->fcg_part && cudaMalloc(&op->fcg_part, sizeof(double2) * zblas_blocks()) != cudaSuccess)
+    return fail(B200_ENOMEM, "cudaMalloc for flexible-CG partials failed");
+  if (!op->fcg_sc && cudaMalloc(&op->fcg_sc, sizeof(double2) * 16) != cudaSuccess)
+    return fail(B200_ENOMEM, "cudaMalloc for flexible-CG scalars failed");
+  void** P = op->fcg_buf.data();
+  void** Q = op->fcg_buf.data() + (M + 1);
+  void* r = op->fcg_buf[2 * (M + 1)];
+  void* z = op->fcg_buf[2 * (M + 1) + 1];
+  void* dx = op->fcg_buf[2 * (M + 1) + 2];
+  void* rf = op->work[10][P32];
+  void* zf = op->work[11][P32];
+  double2* sc = reinterpret_cast<double2*>(op->fcg_sc);   // [1] alpha, [2+i] <p_i,q_i>, [12] beta
+  double* part = reinterpret_cast<double*>(op->fcg_part);
+
+  auto precondition = [&]() -> int {
+    B200_CHECK_CUDA(launch_convert(P32, rf, P64, r, g, st));
+    int rc2 = lp_apply_internal(lp, zf, rf, st);
+    if (rc2) return rc2;
+    B200_CHECK_CUDA(launch_convert(P64, z, P32, zf, g, st));
+    return 0;
+  };
+
+  if (nconv) *nconv = 0;
+  if (nconv_fallback) *nconv_fallback = 0;
+  if (diff) *diff = 0.0;
+  B200_CHECK_CUDA(launch_axpby(P64, g, x, nullptr, 0.0, nullptr, 0.0, nullptr, st));
+  B200_CHECK_CUDA(cudaMemcpyAsync(r, b, fb, cudaMemcpyDeviceToDevice, st));
+  if ((rc = field_norm2_dev(op, P64, r, op->sc + SC_RR_NEW, st))) return rc;
+  double bb = 0.0;
+  if ((rc = host_scalar(op, SC_RR_NEW, &bb, st))) return rc;
+  if (!(bb > 0.0)) return 0;
+  if ((rc = precondition())) return rc;
+  B200_CHECK_CUDA(cudaMemcpyAsync(P[0], z, fb, cudaMemcpyDeviceToDevice, st));
+  double rr = bb;
+  int iters = 0;
+  for (int it = 0; it < maxiter; ++it) {
+    const int k = it % (M + 1);
+    if ((rc = apply_DdagD(op, P64, Q[k], P[k], st))) return rc;
+    B200_CHECK_CUDA(launch_zdot(P[k], Q[k], ncplx, op->fcg_part, sc + 2 + k, nullptr, 1.0, st));
+    B200_CHECK_CUDA(launch_zdot(P[k], r, ncplx, op->fcg_part, sc + 1, sc + 2 + k, 1.0, st));
+    B200_CHECK_CUDA(launch_zcg_update(x, r, P[k], Q[k], ncplx, sc + 1, part, st));
+    B200_CHECK_CUDA(launch_finalize(part, zblas_blocks(), op->sc + SC_RR_NEW, FIN_SUM, st));
+    if ((rc = host_scalar(op, SC_RR_NEW, &rr, st))) return rc;
+    iters = it + 1;
+    if (!(rr == rr)) return fail(B200_ENOCONV, "flexible CG breakdown: NaN residual at iteration %d", iters);
+    if (rr / bb < tol2) break;
+    if ((rc = precondition())) return rc;
+    const int kn = (it + 1) % (M + 1);
+    B200_CHECK_CUDA(cudaMemcpyAsync(P[kn], z, fb, cudaMemcpyDeviceToDevice, st));
+    for (int j = (it - M + 1 > 0 ? it - M + 1 : 0); j <= it; ++j) {
+      const int sj = j % (M + 1);
+      B200_CHECK_CUDA(launch_zdot(Q[sj], z, ncplx, op->fcg_part, sc + 12, sc + 2 + sj, -1.0, st));
+      B200_CHECK_CUDA(launch_zaxpy(P[kn], P[sj], ncplx, sc + 12, st));
+    }
+  }
+  if (nconv) *nconv = iters;
+  double d = 0.0;
+  if ((rc = true_residual(op, P64, x, b, 0.0, &d, st))) return rc;
+  if (!(d * d < tol2)) {
+    // r = b - DdagD x, then plain CG on DdagD dx = r to the remaining tolerance
+    if ((rc = apply_DdagD(op, P64, r, x, st))) return rc;
+    B200_CHECK_CUDA(launch_axpby(P64, g, r, b, 1.0, nullptr, -1.0, nullptr, st));
+    const double r2 = d * d * bb;
+    int nfb = 0;
+    double rel = 0.0;
+    rc = cg_core(op, P64, dx, r, kFallbackMaxiter, tol2 * bb / r2, &nfb, &rel, st);
+    if (rc && rc != B200_ENOCONV) return rc;
+    B200_CHECK_CUDA(launch_axpby(P64, g, x, dx, 1.0, nullptr, 1.0, nullptr, st));
+    if (nconv_fallback) *nconv_fallback = nfb;
+    if ((rc = true_residual(op, P64, x, b, 0.0, &d, st))) return rc;
+  }
+  if (diff) *diff = d;
+  if (!(d * d < tol2))
+    return fail(B200_ENOCONV, "flexible CG and its CG fallback missed the tolerance: |r|/|b| = %.3e", d);
+  return 0;
+}
+
 // Force_F_Domainwall_eo (src/lib/Force/Fermion/force_F_Domainwall_eo.cpp:
 // 150-327) on the device.  With y_e = M5pre(eta), y_o = M5pre M_oo^-1 D_oe eta,
 // A_e = M_ee^-+ gm5R zeta and A_o = M_oo^-+ D_oe^+ A_e (both fifth-dimension
@@ -1017,3 +1160,18 @@ int b200_tuning_table(char* buf, size_t n) {
 }
 
 }  // extern "C"
+
+// Accessors used by the learned preconditioner (learned.cu).
+namespace b200 {
+int plan_geometry(b200_dwf* op, Geom* g, float bc[4]) {
+  *g = op->g;
+  for (int mu = 0; mu < 4; ++mu) bc[mu] = (float)op->bc[mu];
+  return 0;
+}
+int plan_links_f32(b200_dwf* op, const void** links, cudaStream_t st) {
+  const int rc = ensure_links(op, PREC_F32, st);
+  if (rc) return rc;
+  *links = op->links[LINK_F32_12];
+  return 0;
+}
+}  // namespace b200

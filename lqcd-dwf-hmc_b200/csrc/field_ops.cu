@@ -84,7 +84,7 @@ sop_kernel(SopParams p, const __grid_constant__ ChainCoef<typename Store<P>::R> 
   using R = typename St::R;
   constexpr int G = 32 / LS;
   constexpr int WARPS = 4;
-  extern __shared__ unsigned char smem_raw[];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   R* tile_all = reinterpret_cast<R*>(smem_raw);
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
@@ -93,7 +93,7 @@ sop_kernel(SopParams p, const __grid_constant__ ChainCoef<typename Store<P>::R> 
   const int site = (blockIdx.x * WARPS + warp) * G + g;
   const bool active = (g < G) && (site < p.g.vh);
   const size_t vh = p.g.vh;
-  R* tile = tile_all + warp * G * LS * 24;
+  R* tile = tile_all + warp * G * LS * TileStride<R>::v;
 
   R v[24];
 #pragma unroll
@@ -102,7 +102,7 @@ sop_kernel(SopParams p, const __grid_constant__ ChainCoef<typename Store<P>::R> 
   if (OPA != SOP_ID) {
     if (g < G) {
 #pragma unroll
-      for (int i = 0; i < 24; ++i) tile[(g * LS + s) * 24 + i] = v[i];
+      tile_put(tile + (g * LS + s) * TileStride<R>::v, v);
     }
     __syncwarp();
     tile_chiral<R, LS, G>(tile, lane, [&](R* xp, R* xm) {
@@ -112,7 +112,7 @@ sop_kernel(SopParams p, const __grid_constant__ ChainCoef<typename Store<P>::R> 
     __syncwarp();
     if (g < G) {
 #pragma unroll
-      for (int i = 0; i < 24; ++i) v[i] = tile[(g * LS + s) * 24 + i];
+      tile_get(tile + (g * LS + s) * TileStride<R>::v, v);
     }
   }
   double nrm = 0.0;
@@ -144,7 +144,7 @@ sop_kernel(SopParams p, const __grid_constant__ ChainCoef<typename Store<P>::R> 
     __syncwarp();
     if (g < G) {
 #pragma unroll
-      for (int i = 0; i < 24; ++i) tile[(g * LS + s) * 24 + i] = v[i];
+      tile_put(tile + (g * LS + s) * TileStride<R>::v, v);
     }
     __syncwarp();
     tile_chiral<R, LS, G>(tile, lane, [&](R* xp, R* xm) {
@@ -155,7 +155,7 @@ sop_kernel(SopParams p, const __grid_constant__ ChainCoef<typename Store<P>::R> 
     if (active) {
       R o2[24];
 #pragma unroll
-      for (int i = 0; i < 24; ++i) o2[i] = tile[(g * LS + s) * 24 + i];
+      tile_get(tile + (g * LS + s) * TileStride<R>::v, o2);
       St::store(p.out2, vh, LS, site, s, o2);
     }
   }
@@ -165,7 +165,7 @@ sop_kernel(SopParams p, const __grid_constant__ ChainCoef<typename Store<P>::R> 
 template <int LS, int P, int OPA, int OPB>
 cudaError_t run_sop(const SopParams& p, const ChainCoefs& c, cudaStream_t st) {
   using R = typename Store<P>::R;
-  constexpr size_t smem = sizeof(R) * (4 * (32 / LS) * LS * 24);
+  constexpr size_t smem = sizeof(R) * (4 * (32 / LS) * LS * TileStride<R>::v);
   auto k = sop_kernel<LS, P, OPA, OPB>;
   static bool attr_done = false;
   if (!attr_done) {
@@ -231,7 +231,7 @@ cg_update_kernel(CgUpdParams p, const __grid_constant__ ChainCoef<typename Store
   using R = typename St::R;
   constexpr int G = 32 / LS;
   constexpr int WARPS = 4;
-  extern __shared__ unsigned char smem_raw[];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   R* tile_all = reinterpret_cast<R*>(smem_raw);
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
@@ -240,7 +240,7 @@ cg_update_kernel(CgUpdParams p, const __grid_constant__ ChainCoef<typename Store
   const int site = (blockIdx.x * WARPS + warp) * G + g;
   const bool active = (g < G) && (site < p.g.vh);
   const size_t vh = p.g.vh;
-  R* tile = tile_all + warp * G * LS * 24;
+  R* tile = tile_all + warp * G * LS * TileStride<R>::v;
   R pv[24];
 #pragma unroll
   for (int i = 0; i < 24; ++i) pv[i] = 0;
@@ -260,7 +260,7 @@ cg_update_kernel(CgUpdParams p, const __grid_constant__ ChainCoef<typename Store
   }
   if (g < G) {
 #pragma unroll
-    for (int i = 0; i < 24; ++i) tile[(g * LS + s) * 24 + i] = pv[i];
+    tile_put(tile + (g * LS + s) * TileStride<R>::v, pv);
   }
   __syncwarp();
   tile_chiral<R, LS, G>(tile, lane, [&](R* xp, R* xm) {
@@ -271,7 +271,7 @@ cg_update_kernel(CgUpdParams p, const __grid_constant__ ChainCoef<typename Store
   if (active) {
     R o[24];
 #pragma unroll
-    for (int i = 0; i < 24; ++i) o[i] = tile[(g * LS + s) * 24 + i];
+    tile_get(tile + (g * LS + s) * TileStride<R>::v, o);
     St::store(p.y, vh, LS, site, s, o);
   }
 }
@@ -279,7 +279,7 @@ cg_update_kernel(CgUpdParams p, const __grid_constant__ ChainCoef<typename Store
 template <int LS, int P>
 cudaError_t run_cgu(const CgUpdParams& p, const ChainCoefs& c, cudaStream_t st) {
   using R = typename Store<P>::R;
-  constexpr size_t smem = sizeof(R) * (4 * (32 / LS) * LS * 24);
+  constexpr size_t smem = sizeof(R) * (4 * (32 / LS) * LS * TileStride<R>::v);
   auto k = cg_update_kernel<LS, P>;
   static bool attr_done = false;
   if (!attr_done) {
@@ -326,7 +326,7 @@ ms_update_kernel(MsUpdParams p, const __grid_constant__ ChainCoef<typename Store
   using R = typename St::R;
   constexpr int G = 32 / LS;
   constexpr int WARPS = 4;
-  extern __shared__ unsigned char smem_raw[];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   R* tile_all = reinterpret_cast<R*>(smem_raw);
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
@@ -335,7 +335,7 @@ ms_update_kernel(MsUpdParams p, const __grid_constant__ ChainCoef<typename Store
   const int site = (blockIdx.x * WARPS + warp) * G + g;
   const bool active = (g < G) && (site < p.g.vh);
   const size_t vh = p.g.vh;
-  R* tile = tile_all + warp * G * LS * 24;
+  R* tile = tile_all + warp * G * LS * TileStride<R>::v;
   const int nact = (int)p.st[MS_NACT];
   const R beta = (R)p.st[MS_BETA], alpha = (R)p.st[MS_ALPHA];
   R rv[24], pv[24];
@@ -358,7 +358,7 @@ ms_update_kernel(MsUpdParams p, const __grid_constant__ ChainCoef<typename Store
   }
   if (g < G) {
 #pragma unroll
-    for (int i = 0; i < 24; ++i) tile[(g * LS + s) * 24 + i] = pv[i];
+    tile_put(tile + (g * LS + s) * TileStride<R>::v, pv);
   }
   __syncwarp();
   tile_chiral<R, LS, G>(tile, lane, [&](R* xp, R* xm) {
@@ -369,7 +369,7 @@ ms_update_kernel(MsUpdParams p, const __grid_constant__ ChainCoef<typename Store
   if (active) {
     R o[24];
 #pragma unroll
-    for (int i = 0; i < 24; ++i) o[i] = tile[(g * LS + s) * 24 + i];
+    tile_get(tile + (g * LS + s) * TileStride<R>::v, o);
     St::store(p.y0, vh, LS, site, s, o);
   }
   block_reduce_store(nrm, p.red);
@@ -399,7 +399,7 @@ ms_update_kernel(MsUpdParams p, const __grid_constant__ ChainCoef<typename Store
 template <int LS, int P>
 cudaError_t run_msu(const MsUpdParams& p, const ChainCoefs& c, cudaStream_t st) {
   using R = typename Store<P>::R;
-  constexpr size_t smem = sizeof(R) * (4 * (32 / LS) * LS * 24);
+  constexpr size_t smem = sizeof(R) * (4 * (32 / LS) * LS * TileStride<R>::v);
   auto k = ms_update_kernel<LS, P>;
   static bool attr_done = false;
   if (!attr_done) {
@@ -755,6 +755,112 @@ cudaError_t launch_links_from_lex(int lf, void* out, const double* u_lex_dev, co
 
 cudaError_t launch_finalize(const double* partials, int n, double* out, int op, cudaStream_t st) {
   finalize_kernel<<<1, 1024, 0, st>>>(partials, n, out, op);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------ complex BLAS (f64)
+// The FP64 field is an array of n complex numbers (double2).  Used by the
+// flexible CG, whose step sizes are complex once the preconditioner is not
+// Hermitian.
+namespace {
+constexpr int kZBlocks = 296;
+
+__global__ void zdot_kernel(const double2* x, const double2* y, size_t n, double2* partial) {
+  __shared__ double sr[256], si[256];
+  double re = 0.0, im = 0.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double2 a = x[i], b = y[i];
+    re = fma(a.x, b.x, re); re = fma(a.y, b.y, re);   // conj(a) * b
+    im = fma(a.x, b.y, im); im = fma(-a.y, b.x, im);
+  }
+  sr[threadIdx.x] = re; si[threadIdx.x] = im;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) { sr[threadIdx.x] += sr[threadIdx.x + o]; si[threadIdx.x] += si[threadIdx.x + o]; }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = make_double2(sr[0], si[0]);
+}
+
+// out = sum of partials; with den != nullptr, out = sign * sum / Re(den[0]).
+__global__ void zfinal_kernel(const double2* partial, int nb, double2* out, const double2* den,
+                              double sign) {
+  __shared__ double sr[256], si[256];
+  double re = 0.0, im = 0.0;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) { re += partial[i].x; im += partial[i].y; }
+  sr[threadIdx.x] = re; si[threadIdx.x] = im;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) { sr[threadIdx.x] += sr[threadIdx.x + o]; si[threadIdx.x] += si[threadIdx.x + o]; }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    double2 v = make_double2(sr[0], si[0]);
+    if (den) {
+      const double d = den[0].x;
+      const double f = (d != 0.0) ? sign / d : 0.0;
+      v = make_double2(f * v.x, f * v.y);
+    }
+    out[0] = v;
+  }
+}
+
+// y += c * x  (c complex, read from the device)
+__global__ void zaxpy_kernel(double2* y, const double2* x, size_t n, const double2* c) {
+  const double2 cc = c[0];
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double2 a = x[i];
+    double2 v = y[i];
+    v.x = fma(cc.x, a.x, v.x); v.x = fma(-cc.y, a.y, v.x);
+    v.y = fma(cc.x, a.y, v.y); v.y = fma(cc.y, a.x, v.y);
+    y[i] = v;
+  }
+}
+
+// x += alpha p ; r -= alpha q ; per-block |r|^2
+__global__ void zcg_update_kernel(double2* x, double2* r, const double2* p, const double2* q, size_t n,
+                                  const double2* alpha, double* partial) {
+  __shared__ double sh[256];
+  const double2 a = alpha[0];
+  double acc = 0.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double2 pv = p[i], qv = q[i];
+    double2 xv = x[i], rv = r[i];
+    xv.x = fma(a.x, pv.x, xv.x); xv.x = fma(-a.y, pv.y, xv.x);
+    xv.y = fma(a.x, pv.y, xv.y); xv.y = fma(a.y, pv.x, xv.y);
+    rv.x = fma(-a.x, qv.x, rv.x); rv.x = fma(a.y, qv.y, rv.x);
+    rv.y = fma(-a.x, qv.y, rv.y); rv.y = fma(-a.y, qv.x, rv.y);
+    x[i] = xv; r[i] = rv;
+    acc = fma(rv.x, rv.x, acc); acc = fma(rv.y, rv.y, acc);
+  }
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = sh[0];
+}
+}  // namespace
+
+int zblas_blocks() { return kZBlocks; }
+
+cudaError_t launch_zdot(const void* x, const void* y, size_t n, void* partial, void* out,
+                        const void* den, double sign, cudaStream_t st) {
+  zdot_kernel<<<kZBlocks, 256, 0, st>>>((const double2*)x, (const double2*)y, n, (double2*)partial);
+  zfinal_kernel<<<1, 256, 0, st>>>((const double2*)partial, kZBlocks, (double2*)out, (const double2*)den, sign);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_zaxpy(void* y, const void* x, size_t n, const void* c, cudaStream_t st) {
+  zaxpy_kernel<<<kZBlocks, 256, 0, st>>>((double2*)y, (const double2*)x, n, (const double2*)c);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_zcg_update(void* x, void* r, const void* p, const void* q, size_t n,
+                              const void* alpha, double* partial, cudaStream_t st) {
+  zcg_update_kernel<<<kZBlocks, 256, 0, st>>>((double2*)x, (double2*)r, (const double2*)p,
+                                              (const double2*)q, n, (const double2*)alpha, partial);
   return cudaGetLastError();
 }
 

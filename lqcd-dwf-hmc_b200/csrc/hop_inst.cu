@@ -37,12 +37,12 @@ cudaError_t run_mb(const HopParams& p, const ChainCoefs& c, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-template <int LS, int P, int EPI, int FK, int S>
+template <int LS, int P, int EPI, int FK, int S, int MB>
 cudaError_t run_tma(const HopParams& p, const ChainCoefs& c, cudaStream_t st) {
   using R = typename Store<P>::R;
   constexpr int LF = DefaultLink<P>::v;
   constexpr size_t smem = hop_tma_smem_bytes<LS, P, LF, S>();
-  auto k = dwf_hop_tma_kernel<LS, P, LF, EPI, FK, S>;
+  auto k = dwf_hop_tma_kernel<LS, P, LF, EPI, FK, S, MB>;
   static bool attr_done = false;
   if (!attr_done) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -55,11 +55,15 @@ cudaError_t run_tma(const HopParams& p, const ChainCoefs& c, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-// variant 0: direct loads; 1: TMA-staged, 2 stages; 2: TMA-staged, 3 stages
+// variant 0: direct loads; 1: TMA-staged, 2 stages; 2: TMA-staged, 3 stages;
+// 3: TMA-staged, 2 stages, register budget for HopMinBlocks::v1 resident
+// blocks; 4: direct loads with that register budget.
 template <int LS, int P, int EPI, int FK>
 cudaError_t run(const HopParams& p, const ChainCoefs& c, cudaStream_t st) {
-  if (p.variant == 1) return run_tma<LS, P, EPI, FK, 2>(p, c, st);
-  if (p.variant == 2) return run_tma<LS, P, EPI, FK, 3>(p, c, st);
+  if (p.variant == 1) return run_tma<LS, P, EPI, FK, 2, 1>(p, c, st);
+  if (p.variant == 2) return run_tma<LS, P, EPI, FK, 3, 1>(p, c, st);
+  if (p.variant == 3) return run_tma<LS, P, EPI, FK, 2, HopMinBlocks<P>::v1>(p, c, st);
+  if (p.variant == 4) return run_mb<LS, P, EPI, FK, HopMinBlocks<P>::v1>(p, c, st);
   return run_mb<LS, P, EPI, FK, HopMinBlocks<P>::v0>(p, c, st);
 }
 

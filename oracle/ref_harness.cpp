@@ -277,6 +277,7 @@ int main(int argc, char **argv)
     // "Deo"/"Doe"/... use mult(v, w, mode); "dag_<mode>" uses mult_dag;
     // composite modes (D, DdagD, ...) use set_mode + mult.
     const int reps = geti(kv, "reps", 10);
+    const int warm = geti(kv, "warmup", 1);
     for (size_t i = 0; i < modes.size(); ++i) {
       std::string m = modes[i];
       bool dag = false;
@@ -284,9 +285,9 @@ int main(int argc, char **argv)
       const bool explicit_mode = (m == "Deo" || m == "Doe" || m == "Dee" || m == "Doo" ||
                                   m == "Dee_inv" || m == "Doo_inv");
       if (!explicit_mode) fopr.set_mode(m);
-      // r = -1 is one untimed call that touches all memory first
+      // r < 0: `warm` untimed calls that touch all memory first
       std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
-      for (int r = -1; r < reps; ++r) {
+      for (int r = -warm; r < reps; ++r) {
         if (r == 0) t0 = std::chrono::steady_clock::now();
 #pragma omp parallel
         {
