@@ -218,14 +218,18 @@ int b200_lp_set_weights(b200_lp_t *lp, const float *w, int nfloat);
 int b200_lp_get_weights(b200_lp_t *lp, float *w, int nfloat, int deployed);
 /* z = N(r). */
 int b200_lp_apply(b200_lp_t *lp, void *z, const void *r, void *stream);
-/* loss = |N(r) - e|^2 / |e|^2 and its gradient dL/dRe(w) + i dL/dIm(w),
- * kept on the device (b200_lp_get_grad copies it out).  Synchronous. */
+/* For a pair with DdagD e = r: loss = |DdagD (N(r) - e)|^2 / |r|^2 (the
+ * error of N measured in the residual norm) and its gradient
+ * dL/dRe(w) + i dL/dIm(w), kept on the device (b200_lp_get_grad copies it
+ * out).  Synchronous. */
 int b200_lp_loss_grad(b200_lp_t *lp, const void *r, const void *e, double *loss, void *stream);
 int b200_lp_get_grad(b200_lp_t *lp, float *g, int nfloat);
 /* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on the master weights. */
 int b200_lp_adam_step(b200_lp_t *lp, double lr, void *stream);
 /* `epochs` passes of loss_grad + adam_step over the pairs in a seeded
- * shuffled order; mean loss of the first and the last epoch. */
+ * shuffled order; mean loss of the first and the last epoch.  A network that
+ * has not taken a step yet first scales its last layer by the least-squares
+ * factor Re<DdagD N r, r> / |DdagD N r|^2 of the first pair. */
 int b200_lp_train(b200_lp_t *lp, int npairs, const void *const *r, const void *const *e,
                   int epochs, double lr, unsigned long long seed, double *loss_first,
                   double *loss_last, void *stream);

@@ -1168,6 +1168,9 @@ int plan_geometry(b200_dwf* op, Geom* g, float bc[4]) {
   for (int mu = 0; mu < 4; ++mu) bc[mu] = (float)op->bc[mu];
   return 0;
 }
+int plan_apply_ddagd(b200_dwf* op, void* v, const void* w, cudaStream_t st) {
+  return apply_mode(op, PREC_F32, v, w, "DdagD", 0, st);
+}
 int plan_links_f32(b200_dwf* op, const void** links, cudaStream_t st) {
   const int rc = ensure_links(op, PREC_F32, st);
   if (rc) return rc;

@@ -10,10 +10,15 @@
 //
 // The deployed weights are the FP32 master weights rounded to BF16 (held as
 // FP32 values that BF16 represents exactly); every kernel accumulates in
-// FP32.  Training (forward, loss, backward through the layers, weight
-// gradients as site-reduced outer products, Adam on the FP32 master copy)
-// runs entirely in these kernels.  The network has no counterpart in the
-// reference; it plugs in where its solver framework takes a preconditioner
+// FP32.  Training runs entirely in these kernels: forward, the loss
+// L = |A (N r - e)|^2 / |r|^2 on a pair with A e = r (A = DdagD applied by
+// the operator's own FP32 kernels; measuring the error in the residual norm
+// makes A N ~ 1 on every mode, which is what a Krylov solver needs -- the
+// plain error norm lets N neglect the high modes, and the flexible solver
+// then stagnates on them), backward through the layers, weight gradients as
+// site-reduced outer products, and Adam on the FP32 master copy.  The
+// network has no counterpart in the reference; it plugs in where its solver
+// framework takes a preconditioner
 // (APrecond<AFIELD>::mult, src/lib_alt/Solver/aprecond.h:28-47) and is used by
 // the flexible CG in dwf_plan.cu.
 #include <cuda_bf16.h>
@@ -305,20 +310,40 @@ __global__ void lp_norm_kernel(const float4* x, size_t n4, double* partial) {
   if (threadIdx.x == 0) partial[blockIdx.x] = sh[0];
 }
 
-// delta = 2 (y - e) / |e|^2 ; partial sums of |y - e|^2 / |e|^2
-__global__ void lp_loss_kernel(const float4* y, const float4* e, float4* delta, size_t n4,
-                               const double* e2, double* partial) {
-  __shared__ double sh[256];
-  const double inv = (e2[0] > 0.0) ? 1.0 / e2[0] : 0.0;
-  const float two_inv = (float)(2.0 * inv);
-  double acc = 0.0;
+// t = y - e
+__global__ void lp_sub_kernel(const float4* y, const float4* e, float4* t, size_t n4) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n4; i += (size_t)gridDim.x * blockDim.x) {
     const float4 a = y[i], b = e[i];
-    const float4 d = make_float4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w);
-    delta[i] = make_float4(two_inv * d.x, two_inv * d.y, two_inv * d.z, two_inv * d.w);
-    acc += (double)d.x * d.x + (double)d.y * d.y + (double)d.z * d.z + (double)d.w * d.w;
+    t[i] = make_float4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w);
   }
-  sh[threadIdx.x] = acc * inv;
+}
+
+// out = num * x / den[0] (den a device scalar; zero if den is not positive)
+__global__ void lp_scale_kernel(const float4* x, float4* out, size_t n4, const double* den, double num) {
+  const float f = (den[0] > 0.0) ? (float)(num / den[0]) : 0.f;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n4; i += (size_t)gridDim.x * blockDim.x) {
+    const float4 a = x[i];
+    out[i] = make_float4(f * a.x, f * a.y, f * a.z, f * a.w);
+  }
+}
+
+// w *= c[0] / c[1] on n complex weights (c: device scalars)
+__global__ void lp_rescale_kernel(float2* w, int n, const double* c) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || !(c[1] > 0.0)) return;
+  const float f = (float)(c[0] / c[1]);
+  w[i] = make_float2(f * w[i].x, f * w[i].y);
+}
+
+// out[0] = Re <x, y> over n4 float4 (complex pairs), per-block partials
+__global__ void lp_redot_kernel(const float4* x, const float4* y, size_t n4, double* partial) {
+  __shared__ double sh[256];
+  double acc = 0.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n4; i += (size_t)gridDim.x * blockDim.x) {
+    const float4 a = x[i], b = y[i];
+    acc += (double)a.x * b.x + (double)a.y * b.y + (double)a.z * b.z + (double)a.w * b.w;
+  }
+  sh[threadIdx.x] = acc;
   __syncthreads();
   for (int o = blockDim.x / 2; o > 0; o >>= 1) {
     if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
@@ -443,7 +468,7 @@ struct b200_lp {
   float2* wadj = nullptr;               // deployed adjoint weights
   bool prepped = false;
   int t = 0;                            // Adam step
-  float4* act[10] = {};                 // y1e y1o y2e y2o y3 d3 d2e d2o d1e d1o
+  float4* act[12] = {};                 // y1e y1o y2e y2o y3 d3 d2e d2o d1e d1o t ad
   float2* partial = nullptr;
   int max_blocks = 0;
   double* red = nullptr;                // reduction partials
@@ -453,7 +478,7 @@ struct b200_lp {
 
 namespace {
 
-enum { Y1E = 0, Y1O, Y2E, Y2O, Y3, D3, D2E, D2O, D1E, D1O };
+enum { Y1E = 0, Y1O, Y2E, Y2O, Y3, D3, D2E, D2O, D1E, D1O, T4, AD4, NACT };
 constexpr int kRedBlocks = 296;
 
 int lp_fail(int code, const char* msg) {
@@ -606,8 +631,8 @@ int b200_lp_create(b200_lp_t** out, b200_dwf_t* op, int hidden, unsigned long lo
   bool ok = cudaMalloc(&lp->master, pb) == cudaSuccess && cudaMalloc(&lp->adam_m, pb) == cudaSuccess &&
             cudaMalloc(&lp->adam_v, pb) == cudaSuccess && cudaMalloc(&lp->grad, pb) == cudaSuccess &&
             cudaMalloc(&lp->wf, pb) == cudaSuccess && cudaMalloc(&lp->wadj, pb) == cudaSuccess;
-  for (int i = 0; ok && i < 10; ++i) {
-    const int ch = (i == Y3 || i == D3) ? kLpIn : hidden;
+  for (int i = 0; ok && i < NACT; ++i) {
+    const int ch = (i == Y3 || i == D3 || i == T4 || i == AD4) ? kLpIn : hidden;
     ok = cudaMalloc(&lp->act[i], act_bytes(lp, ch)) == cudaSuccess;
   }
   lp->max_blocks = 148 * 3;
@@ -633,7 +658,7 @@ int b200_lp_destroy(b200_lp_t* lp) {
   if (!lp) return 0;
   cudaFree(lp->master); cudaFree(lp->adam_m); cudaFree(lp->adam_v); cudaFree(lp->grad);
   cudaFree(lp->wf); cudaFree(lp->wadj);
-  for (int i = 0; i < 10; ++i) cudaFree(lp->act[i]);
+  for (int i = 0; i < NACT; ++i) cudaFree(lp->act[i]);
   cudaFree(lp->partial); cudaFree(lp->red); cudaFree(lp->sc);
   if (lp->sc_host) cudaFreeHost(lp->sc_host);
   delete lp;
@@ -669,8 +694,10 @@ int b200_lp_apply(b200_lp_t* lp, void* z_f32, const void* r_f32, void* stream) {
   return lp_apply_internal(lp, z_f32, r_f32, (cudaStream_t)stream);
 }
 
-// Forward, loss L = |N(r) - e|^2 / |e|^2 and the gradient dL/dRe W + i dL/dIm W
-// of every weight (kept on the device; b200_lp_get_grad copies it out).
+// Forward, loss L = |A (N r - e)|^2 / |r|^2 (A = DdagD, r = A e) and the
+// gradient dL/dRe W + i dL/dIm W of every weight (kept on the device;
+// b200_lp_get_grad copies it out).  dL/dy = 2 A A (y - e) / |r|^2 since A is
+// Hermitian: two FP32 DdagD applications per step.
 int b200_lp_loss_grad(b200_lp_t* lp, const void* r_f32, const void* e_f32, double* loss,
                       void* stream) {
   if (!lp || bad_ptr(r_f32) || bad_ptr(e_f32)) return lp_fail(B200_EINVAL, "invalid argument");
@@ -683,10 +710,15 @@ int b200_lp_loss_grad(b200_lp_t* lp, const void* r_f32, const void* e_f32, doubl
   float4** a = lp->act;
   if ((rc = forward(lp, links, r, a[Y3], st))) return rc;
   const size_t n4 = act_bytes(lp, kLpIn) / sizeof(float4);
-  lp_norm_kernel<<<kRedBlocks, 256, 0, st>>>(e, n4, lp->red);
-  lp_sum_kernel<<<1, 256, 0, st>>>(lp->red, kRedBlocks, lp->sc);
-  lp_loss_kernel<<<kRedBlocks, 256, 0, st>>>(a[Y3], e, a[D3], n4, lp->sc, lp->red);
-  lp_sum_kernel<<<1, 256, 0, st>>>(lp->red, kRedBlocks, lp->sc + 1);
+  lp_norm_kernel<<<kRedBlocks, 256, 0, st>>>(r, n4, lp->red);
+  lp_sum_kernel<<<1, 256, 0, st>>>(lp->red, kRedBlocks, lp->sc);          // |r|^2
+  lp_sub_kernel<<<kRedBlocks, 256, 0, st>>>(a[Y3], e, a[T4], n4);         // t = y - e
+  LP_CHECK(cudaGetLastError());
+  if ((rc = plan_apply_ddagd(lp->op, a[AD4], a[T4], st))) return rc;       // d = A t
+  lp_norm_kernel<<<kRedBlocks, 256, 0, st>>>(a[AD4], n4, lp->red);
+  lp_sum_kernel<<<1, 256, 0, st>>>(lp->red, kRedBlocks, lp->sc + 1);      // |d|^2
+  if ((rc = plan_apply_ddagd(lp->op, a[T4], a[AD4], st))) return rc;       // A d
+  lp_scale_kernel<<<kRedBlocks, 256, 0, st>>>(a[T4], a[D3], n4, lp->sc, 2.0);
   LP_CHECK(cudaGetLastError());
   // layer 3 (output even only)
   if ((rc = gradw(lp, links, 2, 0, a[D3], a[Y2E], a[Y2O], false, st))) return rc;
@@ -702,8 +734,8 @@ int b200_lp_loss_grad(b200_lp_t* lp, const void* r_f32, const void* e_f32, doubl
   if ((rc = gradw(lp, links, 0, 1, a[D1O], nullptr, r, true, st))) return rc;
   LP_CHECK(cudaMemcpyAsync(lp->sc_host, lp->sc, sizeof(double) * 2, cudaMemcpyDeviceToHost, st));
   LP_CHECK(cudaStreamSynchronize(st));
-  if (loss) *loss = lp->sc_host[1];
-  if (!(lp->sc_host[0] > 0.0)) return lp_fail(B200_EINVAL, "target field e is zero");
+  if (!(lp->sc_host[0] > 0.0)) return lp_fail(B200_EINVAL, "residual field r is zero");
+  if (loss) *loss = lp->sc_host[1] / lp->sc_host[0];
   return 0;
 }
 
@@ -736,6 +768,27 @@ int b200_lp_train(b200_lp_t* lp, int npairs, const void* const* r_f32, const voi
   std::vector<int> order(npairs);
   for (int i = 0; i < npairs; ++i) order[i] = i;
   uint64_t s = seed ? seed : 0xABCDEFull;
+  if (lp->t == 0) {
+    // Fresh network: scale the last layer by the least-squares factor
+    // c = Re<A N r, r> / |A N r|^2 on the first pair, so training starts from
+    // the best multiple of the initial N.
+    cudaStream_t st = (cudaStream_t)stream;
+    const void* links = nullptr;
+    int rc;
+    if ((rc = plan_links_f32(lp->op, &links, st))) return rc;
+    float4** a = lp->act;
+    const size_t n4 = act_bytes(lp, kLpIn) / sizeof(float4);
+    if ((rc = forward(lp, links, reinterpret_cast<const float4*>(r_f32[0]), a[Y3], st))) return rc;
+    if ((rc = plan_apply_ddagd(lp->op, a[AD4], a[Y3], st))) return rc;
+    lp_redot_kernel<<<kRedBlocks, 256, 0, st>>>(a[AD4], reinterpret_cast<const float4*>(r_f32[0]), n4, lp->red);
+    lp_sum_kernel<<<1, 256, 0, st>>>(lp->red, kRedBlocks, lp->sc + 2);
+    lp_norm_kernel<<<kRedBlocks, 256, 0, st>>>(a[AD4], n4, lp->red);
+    lp_sum_kernel<<<1, 256, 0, st>>>(lp->red, kRedBlocks, lp->sc + 3);
+    const int n3 = kLpPaths * lp->cin[2] * lp->cout[2];
+    lp_rescale_kernel<<<(n3 + 255) / 256, 256, 0, st>>>(lp->master + lp->off[2], n3, lp->sc + 2);
+    LP_CHECK(cudaGetLastError());
+    lp->prepped = false;
+  }
   for (int ep = 0; ep < epochs; ++ep) {
     for (int i = npairs - 1; i > 0; --i) {
       const int j = (int)(splitmix(s) % (uint64_t)(i + 1));

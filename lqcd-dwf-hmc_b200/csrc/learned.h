@@ -52,5 +52,7 @@ int lp_apply_internal(b200_lp* lp, void* z_f32, const void* r_f32, cudaStream_t 
 // Accessors into the operator plan for learned.cu.
 int plan_geometry(b200_dwf* op, Geom* g, float bc[4]);
 int plan_links_f32(b200_dwf* op, const void** links, cudaStream_t st);
+// v = DdagD w on FP32 fields of the plan (the operator's own kernels).
+int plan_apply_ddagd(b200_dwf* op, void* v, const void* w, cudaStream_t st);
 
 }  // namespace b200

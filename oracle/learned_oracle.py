@@ -17,7 +17,9 @@ Definition (per parity p of the even/odd 5D half lattice, fields shaped
   (11, Cout, Cin) acting on channels only.
   N(r): y1e = L1(r, -), y1o = L1(-, r), y2e = L2(y1e, y1o), y2o = L2(y1o, y1e),
         N(r) = y3e = L3(y2e, y2o).
-  loss(r, e) = |N(r) - e|^2 / |e|^2; gradient G = dL/dRe W + i dL/dIm W.
+  loss(r, e) = |A (N(r) - e)|^2 / |r|^2 for a pair with A e = r, A = DdagD
+  (the error of N in the residual norm); gradient G = dL/dRe W + i dL/dIm W,
+  with dL/dy = 2 A A (N(r) - e) / |r|^2 (A Hermitian).
 Site order within a parity: x/2 + Nx/2*(y + Ny*(z + Nz*t)) (index_eo.h of
 the reference); spinor fields in the reference host layout
 Field(24, Vh, Ls): ri + 2*(color + 3*spin) + 24*(site + Vh*s).
@@ -145,13 +147,14 @@ def grad_w(geo, p_out, delta, same, other, cin):
     return G
 
 
-def loss_and_grad(geo, Ws, r, e):
+def loss_and_grad(geo, Ws, r, e, A):
+    """A: the Hermitian operator DdagD as a function on (Vh, Ls, 4, 3) fields."""
     W1, W2, W3 = Ws
     y3, (y1e, y1o, y2e, y2o) = forward(geo, Ws, r)
-    e2 = np.vdot(e, e).real
-    d = y3 - e
-    loss = np.vdot(d, d).real / e2
-    d3 = 2.0 * d / e2
+    rr = np.vdot(r, r).real
+    d = A(y3 - e)
+    loss = np.vdot(d, d).real / rr
+    d3 = 2.0 * A(d) / rr
     G3 = grad_w(geo, 0, d3, y2e, y2o, W3.shape[2])
     A3 = adjoint_weights(W3)
     d2e = layer(geo, A3, 0, d3, None)

@@ -13,6 +13,15 @@ LS = 4
 H = 8
 
 
+def ddagd(u):
+    """DdagD of the operator oracle (pinned to the reference) on network fields."""
+    from oracle.oracle import OracleDWF
+    ora = OracleDWF(LAT, LS, 0.05, 1.8)
+    ora.set_links(u)
+    vh = int(np.prod(LAT)) // 2
+    return lambda a: lo.spinor_to_act(ora.mult("DdagD", lo.act_to_spinor(a)), vh, LS)
+
+
 def setup(seed=3, kind="hot"):
     u = synth.gauge_field(LAT, 200 + seed, kind)
     geo = lo.Geometry(LAT, u, bc=(1, 1, 1, -1))
@@ -26,8 +35,9 @@ def setup(seed=3, kind="hot"):
 
 
 def test_gradient_matches_finite_differences():
-    _, geo, Ws, r, e = setup()
-    loss, G, _ = lo.loss_and_grad(geo, Ws, r, e)
+    u, geo, Ws, r, e = setup()
+    A = ddagd(u)
+    loss, G, _ = lo.loss_and_grad(geo, Ws, r, e, A)
     rng = np.random.default_rng(11)
     h = 1e-6
     for layer in range(3):
@@ -38,8 +48,8 @@ def test_gradient_matches_finite_differences():
                 Wm = [w.copy() for w in Ws]
                 Wp[layer][idx] += h * unit
                 Wm[layer][idx] -= h * unit
-                lp_, _, _ = lo.loss_and_grad(geo, Wp, r, e)
-                lm_, _, _ = lo.loss_and_grad(geo, Wm, r, e)
+                lp_, _, _ = lo.loss_and_grad(geo, Wp, r, e, A)
+                lm_, _, _ = lo.loss_and_grad(geo, Wm, r, e, A)
                 fd = (lp_ - lm_) / (2 * h)
                 an = G[layer][idx].real if part == "re" else G[layer][idx].imag
                 assert abs(fd - an) <= 1e-6 * max(1.0, abs(an)), (layer, idx, part, fd, an)
