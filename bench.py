@@ -53,6 +53,13 @@ def parse():
     ap.add_argument("--no-solvers", action="store_true",
                     help="skip the mixed-precision Richardson and multishift timings")
     ap.add_argument("--lattice", type=int, nargs=4, default=LATTICE)
+    ap.add_argument("--no-learned", action="store_true",
+                    help="skip training and timing the learned preconditioner")
+    ap.add_argument("--learned-configs", type=int, default=4,
+                    help="gauge configurations the network is trained on")
+    ap.add_argument("--learned-pairs", type=int, default=16,
+                    help="(residual, error) pairs per configuration")
+    ap.add_argument("--learned-epochs", type=int, default=2)
     return ap.parse_args()
 
 
@@ -204,6 +211,72 @@ def reference_arm(args, rank, world):
     print(json.dumps(line))
 
 
+# ------------------------------------------------------------------ learned preconditioner
+def learned_section(op, lattice, w, u_workload, args):
+    """Train the gauge-covariant network on CG (residual, error) pairs of
+    seeded configurations (near-unit links + 2 stout steps, other seeds than
+    the workload's) and compare flexible CG with it against plain FP64 CG on
+    the workload configuration and RHS, both to |r|/|b| < 1e-10."""
+    import torch
+    import b200dwf
+    from b200dwf import synth
+    lp = b200dwf.LearnedPrecond(op, hidden=8, seed=11)
+    sm = b200dwf.StoutSmear(lattice, 0.1, 2)
+    losses = []
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    npairs = 0
+    for c in range(args.learned_configs):
+        sm.set_config(synth.gauge_field(lattice, SEED_U + 1000 + c, "near", 0.3))
+        op.set_config(sm.config(2))
+        b = op.new_field(0)
+        op.convert(b, synth.spinor_field(lattice, LS, SEED_B + 1000 + c))
+        n_ref, _, _ = op.cg(op.new_field(0), b, 1e-20, 20000)
+        iters = sorted(set(int(v) for v in np.linspace(2, max(3, n_ref - 2), args.learned_pairs)))
+        rs, es = b200dwf.cg_training_pairs(op, b, iters)
+        npairs += len(rs)
+        losses.append(lp.train(rs, es, args.learned_epochs, 3e-3, seed=c + 1))
+        del rs, es
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    op.set_config(u_workload)
+    # network apply alone, CUDA events
+    r32 = op.new_field(1)
+    z32 = op.new_field(1)
+    op.copy_convert(r32, w)
+    lp.apply(z32, r32)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(10):
+        lp.apply(z32, r32)
+    ev1.record()
+    torch.cuda.synchronize()
+    t_apply = ev0.elapsed_time(ev1) / 10 / 1e3
+    res = {}
+    for name, fn in (("cg_f64", lambda x: op.cg(x, w, 1e-20, 20000)),
+                     ("fcg_learned", lambda x: op.fcg(x, w, lp, 1e-20, 20000, 8))):
+        x = op.new_field(0)
+        torch.cuda.synchronize()
+        c0 = time.perf_counter()
+        out = fn(x)
+        torch.cuda.synchronize()
+        c1 = time.perf_counter()
+        if name == "cg_f64":
+            res[name] = {"iterations": out[0], "true_rel_residual": out[1], "seconds": c1 - c0,
+                         "converged": out[2] == 0}
+        else:
+            res[name] = {"iterations": out[0], "fallback_cg_iterations": out[1],
+                         "true_rel_residual": out[2], "seconds": c1 - c0, "converged": out[3] == 0}
+    return {"network": "3 layers, 4->8->4 channels per color, 11 paths, BF16 weights, FP32 accumulate",
+            "train_configs": args.learned_configs, "train_pairs": npairs,
+            "epochs_per_config": args.learned_epochs,
+            "loss_first_last_per_config": losses, "train_seconds": t_train,
+            "apply_ms": t_apply * 1e3, "tol_rel_residual": 1e-10, **res,
+            "iteration_ratio": res["cg_f64"]["iterations"] / max(1, res["fcg_learned"]["iterations"]
+                                                                 + res["fcg_learned"]["fallback_cg_iterations"]),
+            "time_ratio": res["cg_f64"]["seconds"] / res["fcg_learned"]["seconds"]}
+
+
 # ------------------------------------------------------------------ B200 arm
 def b200_arm(args, rank, world, local_rank):
     import torch
@@ -339,6 +412,10 @@ def b200_arm(args, rank, world, local_rank):
                                  "converged": rc == 0}
         del xs
 
+    learned = None
+    if not args.no_learned:
+        learned = learned_section(op, lattice, w, u, args)
+
     if rank != 0:
         return
     cpu = None
@@ -369,6 +446,7 @@ def b200_arm(args, rank, world, local_rank):
                 "d2h_bytes_per_step": 2 * nbytes},
         "cg_f64": cg,
         "solvers": solvers,
+        "learned_preconditioner": learned,
         "autotune": b200dwf.tuning_table().strip().splitlines(),
         "cpu_baseline": cpu,
     }
