@@ -189,6 +189,22 @@ __device__ __forceinline__ void apply_f(const ChainCoef<R>& k, R* x) {
 template <typename R> struct TileStride { static constexpr int v = 26; };
 template <> struct TileStride<float> { static constexpr int v = 28; };
 
+// Elements between the tiles of consecutive sites g of a warp: LS rows plus a
+// pad that puts site g+1's columns half a bank cycle away from site g's, so
+// the column walks of tile_chiral for two sites do not collide.
+template <typename R, int LS> struct TileGroup {
+  static constexpr int rows = LS * TileStride<R>::v;
+  static constexpr int mod = sizeof(R) == 8 ? 16 : 32;       // elements per bank cycle
+  static constexpr int target = sizeof(R) == 8 ? 12 : 16;
+  static constexpr int v = rows + ((target - rows % mod) % mod + mod) % mod;
+};
+template <typename R, int LS, int G> struct TileWarp { static constexpr int v = G * TileGroup<R, LS>::v; };
+
+template <typename R, int LS>
+__device__ __forceinline__ R* tile_row(R* tile, int g, int s) {
+  return tile + g * TileGroup<R, LS>::v + s * TileStride<R>::v;
+}
+
 __device__ __forceinline__ void tile_put(double* row, const double* v) {
 #pragma unroll
   for (int k = 0; k < 12; ++k) reinterpret_cast<double2*>(row)[k] = make_double2(v[2 * k], v[2 * k + 1]);
@@ -224,7 +240,7 @@ __device__ __forceinline__ void tile_chiral(R* tile, int lane, Op op) {
     const int r = u - 12 * g;
     const int pair = r / 6;
     const int cr = r - 6 * pair;
-    R* t = tile + g * LS * TS + 6 * pair + cr;
+    R* t = tile + g * TileGroup<R, LS>::v + 6 * pair + cr;
     R xp[LS], xm[LS];
 #pragma unroll
     for (int s = 0; s < LS; ++s) {

@@ -238,10 +238,37 @@ __device__ __forceinline__ void hop_epilogue(const HopParams& p, const ChainCoef
   if (EPI == EPI_HALF) {
 #pragma unroll
     for (int i = 0; i < 24; ++i) o1[i] = R(-0.5) * acc[i];
+  } else if (EPI == EPI_DDAGEO || EPI == EPI_K4N) {
+    // c * M5^+ g5 acc (c = -1/2 or +1/2): in the chiral basis M5^+ couples s
+    // only to s+1 (x+) or s-1 (x-) of the same site, whose values sit in the
+    // neighbouring lanes, so the chain is two warp shuffles per component and
+    // needs no shared-memory tile.  Coefficients as in chain_m5dag, with the
+    // g5 sign, the 1/2 of the back transform and c folded in.
+    const R c = (EPI == EPI_DDAGEO) ? R(-0.5) : R(0.5);
+    const int sp = (s + 1 == LS) ? 0 : s + 1;
+    const int sm = (s == 0) ? LS - 1 : s - 1;
+    const R wf0 = (s == LS - 1) ? R(1) : k.alpha;
+    const R wf1 = (s == 0) ? R(1) : k.alpha;
+    const R fdn = (sp == 0) ? k.mhalf_mq : k.half_alpha;
+    const R fup = (sm == LS - 1) ? k.mhalf_mq : k.half_alpha;
+    const R hc = R(0.5) * c;
+    const R a0 = hc * k.wb[s] * wf0, b0 = hc * k.wc2[sp] * fdn;
+    const R a1 = -hc * k.wb[s] * wf1, b1 = -hc * k.wc2[sm] * fup;
+    const int lup = g * LS + sp, ldn = g * LS + sm;
+#pragma unroll
+    for (int i = 0; i < 12; ++i) {
+      const R xp = acc[i] + acc[i + 12];
+      const R xm = acc[i] - acc[i + 12];
+      const R xpu = __shfl_sync(0xffffffffu, xp, lup);
+      const R xmd = __shfl_sync(0xffffffffu, xm, ldn);
+      const R yp = fma(a0, xp, b0 * xpu);
+      const R ym = fma(a1, xm, b1 * xmd);
+      o1[i] = yp + ym;
+      o1[i + 12] = yp - ym;
+    }
   } else {
     if (g < G) {
-#pragma unroll
-      tile_put(tile + (g * LS + s) * TileStride<R>::v, acc);
+      tile_put(tile_row<R, LS>(tile, g, s), acc);
     }
     __syncwarp();
     tile_chiral<R, LS, G>(tile, lane, [&](R* xp, R* xm) {
@@ -250,8 +277,7 @@ __device__ __forceinline__ void hop_epilogue(const HopParams& p, const ChainCoef
     });
     __syncwarp();
     if (g < G) {
-#pragma unroll
-      tile_get(tile + (g * LS + s) * TileStride<R>::v, o1);
+      tile_get(tile_row<R, LS>(tile, g, s), o1);
     }
   }
 
@@ -290,8 +316,7 @@ __device__ __forceinline__ void hop_epilogue(const HopParams& p, const ChainCoef
   if (FK != F_NONE) {
     __syncwarp();
     if (g < G) {
-#pragma unroll
-      tile_put(tile + (g * LS + s) * TileStride<R>::v, o1);
+      tile_put(tile_row<R, LS>(tile, g, s), o1);
     }
     __syncwarp();
     tile_chiral<R, LS, G>(tile, lane, [&](R* xp, R* xm) {
@@ -301,8 +326,7 @@ __device__ __forceinline__ void hop_epilogue(const HopParams& p, const ChainCoef
     __syncwarp();
     if (active) {
       R o2[24];
-#pragma unroll
-      tile_get(tile + (g * LS + s) * TileStride<R>::v, o2);
+      tile_get(tile_row<R, LS>(tile, g, s), o2);
       St::store(p.out2, vh, LS, site, s, o2);
     }
   }
@@ -338,7 +362,7 @@ dwf_hop_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename Sto
   constexpr bool kTile = (EPI != EPI_HALF) || (FK != F_NONE);
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  R* tile_all = reinterpret_cast<R*>(smem_raw);        // WARPS * G * LS * TileStride
+  R* tile_all = reinterpret_cast<R*>(smem_raw);        // WARPS * TileWarp
   __shared__ double red_warp[WARPS];
 
   const int tid = threadIdx.x;
@@ -417,7 +441,7 @@ dwf_hop_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename Sto
 #undef B200_HOP_DIR
   }
 
-  hop_epilogue<LS, P, EPI, FK>(p, k, acc, tile_all + (size_t)warp * G * LS * TileStride<R>::v, red_warp, tid, lane,
+  hop_epilogue<LS, P, EPI, FK>(p, k, acc, tile_all + (size_t)warp * TileWarp<R, LS, G>::v, red_warp, tid, lane,
                                warp, g, s, site, active);
 }
 
@@ -439,9 +463,9 @@ template <int LS, int P, int LF> struct TmaGeom {
   template <int S> static constexpr int warp_bytes() {
     // stages, and the epilogue tile (reuses the stage area)
     using R = typename Store<P>::R;
-    return (S * G * SLOT > G * LS * TileStride<R>::v * (int)sizeof(R))
+    return (S * G * SLOT > TileWarp<R, LS, G>::v * (int)sizeof(R))
                ? S * G * SLOT
-               : G * LS * TileStride<R>::v * (int)sizeof(R);
+               : TileWarp<R, LS, G>::v * (int)sizeof(R);
   }
 };
 
@@ -600,7 +624,7 @@ constexpr size_t hop_tma_smem_bytes() {
 template <int LS, int P>
 constexpr size_t hop_smem_bytes() {
   using R = typename Store<P>::R;
-  return sizeof(R) * (4 * (32 / LS) * LS * TileStride<R>::v);
+  return sizeof(R) * (4 * TileWarp<R, LS, 32 / LS>::v);
 }
 
 }  // namespace b200

@@ -93,7 +93,7 @@ sop_kernel(SopParams p, const __grid_constant__ ChainCoef<typename Store<P>::R> 
   const int site = (blockIdx.x * WARPS + warp) * G + g;
   const bool active = (g < G) && (site < p.g.vh);
   const size_t vh = p.g.vh;
-  R* tile = tile_all + warp * G * LS * TileStride<R>::v;
+  R* tile = tile_all + warp * TileWarp<R, LS, G>::v;
 
   R v[24];
 #pragma unroll
@@ -101,8 +101,7 @@ sop_kernel(SopParams p, const __grid_constant__ ChainCoef<typename Store<P>::R> 
   if (active && p.in) St::load(p.in, vh, LS, site, s, v);
   if (OPA != SOP_ID) {
     if (g < G) {
-#pragma unroll
-      tile_put(tile + (g * LS + s) * TileStride<R>::v, v);
+      tile_put(tile_row<R, LS>(tile, g, s), v);
     }
     __syncwarp();
     tile_chiral<R, LS, G>(tile, lane, [&](R* xp, R* xm) {
@@ -111,8 +110,7 @@ sop_kernel(SopParams p, const __grid_constant__ ChainCoef<typename Store<P>::R> 
     });
     __syncwarp();
     if (g < G) {
-#pragma unroll
-      tile_get(tile + (g * LS + s) * TileStride<R>::v, v);
+      tile_get(tile_row<R, LS>(tile, g, s), v);
     }
   }
   double nrm = 0.0;
@@ -143,8 +141,7 @@ sop_kernel(SopParams p, const __grid_constant__ ChainCoef<typename Store<P>::R> 
   if (OPB != SOP_ID) {
     __syncwarp();
     if (g < G) {
-#pragma unroll
-      tile_put(tile + (g * LS + s) * TileStride<R>::v, v);
+      tile_put(tile_row<R, LS>(tile, g, s), v);
     }
     __syncwarp();
     tile_chiral<R, LS, G>(tile, lane, [&](R* xp, R* xm) {
@@ -154,8 +151,7 @@ sop_kernel(SopParams p, const __grid_constant__ ChainCoef<typename Store<P>::R> 
     __syncwarp();
     if (active) {
       R o2[24];
-#pragma unroll
-      tile_get(tile + (g * LS + s) * TileStride<R>::v, o2);
+      tile_get(tile_row<R, LS>(tile, g, s), o2);
       St::store(p.out2, vh, LS, site, s, o2);
     }
   }
@@ -165,7 +161,7 @@ sop_kernel(SopParams p, const __grid_constant__ ChainCoef<typename Store<P>::R> 
 template <int LS, int P, int OPA, int OPB>
 cudaError_t run_sop(const SopParams& p, const ChainCoefs& c, cudaStream_t st) {
   using R = typename Store<P>::R;
-  constexpr size_t smem = sizeof(R) * (4 * (32 / LS) * LS * TileStride<R>::v);
+  constexpr size_t smem = sizeof(R) * (4 * TileWarp<R, LS, 32 / LS>::v);
   auto k = sop_kernel<LS, P, OPA, OPB>;
   static bool attr_done = false;
   if (!attr_done) {
@@ -240,7 +236,7 @@ cg_update_kernel(CgUpdParams p, const __grid_constant__ ChainCoef<typename Store
   const int site = (blockIdx.x * WARPS + warp) * G + g;
   const bool active = (g < G) && (site < p.g.vh);
   const size_t vh = p.g.vh;
-  R* tile = tile_all + warp * G * LS * TileStride<R>::v;
+  R* tile = tile_all + warp * TileWarp<R, LS, G>::v;
   R pv[24];
 #pragma unroll
   for (int i = 0; i < 24; ++i) pv[i] = 0;
@@ -259,8 +255,7 @@ cg_update_kernel(CgUpdParams p, const __grid_constant__ ChainCoef<typename Store
     St::store(p.p, vh, LS, site, s, pv);
   }
   if (g < G) {
-#pragma unroll
-    tile_put(tile + (g * LS + s) * TileStride<R>::v, pv);
+    tile_put(tile_row<R, LS>(tile, g, s), pv);
   }
   __syncwarp();
   tile_chiral<R, LS, G>(tile, lane, [&](R* xp, R* xm) {
@@ -270,8 +265,7 @@ cg_update_kernel(CgUpdParams p, const __grid_constant__ ChainCoef<typename Store
   __syncwarp();
   if (active) {
     R o[24];
-#pragma unroll
-    tile_get(tile + (g * LS + s) * TileStride<R>::v, o);
+    tile_get(tile_row<R, LS>(tile, g, s), o);
     St::store(p.y, vh, LS, site, s, o);
   }
 }
@@ -279,7 +273,7 @@ cg_update_kernel(CgUpdParams p, const __grid_constant__ ChainCoef<typename Store
 template <int LS, int P>
 cudaError_t run_cgu(const CgUpdParams& p, const ChainCoefs& c, cudaStream_t st) {
   using R = typename Store<P>::R;
-  constexpr size_t smem = sizeof(R) * (4 * (32 / LS) * LS * TileStride<R>::v);
+  constexpr size_t smem = sizeof(R) * (4 * TileWarp<R, LS, 32 / LS>::v);
   auto k = cg_update_kernel<LS, P>;
   static bool attr_done = false;
   if (!attr_done) {
@@ -335,7 +329,7 @@ ms_update_kernel(MsUpdParams p, const __grid_constant__ ChainCoef<typename Store
   const int site = (blockIdx.x * WARPS + warp) * G + g;
   const bool active = (g < G) && (site < p.g.vh);
   const size_t vh = p.g.vh;
-  R* tile = tile_all + warp * G * LS * TileStride<R>::v;
+  R* tile = tile_all + warp * TileWarp<R, LS, G>::v;
   const int nact = (int)p.st[MS_NACT];
   const R beta = (R)p.st[MS_BETA], alpha = (R)p.st[MS_ALPHA];
   R rv[24], pv[24];
@@ -357,8 +351,7 @@ ms_update_kernel(MsUpdParams p, const __grid_constant__ ChainCoef<typename Store
     St::store(p.ps[0], vh, LS, site, s, pv);
   }
   if (g < G) {
-#pragma unroll
-    tile_put(tile + (g * LS + s) * TileStride<R>::v, pv);
+    tile_put(tile_row<R, LS>(tile, g, s), pv);
   }
   __syncwarp();
   tile_chiral<R, LS, G>(tile, lane, [&](R* xp, R* xm) {
@@ -368,8 +361,7 @@ ms_update_kernel(MsUpdParams p, const __grid_constant__ ChainCoef<typename Store
   __syncwarp();
   if (active) {
     R o[24];
-#pragma unroll
-    tile_get(tile + (g * LS + s) * TileStride<R>::v, o);
+    tile_get(tile_row<R, LS>(tile, g, s), o);
     St::store(p.y0, vh, LS, site, s, o);
   }
   block_reduce_store(nrm, p.red);
@@ -399,7 +391,7 @@ ms_update_kernel(MsUpdParams p, const __grid_constant__ ChainCoef<typename Store
 template <int LS, int P>
 cudaError_t run_msu(const MsUpdParams& p, const ChainCoefs& c, cudaStream_t st) {
   using R = typename Store<P>::R;
-  constexpr size_t smem = sizeof(R) * (4 * (32 / LS) * LS * TileStride<R>::v);
+  constexpr size_t smem = sizeof(R) * (4 * TileWarp<R, LS, 32 / LS>::v);
   auto k = ms_update_kernel<LS, P>;
   static bool attr_done = false;
   if (!attr_done) {
