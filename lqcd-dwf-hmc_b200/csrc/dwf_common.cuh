@@ -76,6 +76,10 @@ template <> struct Store<PREC_F32> {
       v[4 * k] = c.x; v[4 * k + 1] = c.y; v[4 * k + 2] = c.z; v[4 * k + 3] = c.w;
     }
   }
+  __device__ static void load_col_raw(const void* col, int ls, int s, R* v, float* sc) {
+    load_col(col, ls, s, v);
+    *sc = 1.f;
+  }
   __device__ static void load(const void* base, size_t vh, int ls, int site, int s, R* v) {
     const float4* p = reinterpret_cast<const float4*>(base) + (size_t)site * K * ls;
 #pragma unroll
@@ -83,6 +87,11 @@ template <> struct Store<PREC_F32> {
       float4 c = __ldg(p + k * ls + s);
       v[4 * k] = c.x; v[4 * k + 1] = c.y; v[4 * k + 2] = c.z; v[4 * k + 3] = c.w;
     }
+  }
+  // unscaled components and the slice's scale (1 for this unscaled storage)
+  __device__ static void load_raw(const void* base, size_t vh, int ls, int site, int s, R* v, float* sc) {
+    load(base, vh, ls, site, s, v);
+    *sc = 1.f;
   }
   __device__ static void store(void* base, size_t vh, int ls, int site, int s, const R* v) {
     float4* p = reinterpret_cast<float4*>(base) + (size_t)site * K * ls;
@@ -140,6 +149,19 @@ template <typename H> struct StoreHalf {
     const float sc = reinterpret_cast<const float*>(p + K * ls)[s];
     decode(p, sc, ls, s, v);
   }
+  // stored components without their scale, and the scale of slice s
+  __device__ static void load_col_raw(const void* col, int ls, int s, R* v, float* sc) {
+    const uint4* p = reinterpret_cast<const uint4*>(col);
+    *sc = reinterpret_cast<const float*>(p + K * ls)[s];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      uint4 c = p[k * ls + s];
+      float2 a = HalfOps<H>::to2(c.x), b = HalfOps<H>::to2(c.y);
+      float2 d = HalfOps<H>::to2(c.z), e = HalfOps<H>::to2(c.w);
+      v[8 * k + 0] = a.x; v[8 * k + 1] = a.y; v[8 * k + 2] = b.x; v[8 * k + 3] = b.y;
+      v[8 * k + 4] = d.x; v[8 * k + 5] = d.y; v[8 * k + 6] = e.x; v[8 * k + 7] = e.y;
+    }
+  }
   __device__ static void load(const void* base, size_t vh, int ls, int site, int s, R* v) {
     const unsigned char* colp = reinterpret_cast<const unsigned char*>(base) + (size_t)site * col_bytes(ls);
     const uint4* p = reinterpret_cast<const uint4*>(colp);
@@ -153,6 +175,20 @@ template <typename H> struct StoreHalf {
       v[8 * k + 2] = b.x * sc; v[8 * k + 3] = b.y * sc;
       v[8 * k + 4] = d.x * sc; v[8 * k + 5] = d.y * sc;
       v[8 * k + 6] = e.x * sc; v[8 * k + 7] = e.y * sc;
+    }
+  }
+  // stored components without their scale, and the scale of slice s
+  __device__ static void load_raw(const void* base, size_t vh, int ls, int site, int s, R* v, float* sc) {
+    const unsigned char* colp = reinterpret_cast<const unsigned char*>(base) + (size_t)site * col_bytes(ls);
+    const uint4* p = reinterpret_cast<const uint4*>(colp);
+    *sc = __ldg(reinterpret_cast<const float*>(p + K * ls) + s);
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      uint4 c = __ldg(p + k * ls + s);
+      float2 a = HalfOps<H>::to2(c.x), b = HalfOps<H>::to2(c.y);
+      float2 d = HalfOps<H>::to2(c.z), e = HalfOps<H>::to2(c.w);
+      v[8 * k + 0] = a.x; v[8 * k + 1] = a.y; v[8 * k + 2] = b.x; v[8 * k + 3] = b.y;
+      v[8 * k + 4] = d.x; v[8 * k + 5] = d.y; v[8 * k + 6] = e.x; v[8 * k + 7] = e.y;
     }
   }
   __device__ static void store(void* base, size_t vh, int ls, int site, int s, const R* v) {

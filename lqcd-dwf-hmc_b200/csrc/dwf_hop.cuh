@@ -221,29 +221,36 @@ struct HopParams {
   double bc[4];
 };
 
-// Epilogue shared by both hop kernels: chain E on the site column, axpy with
+// Epilogue shared by the hop kernels: chain E on the site column, axpy with
 // up to three fields, store o1, optional F map -> o2, |o1|^2 block partials.
-template <int LS, int P, int EPI, int FK>
-__device__ __forceinline__ void hop_epilogue(const HopParams& p, const ChainCoef<typename Store<P>::R>& k,
-                                             typename Store<P>::R* acc,
-                                             typename Store<P>::R* tile, double* red_warp,
-                                             int tid, int lane, int warp, int g, int s, int site,
-                                             bool active) {
+// Each thread finishes NR rows (slices srow[r]) of its site; GT sites per warp.
+// With NR = 2 a block covers the sites of two one-row blocks and writes its
+// |o1|^2 partial to red[2*block] (and zero to red[2*block + 1]), so the host
+// reduces the same number of partials for either kernel shape.
+template <int LS, int P, int EPI, int FK, int NR, int GT>
+__device__ __forceinline__ void hop_epilogue_rows(const HopParams& p,
+                                                  const ChainCoef<typename Store<P>::R>& k,
+                                                  typename Store<P>::R (*acc)[24],
+                                                  typename Store<P>::R* tile, double* red_warp,
+                                                  int tid, int lane, int warp, int g,
+                                                  const int* srow, int site, bool active) {
   using St = Store<P>;
   using R = typename St::R;
-  constexpr int G = 32 / LS;
   constexpr int WARPS = 4;
   const size_t vh = p.vh;
-  R o1[24];
+  R o1[NR][24];
   if (EPI == EPI_HALF) {
 #pragma unroll
-    for (int i = 0; i < 24; ++i) o1[i] = R(-0.5) * acc[i];
-  } else if (EPI == EPI_DDAGEO || EPI == EPI_K4N) {
+    for (int r = 0; r < NR; ++r)
+#pragma unroll
+      for (int i = 0; i < 24; ++i) o1[r][i] = R(-0.5) * acc[r][i];
+  } else if (NR == 1 && (EPI == EPI_DDAGEO || EPI == EPI_K4N)) {
     // c * M5^+ g5 acc (c = -1/2 or +1/2): in the chiral basis M5^+ couples s
     // only to s+1 (x+) or s-1 (x-) of the same site, whose values sit in the
     // neighbouring lanes, so the chain is two warp shuffles per component and
     // needs no shared-memory tile.  Coefficients as in chain_m5dag, with the
     // g5 sign, the 1/2 of the back transform and c folded in.
+    const int s = srow[0];
     const R c = (EPI == EPI_DDAGEO) ? R(-0.5) : R(0.5);
     const int sp = (s + 1 == LS) ? 0 : s + 1;
     const int sm = (s == 0) ? LS - 1 : s - 1;
@@ -257,77 +264,87 @@ __device__ __forceinline__ void hop_epilogue(const HopParams& p, const ChainCoef
     const int lup = g * LS + sp, ldn = g * LS + sm;
 #pragma unroll
     for (int i = 0; i < 12; ++i) {
-      const R xp = acc[i] + acc[i + 12];
-      const R xm = acc[i] - acc[i + 12];
+      const R xp = acc[0][i] + acc[0][i + 12];
+      const R xm = acc[0][i] - acc[0][i + 12];
       const R xpu = __shfl_sync(0xffffffffu, xp, lup);
       const R xmd = __shfl_sync(0xffffffffu, xm, ldn);
       const R yp = fma(a0, xp, b0 * xpu);
       const R ym = fma(a1, xm, b1 * xmd);
-      o1[i] = yp + ym;
-      o1[i + 12] = yp - ym;
+      o1[0][i] = yp + ym;
+      o1[0][i + 12] = yp - ym;
     }
   } else {
-    if (g < G) {
-      tile_put(tile_row<R, LS>(tile, g, s), acc);
+    if (g < GT) {
+#pragma unroll
+      for (int r = 0; r < NR; ++r) tile_put(tile_row<R, LS>(tile, g, srow[r]), acc[r]);
     }
     __syncwarp();
-    tile_chiral<R, LS, G>(tile, lane, [&](R* xp, R* xm) {
+    tile_chiral<R, LS, GT>(tile, lane, [&](R* xp, R* xm) {
       apply_epi<R, LS, 0, EPI>(k, xp);
       apply_epi<R, LS, 1, EPI>(k, xm);
     });
     __syncwarp();
-    if (g < G) {
-      tile_get(tile_row<R, LS>(tile, g, s), o1);
+    if (g < GT) {
+#pragma unroll
+      for (int r = 0; r < NR; ++r) tile_get(tile_row<R, LS>(tile, g, srow[r]), o1[r]);
     }
   }
 
   double nrm = 0.0;
   if (active) {
     const R ce = (R)(p.ce * (p.ce_dev ? *p.ce_dev : 1.0));
+    const R c1 = (R)(p.c_x1 * (p.c_x1_dev ? *p.c_x1_dev : 1.0));
+    const R c2 = (R)(p.c_x2 * (p.c_x2_dev ? *p.c_x2_dev : 1.0));
+    const R c3 = (R)(p.c_x3 * (p.c_x3_dev ? *p.c_x3_dev : 1.0));
 #pragma unroll
-    for (int i = 0; i < 24; ++i) o1[i] *= ce;
-    if (p.x1) {
-      R xv[24];
-      St::load(p.x1, vh, LS, site, s, xv);
-      const R c = (R)(p.c_x1 * (p.c_x1_dev ? *p.c_x1_dev : 1.0));
+    for (int r = 0; r < NR; ++r) {
+      const int s = srow[r];
 #pragma unroll
-      for (int i = 0; i < 24; ++i) o1[i] = fma(c, xv[i], o1[i]);
-    }
-    if (p.x2) {
-      R xv[24];
-      St::load(p.x2, vh, LS, site, s, xv);
-      const R c = (R)(p.c_x2 * (p.c_x2_dev ? *p.c_x2_dev : 1.0));
+      for (int i = 0; i < 24; ++i) o1[r][i] *= ce;
+      if (p.x1) {
+        R xv[24];
+        St::load(p.x1, vh, LS, site, s, xv);
 #pragma unroll
-      for (int i = 0; i < 24; ++i) o1[i] = fma(c, xv[i], o1[i]);
-    }
-    if (p.x3) {
-      R xv[24];
-      St::load(p.x3, vh, LS, site, s, xv);
-      const R c = (R)(p.c_x3 * (p.c_x3_dev ? *p.c_x3_dev : 1.0));
+        for (int i = 0; i < 24; ++i) o1[r][i] = fma(c1, xv[i], o1[r][i]);
+      }
+      if (p.x2) {
+        R xv[24];
+        St::load(p.x2, vh, LS, site, s, xv);
 #pragma unroll
-      for (int i = 0; i < 24; ++i) o1[i] = fma(c, xv[i], o1[i]);
-    }
-    if (p.out1) St::store(p.out1, vh, LS, site, s, o1);
-    if (p.red) {
+        for (int i = 0; i < 24; ++i) o1[r][i] = fma(c2, xv[i], o1[r][i]);
+      }
+      if (p.x3) {
+        R xv[24];
+        St::load(p.x3, vh, LS, site, s, xv);
 #pragma unroll
-      for (int i = 0; i < 24; ++i) nrm += (double)o1[i] * (double)o1[i];
+        for (int i = 0; i < 24; ++i) o1[r][i] = fma(c3, xv[i], o1[r][i]);
+      }
+      if (p.out1) St::store(p.out1, vh, LS, site, s, o1[r]);
+      if (p.red) {
+#pragma unroll
+        for (int i = 0; i < 24; ++i) nrm += (double)o1[r][i] * (double)o1[r][i];
+      }
     }
   }
   if (FK != F_NONE) {
     __syncwarp();
-    if (g < G) {
-      tile_put(tile_row<R, LS>(tile, g, s), o1);
+    if (g < GT) {
+#pragma unroll
+      for (int r = 0; r < NR; ++r) tile_put(tile_row<R, LS>(tile, g, srow[r]), o1[r]);
     }
     __syncwarp();
-    tile_chiral<R, LS, G>(tile, lane, [&](R* xp, R* xm) {
+    tile_chiral<R, LS, GT>(tile, lane, [&](R* xp, R* xm) {
       apply_f<R, LS, 0, FK>(k, xp);
       apply_f<R, LS, 1, FK>(k, xm);
     });
     __syncwarp();
     if (active) {
-      R o2[24];
-      tile_get(tile_row<R, LS>(tile, g, s), o2);
-      St::store(p.out2, vh, LS, site, s, o2);
+#pragma unroll
+      for (int r = 0; r < NR; ++r) {
+        R o2[24];
+        tile_get(tile_row<R, LS>(tile, g, srow[r]), o2);
+        St::store(p.out2, vh, LS, site, srow[r], o2);
+      }
     }
   }
   if (p.red) {
@@ -339,9 +356,28 @@ __device__ __forceinline__ void hop_epilogue(const HopParams& p, const ChainCoef
       double b = 0.0;
 #pragma unroll
       for (int w = 0; w < WARPS; ++w) b += red_warp[w];
-      p.red[blockIdx.x] = b;
+      if (NR == 1) {
+        p.red[blockIdx.x] = b;
+      } else {
+        const int nb1 = (p.vh + WARPS * (32 / LS) - 1) / (WARPS * (32 / LS));
+        p.red[2 * blockIdx.x] = b;
+        if (2 * (int)blockIdx.x + 1 < nb1) p.red[2 * blockIdx.x + 1] = 0.0;
+      }
     }
   }
+}
+
+template <int LS, int P, int EPI, int FK>
+__device__ __forceinline__ void hop_epilogue(const HopParams& p, const ChainCoef<typename Store<P>::R>& k,
+                                             typename Store<P>::R* acc,
+                                             typename Store<P>::R* tile, double* red_warp,
+                                             int tid, int lane, int warp, int g, int s, int site,
+                                             bool active) {
+  using R = typename Store<P>::R;
+  R (*rows)[24] = reinterpret_cast<R (*)[24]>(acc);
+  const int srow[1] = {s};
+  hop_epilogue_rows<LS, P, EPI, FK, 1, 32 / LS>(p, k, rows, tile, red_warp, tid, lane, warp, g, srow,
+                                                site, active);
 }
 
 // Occupancy variants (minimum resident 128-thread blocks per SM requested from
@@ -446,6 +482,198 @@ dwf_hop_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename Sto
 }
 
 // ---------------------------------------------------------------------------
+// Packed variant for FP32 arithmetic (f32, f16, bf16 storage).  One thread per
+// (site, slice pair): slices s0 = j and s1 = j + Ls/2 undergo exactly the same
+// operations (same links, same projections), so every value is held as a
+// float2 (value at s0, value at s1) and the hop runs on Blackwell's packed
+// FP32x2 instructions: the SU(3) products and the reconstruction issue half
+// the instructions of the one-slice kernel, and each link is loaded and its
+// third row rebuilt once per two slices.  The projection is done per slice in
+// scalar code so that its outputs land directly in the packed pairs; the
+// per-slice scale of f16/bf16 storage is applied to the projected pairs.
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+
+// out (half spinor pairs) = U h or U^+ h on both slices
+template <bool kDag>
+__device__ __forceinline__ void su3_mult_half2(const float* u, const float2* h, float2* o) {
+#pragma unroll
+  for (int a = 0; a < 2; ++a) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      float2 re = make_float2(0.f, 0.f), im = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const float ur = kDag ? u[2 * (i + 3 * j)] : u[2 * (j + 3 * i)];
+        const float ui = kDag ? -u[2 * (i + 3 * j) + 1] : u[2 * (j + 3 * i) + 1];
+        const float2 hr = h[6 * a + 2 * j], hi = h[6 * a + 2 * j + 1];
+        re = __ffma2_rn(f2(ur), hr, re);
+        re = __ffma2_rn(f2(-ui), hi, re);
+        im = __ffma2_rn(f2(ur), hi, im);
+        im = __ffma2_rn(f2(ui), hr, im);
+      }
+      o[6 * a + 2 * i] = re;
+      o[6 * a + 2 * i + 1] = im;
+    }
+  }
+}
+
+// acc (pairs) += ph * (1 - sign*gamma_mu)-shaped result; same algebra as
+// reconstruct_acc, the factor i only selects the re/im pair.
+template <int MU, int SIGN>
+__device__ __forceinline__ void reconstruct_acc2(float2* acc, const float2* o, float ph) {
+  const float2 pp = f2(ph);
+  const float2 sp = f2(SIGN > 0 ? ph : -ph);
+  const float2 sm = f2(SIGN > 0 ? -ph : ph);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const float2 a0r = o[2 * c], a0i = o[2 * c + 1];
+    const float2 a1r = o[6 + 2 * c], a1i = o[6 + 2 * c + 1];
+    float2* r0 = acc + 2 * c;
+    float2* r1 = acc + 2 * (c + 3);
+    float2* r2 = acc + 2 * (c + 6);
+    float2* r3 = acc + 2 * (c + 9);
+    if (MU == 3) {
+      if (SIGN > 0) {
+        r2[0] = __ffma2_rn(pp, a0r, r2[0]); r2[1] = __ffma2_rn(pp, a0i, r2[1]);
+        r3[0] = __ffma2_rn(pp, a1r, r3[0]); r3[1] = __ffma2_rn(pp, a1i, r3[1]);
+      } else {
+        r0[0] = __ffma2_rn(pp, a0r, r0[0]); r0[1] = __ffma2_rn(pp, a0i, r0[1]);
+        r1[0] = __ffma2_rn(pp, a1r, r1[0]); r1[1] = __ffma2_rn(pp, a1i, r1[1]);
+      }
+      continue;
+    }
+    r0[0] = __ffma2_rn(pp, a0r, r0[0]); r0[1] = __ffma2_rn(pp, a0i, r0[1]);
+    r1[0] = __ffma2_rn(pp, a1r, r1[0]); r1[1] = __ffma2_rn(pp, a1i, r1[1]);
+    if (MU == 0) {        // rows 2,3 = -+ i h1, -+ i h0
+      r2[0] = __ffma2_rn(sp, a1i, r2[0]); r2[1] = __ffma2_rn(sm, a1r, r2[1]);
+      r3[0] = __ffma2_rn(sp, a0i, r3[0]); r3[1] = __ffma2_rn(sm, a0r, r3[1]);
+    } else if (MU == 1) { // rows 2,3 = -+ h1, +- h0
+      r2[0] = __ffma2_rn(sm, a1r, r2[0]); r2[1] = __ffma2_rn(sm, a1i, r2[1]);
+      r3[0] = __ffma2_rn(sp, a0r, r3[0]); r3[1] = __ffma2_rn(sp, a0i, r3[1]);
+    } else {              // MU==2: rows 2,3 = -+ i h0, +- i h1
+      r2[0] = __ffma2_rn(sp, a0i, r2[0]); r2[1] = __ffma2_rn(sm, a0r, r2[1]);
+      r3[0] = __ffma2_rn(sm, a1i, r3[0]); r3[1] = __ffma2_rn(sp, a1r, r3[1]);
+    }
+  }
+}
+
+template <int LS, int P, int LF, int EPI, int FK, int MB>
+__global__ void __launch_bounds__(128, MB)
+dwf_hop_pair_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename Store<P>::R> k) {
+  using St = Store<P>;
+  using R = typename St::R;
+  static_assert(sizeof(R) == 4, "packed kernel is for FP32 arithmetic");
+  static_assert(32 % LS == 0 && LS % 2 == 0, "packed kernel needs Ls | 32");
+  constexpr bool kDagHop = EpiIsDag<EPI>::v;
+  constexpr int H = LS / 2;               // lanes per site
+  constexpr int G = 32 / H;               // sites per warp
+  constexpr int WARPS = 4;
+
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R* tile_all = reinterpret_cast<R*>(smem_raw);
+  __shared__ double red_warp[WARPS];
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const int g = lane / H;
+  const int j = lane - g * H;
+  const int site = (blockIdx.x * WARPS + warp) * G + g;
+  const bool active = (g < G) && (site < p.vh);
+  const size_t vh = p.vh;
+  const int s0 = j, s1 = j + H;
+
+  float2 acc[24];
+#pragma unroll
+  for (int i = 0; i < 24; ++i) acc[i] = make_float2(0.f, 0.f);
+
+  if (active) {
+    const int ix2 = site % p.nx2;
+    const int iyzt = site / p.nx2;
+    const int y = iyzt % p.ny;
+    const int izt = iyzt / p.ny;
+    const int z = izt % p.nz;
+    const int t = izt / p.nz;
+    const int keo = (p.ieo + y + z + t) & 1;
+    const int x = 2 * ix2 + keo;
+    const int nx = 2 * p.nx2;
+    const int ieo = p.ieo;
+
+#define B200_PAIR_HALF(MU, SIGN, NB, PH, LIDX)                                       \
+    {                                                                                \
+      float w0[24], w1[24], h0[12], h1[12], u[18];                                   \
+      float sc0, sc1;                                                                \
+      St::load_raw(p.in, vh, LS, NB, s0, w0, &sc0);                                  \
+      St::load_raw(p.in, vh, LS, NB, s1, w1, &sc1);                                  \
+      if (kDagHop) {                                                                 \
+        _Pragma("unroll") for (int q = 0; q < 12; ++q) {                             \
+          float t0 = w0[q]; w0[q] = w0[q + 12]; w0[q + 12] = t0;                     \
+          float t1 = w1[q]; w1[q] = w1[q + 12]; w1[q + 12] = t1; }                   \
+      }                                                                              \
+      project<float, MU, SIGN>(w0, h0);                                              \
+      project<float, MU, SIGN>(w1, h1);                                              \
+      float2 h[12], o[12];                                                           \
+      _Pragma("unroll") for (int q = 0; q < 12; ++q) h[q] = make_float2(h0[q], h1[q]); \
+      if (St::kScaled) {                                                             \
+        const float2 sc = make_float2(sc0, sc1);                                     \
+        _Pragma("unroll") for (int q = 0; q < 12; ++q) h[q] = __fmul2_rn(h[q], sc);  \
+      }                                                                              \
+      LinkLoad<LF>::load(p.links, LIDX, u);                                          \
+      su3_mult_half2<(SIGN < 0)>(u, h, o);                                           \
+      reconstruct_acc2<MU, SIGN>(acc, o, PH);                                        \
+    }
+
+#define B200_PAIR_DIR(MU, COORD, EXT, NBP, NBM)                                      \
+    {                                                                                \
+      const int nbp = NBP;                                                           \
+      const float php = (COORD == EXT - 1) ? (float)p.bc[MU] : 1.f;                  \
+      B200_PAIR_HALF(MU, 1, nbp, php, (size_t)(ieo + 2 * MU) * vh + site)            \
+      const int nbm = NBM;                                                           \
+      const float phm = (COORD == 0) ? (float)p.bc[MU] : 1.f;                        \
+      B200_PAIR_HALF(MU, -1, nbm, phm, (size_t)(1 - ieo + 2 * MU) * vh + nbm)        \
+    }
+
+    const int row = p.nx2 * iyzt;
+    B200_PAIR_DIR(0, x, nx,
+                  row + ((ix2 + keo == p.nx2) ? 0 : ix2 + keo),
+                  row + ((ix2 - 1 + keo < 0) ? p.nx2 - 1 : ix2 - 1 + keo));
+    const int sy = p.nx2;
+    B200_PAIR_DIR(1, y, p.ny,
+                  (y == p.ny - 1) ? site - (p.ny - 1) * sy : site + sy,
+                  (y == 0) ? site + (p.ny - 1) * sy : site - sy);
+    const int sz = p.nx2 * p.ny;
+    B200_PAIR_DIR(2, z, p.nz,
+                  (z == p.nz - 1) ? site - (p.nz - 1) * sz : site + sz,
+                  (z == 0) ? site + (p.nz - 1) * sz : site - sz);
+    const int st = p.nx2 * p.ny * p.nz;
+    B200_PAIR_DIR(3, t, p.nt,
+                  (t == p.nt - 1) ? site - (p.nt - 1) * st : site + st,
+                  (t == 0) ? site + (p.nt - 1) * st : site - st);
+#undef B200_PAIR_DIR
+#undef B200_PAIR_HALF
+  }
+
+  float rows[2][24];
+#pragma unroll
+  for (int i = 0; i < 24; ++i) { rows[0][i] = acc[i].x; rows[1][i] = acc[i].y; }
+  const int srow[2] = {s0, s1};
+  hop_epilogue_rows<LS, P, EPI, FK, 2, G>(p, k, rows, tile_all + (size_t)warp * TileWarp<R, LS, G>::v,
+                                          red_warp, tid, lane, warp, g, srow, site, active);
+}
+
+template <int LS, int P>
+constexpr size_t hop_pair_smem_bytes() {
+  using R = typename Store<P>::R;
+  return sizeof(R) * (4 * TileWarp<R, LS, 64 / LS>::v);
+}
+
+// Blocks of the packed kernel: 4 warps of 64/Ls sites each.
+inline int hop_pair_grid(int ls, int vh) {
+  const int per_block = 4 * (64 / ls);
+  return (vh + per_block - 1) / per_block;
+}
+
+// ---------------------------------------------------------------------------
 // TMA-staged variant.  Each warp keeps an S-deep pipeline over the 8 hop
 // directions: for every one of its G sites the lane with s == 0 issues two
 // bulk asynchronous copies per direction -- the neighbour site's whole
@@ -455,8 +683,8 @@ dwf_hop_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename Sto
 // flight, without holding registers.  Stage buffers are reused after the
 // warp's lanes have finished reading them (__syncwarp + proxy fence).
 // All waits are bounded; on timeout the kernel sets p.err and skips its work.
-template <int LS, int P, int LF> struct TmaGeom {
-  static constexpr int G = 32 / LS;
+template <int LS, int P, int LF, int GS = 32 / LS> struct TmaGeom {
+  static constexpr int G = GS;              // sites per warp
   static constexpr int COL = (int)Store<P>::col_bytes(LS);
   static constexpr int LNK = LinkLoad<LF>::kChunks * 16;
   static constexpr int SLOT = COL + LNK;                       // one site, one direction
@@ -614,6 +842,176 @@ dwf_hop_tma_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename
   if (!__syncthreads_and(ok ? 1 : 0)) return;
   hop_epilogue<LS, P, EPI, FK>(p, k, acc, reinterpret_cast<R*>(wbase), red_warp, tid, lane, warp, g, s,
                                site, active);
+}
+
+// TMA-staged packed kernel: the bulk-copy pipeline of dwf_hop_tma_kernel
+// (neighbour column + link per site and direction, S-deep per warp, bounded
+// mbarrier waits, device error word on timeout) feeding the two-slice FP32x2
+// arithmetic of dwf_hop_pair_kernel.  64/Ls sites per warp.
+template <int LS, int P, int LF, int EPI, int FK, int S, int MB>
+__global__ void __launch_bounds__(128, MB)
+dwf_hop_tma_pair_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename Store<P>::R> k) {
+  using St = Store<P>;
+  using R = typename St::R;
+  static_assert(sizeof(R) == 4, "packed kernel is for FP32 arithmetic");
+  static_assert(32 % LS == 0 && LS % 2 == 0, "packed kernel needs Ls | 32");
+  constexpr int H = LS / 2;
+  constexpr int G = 32 / H;
+  using TG = TmaGeom<LS, P, LF, G>;
+  constexpr bool kDagHop = EpiIsDag<EPI>::v;
+  constexpr int WARPS = 4;
+  constexpr int WB = TG::template warp_bytes<S>();
+  constexpr int WBA = (WB + 127) / 128 * 128;
+
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ double red_warp[WARPS];
+  __shared__ __align__(8) uint64_t bars[WARPS][S];
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const int g = lane / H;
+  const int j = lane - g * H;
+  const int site = (blockIdx.x * WARPS + warp) * G + g;
+  const bool active = (g < G) && (site < p.vh);
+  const bool issuer = (g < G) && (j == 0);
+  unsigned char* wbase = smem_raw + (size_t)warp * WBA;
+  const size_t vh = p.vh;
+  const int s0 = j, s1 = j + H;
+
+  if (lane == 0) {
+#pragma unroll
+    for (int st = 0; st < S; ++st) mbar_init(smem_u32(&bars[warp][st]), G);
+    mbar_fence_init();
+  }
+  __syncwarp();
+
+  int nb[8];
+  float ph[8];
+  if (active) {
+    const int ix2 = site % p.nx2;
+    const int iyzt = site / p.nx2;
+    const int y = iyzt % p.ny;
+    const int izt = iyzt / p.ny;
+    const int z = izt % p.nz;
+    const int t = izt / p.nz;
+    const int keo = (p.ieo + y + z + t) & 1;
+    const int x = 2 * ix2 + keo;
+    const int row = p.nx2 * iyzt;
+    nb[0] = row + ((ix2 + keo == p.nx2) ? 0 : ix2 + keo);
+    nb[1] = row + ((ix2 - 1 + keo < 0) ? p.nx2 - 1 : ix2 - 1 + keo);
+    ph[0] = (x == 2 * p.nx2 - 1) ? (float)p.bc[0] : 1.f;
+    ph[1] = (x == 0) ? (float)p.bc[0] : 1.f;
+    const int sy = p.nx2, sz = p.nx2 * p.ny, st4 = p.nx2 * p.ny * p.nz;
+    nb[2] = (y == p.ny - 1) ? site - (p.ny - 1) * sy : site + sy;
+    nb[3] = (y == 0) ? site + (p.ny - 1) * sy : site - sy;
+    ph[2] = (y == p.ny - 1) ? (float)p.bc[1] : 1.f;
+    ph[3] = (y == 0) ? (float)p.bc[1] : 1.f;
+    nb[4] = (z == p.nz - 1) ? site - (p.nz - 1) * sz : site + sz;
+    nb[5] = (z == 0) ? site + (p.nz - 1) * sz : site - sz;
+    ph[4] = (z == p.nz - 1) ? (float)p.bc[2] : 1.f;
+    ph[5] = (z == 0) ? (float)p.bc[2] : 1.f;
+    nb[6] = (t == p.nt - 1) ? site - (p.nt - 1) * st4 : site + st4;
+    nb[7] = (t == 0) ? site + (p.nt - 1) * st4 : site - st4;
+    ph[6] = (t == p.nt - 1) ? (float)p.bc[3] : 1.f;
+    ph[7] = (t == 0) ? (float)p.bc[3] : 1.f;
+  } else {
+#pragma unroll
+    for (int d = 0; d < 8; ++d) { nb[d] = 0; ph[d] = 0.f; }
+  }
+
+  auto col_ptr = [&](int st) { return wbase + (size_t)(st * G + g) * TG::SLOT; };
+  int nissued = 0;
+  auto issue = [&](int d, int st) {
+    ++nissued;
+    if (!issuer) return;
+    const uint32_t bar = smem_u32(&bars[warp][st]);
+    if (!active) { mbar_arrive(bar); return; }
+    const int mu = d >> 1;
+    const bool fwd = (d & 1) == 0;
+    const size_t lidx = fwd ? (size_t)(p.ieo + 2 * mu) * vh + site : (size_t)(1 - p.ieo + 2 * mu) * vh + nb[d];
+    unsigned char* dst = col_ptr(st);
+    mbar_arrive_expect_tx(bar, TG::SLOT);
+    bulk_g2s(smem_u32(dst), reinterpret_cast<const unsigned char*>(p.in) + (size_t)nb[d] * TG::COL,
+             TG::COL, bar);
+    bulk_g2s(smem_u32(dst + TG::COL), reinterpret_cast<const unsigned char*>(p.links) + lidx * TG::LNK,
+             TG::LNK, bar);
+  };
+
+#pragma unroll
+  for (int d = 0; d < S; ++d) issue(d, d);
+
+  float2 acc[24];
+#pragma unroll
+  for (int i = 0; i < 24; ++i) acc[i] = make_float2(0.f, 0.f);
+  bool ok = true;
+  int ndone = 0;
+
+#define B200_TMAP_STEP(D, MU, SIGN)                                                  \
+  {                                                                                  \
+    constexpr int st = (D) % S;                                                      \
+    const uint32_t parity = ((D) / S) & 1;                                           \
+    if (ok) {                                                                        \
+      const bool got = mbar_wait_bounded(smem_u32(&bars[warp][st]), parity);         \
+      ok = __all_sync(0xffffffffu, got);                                             \
+      if (ok) ndone = (D) + 1;                                                       \
+      else if (lane == 0 && p.err) atomicExch(p.err, 1);                             \
+    }                                                                                \
+    if (ok && active) {                                                              \
+      float w0[24], w1[24], h0[12], h1[12], u[18];                                   \
+      float sc0, sc1;                                                                \
+      const unsigned char* c = col_ptr(st);                                          \
+      St::load_col_raw(c, LS, s0, w0, &sc0);                                         \
+      St::load_col_raw(c, LS, s1, w1, &sc1);                                         \
+      if (kDagHop) {                                                                 \
+        _Pragma("unroll") for (int q = 0; q < 12; ++q) {                             \
+          float t0 = w0[q]; w0[q] = w0[q + 12]; w0[q + 12] = t0;                     \
+          float t1 = w1[q]; w1[q] = w1[q + 12]; w1[q + 12] = t1; }                   \
+      }                                                                              \
+      project<float, MU, SIGN>(w0, h0);                                              \
+      project<float, MU, SIGN>(w1, h1);                                              \
+      float2 h[12], o[12];                                                           \
+      _Pragma("unroll") for (int q = 0; q < 12; ++q) h[q] = make_float2(h0[q], h1[q]); \
+      if (St::kScaled) {                                                             \
+        const float2 sc = make_float2(sc0, sc1);                                     \
+        _Pragma("unroll") for (int q = 0; q < 12; ++q) h[q] = __fmul2_rn(h[q], sc);  \
+      }                                                                              \
+      LinkLoad<LF>::load_plain(c + TG::COL, u);                                      \
+      su3_mult_half2<(SIGN < 0)>(u, h, o);                                           \
+      reconstruct_acc2<MU, SIGN>(acc, o, ph[D]);                                     \
+    }                                                                                \
+    __syncwarp();                                                                    \
+    if ((D) + S < 8 && ok) {                                                         \
+      fence_proxy_async_smem();                                                      \
+      issue((D) + S, st);                                                            \
+    }                                                                                \
+  }
+
+  B200_TMAP_STEP(0, 0, 1)
+  B200_TMAP_STEP(1, 0, -1)
+  B200_TMAP_STEP(2, 1, 1)
+  B200_TMAP_STEP(3, 1, -1)
+  B200_TMAP_STEP(4, 2, 1)
+  B200_TMAP_STEP(5, 2, -1)
+  B200_TMAP_STEP(6, 3, 1)
+  B200_TMAP_STEP(7, 3, -1)
+#undef B200_TMAP_STEP
+
+  if (!ok) {
+    for (int d = ndone; d < nissued; ++d) mbar_wait_bounded(smem_u32(&bars[warp][d % S]), (d / S) & 1);
+  }
+  if (!__syncthreads_and(ok ? 1 : 0)) return;
+  float rows[2][24];
+#pragma unroll
+  for (int i = 0; i < 24; ++i) { rows[0][i] = acc[i].x; rows[1][i] = acc[i].y; }
+  const int srow[2] = {s0, s1};
+  hop_epilogue_rows<LS, P, EPI, FK, 2, G>(p, k, rows, reinterpret_cast<R*>(wbase), red_warp, tid, lane,
+                                          warp, g, srow, site, active);
+}
+
+template <int LS, int P, int LF, int S>
+constexpr size_t hop_tma_pair_smem_bytes() {
+  return (size_t)4 * ((TmaGeom<LS, P, LF, 64 / LS>::template warp_bytes<S>() + 127) / 128 * 128);
 }
 
 template <int LS, int P, int LF, int S>

@@ -178,7 +178,15 @@ SopParams sop_base(const b200_dwf* op) {
 // B200_AUTOTUNE=0 disables tuning (variant 0).  The first call of a
 // combination must not be inside a CUDA graph capture.
 typedef std::tuple<int, int, int, int, int> TuneKey;   // vh, ls, prec, epi, fk
-constexpr int kHopVariants = 5;   // direct, TMA 2-stage, TMA 3-stage, TMA 2-stage + direct at higher occupancy
+constexpr int kHopVariants = 9;   // direct, TMA 2-stage, TMA 3-stage, TMA 2-stage + direct at
+                                  // higher occupancy, packed two-slice FP32x2 (direct, TMA),
+                                  // 4-deep TMA, packed with all directions in flight
+
+bool variant_supported(int prec, int ls, int v) {
+  if (v < 5) return true;
+  if (v == 7 && prec == PREC_F64) return true;
+  return prec != PREC_F64 && 32 % ls == 0;
+}
 std::map<TuneKey, std::pair<int, float> > g_tune;
 std::mutex g_tune_mu;
 
@@ -203,6 +211,7 @@ int tune_hop(b200_dwf* op, int prec, const HopParams& p0, cudaStream_t st, int* 
   float best_ms = 1e30f;
   *best = 0;
   for (int v = 0; v < kHopVariants; ++v) {
+    if (!variant_supported(prec, op->g.ls, v)) continue;
     p.variant = v;
     B200_CHECK_CUDA(launch_hop(prec, p, op->coefs, st));
     B200_CHECK_CUDA(cudaEventRecord(a, st));
@@ -231,7 +240,7 @@ int forced_variant() {
 int run_hop(b200_dwf* op, int prec, HopParams& p, cudaStream_t st) {
   int variant = 0;
   const int fv = forced_variant();
-  if (fv >= 0) {
+  if (fv >= 0 && variant_supported(prec, op->g.ls, fv)) {
     variant = fv;
   } else if (tuning_enabled()) {
     const TuneKey key(op->g.vh, op->g.ls, prec, p.epi, p.fk);

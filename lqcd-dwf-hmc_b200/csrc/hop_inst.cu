@@ -55,15 +55,62 @@ cudaError_t run_tma(const HopParams& p, const ChainCoefs& c, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+template <int LS, int P, int EPI, int FK>
+cudaError_t run_pair(const HopParams& p, const ChainCoefs& c, cudaStream_t st) {
+  using R = typename Store<P>::R;
+  constexpr int LF = DefaultLink<P>::v;
+  constexpr size_t smem = hop_pair_smem_bytes<LS, P>();
+  auto k = dwf_hop_pair_kernel<LS, P, LF, EPI, FK, HopMinBlocks<P>::v0>;
+  static bool attr_done = false;
+  if (!attr_done) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr_done = true;
+  }
+  const ChainCoef<R>& kc = *reinterpret_cast<const ChainCoef<R>*>(&c.f);
+  k<<<hop_pair_grid(LS, p.vh), 128, smem, st>>>(p, kc);
+  return cudaGetLastError();
+}
+
+template <int LS, int P, int EPI, int FK, int S, int MB>
+cudaError_t run_tma_pair(const HopParams& p, const ChainCoefs& c, cudaStream_t st) {
+  using R = typename Store<P>::R;
+  constexpr int LF = DefaultLink<P>::v;
+  constexpr size_t smem = hop_tma_pair_smem_bytes<LS, P, LF, S>();
+  auto k = dwf_hop_tma_pair_kernel<LS, P, LF, EPI, FK, S, MB>;
+  static bool attr_done = false;
+  if (!attr_done) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr_done = true;
+  }
+  const ChainCoef<R>& kc = *reinterpret_cast<const ChainCoef<R>*>(&c.f);
+  k<<<hop_pair_grid(LS, p.vh), 128, smem, st>>>(p, kc);
+  return cudaGetLastError();
+}
+
 // variant 0: direct loads; 1: TMA-staged, 2 stages; 2: TMA-staged, 3 stages;
 // 3: TMA-staged, 2 stages, register budget for HopMinBlocks::v1 resident
-// blocks; 4: direct loads with that register budget.
+// blocks; 4: direct loads with that register budget; 5: packed FP32x2 kernel,
+// two slices per thread, direct loads; 6: the packed kernel fed by the TMA
+// pipeline; 7: a 4-deep TMA pipeline (FP64: the one-slice kernel; FP32
+// arithmetic: the packed kernel) at 2 resident blocks; 8: the packed kernel
+// with all 8 directions in flight at once (5-8 packed: FP32 arithmetic and
+// Ls dividing 32 only).
 template <int LS, int P, int EPI, int FK>
 cudaError_t run(const HopParams& p, const ChainCoefs& c, cudaStream_t st) {
   if (p.variant == 1) return run_tma<LS, P, EPI, FK, 2, 1>(p, c, st);
   if (p.variant == 2) return run_tma<LS, P, EPI, FK, 3, 1>(p, c, st);
   if (p.variant == 3) return run_tma<LS, P, EPI, FK, 2, HopMinBlocks<P>::v1>(p, c, st);
   if (p.variant == 4) return run_mb<LS, P, EPI, FK, HopMinBlocks<P>::v1>(p, c, st);
+  if constexpr (P != PREC_F64 && 32 % LS == 0) {
+    if (p.variant == 5) return run_pair<LS, P, EPI, FK>(p, c, st);
+    if (p.variant == 6) return run_tma_pair<LS, P, EPI, FK, 2, HopMinBlocks<P>::v0>(p, c, st);
+    if (p.variant == 7) return run_tma_pair<LS, P, EPI, FK, 4, 2>(p, c, st);
+    if (p.variant == 8) return run_tma_pair<LS, P, EPI, FK, 8, 2>(p, c, st);
+  }
+  if constexpr (P == PREC_F64)
+    if (p.variant == 7) return run_tma<LS, P, EPI, FK, 4, 2>(p, c, st);
   return run_mb<LS, P, EPI, FK, HopMinBlocks<P>::v0>(p, c, st);
 }
 
