@@ -255,7 +255,8 @@ def learned_section(op, lattice, w, u_workload, args):
     op.fcg(op.new_field(0), w, lp, 1.0, 20000, 8)     # untimed: flexible-CG buffers
     res = {}
     for name, fn in (("cg_f64", lambda x: op.cg(x, w, 1e-20, 20000)),
-                     ("fcg_learned", lambda x: op.fcg(x, w, lp, 1e-20, 20000, 8))):
+                     ("fcg_learned", lambda x: op.fcg(x, w, lp, 1e-20, 20000, 8)),
+                     ("fcg_learned_m2", lambda x: op.fcg(x, w, lp, 1e-20, 20000, 2))):
         x = op.new_field(0)
         torch.cuda.synchronize()
         c0 = time.perf_counter()
@@ -267,7 +268,8 @@ def learned_section(op, lattice, w, u_workload, args):
                          "converged": out[2] == 0}
         else:
             res[name] = {"iterations": out[0], "fallback_cg_iterations": out[1],
-                         "true_rel_residual": out[2], "seconds": c1 - c0, "converged": out[3] == 0}
+                         "true_rel_residual": out[2], "seconds": c1 - c0, "converged": out[3] == 0,
+                         "orthogonalised_against": 8 if name == "fcg_learned" else 2}
     return {"network": "3 layers, 4->8->4 channels per color, 11 paths, BF16 weights, FP32 accumulate",
             "train_configs": args.learned_configs, "train_pairs": npairs,
             "epochs_per_config": args.learned_epochs,

@@ -152,6 +152,19 @@ int zblas_blocks();
 cudaError_t launch_zdot(const void* x, const void* y, size_t n, void* partial, void* out,
                         const void* den, double sign, cudaStream_t st);
 cudaError_t launch_zaxpy(void* y, const void* x, size_t n, const void* c, cudaStream_t st);
+// Up to kZMaxMulti fields at once (passed by value).
+constexpr int kZMaxMulti = 8;
+struct ZMulti {
+  const double2* v[kZMaxMulti];
+  int m;
+};
+// out[j] = sign * <Q_j, z> / Re(den[j]) for j < q.m in one pass over z
+// (partial: zblas_blocks() * kZMaxMulti double2 scratch).
+cudaError_t launch_zmdot(const ZMulti& q, const void* z, size_t n, void* partial, void* out,
+                         const void* den, double sign, cudaStream_t st);
+// y = z + sum_j c[j] P_j in one pass
+cudaError_t launch_zmaxpy(void* y, const void* z, const ZMulti& pv, const void* c, size_t n,
+                          cudaStream_t st);
 // x += alpha p ; r -= alpha q ; partial[block] = |r|^2 (zblas_blocks() doubles)
 cudaError_t launch_zcg_update(void* x, void* r, const void* p, const void* q, size_t n,
                               const void* alpha, double* partial, cudaStream_t st);

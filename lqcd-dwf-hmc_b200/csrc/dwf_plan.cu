@@ -979,9 +979,9 @@ int b200_fcg_solve(b200_dwf_t* op, b200_lp_t* lp, void* x, const void* b, int ma
     if (cudaMalloc(&q, fb) != cudaSuccess) return fail(B200_ENOMEM, "cudaMalloc for a flexible-CG field failed");
     op->fcg_buf.push_back(q);
   }
-  if (!op->fcg_part && cudaMalloc(&op->fcg_part, sizeof(double2) * zblas_blocks()) != cudaSuccess)
+  if (!op->fcg_part && cudaMalloc(&op->fcg_part, sizeof(double2) * zblas_blocks() * kZMaxMulti) != cudaSuccess)
     return fail(B200_ENOMEM, "cudaMalloc for flexible-CG partials failed");
-  if (!op->fcg_sc && cudaMalloc(&op->fcg_sc, sizeof(double2) * 16) != cudaSuccess)
+  if (!op->fcg_sc && cudaMalloc(&op->fcg_sc, sizeof(double2) * 32) != cudaSuccess)
     return fail(B200_ENOMEM, "cudaMalloc for flexible-CG scalars failed");
   void** P = op->fcg_buf.data();
   void** Q = op->fcg_buf.data() + (M + 1);
@@ -990,7 +990,8 @@ int b200_fcg_solve(b200_dwf_t* op, b200_lp_t* lp, void* x, const void* b, int ma
   void* dx = op->fcg_buf[2 * (M + 1) + 2];
   void* rf = op->work[10][P32];
   void* zf = op->work[11][P32];
-  double2* sc = reinterpret_cast<double2*>(op->fcg_sc);   // [1] alpha, [2+i] <p_i,q_i>, [12] beta
+  double2* sc = reinterpret_cast<double2*>(op->fcg_sc);   // [1] alpha, [2+i] <p_i,q_i>, [16+j] betas
+  double2* pqw = sc + 24;                                  // <p_j,q_j> of the current window
   double* part = reinterpret_cast<double*>(op->fcg_part);
 
   auto precondition = [&]() -> int {
@@ -1026,13 +1027,21 @@ int b200_fcg_solve(b200_dwf_t* op, b200_lp_t* lp, void* x, const void* b, int ma
     if (!(rr == rr)) return fail(B200_ENOCONV, "flexible CG breakdown: NaN residual at iteration %d", iters);
     if (rr / bb < tol2) break;
     if ((rc = precondition())) return rc;
+    // p_new = z - sum_j (<q_j, z> / <p_j, q_j>) p_j over the window, as two
+    // passes: all dot products at once, then one combined update
     const int kn = (it + 1) % (M + 1);
-    B200_CHECK_CUDA(cudaMemcpyAsync(P[kn], z, fb, cudaMemcpyDeviceToDevice, st));
-    for (int j = (it - M + 1 > 0 ? it - M + 1 : 0); j <= it; ++j) {
+    const int j0 = (it - M + 1 > 0 ? it - M + 1 : 0);
+    ZMulti qv, pv;
+    qv.m = pv.m = it - j0 + 1;
+    for (int j = j0; j <= it; ++j) {
       const int sj = j % (M + 1);
-      B200_CHECK_CUDA(launch_zdot(Q[sj], z, ncplx, op->fcg_part, sc + 12, sc + 2 + sj, -1.0, st));
-      B200_CHECK_CUDA(launch_zaxpy(P[kn], P[sj], ncplx, sc + 12, st));
+      qv.v[j - j0] = reinterpret_cast<const double2*>(Q[sj]);
+      pv.v[j - j0] = reinterpret_cast<const double2*>(P[sj]);
+      B200_CHECK_CUDA(cudaMemcpyAsync(pqw + (j - j0), sc + 2 + sj, sizeof(double2),
+                                      cudaMemcpyDeviceToDevice, st));
     }
+    B200_CHECK_CUDA(launch_zmdot(qv, z, ncplx, op->fcg_part, sc + 16, pqw, -1.0, st));
+    B200_CHECK_CUDA(launch_zmaxpy(P[kn], z, pv, sc + 16, ncplx, st));
   }
   if (nconv) *nconv = iters;
   double d = 0.0;

@@ -833,9 +833,87 @@ __global__ void zcg_update_kernel(double2* x, double2* r, const double2* p, cons
   }
   if (threadIdx.x == 0) partial[blockIdx.x] = sh[0];
 }
+// partial[blk * m + j] = sum over the block's elements of conj(Q_j) z, j < m
+__global__ void zmdot_kernel(ZMulti q, const double2* z, size_t n, double2* partial) {
+  __shared__ double sr[kZMaxMulti][128], si[kZMaxMulti][128];
+  double re[kZMaxMulti], im[kZMaxMulti];
+#pragma unroll
+  for (int j = 0; j < kZMaxMulti; ++j) { re[j] = 0.0; im[j] = 0.0; }
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double2 b = z[i];
+#pragma unroll
+    for (int j = 0; j < kZMaxMulti; ++j) {
+      if (j < q.m) {
+        const double2 a = q.v[j][i];
+        re[j] = fma(a.x, b.x, re[j]); re[j] = fma(a.y, b.y, re[j]);
+        im[j] = fma(a.x, b.y, im[j]); im[j] = fma(-a.y, b.x, im[j]);
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < kZMaxMulti; ++j) { sr[j][threadIdx.x] = re[j]; si[j][threadIdx.x] = im[j]; }
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o)
+#pragma unroll
+      for (int j = 0; j < kZMaxMulti; ++j) {
+        sr[j][threadIdx.x] += sr[j][threadIdx.x + o];
+        si[j][threadIdx.x] += si[j][threadIdx.x + o];
+      }
+    __syncthreads();
+  }
+  if (threadIdx.x < q.m) partial[blockIdx.x * kZMaxMulti + threadIdx.x] = make_double2(sr[threadIdx.x][0], si[threadIdx.x][0]);
+}
+
+// out[j] = sign * (sum over blocks of partial[.][j]) / Re(den[j]), j < m
+__global__ void zmfinal_kernel(const double2* partial, int nb, int m, double2* out, const double2* den,
+                               double sign) {
+  const int j = threadIdx.x;
+  if (j >= m) return;
+  double re = 0.0, im = 0.0;
+  for (int b = 0; b < nb; ++b) { re += partial[b * kZMaxMulti + j].x; im += partial[b * kZMaxMulti + j].y; }
+  const double d = den[j].x;
+  const double f = (d != 0.0) ? sign / d : 0.0;
+  out[j] = make_double2(f * re, f * im);
+}
+
+// y = z + sum_j c[j] * P_j
+__global__ void zmaxpy_kernel(double2* y, const double2* z, ZMulti pv, const double2* c, size_t n) {
+  double2 cc[kZMaxMulti];
+#pragma unroll
+  for (int j = 0; j < kZMaxMulti; ++j) cc[j] = (j < pv.m) ? c[j] : make_double2(0.0, 0.0);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    double2 v = z[i];
+#pragma unroll
+    for (int j = 0; j < kZMaxMulti; ++j) {
+      if (j < pv.m) {
+        const double2 a = pv.v[j][i];
+        v.x = fma(cc[j].x, a.x, v.x); v.x = fma(-cc[j].y, a.y, v.x);
+        v.y = fma(cc[j].x, a.y, v.y); v.y = fma(cc[j].y, a.x, v.y);
+      }
+    }
+    y[i] = v;
+  }
+}
 }  // namespace
 
 int zblas_blocks() { return kZBlocks; }
+
+cudaError_t launch_zmdot(const ZMulti& q, const void* z, size_t n, void* partial, void* out,
+                         const void* den, double sign, cudaStream_t st) {
+  if (q.m < 1 || q.m > kZMaxMulti) return cudaErrorInvalidValue;
+  zmdot_kernel<<<kZBlocks, 128, 0, st>>>(q, (const double2*)z, n, (double2*)partial);
+  zmfinal_kernel<<<1, 32, 0, st>>>((const double2*)partial, kZBlocks, q.m, (double2*)out,
+                                    (const double2*)den, sign);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_zmaxpy(void* y, const void* z, const ZMulti& pv, const void* c, size_t n,
+                          cudaStream_t st) {
+  if (pv.m < 1 || pv.m > kZMaxMulti) return cudaErrorInvalidValue;
+  zmaxpy_kernel<<<kZBlocks, 256, 0, st>>>((double2*)y, (const double2*)z, pv, (const double2*)c, n);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_zdot(const void* x, const void* y, size_t n, void* partial, void* out,
                         const void* den, double sign, cudaStream_t st) {

@@ -152,41 +152,70 @@ __device__ __forceinline__ void lp_path_input(const PP& p, const float4* in_same
 }
 
 // ------------------------------------------------------------ forward layer
-// One thread per (output site, s): acc = sum_path W_path (T_path in).
+// One thread per (output site, s): acc = sum_path W_path (T_path in).  The
+// channel mixing runs on packed FP32x2 instructions over pairs of output
+// channels (a, a+1): the weights sit in shared memory as float4
+// (Re W[a][b], Re W[a+1][b], Im W[a][b], Im W[a+1][b]) and each input
+// component is broadcast to a pair, so one complex multiply-add of two output
+// channels is four FFMA2.
 template <int CIN, int COUT>
-__global__ void __launch_bounds__(128) lp_conv_kernel(LpConvParams p) {
-  constexpr int NW = kLpPaths * COUT * CIN;
-  __shared__ float2 w[NW];
-  for (int i = threadIdx.x; i < NW; i += blockDim.x) w[i] = p.w[i];
+__global__ void __launch_bounds__(128) lp_conv_kernel(const __grid_constant__ LpConvParams p) {
+  static_assert(COUT % 2 == 0, "output channels are processed in pairs");
+  constexpr int NA = COUT / 2;
+  constexpr int NW = kLpPaths * NA * CIN;
+  __shared__ float4 w[NW];                       // [path][a/2][b]
+  for (int i = threadIdx.x; i < NW; i += blockDim.x) {
+    const int path = i / (NA * CIN);
+    const int a2 = (i / CIN) % NA;
+    const int b = i % CIN;
+    const float2 lo = p.w[(path * COUT + 2 * a2) * CIN + b];
+    const float2 hi = p.w[(path * COUT + 2 * a2 + 1) * CIN + b];
+    w[i] = make_float4(lo.x, hi.x, lo.y, hi.y);
+  }
   __syncthreads();
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= p.vh * p.ls) return;
   const int site = idx / p.ls;
   const int s = idx - site * p.ls;
 
-  float2 acc[COUT][3];
-  lp_zero<COUT>(acc);
+  float2 accr[NA][3], acci[NA][3];   // (channel 2a, channel 2a+1) real / imaginary parts
+#pragma unroll
+  for (int a = 0; a < NA; ++a)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) { accr[a][c] = make_float2(0.f, 0.f); acci[a][c] = accr[a][c]; }
 #pragma unroll 1
   for (int path = 0; path < kLpPaths; ++path) {
     if (path < 3 && !p.in_same) continue;
     if (path >= 3 && !p.in_other) break;
     float2 u[CIN][3];
     lp_path_input<CIN>(p, p.in_same, p.in_other, path, site, s, u);
-    const float2* wp = w + path * COUT * CIN;
+    const float4* wp = w + path * NA * CIN;
 #pragma unroll
-    for (int a = 0; a < COUT; ++a)
+    for (int b = 0; b < CIN; ++b)
 #pragma unroll
-      for (int b = 0; b < CIN; ++b) {
-        const float2 wab = wp[a * CIN + b];
+      for (int c = 0; c < 3; ++c) {
+        const float2 ur = make_float2(u[b][c].x, u[b][c].x);
+        const float2 ui = make_float2(u[b][c].y, u[b][c].y);
+        const float2 mui = make_float2(-u[b][c].y, -u[b][c].y);
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          acc[a][c].x = fmaf(wab.x, u[b][c].x, acc[a][c].x);
-          acc[a][c].x = fmaf(-wab.y, u[b][c].y, acc[a][c].x);
-          acc[a][c].y = fmaf(wab.x, u[b][c].y, acc[a][c].y);
-          acc[a][c].y = fmaf(wab.y, u[b][c].x, acc[a][c].y);
+        for (int a = 0; a < NA; ++a) {
+          const float4 wv = wp[a * CIN + b];
+          const float2 wr = make_float2(wv.x, wv.y), wi = make_float2(wv.z, wv.w);
+          accr[a][c] = __ffma2_rn(wr, ur, accr[a][c]);
+          accr[a][c] = __ffma2_rn(wi, mui, accr[a][c]);
+          acci[a][c] = __ffma2_rn(wr, ui, acci[a][c]);
+          acci[a][c] = __ffma2_rn(wi, ur, acci[a][c]);
         }
       }
   }
+  float2 acc[COUT][3];
+#pragma unroll
+  for (int a = 0; a < NA; ++a)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      acc[2 * a][c] = make_float2(accr[a][c].x, acci[a][c].x);
+      acc[2 * a + 1][c] = make_float2(accr[a][c].y, acci[a][c].y);
+    }
   lp_store<COUT>(p.out, p.ls, site, s, acc);
 }
 
@@ -204,7 +233,7 @@ constexpr size_t lp_gradw_smem() {
 }
 
 template <int CIN, int COUT>
-__global__ void __launch_bounds__(kGradThreads) lp_gradw_kernel(LpGradParams p) {
+__global__ void __launch_bounds__(kGradThreads) lp_gradw_kernel(const __grid_constant__ LpGradParams p) {
   constexpr int NE = kLpPaths * COUT * CIN;
   constexpr int EPT = (NE + kGradThreads - 1) / kGradThreads;
   extern __shared__ float2 sm[];
