@@ -216,6 +216,8 @@ struct HopParams {
   const double* c_x3_dev;
   double* red;           // per-block partials of |o1|^2 (nullable)
   int* err;              // device error word: set when a bounded wait gives up
+  const double* skip;    // when non-null and *skip != 0 the launch does nothing
+                         // (lets a captured solver iteration replay as a no-op)
   int vh, nx2, ny, nz, nt, ls;
   int ieo;               // output parity (0 even, 1 odd)
   double bc[4];
@@ -390,6 +392,7 @@ template <> struct HopMinBlocks<PREC_BF16> { static constexpr int v0 = 4, v1 = 6
 template <int LS, int P, int LF, int EPI, int FK, int MB>
 __global__ void __launch_bounds__(128, MB)
 dwf_hop_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename Store<P>::R> k) {
+  if (p.skip && *p.skip != 0.0) return;
   using St = Store<P>;
   using R = typename St::R;
   constexpr bool kDagHop = EpiIsDag<EPI>::v;
@@ -560,6 +563,7 @@ __device__ __forceinline__ void reconstruct_acc2(float2* acc, const float2* o, f
 template <int LS, int P, int LF, int EPI, int FK, int MB>
 __global__ void __launch_bounds__(128, MB)
 dwf_hop_pair_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename Store<P>::R> k) {
+  if (p.skip && *p.skip != 0.0) return;
   using St = Store<P>;
   using R = typename St::R;
   static_assert(sizeof(R) == 4, "packed kernel is for FP32 arithmetic");
@@ -700,6 +704,7 @@ template <int LS, int P, int LF, int GS = 32 / LS> struct TmaGeom {
 template <int LS, int P, int LF, int EPI, int FK, int S, int MB>
 __global__ void __launch_bounds__(128, MB)
 dwf_hop_tma_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename Store<P>::R> k) {
+  if (p.skip && *p.skip != 0.0) return;
   using St = Store<P>;
   using R = typename St::R;
   using TG = TmaGeom<LS, P, LF>;
@@ -851,6 +856,7 @@ dwf_hop_tma_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename
 template <int LS, int P, int LF, int EPI, int FK, int S, int MB>
 __global__ void __launch_bounds__(128, MB)
 dwf_hop_tma_pair_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename Store<P>::R> k) {
+  if (p.skip && *p.skip != 0.0) return;
   using St = Store<P>;
   using R = typename St::R;
   static_assert(sizeof(R) == 4, "packed kernel is for FP32 arithmetic");

@@ -65,7 +65,11 @@ struct ChainCoefs {
 constexpr int kMaxShift = 32;
 enum MsScalar {
   MS_RR = 0, MS_RR_NEW, MS_PQ, MS_BETA, MS_ALPHA, MS_ALPHA_P, MS_BETA_P, MS_PP0,
-  MS_SNORM, MS_SIGMA0, MS_TOL2, MS_NACT, MS_N = 16
+  MS_SNORM, MS_SIGMA0, MS_TOL2, MS_NACT,
+  MS_DONE,      // 0 while iterating; 1 converged, 2 NaN, 3 iteration cap (set by MSS_PRUNE)
+  MS_ITER,      // iterations completed (counted on the device)
+  MS_MAXITER,
+  MS_N = 16
 };
 // per-shift arrays follow the scalars: [MS_N + a*kMaxShift + i]
 enum MsArray { MSA_ZETA1 = 0, MSA_ZETA2, MSA_CSH2, MSA_BETAS, MSA_ALPHAS, MSA_ZETA, MSA_PP, MSA_COUNT };

@@ -106,7 +106,7 @@ struct b200_dwf {
   int* err = nullptr;           // device error word of the bounded waits
   int red_n = 0;
   double* sc = nullptr;         // solver scalars (device)
-  double* sc_host = nullptr;    // pinned mirror
+  double* sc_host = nullptr;    // pinned mirror (also of the multishift scalars)
   int* err_host = nullptr;      // pinned mirror of err
   double* stage = nullptr;      // device f64 staging for convert/reverse
   void* work[12][4] = {};       // work fields per precision
@@ -119,6 +119,7 @@ struct b200_dwf {
   std::vector<void*> fcg_buf;   // flexible-CG fields (FP64 ring of directions)
   void* fcg_part = nullptr;     // complex reduction partials
   void* fcg_sc = nullptr;       // complex device scalars
+  cudaStream_t gst = nullptr;   // private stream for captured solver iterations
 };
 
 namespace {
@@ -483,7 +484,7 @@ int b200_dwf_create(b200_dwf_t** out, const int lattice[4], int Ls, double mq, d
       cudaMalloc(&op->sc, SC_N * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&op->err, sizeof(int)) != cudaSuccess ||
       cudaMallocHost(&op->err_host, sizeof(int)) != cudaSuccess ||
-      cudaMallocHost(&op->sc_host, SC_N * sizeof(double)) != cudaSuccess) {
+      cudaMallocHost(&op->sc_host, (SC_N > MS_N ? SC_N : MS_N) * sizeof(double)) != cudaSuccess) {
     b200_dwf_destroy(op);
     return fail(B200_ENOMEM, "device allocation for the operator plan failed");
   }
@@ -514,6 +515,7 @@ int b200_dwf_destroy(b200_dwf_t* op) {
   for (void* q : op->fcg_buf) cudaFree(q);
   cudaFree(op->fcg_part);
   cudaFree(op->fcg_sc);
+  if (op->gst) cudaStreamDestroy(op->gst);
   for (int i = 0; i < 2; ++i)
     for (int p = 0; p < 4; ++p) cudaFree(op->tune_out[i][p]);
   delete op;
@@ -810,6 +812,9 @@ int b200_shiftcg_solve(b200_dwf_t* op, void* const* x, const double* sigma, int 
   h[MS_SIGMA0] = sigma[0];
   h[MS_TOL2] = tol2;
   h[MS_NACT] = nshift;
+  h[MS_DONE] = 0.0;
+  h[MS_ITER] = 0.0;
+  h[MS_MAXITER] = (double)maxiter;
   for (int i = 0; i < nshift; ++i) {
     h[MS_N + MSA_ZETA1 * kMaxShift + i] = 1.0;
     h[MS_N + MSA_ZETA2 * kMaxShift + i] = 1.0;
@@ -822,19 +827,22 @@ int b200_shiftcg_solve(b200_dwf_t* op, void* const* x, const double* sigma, int 
   if ((rc = apply_sop(op, prec, y0, p0, SOP_M5PRE, st))) return rc;
   double* S = op->ms_state;
 
-  int it_conv = -1;
-  double rr = bnorm2;
-  for (int it = 0; it < maxiter; ++it) {
+  // One iteration: the four fused DdagD hops, the scalar steps and the fused
+  // update of every active shift.  Every kernel skips itself once S[MS_DONE]
+  // is set, so iterations can be replayed past convergence as no-ops.
+  auto iteration = [&](cudaStream_t s) -> int {
+    int rc2;
     HopParams p1 = hop_base(op, prec, 1, EPI_K1);
-    p1.in = y0; p1.out1 = y1;
-    if ((rc = run_hop(op, prec, p1, st))) return rc;
+    p1.in = y0; p1.out1 = y1; p1.skip = S + MS_DONE;
+    if ((rc2 = run_hop(op, prec, p1, s))) return rc2;
     HopParams p2 = hop_base(op, prec, 0, EPI_K2N, F_LUDAG);
     p2.in = y1; p2.out1 = t2; p2.x1 = p0; p2.c_x1 = 1.0; p2.out2 = u; p2.red = op->red;
-    if ((rc = run_hop(op, prec, p2, st))) return rc;
-    B200_CHECK_CUDA(launch_ms_scalar(MSS_BETA, op->red, nb_hop, S, nshift, st));
+    p2.skip = S + MS_DONE;
+    if ((rc2 = run_hop(op, prec, p2, s))) return rc2;
+    B200_CHECK_CUDA(launch_ms_scalar(MSS_BETA, op->red, nb_hop, S, nshift, s));
     HopParams p3 = hop_base(op, prec, 1, EPI_K3);
-    p3.in = u; p3.out1 = t3;
-    if ((rc = run_hop(op, prec, p3, st))) return rc;
+    p3.in = u; p3.out1 = t3; p3.skip = S + MS_DONE;
+    if ((rc2 = run_hop(op, prec, p3, s))) return rc2;
     // r += beta (DdagD p0 + sigma0 p0) = r + beta t2 + beta sigma0 p0 + beta K4N(hop)
     HopParams p4 = hop_base(op, prec, 0, EPI_K4N);
     p4.in = t3; p4.out1 = r;
@@ -842,20 +850,65 @@ int b200_shiftcg_solve(b200_dwf_t* op, void* const* x, const double* sigma, int 
     p4.x1 = r; p4.c_x1 = 1.0;
     p4.x2 = t2; p4.c_x2 = 1.0; p4.c_x2_dev = S + MS_BETA;
     p4.x3 = p0; p4.c_x3 = sigma[0]; p4.c_x3_dev = S + MS_BETA;
-    p4.red = op->red;
-    if ((rc = run_hop(op, prec, p4, st))) return rc;
-    B200_CHECK_CUDA(launch_ms_scalar(MSS_ALPHA, op->red, nb_hop, S, nshift, st));
+    p4.red = op->red; p4.skip = S + MS_DONE;
+    if ((rc2 = run_hop(op, prec, p4, s))) return rc2;
+    B200_CHECK_CUDA(launch_ms_scalar(MSS_ALPHA, op->red, nb_hop, S, nshift, s));
     MsUpdParams mu;
     mu.xs = op->ms_ptrs; mu.ps = op->ms_ptrs + kMaxShift; mu.r = r; mu.y0 = y0;
     mu.st = S; mu.red = op->ms_red; mu.nblocks = nb_hop; mu.g = g;
-    B200_CHECK_CUDA(launch_ms_update(prec, mu, op->coefs, st));
-    B200_CHECK_CUDA(launch_ms_scalar(MSS_PRUNE, op->ms_red, nb_hop, S, nshift, st));
-    B200_CHECK_CUDA(cudaMemcpyAsync(op->sc_host, S + MS_RR, sizeof(double), cudaMemcpyDeviceToHost, st));
-    B200_CHECK_CUDA(cudaStreamSynchronize(st));
-    rr = op->sc_host[0];
-    if (!(rr == rr)) return fail(B200_ENOCONV, "multishift CG breakdown: NaN at iteration %d", it + 1);
-    if (rr / bnorm2 < tol2) { it_conv = it + 1; break; }
+    B200_CHECK_CUDA(launch_ms_update(prec, mu, op->coefs, s));
+    B200_CHECK_CUDA(launch_ms_scalar(MSS_PRUNE, op->ms_red, nb_hop, S, nshift, s));
+    return 0;
+  };
+  // host view of S[MS_RR .. MS_MAXITER]
+  auto read_state = [&](cudaStream_t s, double* done, double* iters, double* rr_out) -> int {
+    B200_CHECK_CUDA(cudaMemcpyAsync(op->sc_host, S, (MS_MAXITER + 1) * sizeof(double),
+                                    cudaMemcpyDeviceToHost, s));
+    B200_CHECK_CUDA(cudaMemcpyAsync(op->err_host, op->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    B200_CHECK_CUDA(cudaStreamSynchronize(s));
+    if (*op->err_host != 0)
+      return fail(B200_ECUDA, "a kernel gave up waiting for its bulk copies (device error word %d)",
+                  *op->err_host);
+    *done = op->sc_host[MS_DONE];
+    *iters = op->sc_host[MS_ITER];
+    *rr_out = op->sc_host[MS_RR];
+    return 0;
+  };
+
+  double done = 0.0, iters = 0.0, rr = bnorm2;
+  if (maxiter > 0) {
+    // the first iteration runs on the caller's stream (it may autotune the
+    // four hop epilogues); the rest replay a captured CUDA graph of kBatch
+    // iterations on a private stream, checking the device's stop flag after
+    // each replay
+    if ((rc = iteration(st))) return rc;
+    if ((rc = read_state(st, &done, &iters, &rr))) return rc;
+    if (done == 0.0) {
+      constexpr int kBatch = 16;
+      if (!op->gst && cudaStreamCreateWithFlags(&op->gst, cudaStreamNonBlocking) != cudaSuccess)
+        return fail(B200_ECUDA, "cudaStreamCreate failed");
+      cudaGraph_t graph = nullptr;
+      cudaGraphExec_t exec = nullptr;
+      B200_CHECK_CUDA(cudaStreamBeginCapture(op->gst, cudaStreamCaptureModeThreadLocal));
+      int rc_cap = 0;
+      for (int b2 = 0; b2 < kBatch && !rc_cap; ++b2) rc_cap = iteration(op->gst);
+      const cudaError_t ec = cudaStreamEndCapture(op->gst, &graph);
+      if (rc_cap) { if (graph) cudaGraphDestroy(graph); return rc_cap; }
+      B200_CHECK_CUDA(ec);
+      const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+      cudaGraphDestroy(graph);
+      B200_CHECK_CUDA(ei);
+      while (done == 0.0) {
+        const cudaError_t el = cudaGraphLaunch(exec, op->gst);
+        if (el != cudaSuccess) { cudaGraphExecDestroy(exec); B200_CHECK_CUDA(el); }
+        if ((rc = read_state(op->gst, &done, &iters, &rr))) { cudaGraphExecDestroy(exec); return rc; }
+      }
+      cudaGraphExecDestroy(exec);
+    }
+    if (done == 2.0)
+      return fail(B200_ENOCONV, "multishift CG breakdown: NaN at iteration %d", (int)iters);
   }
+  const int it_conv = (done == 1.0) ? (int)iters : -1;
   double dmax = 0.0;
   for (int i = 0; i < nshift; ++i) {
     double d = 0.0;

@@ -318,6 +318,7 @@ __global__ void __launch_bounds__(128)
 ms_update_kernel(MsUpdParams p, const __grid_constant__ ChainCoef<typename Store<P>::R> k) {
   using St = Store<P>;
   using R = typename St::R;
+  if (p.st[MS_DONE] != 0.0) return;   // solve finished: replayed iteration is a no-op
   constexpr int G = 32 / LS;
   constexpr int WARPS = 4;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -444,6 +445,7 @@ __device__ double block_sum_partials(const double* partials, int n) {
 }
 
 __global__ void ms_scalar_kernel(int step, const double* partials, int n, double* st, int nshift) {
+  if (st[MS_DONE] != 0.0) return;     // solve finished: a replayed iteration is a no-op
   double* zeta1 = st + MS_N + MSA_ZETA1 * kMaxShift;
   double* zeta2 = st + MS_N + MSA_ZETA2 * kMaxShift;
   double* csh2 = st + MS_N + MSA_CSH2 * kMaxShift;
@@ -497,6 +499,14 @@ __global__ void ms_scalar_kernel(int step, const double* partials, int n, double
         if (pp[i] > st[MS_TOL2]) { ish1 = i + 1; break; }
       }
       st[MS_NACT] = (double)ish1;
+      // end of an iteration: count it and decide on the device whether the
+      // solve is over, so that iterations can be replayed without the host
+      const double it = st[MS_ITER] + 1.0;
+      st[MS_ITER] = it;
+      const double rel = st[MS_RR] * st[MS_SNORM];
+      if (!(rel == rel)) st[MS_DONE] = 2.0;
+      else if (rel < st[MS_TOL2]) st[MS_DONE] = 1.0;
+      else if (it >= st[MS_MAXITER]) st[MS_DONE] = 3.0;
     }
   }
 }

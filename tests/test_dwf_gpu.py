@@ -99,3 +99,31 @@ def test_cg_f64_matches_oracle():
     assert abs(nconv - nr) <= 2
     assert diff < 1e-11
     assert rel(dev.reverse(fx), xr) < 1e-10
+
+
+@pytest.mark.parametrize("variant", [5, 6, 7, 8])
+@pytest.mark.parametrize("ci", [1, 4])
+def test_packed_variants_reduced_precision(variant, ci):
+    """The packed two-slice FP32x2 hop kernels (direct, and 2/4/8-deep TMA
+    feeds) on every reduced storage precision, pinned with B200_HOP_VARIANT,
+    against the FP64 oracle; Ls = 8 and 16 (the packed kernels need Ls | 32)."""
+    import os
+    case = CASES[ci]
+    ora, dev = make(case, 5)
+    w = synth.spinor_field(case[0], case[1], 13)
+    old = os.environ.get("B200_HOP_VARIANT")
+    os.environ["B200_HOP_VARIANT"] = str(variant)
+    try:
+        for prec in (1, 2, 3):
+            fw, fv = dev.new_field(prec), dev.new_field(prec)
+            dev.convert(fw, w)
+            for mode in ("Deo", "Doe", "D", "DdagD", "H", "Hdag"):
+                for dag in (False, True):
+                    (dev.mult_dag if dag else dev.mult)(fv, fw, mode)
+                    ref = ora.mult(mode, w, dag)
+                    assert rel(dev.reverse(fv), ref) < 4 * TOL[prec], (variant, prec, mode, dag)
+    finally:
+        if old is None:
+            del os.environ["B200_HOP_VARIANT"]
+        else:
+            os.environ["B200_HOP_VARIANT"] = old
