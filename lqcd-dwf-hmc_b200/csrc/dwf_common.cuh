@@ -125,6 +125,7 @@ template <> struct HalfOps<__nv_bfloat16> {
 
 template <typename H> struct StoreHalf {
   using R = float;
+  using Half = H;
   using Chunk = uint4;
   static constexpr int K = 3;
   static constexpr bool kScaled = true;

@@ -665,6 +665,167 @@ dwf_hop_pair_kernel(const HopParams p, const __grid_constant__ ChainCoef<typenam
                                           red_warp, tid, lane, warp, g, srow, site, active);
 }
 
+// Packed kernel for f16/bf16 storage with the next direction's raw data
+// (two slices' stored chunks and scales, the link record) fetched into
+// registers while the current direction is computed, so every warp keeps two
+// directions of loads in flight.
+template <int P>
+struct PairRaw {
+  uint4 c0[3], c1[3];   // stored chunks of slices s0 and s1
+  float sc0, sc1;       // their scales
+  uint4 l0, l1;         // link record (two rows, 12 halves)
+};
+
+template <int LS, int P>
+__device__ __forceinline__ void pair_fetch(const HopParams& p, int nb, size_t lidx, int s0, int s1,
+                                           PairRaw<P>& r) {
+  using St = Store<P>;
+  const unsigned char* colp = reinterpret_cast<const unsigned char*>(p.in) + (size_t)nb * St::col_bytes(LS);
+  const uint4* c = reinterpret_cast<const uint4*>(colp);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    r.c0[k] = __ldg(c + k * LS + s0);
+    r.c1[k] = __ldg(c + k * LS + s1);
+  }
+  const float* scp = reinterpret_cast<const float*>(c + 3 * LS);
+  r.sc0 = __ldg(scp + s0);
+  r.sc1 = __ldg(scp + s1);
+  const uint4* lp = reinterpret_cast<const uint4*>(p.links) + lidx * 2;
+  r.l0 = __ldg(lp);
+  r.l1 = __ldg(lp + 1);
+}
+
+template <int P>
+__device__ __forceinline__ void pair_decode(const uint4 (&c)[3], float* v) {
+  using HO = HalfOps<typename Store<P>::Half>;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float2 a = HO::to2(c[k].x), b = HO::to2(c[k].y), d = HO::to2(c[k].z), e = HO::to2(c[k].w);
+    v[8 * k + 0] = a.x; v[8 * k + 1] = a.y; v[8 * k + 2] = b.x; v[8 * k + 3] = b.y;
+    v[8 * k + 4] = d.x; v[8 * k + 5] = d.y; v[8 * k + 6] = e.x; v[8 * k + 7] = e.y;
+  }
+}
+
+template <int P, int MU, int SIGN, bool kDagHop>
+__device__ __forceinline__ void pair_compute(const PairRaw<P>& r, float ph, float2* acc) {
+  float w0[24], w1[24], h0[12], h1[12], u[18];
+  pair_decode<P>(r.c0, w0);
+  pair_decode<P>(r.c1, w1);
+  if (kDagHop) {
+#pragma unroll
+    for (int q = 0; q < 12; ++q) {
+      float t0 = w0[q]; w0[q] = w0[q + 12]; w0[q + 12] = t0;
+      float t1 = w1[q]; w1[q] = w1[q + 12]; w1[q + 12] = t1;
+    }
+  }
+  project<float, MU, SIGN>(w0, h0);
+  project<float, MU, SIGN>(w1, h1);
+  float2 h[12], o[12];
+  const float2 sc = make_float2(r.sc0, r.sc1);
+#pragma unroll
+  for (int q = 0; q < 12; ++q) h[q] = __fmul2_rn(make_float2(h0[q], h1[q]), sc);
+  {
+    const unsigned int wl[6] = {r.l0.x, r.l0.y, r.l0.z, r.l0.w, r.l1.x, r.l1.y};
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      const float2 f = HalfOps<__half>::to2(wl[q]);
+      u[2 * q] = f.x; u[2 * q + 1] = f.y;
+    }
+    su3_reconstruct(u);
+  }
+  su3_mult_half2<(SIGN < 0)>(u, h, o);
+  reconstruct_acc2<MU, SIGN>(acc, o, ph);
+}
+
+template <int LS, int P, int EPI, int FK, int MB>
+__global__ void __launch_bounds__(128, MB)
+dwf_hop_pair_pf_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename Store<P>::R> k) {
+  if (p.skip && *p.skip != 0.0) return;
+  using St = Store<P>;
+  using R = typename St::R;
+  static_assert(St::kScaled, "prefetching packed kernel is for f16/bf16 storage");
+  static_assert(32 % LS == 0 && LS % 2 == 0, "packed kernel needs Ls | 32");
+  constexpr bool kDagHop = EpiIsDag<EPI>::v;
+  constexpr int H = LS / 2;
+  constexpr int G = 32 / H;
+  constexpr int WARPS = 4;
+
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R* tile_all = reinterpret_cast<R*>(smem_raw);
+  __shared__ double red_warp[WARPS];
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const int g = lane / H;
+  const int j = lane - g * H;
+  const int site = (blockIdx.x * WARPS + warp) * G + g;
+  const bool active = (g < G) && (site < p.vh);
+  const size_t vh = p.vh;
+  const int s0 = j, s1 = j + H;
+
+  float2 acc[24];
+#pragma unroll
+  for (int i = 0; i < 24; ++i) acc[i] = make_float2(0.f, 0.f);
+
+  if (active) {
+    const int ix2 = site % p.nx2;
+    const int iyzt = site / p.nx2;
+    const int y = iyzt % p.ny;
+    const int izt = iyzt / p.ny;
+    const int z = izt % p.nz;
+    const int t = izt / p.nz;
+    const int keo = (p.ieo + y + z + t) & 1;
+    const int x = 2 * ix2 + keo;
+    const int ieo = p.ieo;
+    int nb[8];
+    float ph[8];
+    const int row = p.nx2 * iyzt;
+    nb[0] = row + ((ix2 + keo == p.nx2) ? 0 : ix2 + keo);
+    nb[1] = row + ((ix2 - 1 + keo < 0) ? p.nx2 - 1 : ix2 - 1 + keo);
+    ph[0] = (x == 2 * p.nx2 - 1) ? (float)p.bc[0] : 1.f;
+    ph[1] = (x == 0) ? (float)p.bc[0] : 1.f;
+    const int sy = p.nx2, sz = p.nx2 * p.ny, st4 = p.nx2 * p.ny * p.nz;
+    nb[2] = (y == p.ny - 1) ? site - (p.ny - 1) * sy : site + sy;
+    nb[3] = (y == 0) ? site + (p.ny - 1) * sy : site - sy;
+    ph[2] = (y == p.ny - 1) ? (float)p.bc[1] : 1.f;
+    ph[3] = (y == 0) ? (float)p.bc[1] : 1.f;
+    nb[4] = (z == p.nz - 1) ? site - (p.nz - 1) * sz : site + sz;
+    nb[5] = (z == 0) ? site + (p.nz - 1) * sz : site - sz;
+    ph[4] = (z == p.nz - 1) ? (float)p.bc[2] : 1.f;
+    ph[5] = (z == 0) ? (float)p.bc[2] : 1.f;
+    nb[6] = (t == p.nt - 1) ? site - (p.nt - 1) * st4 : site + st4;
+    nb[7] = (t == 0) ? site + (p.nt - 1) * st4 : site - st4;
+    ph[6] = (t == p.nt - 1) ? (float)p.bc[3] : 1.f;
+    ph[7] = (t == 0) ? (float)p.bc[3] : 1.f;
+    auto lidx = [&](int d) -> size_t {
+      const int mu = d >> 1;
+      return (d & 1) ? (size_t)(1 - ieo + 2 * mu) * vh + nb[d] : (size_t)(ieo + 2 * mu) * vh + site;
+    };
+    PairRaw<P> ra, rb;
+    pair_fetch<LS, P>(p, nb[0], lidx(0), s0, s1, ra);
+#define B200_PF_STEP(D, MU, SIGN, CUR, NXT)                                          \
+    if ((D) < 7) pair_fetch<LS, P>(p, nb[(D) + 1], lidx((D) + 1), s0, s1, NXT);      \
+    pair_compute<P, MU, SIGN, kDagHop>(CUR, ph[D], acc);
+    B200_PF_STEP(0, 0, 1, ra, rb)
+    B200_PF_STEP(1, 0, -1, rb, ra)
+    B200_PF_STEP(2, 1, 1, ra, rb)
+    B200_PF_STEP(3, 1, -1, rb, ra)
+    B200_PF_STEP(4, 2, 1, ra, rb)
+    B200_PF_STEP(5, 2, -1, rb, ra)
+    B200_PF_STEP(6, 3, 1, ra, rb)
+    B200_PF_STEP(7, 3, -1, rb, ra)
+#undef B200_PF_STEP
+  }
+
+  float rows[2][24];
+#pragma unroll
+  for (int i = 0; i < 24; ++i) { rows[0][i] = acc[i].x; rows[1][i] = acc[i].y; }
+  const int srow[2] = {s0, s1};
+  hop_epilogue_rows<LS, P, EPI, FK, 2, G>(p, k, rows, tile_all + (size_t)warp * TileWarp<R, LS, G>::v,
+                                          red_warp, tid, lane, warp, g, srow, site, active);
+}
+
 template <int LS, int P>
 constexpr size_t hop_pair_smem_bytes() {
   using R = typename Store<P>::R;

@@ -179,13 +179,15 @@ SopParams sop_base(const b200_dwf* op) {
 // B200_AUTOTUNE=0 disables tuning (variant 0).  The first call of a
 // combination must not be inside a CUDA graph capture.
 typedef std::tuple<int, int, int, int, int> TuneKey;   // vh, ls, prec, epi, fk
-constexpr int kHopVariants = 9;   // direct, TMA 2-stage, TMA 3-stage, TMA 2-stage + direct at
+constexpr int kHopVariants = 10;   // direct, TMA 2-stage, TMA 3-stage, TMA 2-stage + direct at
                                   // higher occupancy, packed two-slice FP32x2 (direct, TMA),
-                                  // 4-deep TMA, packed with all directions in flight
+                                  // 4-deep TMA, packed with all directions in flight, packed
+                                  // half-storage with register prefetch
 
 bool variant_supported(int prec, int ls, int v) {
   if (v < 5) return true;
   if (v == 7 && prec == PREC_F64) return true;
+  if (v == 9 && (prec == PREC_F64 || prec == PREC_F32)) return false;
   return prec != PREC_F64 && 32 % ls == 0;
 }
 std::map<TuneKey, std::pair<int, float> > g_tune;

@@ -72,6 +72,22 @@ cudaError_t run_pair(const HopParams& p, const ChainCoefs& c, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+template <int LS, int P, int EPI, int FK>
+cudaError_t run_pair_pf(const HopParams& p, const ChainCoefs& c, cudaStream_t st) {
+  using R = typename Store<P>::R;
+  constexpr size_t smem = hop_pair_smem_bytes<LS, P>();
+  auto k = dwf_hop_pair_pf_kernel<LS, P, EPI, FK, 3>;
+  static bool attr_done = false;
+  if (!attr_done) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr_done = true;
+  }
+  const ChainCoef<R>& kc = *reinterpret_cast<const ChainCoef<R>*>(&c.f);
+  k<<<hop_pair_grid(LS, p.vh), 128, smem, st>>>(p, kc);
+  return cudaGetLastError();
+}
+
 template <int LS, int P, int EPI, int FK, int S, int MB>
 cudaError_t run_tma_pair(const HopParams& p, const ChainCoefs& c, cudaStream_t st) {
   using R = typename Store<P>::R;
@@ -95,8 +111,9 @@ cudaError_t run_tma_pair(const HopParams& p, const ChainCoefs& c, cudaStream_t s
 // two slices per thread, direct loads; 6: the packed kernel fed by the TMA
 // pipeline; 7: a 4-deep TMA pipeline (FP64: the one-slice kernel; FP32
 // arithmetic: the packed kernel) at 2 resident blocks; 8: the packed kernel
-// with all 8 directions in flight at once (5-8 packed: FP32 arithmetic and
-// Ls dividing 32 only).
+// with all 8 directions in flight at once; 9: the packed kernel for f16/bf16
+// storage fetching the next direction into registers while computing the
+// current one (5-9 packed: FP32 arithmetic and Ls dividing 32 only).
 template <int LS, int P, int EPI, int FK>
 cudaError_t run(const HopParams& p, const ChainCoefs& c, cudaStream_t st) {
   if (p.variant == 1) return run_tma<LS, P, EPI, FK, 2, 1>(p, c, st);
@@ -108,6 +125,8 @@ cudaError_t run(const HopParams& p, const ChainCoefs& c, cudaStream_t st) {
     if (p.variant == 6) return run_tma_pair<LS, P, EPI, FK, 2, HopMinBlocks<P>::v0>(p, c, st);
     if (p.variant == 7) return run_tma_pair<LS, P, EPI, FK, 4, 2>(p, c, st);
     if (p.variant == 8) return run_tma_pair<LS, P, EPI, FK, 8, 2>(p, c, st);
+    if constexpr (P != PREC_F32)
+      if (p.variant == 9) return run_pair_pf<LS, P, EPI, FK>(p, c, st);
   }
   if constexpr (P == PREC_F64)
     if (p.variant == 7) return run_tma<LS, P, EPI, FK, 4, 2>(p, c, st);

@@ -101,7 +101,7 @@ def test_cg_f64_matches_oracle():
     assert rel(dev.reverse(fx), xr) < 1e-10
 
 
-@pytest.mark.parametrize("variant", [5, 6, 7, 8])
+@pytest.mark.parametrize("variant", [5, 6, 7, 8, 9])
 @pytest.mark.parametrize("ci", [1, 4])
 def test_packed_variants_reduced_precision(variant, ci):
     """The packed two-slice FP32x2 hop kernels (direct, and 2/4/8-deep TMA
