@@ -304,9 +304,10 @@ def b200_arm(args, rank, world, local_rank):
         op.mult(v1, w, "Deo")
         op.mult_dag(v2, w, "Deo")
 
+    from b200dwf import replicas
+
     def barrier():
-        if dist is not None:
-            dist.barrier()
+        replicas.barrier(dist)
 
     for _ in range(args.warmup):
         step()
@@ -322,12 +323,8 @@ def b200_arm(args, rank, world, local_rank):
         torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
-    t_total = e0.elapsed_time(e1) / 1e3
-    if dist is not None:
-        tt = torch.tensor([t_total], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_total = float(tt.item())
-    value = world * step_bytes * args.steps / t_total / 1e9
+    t_total = replicas.max_over_ranks(e0.elapsed_time(e1) / 1e3, dist, "cuda")
+    value = replicas.whole_job_rate(step_bytes * args.steps, t_total, world) / 1e9
 
     # dominant kernel: mult_dag("Deo") is exactly one launch of the fused hop kernel
     nk = max(50, min(args.steps, 500))
@@ -367,12 +364,8 @@ def b200_arm(args, rank, world, local_rank):
         e2e_step()
     q1.record()
     torch.cuda.synchronize()
-    t_e2e = q0.elapsed_time(q1) / 1e3
-    if dist is not None:
-        tt = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_e2e = float(tt.item())
-    e2e_value = world * step_bytes * ne / t_e2e / 1e9
+    t_e2e = replicas.max_over_ranks(q0.elapsed_time(q1) / 1e3, dist, "cuda")
+    e2e_value = replicas.whole_job_rate(step_bytes * ne, t_e2e, world) / 1e9
 
     # FP64 CG time to solution, |r|/|b| < 1e-10
     cg = None
