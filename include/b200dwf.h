@@ -197,6 +197,30 @@ int b200_smear_jacobian(b200_smear_t *sm, double *sigma, void *stream);
  * force <- -2 * (traceless anti-Hermitian part of U force), per link. */
 int b200_force_mult_generator(const int lattice[4], double *force, const double *u, void *stream);
 
+/* ---------------------------------------------------------------- gauge side of the HMC step
+ * Device arrays in the lexical Field_G(Nvol, 4) layout (18 reals per link),
+ * FP64.  Iwasaki / rectangle gauge action with beta, c_plaq, c_rect.
+ * Force_G_Rectangle::force_core (src/lib/Force/Gauge/force_G_Rectangle.cpp:
+ * 84-220): force = -(beta/3) TA(U_mu sum of staples^+), overwritten. */
+int b200_gauge_force_rect(const int lattice[4], double beta, double c_plaq, double c_rect,
+                          double *force, const double *u, void *stream);
+/* Action_G_Rectangle::calcH (src/lib/Action/Gauge/action_G_Rectangle.cpp:97-200);
+ * synchronous. */
+int b200_gauge_action_rect(const int lattice[4], double beta, double c_plaq, double c_rect,
+                           const double *u, double *H, void *stream);
+/* Integrator_UpdateU::evolve (src/lib/HMC/integrator_UpdateU.cpp:79-86 ->
+ * mult_exp_Field_G, SU_N::mat_exp, reunit_SU3): u <- exp(alpha iP) u in place,
+ * Taylor order nprec, reunitarised. */
+int b200_link_update(const int lattice[4], double alpha, const double *ip, double *u, int nprec,
+                     void *stream);
+/* Integrator_UpdateP::evolve (src/lib/HMC/integrator_UpdateP.cpp:44-66):
+ * ip += eps * force. */
+int b200_momentum_update(const int lattice[4], double eps, const double *force, double *ip,
+                         void *stream);
+/* HMC_General::calcH_P (src/lib/HMC/hmc_General.cpp:340-346): H = |iP|^2 / 2;
+ * synchronous. */
+int b200_momentum_energy(const int lattice[4], const double *ip, double *H, void *stream);
+
 /* ---------------------------------------------------------------- learned preconditioner
  * No reference counterpart.  A 3-layer linear gauge-covariant 5D convolution
  * network N ~ (DdagD)^-1 for the even-parity system: channels 4 -> hidden ->

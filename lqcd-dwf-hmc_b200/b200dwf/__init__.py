@@ -78,6 +78,12 @@ def lib():
     L.b200_tuning_table.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
     L.b200_cg_solve.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_double,
                                 ip, dp, vp]
+    d_ = ctypes.c_double
+    L.b200_gauge_force_rect.argtypes = [ip, d_, d_, d_, vp, vp, vp]
+    L.b200_gauge_action_rect.argtypes = [ip, d_, d_, d_, vp, dp, vp]
+    L.b200_link_update.argtypes = [ip, d_, vp, vp, ctypes.c_int, vp]
+    L.b200_momentum_update.argtypes = [ip, d_, vp, vp, vp]
+    L.b200_momentum_energy.argtypes = [ip, vp, dp, vp]
     fp = ctypes.POINTER(ctypes.c_float)
     L.b200_lp_create.argtypes = [ctypes.POINTER(vp), vp, ctypes.c_int, ctypes.c_ulonglong,
                                  ctypes.c_double]
@@ -286,6 +292,56 @@ class DomainWall:
         if rc not in (0, -4):
             check(rc)
         return n.value, nf.value, d.value, rc
+
+
+class GaugeRect:
+    """Iwasaki / rectangle gauge action (Force_G_Rectangle, Action_G_Rectangle)
+    and the HMC link/momentum updates (Integrator_UpdateU/UpdateP,
+    HMC_General::calcH_P) on device copies of lexical Field_G arrays."""
+
+    def __init__(self, lattice, beta, c_plaq=3.648, c_rect=-0.331):
+        self.lattice = list(lattice)
+        self.beta, self.c_plaq, self.c_rect = beta, c_plaq, c_rect
+        self._L = (ctypes.c_int * 4)(*lattice)
+
+    @staticmethod
+    def _dev(a):
+        import torch
+        return torch.from_numpy(np.ascontiguousarray(a, np.float64)).cuda()
+
+    def force(self, u_lex):
+        u = self._dev(u_lex)
+        f = u.new_empty(u.shape)
+        check(lib().b200_gauge_force_rect(self._L, self.beta, self.c_plaq, self.c_rect,
+                                          ctypes.c_void_p(f.data_ptr()), ctypes.c_void_p(u.data_ptr()), None))
+        return f.cpu().numpy()
+
+    def action(self, u_lex):
+        u = self._dev(u_lex)
+        h = ctypes.c_double()
+        check(lib().b200_gauge_action_rect(self._L, self.beta, self.c_plaq, self.c_rect,
+                                           ctypes.c_void_p(u.data_ptr()), ctypes.byref(h), None))
+        return h.value
+
+    def link_update(self, u_lex, ip_lex, alpha, nprec=8):
+        u = self._dev(u_lex)
+        ipd = self._dev(ip_lex)
+        check(lib().b200_link_update(self._L, alpha, ctypes.c_void_p(ipd.data_ptr()),
+                                     ctypes.c_void_p(u.data_ptr()), nprec, None))
+        return u.cpu().numpy()
+
+    def momentum_update(self, ip_lex, force_lex, eps):
+        ipd = self._dev(ip_lex)
+        f = self._dev(force_lex)
+        check(lib().b200_momentum_update(self._L, eps, ctypes.c_void_p(f.data_ptr()),
+                                         ctypes.c_void_p(ipd.data_ptr()), None))
+        return ipd.cpu().numpy()
+
+    def momentum_energy(self, ip_lex):
+        ipd = self._dev(ip_lex)
+        h = ctypes.c_double()
+        check(lib().b200_momentum_energy(self._L, ctypes.c_void_p(ipd.data_ptr()), ctypes.byref(h), None))
+        return h.value
 
 
 def _fp(a):

@@ -161,3 +161,22 @@ def stout_smear(links, lattice, rho, nsteps):
         expq = vec @ (np.exp(1j * ev)[..., None] * _dag(vec))
         u = expq @ u
     return _as_real(u)
+
+
+def algebra_field(lattice, seed, scale=1.0):
+    """Momentum-like field iP (anti-Hermitian traceless 3x3 per link, the
+    matrices Integrator_UpdateU exponentiates), scale * i * H with H Gaussian
+    Hermitian traceless; float64 in the Field_G(Nvol, 4) layout."""
+    nvol = int(np.prod(lattice))
+    rng = np.random.default_rng(seed)
+    n = 4 * nvol
+    a = rng.standard_normal((n, 3, 3)) + 1j * rng.standard_normal((n, 3, 3))
+    h = 0.5 * (a + np.conj(np.transpose(a, (0, 2, 1))))
+    tr = np.trace(h, axis1=1, axis2=2) / 3.0
+    h = h - tr[:, None, None] * np.eye(3)[None]
+    ip = 1j * scale * h
+    out = np.empty((n, 3, 3, 2))
+    out[..., 0] = ip.real
+    out[..., 1] = ip.imag
+    return out.reshape(-1)
+

@@ -63,6 +63,8 @@
 #include "Smear/smear_APE.h"
 #include "Smear/forceSmear_APE.h"
 #include "Smear/director_Smear.h"
+#include "Force/Gauge/force_G_Rectangle.h"
+#include "Action/Gauge/action_G_Rectangle.h"
 #include "IO/bridgeIO.h"
 
 using Bridge::vout;
@@ -149,7 +151,7 @@ Parameters dwf_params(const Kv& kv)
 int main(int argc, char **argv)
 {
   if (argc < 5) {
-    fprintf(stderr, "usage: %s <modes|cg|shiftcg|time> params.txt in_dir out_dir\n", argv[0]);
+    fprintf(stderr, "usage: %s <modes|cg|shiftcg|time|force|smear|gauge> params.txt in_dir out_dir\n", argv[0]);
     return 2;
   }
   const std::string cmd = argv[1];
@@ -249,6 +251,34 @@ int main(int argc, char **argv)
     write_bin(out_dir + "/force_Hdag.bin", F.ptr(0), nf);
     force.force_udiv(F, src);
     write_bin(out_dir + "/force_udiv.bin", F.ptr(0), nf);
+  } else if (cmd == "gauge") {
+    // Force_G_Rectangle::force_core, Action_G_Rectangle::calcH and the link
+    // update W = exp(alpha iP) U of Integrator_UpdateU (mult_exp_Field_G)
+    const double beta = getd(kv, "beta", 2.13);
+    const double c_plaq = getd(kv, "c_plaq", 3.648);
+    const double c_rect = getd(kv, "c_rect", -0.331);
+    const double alpha = getd(kv, "alpha", 0.1);
+    const int nprec = geti(kv, "nprec", 8);
+    const size_t ng = size_t(18) * Nvol * 4;
+    Force_G_Rectangle fg;
+    fg.set_parameters(beta, c_plaq, c_rect);
+    fg.set_config(&U);
+    Field_G F(Nvol, 4);
+    F.set(0.0);
+    fg.force_core(F);
+    write_bin(out_dir + "/gforce.bin", F.ptr(0), ng);
+    Action_G_Rectangle act;
+    act.set_parameters(beta, c_plaq, c_rect);
+    act.set_config(&U);
+    const double H = act.calcH();
+    FILE *f = fopen((out_dir + "/gauge_H.txt").c_str(), "w");
+    fprintf(f, "%.17e\n", H);
+    fclose(f);
+    Field_G iP(Nvol, 4);
+    read_bin(in_dir + "/mom.bin", iP.ptr(0), ng);
+    Field_G W(Nvol, 4);
+    mult_exp_Field_G(W, alpha, iP, U, nprec);
+    write_bin(out_dir + "/update.bin", W.ptr(0), ng);
   } else if (cmd == "smear") {
     const double rho = getd(kv, "rho", 0.1);
     const int nsmear = geti(kv, "nsmear", 2);

@@ -43,6 +43,11 @@ SOLVE = dict(case="shamir", tol=1e-24, sigma=[0.05, 0.2, 1.0], maxiter=5000)
 # stout smearing (rho, 2 levels) and its Jacobian chain on a random force
 SMEAR = dict(lattice=[4, 4, 4, 4], Ls=4, mq=0.01, M0=1.8, b=1.0, c=0.0, alpha=1.0,
              bc=[1, 1, 1, -1], gauge=("near", 71), src=72, rho=0.1, nsmear=2, sigma=73)
+# Iwasaki (rectangle) gauge force, gauge Hamiltonian and the link update
+# W = exp(alpha iP) U (Taylor order nprec + reunitarisation), non-cubic lattice
+GAUGE = dict(lattice=[4, 6, 4, 8], Ls=4, mq=0.01, M0=1.8, b=1.0, c=0.0, alpha=1.0,
+             bc=[1, 1, 1, -1], gauge=("near", 81), src=82, beta=2.13, c_plaq=3.648,
+             c_rect=-0.331, step=0.1, nprec=8, mom=83)
 # force: Moebius (alpha must be 1 for Force_F_Domainwall_eo), antiperiodic t
 FORCE = dict(lattice=[4, 4, 4, 4], Ls=4, mq=0.02, M0=1.4, b=1.5, c=0.5, alpha=1.0,
              bc=[1, 1, 1, -1], gauge=("near", 31), src=32, src2=33)
@@ -118,6 +123,16 @@ def main():
         out["jacobian"] = np.fromfile(os.path.join(tmp, "jacobian.bin"))
     np.savez_compressed(os.path.join(HERE, "smear_stout.npz"), meta=json.dumps(SMEAR), **out)
     print("wrote smear_stout.npz")
+    with tempfile.TemporaryDirectory() as tmp:
+        synth.algebra_field(GAUGE["lattice"], GAUGE["mom"]).tofile(os.path.join(tmp, "mom.bin"))
+        run("gauge", GAUGE, {"beta": GAUGE["beta"], "c_plaq": GAUGE["c_plaq"],
+                             "c_rect": GAUGE["c_rect"], "alpha": GAUGE["step"],
+                             "nprec": GAUGE["nprec"]}, tmp)
+        out = {"gforce": np.fromfile(os.path.join(tmp, "gforce.bin")),
+               "update": np.fromfile(os.path.join(tmp, "update.bin")),
+               "H": np.array(float(open(os.path.join(tmp, "gauge_H.txt")).read()))}
+    np.savez_compressed(os.path.join(HERE, "gauge_rect.npz"), meta=json.dumps(GAUGE), **out)
+    print("wrote gauge_rect.npz")
     np.savez_compressed(os.path.join(HERE, "solve_shamir.npz"),
                         meta=json.dumps(meta), cg_x=x,
                         **{"shift_%d" % i: v for i, v in enumerate(xs)})

@@ -1,0 +1,80 @@
+"""GPU parity of the gauge side of the HMC step against the reference
+corelib's own outputs (tests/golden/gauge_rect.npz, made by
+tests/golden/make_golden.py from Force_G_Rectangle, Action_G_Rectangle and
+mult_exp_Field_G): the Iwasaki rectangle force, the gauge Hamiltonian, the
+link update exp(alpha iP) U, plus the momentum update and kinetic energy."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from b200dwf import synth
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def golden():
+    z = np.load(os.path.join(HERE, "golden", "gauge_rect.npz"))
+    meta = json.loads(str(z["meta"]))
+    kind, seed = meta["gauge"]
+    u = synth.gauge_field(meta["lattice"], seed, kind)
+    ip = synth.algebra_field(meta["lattice"], meta["mom"])
+    return meta, u, ip, z
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+def test_rectangle_force_matches_reference():
+    import b200dwf
+    meta, u, _, z = golden()
+    g = b200dwf.GaugeRect(meta["lattice"], meta["beta"], meta["c_plaq"], meta["c_rect"])
+    assert rel(g.force(u), z["gforce"]) < 1e-13
+
+
+def test_gauge_hamiltonian_matches_reference():
+    import b200dwf
+    meta, u, _, z = golden()
+    g = b200dwf.GaugeRect(meta["lattice"], meta["beta"], meta["c_plaq"], meta["c_rect"])
+    h = g.action(u)
+    assert abs(h - float(z["H"])) <= 1e-12 * abs(float(z["H"]))
+
+
+def test_link_update_matches_reference():
+    import b200dwf
+    meta, u, ip, z = golden()
+    g = b200dwf.GaugeRect(meta["lattice"], meta["beta"])
+    w = g.link_update(u, ip, meta["step"], meta["nprec"])
+    assert np.max(np.abs(w - z["update"])) < 1e-14
+
+
+def test_momentum_update_and_energy():
+    import b200dwf
+    meta, u, ip, _ = golden()
+    g = b200dwf.GaugeRect(meta["lattice"], meta["beta"])
+    f = np.random.default_rng(3).standard_normal(ip.size)
+    np.testing.assert_allclose(g.momentum_update(ip, f, 0.05), ip + 0.05 * f, rtol=0, atol=1e-15)
+    assert g.momentum_energy(ip) == pytest.approx(0.5 * float(ip @ ip), rel=1e-13)
+
+
+def test_force_is_minus_gradient_of_action():
+    """Finite-difference check of the device force against the device action
+    along one algebra direction X: dS/dt at t=0 for U -> exp(t X) U."""
+    import b200dwf
+    lat = [4, 4, 4, 4]
+    u = synth.gauge_field(lat, 55, "near", 0.4)
+    g = b200dwf.GaugeRect(lat, 2.13)
+    X = synth.algebra_field(lat, 56, 1.0)
+    h = 1e-5
+    sp = g.action(g.link_update(u, X, h, 16))
+    sm = g.action(g.link_update(u, X, -h, 16))
+    dS = (sp - sm) / (2 * h)
+    F = g.force(u)
+    # F and X are anti-Hermitian traceless: Re tr(F^+ X) = the sum of products
+    # of their reals, and dS/dt = -F.X (what makes H = |iP|^2/2 + S conserved
+    # by the reference's UpdateP / UpdateU)
+    proj = float(F @ X)
+    assert abs(dS + proj) <= 1e-5 * max(1.0, abs(dS)), (dS, proj)
