@@ -69,3 +69,50 @@ class GaugeMD:
         h0 = self.hamiltonian(ip, u)
         self.leapfrog(ip, u, tau, nsteps)
         return self.hamiltonian(ip, u) - h0, u
+
+
+class DwfMD(GaugeMD):
+    """Gauge + two-flavour even/odd domain-wall fermion molecular dynamics on
+    the device, in the shape of Action_F_Standard_eo (src/lib/Action/Fermion/
+    action_F_Standard_eo.cpp:47-150): S_F = Re <psi, (DdagD)^-1 psi> on the
+    even sites, force = mult_generator(force_udiv(eta)) with
+    eta = (DdagD)^-1 psi (Force::force_core, src/lib/Force/Fermion/
+    force_F.cpp:67-79), added to the gauge force."""
+
+    def __init__(self, op, psi, lattice, beta, c_plaq=3.648, c_rect=-0.331, nprec=8, tol2=1e-24):
+        super().__init__(lattice, beta, c_plaq, c_rect, nprec)
+        from . import Field, F64
+        self.op = op
+        self.psi = psi
+        self.tol2 = tol2
+        self.eta = Field(op, F64)
+        self.last_cg = 0
+
+    def _set(self, u):
+        check(lib().b200_dwf_set_config_device(self.op.handle, self._p(u), None))
+
+    def fermion_action(self, u):
+        self._set(u)
+        n, _, rc = self.op.cg(self.eta, self.psi, self.tol2, 100000)
+        self.last_cg = n
+        return self.op.dot(self.psi, self.eta)
+
+    def fermion_force(self, u):
+        """F_F(U) in the lexical Field_G layout (device tensor)."""
+        import torch
+        self._set(u)
+        n, _, rc = self.op.cg(self.eta, self.psi, self.tol2, 100000)
+        self.last_cg = n
+        f = torch.empty(18 * 4 * self.nvol, dtype=torch.float64, device="cuda")
+        check(lib().b200_dwf_force_udiv(self.op.handle, self._p(f), self.eta.ptr, None))
+        check(lib().b200_force_mult_generator(self._L, self._p(f), self._p(u), None))
+        return f
+
+    def update_p(self, ip, u, eps):
+        fg = self.force(u)
+        check(lib().b200_momentum_update(self._L, eps, self._p(fg), self._p(ip), None))
+        ff = self.fermion_force(u)
+        check(lib().b200_momentum_update(self._L, eps, self._p(ff), self._p(ip), None))
+
+    def hamiltonian(self, ip, u):
+        return super().hamiltonian(ip, u) + self.fermion_action(u)
