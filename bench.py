@@ -60,6 +60,13 @@ def parse():
     ap.add_argument("--learned-pairs", type=int, default=16,
                     help="(residual, error) pairs per configuration")
     ap.add_argument("--learned-epochs", type=int, default=2)
+    ap.add_argument("--no-trajectory", action="store_true",
+                    help="skip the molecular-dynamics trajectory timing")
+    ap.add_argument("--traj-steps", type=int, default=5)
+    ap.add_argument("--traj-length", type=float, default=0.05)
+    ap.add_argument("--traj-lattice", type=int, nargs=4, default=None,
+                    help="lattice of the trajectory timing (default: the Dslash workload's); "
+                         "e.g. 24 24 24 48 for the batched-RHMC configuration's volume")
     return ap.parse_args()
 
 
@@ -277,7 +284,68 @@ def learned_section(op, lattice, w, u_workload, args):
             "apply_ms": t_apply * 1e3, "tol_rel_residual": 1e-10, **res,
             "iteration_ratio": res["cg_f64"]["iterations"] / max(1, res["fcg_learned"]["iterations"]
                                                                  + res["fcg_learned"]["fallback_cg_iterations"]),
-            "time_ratio": res["cg_f64"]["seconds"] / res["fcg_learned"]["seconds"]}
+            "time_ratio": res["cg_f64"]["seconds"] / res["fcg_learned"]["seconds"]}, lp
+
+
+# ------------------------------------------------------------------ trajectory
+def trajectory_section(op, lattice, u_workload, args, lp=None):
+    if args.traj_lattice and list(args.traj_lattice) != list(lattice):
+        # another volume: its own operator and configuration (near-unit links +
+        # 2 stout steps, smeared on the device); the trained network's weights
+        # are volume independent and are carried over
+        import b200dwf
+        from b200dwf import synth
+        lattice = list(args.traj_lattice)
+        sm = b200dwf.StoutSmear(lattice, 0.1, 2)
+        sm.set_config(synth.gauge_field(lattice, SEED_U + 3, "near", 0.3))
+        u_workload = sm.config(2)
+        op = b200dwf.DomainWall(lattice, LS, MQ, M0, 1.0, 0.0, 1.0, (1, 1, 1, -1))
+        op.set_config(u_workload)
+        if lp is not None:
+            lp2 = b200dwf.LearnedPrecond(op, hidden=lp.hidden, seed=1)
+            lp2.set_weights(lp.weights(deployed=False))
+            lp = lp2
+    return _trajectory(op, lattice, u_workload, args, lp)
+
+
+def _trajectory(op, lattice, u_workload, args, lp):
+    """One leapfrog molecular-dynamics trajectory of two-flavour domain-wall
+    fermions (the workload's operator) + the Iwasaki gauge action
+    (beta 2.13), every operator, solve, force and update on the device,
+    timed with each fermion solver to |r|/|b| < 1e-10: plain FP64 CG,
+    mixed-precision Richardson (f16 storage, FP32 inner, FP64 outer) and,
+    when a trained network is given, the learned flexible CG."""
+    import torch
+    import b200dwf
+    from b200dwf import synth
+    from b200dwf.hmc import DwfMD
+    ip = synth.algebra_field(lattice, SEED_U + 7, 1.0)
+    xi = op.new_field(0)
+    op.convert(xi, synth.spinor_field(lattice, LS, SEED_B + 7))
+    psi = op.new_field(0)
+    op.set_config(u_workload)
+    op.mult_dag(psi, xi, "D")                 # heatbath: psi = D^+ xi
+    solvers = [("fp64_cg", "cg"), ("mixed_f16", "mixed")]
+    if lp is not None:
+        solvers.append(("learned_fcg", "learned"))
+    res = {}
+    for name, solver in solvers:
+        md = DwfMD(op, psi, lattice, 2.13, tol2=1e-20, solver=solver, lp=lp)
+        md.trajectory_dh(u_workload, ip, args.traj_length, 1)   # untimed warm-up
+        md.iterations = 0
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        dh, _ = md.trajectory_dh(u_workload, ip, args.traj_length, args.traj_steps)
+        torch.cuda.synchronize()
+        res[name] = {"sec_per_trajectory": time.perf_counter() - t0, "dH": dh,
+                     "solver_iterations": md.iterations}
+    op.set_config(u_workload)
+    out = {"lattice": lattice, "Ls": LS, "mq": MQ, "gauge": "Iwasaki beta 2.13",
+           "integrator": "leapfrog", "length": args.traj_length, "steps": args.traj_steps,
+           "solver_tol_rel_residual": 1e-10, **res}
+    for name in res:
+        out["speedup_" + name] = res["fp64_cg"]["sec_per_trajectory"] / res[name]["sec_per_trajectory"]
+    return out
 
 
 # ------------------------------------------------------------------ B200 arm
@@ -411,9 +479,12 @@ def b200_arm(args, rank, world, local_rank):
                                  "converged": rc == 0}
         del xs
 
-    learned = None
+    learned, lp = None, None
     if not args.no_learned:
-        learned = learned_section(op, lattice, w, u, args)
+        learned, lp = learned_section(op, lattice, w, u, args)
+    trajectory = None
+    if not args.no_trajectory:
+        trajectory = trajectory_section(op, lattice, u, args, lp)
 
     if rank != 0:
         return
@@ -446,6 +517,7 @@ def b200_arm(args, rank, world, local_rank):
         "cg_f64": cg,
         "solvers": solvers,
         "learned_preconditioner": learned,
+        "trajectory": trajectory,
         "autotune": b200dwf.tuning_table().strip().splitlines(),
         "cpu_baseline": cpu,
     }

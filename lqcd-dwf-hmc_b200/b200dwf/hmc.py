@@ -79,30 +79,50 @@ class DwfMD(GaugeMD):
     eta = (DdagD)^-1 psi (Force::force_core, src/lib/Force/Fermion/
     force_F.cpp:67-79), added to the gauge force."""
 
-    def __init__(self, op, psi, lattice, beta, c_plaq=3.648, c_rect=-0.331, nprec=8, tol2=1e-24):
+    def __init__(self, op, psi, lattice, beta, c_plaq=3.648, c_rect=-0.331, nprec=8, tol2=1e-24,
+                 solver="cg", inner_prec=None, lp=None):
         super().__init__(lattice, beta, c_plaq, c_rect, nprec)
-        from . import Field, F64
+        from . import Field, F64, F16
         self.op = op
         self.psi = psi
         self.tol2 = tol2
         self.eta = Field(op, F64)
+        self.solver = solver                  # "cg", "mixed" (Richardson) or "learned" (flexible CG)
+        self.inner_prec = F16 if inner_prec is None else inner_prec
+        self.lp = lp
         self.last_cg = 0
+        self.iterations = 0                   # solver iterations summed over the calls
+
+    def solve(self):
+        """eta = (DdagD)^-1 psi with the chosen solver (Fprop 'DdagD_even')."""
+        if self.solver == "cg":
+            n, _, rc = self.op.cg(self.eta, self.psi, self.tol2, 100000)
+        elif self.solver == "mixed":
+            _, n, _, rc = self.op.richardson(self.eta, self.psi, self.inner_prec, self.tol2, 200,
+                                             1e-4 if self.inner_prec != 1 else 1e-8, 100000)
+        elif self.solver == "learned":
+            n0, n1, _, rc = self.op.fcg(self.eta, self.psi, self.lp, self.tol2, 100000, 2)
+            n = n0 + n1
+        else:
+            raise ValueError(self.solver)
+        if rc != 0:
+            raise RuntimeError("fermion solve did not converge (%s)" % self.solver)
+        self.last_cg = n
+        self.iterations += n
 
     def _set(self, u):
         check(lib().b200_dwf_set_config_device(self.op.handle, self._p(u), None))
 
     def fermion_action(self, u):
         self._set(u)
-        n, _, rc = self.op.cg(self.eta, self.psi, self.tol2, 100000)
-        self.last_cg = n
+        self.solve()
         return self.op.dot(self.psi, self.eta)
 
     def fermion_force(self, u):
         """F_F(U) in the lexical Field_G layout (device tensor)."""
         import torch
         self._set(u)
-        n, _, rc = self.op.cg(self.eta, self.psi, self.tol2, 100000)
-        self.last_cg = n
+        self.solve()
         f = torch.empty(18 * 4 * self.nvol, dtype=torch.float64, device="cuda")
         check(lib().b200_dwf_force_udiv(self.op.handle, self._p(f), self.eta.ptr, None))
         check(lib().b200_force_mult_generator(self._L, self._p(f), self._p(u), None))

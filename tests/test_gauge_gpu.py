@@ -140,3 +140,27 @@ def test_dwf_hmc_energy_violation_falls_as_step_squared():
     dh = [abs(md.trajectory_dh(u, ip, 0.25, n)[0]) for n in (4, 8, 16)]
     r1, r2 = dh[0] / dh[1], dh[1] / dh[2]
     assert 3.0 < r1 < 5.0 and 3.0 < r2 < 5.0, dh
+
+
+def test_trajectory_solvers_agree():
+    """The same trajectory with FP64 CG, mixed-precision Richardson (f16
+    inner) and the learned flexible CG as the fermion solver: |dH| agrees to
+    the solver tolerance and the end links agree."""
+    import b200dwf
+    from b200dwf.hmc import DwfMD
+    lat, ls = [4, 4, 4, 8], 8
+    u = synth.gauge_field(lat, 91, "near", 0.3)
+    ip = synth.algebra_field(lat, 92, 1.0)
+    out = {}
+    for solver in ("cg", "mixed", "learned"):
+        op = b200dwf.DomainWall(lat, ls, 0.05, 1.8)
+        op.set_config(u)
+        psi = op.new_field(b200dwf.F64)
+        op.convert(psi, synth.spinor_field(lat, ls, 93))
+        lp = b200dwf.LearnedPrecond(op, hidden=8, seed=3) if solver == "learned" else None
+        md = DwfMD(op, psi, lat, 2.13, tol2=1e-20, solver=solver, lp=lp)
+        dh, uf = md.trajectory_dh(u, ip, 0.2, 4)
+        out[solver] = (dh, uf.cpu().numpy())
+    for s in ("mixed", "learned"):
+        assert abs(out[s][0] - out["cg"][0]) < 1e-6 * max(1.0, abs(out["cg"][0])), (s, out[s][0], out["cg"][0])
+        assert np.max(np.abs(out[s][1] - out["cg"][1])) < 1e-8, s
