@@ -164,3 +164,48 @@ def test_trajectory_solvers_agree():
     for s in ("mixed", "learned"):
         assert abs(out[s][0] - out["cg"][0]) < 1e-6 * max(1.0, abs(out["cg"][0])), (s, out[s][0], out["cg"][0])
         assert np.max(np.abs(out[s][1] - out["cg"][1])) < 1e-8, s
+
+
+def _rhmc_md(lat, ls, seed, mass_l=0.1, mass_s=0.2):
+    import b200dwf
+    from b200dwf.hmc import GaugeMD, TwoFlavour, Rational
+    from b200dwf.rational import inv_sqrt_partial_fractions
+    u = synth.gauge_field(lat, seed, "near", 0.3)
+    opl = b200dwf.DomainWall(lat, ls, mass_l, 1.8)
+    ops = b200dwf.DomainWall(lat, ls, mass_s, 1.8)
+    for op in (opl, ops):
+        op.set_config(u)
+    psi = opl.new_field(b200dwf.F64)
+    opl.convert(psi, synth.spinor_field(lat, ls, seed + 1))
+    phi = ops.new_field(b200dwf.F64)
+    ops.convert(phi, synth.spinor_field(lat, ls, seed + 2))
+    a0, b, c = inv_sqrt_partial_fractions(1e-4, 10.0, 16)
+    rat = Rational(ops, phi, a0, b, c)
+    md = GaugeMD(lat, 2.13, fermions=[TwoFlavour(opl, psi), rat])
+    return u, md, rat
+
+
+def test_rational_force_is_minus_gradient_of_rational_action():
+    lat, ls = [4, 4, 4, 4], 4
+    u, md, rat = _rhmc_md(lat, ls, 101)
+    X = synth.algebra_field(lat, 102, 1.0)
+    h = 1e-5
+    up = md.to_device(u)
+    md.update_u(md.to_device(X), up, h)
+    um = md.to_device(u)
+    md.update_u(md.to_device(X), um, -h)
+    dS = (rat.action(md, up) - rat.action(md, um)) / (2 * h)
+    F = md.fermion_force(md.to_device(u), rat).cpu().numpy()
+    proj = float(F @ X)
+    assert abs(dS + proj) <= 1e-5 * max(1.0, abs(dS)), (dS, proj)
+
+
+def test_two_plus_one_flavour_energy_violation_falls_as_step_squared():
+    """Iwasaki + two-flavour DWF (light) + RHMC one-flavour DWF (strange, 16
+    poles, multishift CG) on the device: |dH| falls ~4x per step doubling."""
+    lat, ls = [4, 4, 4, 4], 4
+    u, md, _ = _rhmc_md(lat, ls, 111)
+    ip = synth.algebra_field(lat, 112, 1.0)
+    dh = [abs(md.trajectory_dh(u, ip, 0.25, n)[0]) for n in (4, 8, 16)]
+    r1, r2 = dh[0] / dh[1], dh[1] / dh[2]
+    assert 3.0 < r1 < 5.0 and 3.0 < r2 < 5.0, dh
