@@ -35,6 +35,7 @@ sys.path.insert(0, os.path.join(REPO, "lqcd-dwf-hmc_b200"))
 LATTICE = [16, 16, 16, 32]
 LS = 16
 MQ, M0 = 0.01, 1.8
+MS = 0.04                   # strange-quark mass of the 2+1-flavour trajectory
 SEED_U, SEED_B = 1234567, 7654321
 BYTES_PER_HALF_SITE = LS * 24 * (8 + 8) + 8 * 18 * 8
 REF_HARNESS = os.path.join(REPO, "oracle", "_ref", "ref_harness")
@@ -63,6 +64,8 @@ def parse():
     ap.add_argument("--no-trajectory", action="store_true",
                     help="skip the molecular-dynamics trajectory timing")
     ap.add_argument("--traj-steps", type=int, default=5)
+    ap.add_argument("--traj-flavours", default="2+1", choices=["2", "2+1"],
+                    help="light two-flavour DWF only, or plus an RHMC strange quark")
     ap.add_argument("--traj-length", type=float, default=0.05)
     ap.add_argument("--traj-lattice", type=int, nargs=4, default=None,
                     help="lattice of the trajectory timing (default: the Dslash workload's); "
@@ -309,28 +312,38 @@ def trajectory_section(op, lattice, u_workload, args, lp=None):
 
 
 def _trajectory(op, lattice, u_workload, args, lp):
-    """One leapfrog molecular-dynamics trajectory of two-flavour domain-wall
-    fermions (the workload's operator) + the Iwasaki gauge action
+    """One leapfrog molecular-dynamics trajectory of 2+1-flavour domain-wall
+    fermions (light: two-flavour action with the workload's operator; strange:
+    one-flavour RHMC over the multishift solver) + the Iwasaki gauge action
     (beta 2.13), every operator, solve, force and update on the device,
-    timed with each fermion solver to |r|/|b| < 1e-10: plain FP64 CG,
+    timed with each light-quark solver to |r|/|b| < 1e-10: plain FP64 CG,
     mixed-precision Richardson (f16 storage, FP32 inner, FP64 outer) and,
     when a trained network is given, the learned flexible CG."""
     import torch
     import b200dwf
     from b200dwf import synth
-    from b200dwf.hmc import DwfMD
+    from b200dwf.hmc import GaugeMD, TwoFlavour, Rational
+    from b200dwf.rational import inv_sqrt_partial_fractions
     ip = synth.algebra_field(lattice, SEED_U + 7, 1.0)
     xi = op.new_field(0)
     op.convert(xi, synth.spinor_field(lattice, LS, SEED_B + 7))
     psi = op.new_field(0)
     op.set_config(u_workload)
     op.mult_dag(psi, xi, "D")                 # heatbath: psi = D^+ xi
+    # strange quark: one-flavour RHMC, 16 poles on [1e-4, 10], FP64 multishift
+    ops = b200dwf.DomainWall(lattice, LS, MS, M0, 1.0, 0.0, 1.0, (1, 1, 1, -1))
+    ops.set_config(u_workload)
+    phi = ops.new_field(0)
+    ops.convert(phi, synth.spinor_field(lattice, LS, SEED_B + 8))
+    ra0, rb, rc = inv_sqrt_partial_fractions(1e-4, 10.0, 16)
     solvers = [("fp64_cg", "cg"), ("mixed_f16", "mixed")]
     if lp is not None:
         solvers.append(("learned_fcg", "learned"))
     res = {}
     for name, solver in solvers:
-        md = DwfMD(op, psi, lattice, 2.13, tol2=1e-20, solver=solver, lp=lp)
+        two = TwoFlavour(op, psi, 1e-20, solver, None, lp)
+        acts = [two] if args.traj_flavours == "2" else [two, Rational(ops, phi, ra0, rb, rc, 1e-20)]
+        md = GaugeMD(lattice, 2.13, fermions=acts)
         md.trajectory_dh(u_workload, ip, args.traj_length, 1)   # untimed warm-up
         md.iterations = 0
         torch.cuda.synchronize()
@@ -338,9 +351,13 @@ def _trajectory(op, lattice, u_workload, args, lp):
         dh, _ = md.trajectory_dh(u_workload, ip, args.traj_length, args.traj_steps)
         torch.cuda.synchronize()
         res[name] = {"sec_per_trajectory": time.perf_counter() - t0, "dH": dh,
-                     "solver_iterations": md.iterations}
+                     "light_solver_iterations": two.iterations,
+                     "strange_multishift_iterations": md.iterations - two.iterations}
     op.set_config(u_workload)
-    out = {"lattice": lattice, "Ls": LS, "mq": MQ, "gauge": "Iwasaki beta 2.13",
+    out = {"lattice": lattice, "Ls": LS, "mq": MQ, "flavours": args.traj_flavours,
+           "strange": None if args.traj_flavours == "2" else
+           {"mq": MS, "rational": "16 poles, x^-1/2 on [1e-4, 10]", "solver": "FP64 multishift CG"},
+           "gauge": "Iwasaki beta 2.13",
            "integrator": "leapfrog", "length": args.traj_length, "steps": args.traj_steps,
            "solver_tol_rel_residual": 1e-10, **res}
     for name in res:
