@@ -170,6 +170,14 @@ int b200_dwf_force_udiv1(b200_dwf_t *op, const char *mode, double *force, const 
 /* force_udiv(force, eta) = force_udiv1_H(H eta, eta) + force_udiv1_Hdag(eta, H eta)
  * (force_F_Domainwall_eo.cpp:150-167), fused: three hops and two force passes. */
 int b200_dwf_force_udiv(b200_dwf_t *op, double *force, const void *eta, void *stream);
+/* Accumulating form: force += scale * force_udiv1(mode "H"/"Hdag", a, b) or
+ * force += scale * force_udiv(a) (mode "DdagD", b unused).  Replaces the
+ * force_udiv + axpy pairs of the reference's ratio and rational forces
+ * (Force_F_Rational_Ratio::force_udiv_impl, src/lib/Force/Fermion/
+ * force_F_Rational_Ratio.cpp:253-292; Action_F_Ratio_eo::force,
+ * src/lib/Action/Fermion/action_F_Ratio_eo.cpp:171-205). */
+int b200_dwf_force_acc(b200_dwf_t *op, const char *mode, double *force, const void *a,
+                       const void *b, double scale, void *stream);
 
 /* ---------------------------------------------------------------- stout
  * Stout smearing levels and the smeared-force Jacobian, on the device.

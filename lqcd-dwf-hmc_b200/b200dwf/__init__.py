@@ -66,6 +66,7 @@ def lib():
                                         ctypes.c_int, ctypes.c_double, ip, ip, dp, vp]
     L.b200_dwf_force_udiv1.argtypes = [vp, ctypes.c_char_p, vp, vp, vp, vp]
     L.b200_dwf_force_udiv.argtypes = [vp, vp, vp, vp]
+    L.b200_dwf_force_acc.argtypes = [vp, ctypes.c_char_p, vp, vp, vp, ctypes.c_double, vp]
     L.b200_smear_create.argtypes = [ctypes.POINTER(vp), ip, ctypes.c_double, ctypes.c_int]
     L.b200_smear_destroy.argtypes = [vp]
     L.b200_smear_set_config.argtypes = [vp, vp, ctypes.c_int, vp]

@@ -206,3 +206,545 @@ class DwfMD(GaugeMD):
 
     def fermion_action(self, u):
         return self.two.action(self, u)
+
+
+# ---------------------------------------------------------------------------
+# The reference's 2+1-flavour HMC (benchmark_hmc_dwf_corelib/hmc_dwf_eo.cpp:
+# 155-352) on the device: stout-smeared links under one director, the
+# rational-ratio one-flavour action, two Hasenbusch ratio actions, the
+# rectangle gauge action, the nested Omelyan integrator and HMC_General.
+# ---------------------------------------------------------------------------
+
+class DirectorSmear:
+    """Director_Smear (src/lib/Smear/director_Smear.cpp): the stout levels of
+    the current thin links, rebuilt lazily after notify_linkv()."""
+
+    def __init__(self, lattice, rho, nsmear):
+        from . import StoutSmear
+        self.lattice, self.nsmear = list(lattice), nsmear
+        self.sm = StoutSmear(lattice, rho, nsmear) if nsmear > 0 else None
+        self.u = None
+        self.version = 0
+        self._smeared = -1
+
+    def set_config(self, u):
+        self.u = u
+        self.notify_linkv()
+
+    def notify_linkv(self):
+        self.version += 1
+
+    def config_ptr(self):
+        """Device pointer of the fully smeared links."""
+        if self.nsmear == 0:
+            return self.u.data_ptr()
+        if self._smeared != self.version:
+            check(lib().b200_smear_set_config(self.sm.handle, _p(self.u), 1, None))
+            self._smeared = self.version
+        return self.sm.config_ptr(self.nsmear)
+
+    def jacobian(self, sigma):
+        """Force_F_Smeared::mult_jacobian, in place (src/lib/Force/Fermion/
+        force_F_Smeared.cpp:77-88)."""
+        if self.nsmear:
+            self.config_ptr()
+            check(lib().b200_smear_jacobian(self.sm.handle, _p(sigma), None))
+
+
+class FoprSmeared:
+    """Fopr_Smeared_eo: a DomainWall operator that sees the director's
+    smeared links (src/lib/Fopr/fopr_Smeared_eo.cpp)."""
+
+    def __init__(self, op, director):
+        self.op, self.dr = op, director
+        self._version = None
+
+    def sync(self):
+        if self._version != self.dr.version or self.dr.nsmear == 0:
+            check(lib().b200_dwf_set_config_device(self.op.handle,
+                                                   ctypes.c_void_p(self.dr.config_ptr()), None))
+            self._version = self.dr.version
+        return self.op
+
+
+class Solver:
+    """Fprop 'DdagD_even' with a chosen method: FP64 CG (the reference's
+    Solver_CG), mixed-precision Richardson, or the learned flexible CG."""
+
+    def __init__(self, kind="cg", tol2=1e-20, maxiter=100000, inner_prec=None, lp=None):
+        from . import F16
+        self.kind, self.tol2, self.maxiter = kind, tol2, maxiter
+        self.inner_prec = F16 if inner_prec is None else inner_prec
+        self.lp = lp
+        self.iterations = 0
+
+    def solve(self, op, x, b):
+        if self.kind == "cg":
+            n, _, rc = op.cg(x, b, self.tol2, self.maxiter)
+        elif self.kind == "mixed":
+            _, n, _, rc = op.richardson(x, b, self.inner_prec, self.tol2, 200,
+                                        1e-4 if self.inner_prec != 1 else 1e-8, self.maxiter)
+        elif self.kind == "learned":
+            n0, n1, _, rc = op.fcg(x, b, self.lp, self.tol2, self.maxiter, 2)
+            n = n0 + n1
+        else:
+            raise ValueError(self.kind)
+        if rc != 0:
+            raise RuntimeError("fermion solve did not converge (%s)" % self.kind)
+        self.iterations += n
+        return n
+
+
+class FoprRational:
+    """Fopr_Rational (src/lib/Fopr/afopr_Rational-tmpl.h:181-219):
+    v = a0 b + sum_i b_i (DdagD + c_i)^-1 b from one multishift solve."""
+
+    def __init__(self, fopr, rational, tol2, maxiter=100000):
+        self.fopr, self.r = fopr, rational
+        self.tol2, self.maxiter = tol2, maxiter
+        self.xs = None
+        self.iterations = 0
+
+    def shifts(self, b):
+        """x_i = (DdagD + c_i)^-1 b (kept in self.xs)."""
+        from . import Field
+        op = self.fopr.sync()
+        if self.xs is None:
+            self.xs = [Field(op) for _ in self.r.c]
+        n, _, rc = op.shiftcg(self.xs, self.r.c, b, self.tol2, self.maxiter)
+        if rc != 0:
+            raise RuntimeError("multishift solve did not converge")
+        self.iterations += n
+        return self.xs
+
+    def mult(self, v, b):
+        xs = self.shifts(b)
+        op = self.fopr.op
+        op.axpby(v, self.r.a0, b, 0.0)
+        for bi, x in zip(self.r.b, xs):
+            op.axpby(v, bi, x, 1.0)
+        return v
+
+
+class ActionFRatio:
+    """Action_F_Ratio_eo (src/lib/Action/Fermion/action_F_Ratio_eo.cpp):
+    S = <psi, H_p (DdagD)^-1 H_p^dag psi> for det[DdagD / DdagD_p], the
+    Hasenbusch ratio of a lighter (fopr) over a heavier (fopr_prec) operator.
+    The three solves follow the reference's Fprop roles: solver_h_prec in the
+    heatbath, solver_md in the force, solver_h in the Hamiltonian."""
+
+    def __init__(self, fopr_prec, fopr, solver_md, solver_h, solver_h_prec, label=""):
+        from . import Field
+        self.fp, self.f = fopr_prec, fopr
+        self.solver_md, self.solver_h, self.solver_h_prec = solver_md, solver_h, solver_h_prec
+        self.label = label
+        op = fopr.op
+        self.psf, self.v1, self.v2 = Field(op), Field(op), Field(op)
+        self.fermion = True
+
+    def langevin(self, xi):
+        f, fp = self.f.sync(), self.fp.sync()
+        f.mult_dag(self.v2, xi, "H")
+        self.v1.buf.zero_()
+        self.solver_h_prec.solve(fp, self.v1, self.v2)
+        fp.mult(self.psf, self.v1, "H")
+        return f.norm2(xi)
+
+    def calcH(self):
+        f, fp = self.f.sync(), self.fp.sync()
+        fp.mult_dag(self.v1, self.psf, "H")
+        self.v2.buf.zero_()
+        self.solver_h.solve(f, self.v2, self.v1)
+        return f.dot(self.v1, self.v2)
+
+    def force_udiv(self, acc):
+        """acc += this action's force_udiv on the smeared links
+        (action_F_Ratio_eo.cpp:171-205 before mult_generator)."""
+        f, fp = self.f.sync(), self.fp.sync()
+        fp.mult_dag(self.v1, self.psf, "H")
+        self.v2.buf.zero_()
+        self.solver_md.solve(f, self.v2, self.v1)
+        L = lib()
+        check(L.b200_dwf_force_acc(f.handle, b"DdagD", _p(acc), self.v2.ptr, None, 1.0, None))
+        check(L.b200_dwf_force_acc(fp.handle, b"Hdag", _p(acc), self.v2.ptr, self.psf.ptr, -1.0, None))
+        check(L.b200_dwf_force_acc(fp.handle, b"H", _p(acc), self.psf.ptr, self.v2.ptr, -1.0, None))
+
+
+class ActionFRationalRatio:
+    """Action_F_Rational_Ratio_eo + Force_F_Rational_Ratio (src/lib/Action/
+    Fermion/action_F_Rational_Ratio_eo.cpp:73-170, src/lib/Force/Fermion/
+    force_F_Rational_Ratio.cpp:187-292): one flavour as
+    det[(B^dag B)^(1/2) / (A^dag A)^(1/2)], A = fopr_numer (Pauli-Villars),
+    B = fopr_denom.  rats: dict of Rational coefficient sets
+    'md_numer' x^(1/4), 'md_denom' x^(-1/2), 'h_numer' x^(1/4),
+    'h_denom' x^(-1/2), 'psf_denom' x^(1/4), 'psf_numer' x^(-1/4)."""
+
+    def __init__(self, fopr_numer, fopr_denom, rats, tol2_md, tol2_h, label=""):
+        from . import Field
+        self.fa, self.fb = fopr_numer, fopr_denom
+        self.label = label
+        self.md_numer = FoprRational(fopr_numer, rats["md_numer"], tol2_md)
+        self.md_denom = FoprRational(fopr_denom, rats["md_denom"], tol2_md)
+        self.md_numer2 = FoprRational(fopr_numer, rats["md_numer"], tol2_md)
+        self.h_numer = FoprRational(fopr_numer, rats["h_numer"], tol2_h)
+        self.h_denom = FoprRational(fopr_denom, rats["h_denom"], tol2_h)
+        self.psf_denom = FoprRational(fopr_denom, rats["psf_denom"], tol2_h)
+        self.psf_numer = FoprRational(fopr_numer, rats["psf_numer"], tol2_h)
+        op = fopr_denom.op
+        self.psf, self.v1, self.v2 = Field(op), Field(op), Field(op)
+        self.t1, self.t2 = Field(op), Field(op)
+        self.fermion = True
+
+    @property
+    def iterations(self):
+        return sum(r.iterations for r in (self.md_numer, self.md_denom, self.md_numer2, self.h_numer,
+                                          self.h_denom, self.psf_denom, self.psf_numer))
+
+    def langevin(self, xi):
+        self.psf_denom.mult(self.v1, xi)          # (B^dag B)^(1/4) xi
+        self.psf_numer.mult(self.psf, self.v1)    # (A^dag A)^(-1/4)
+        return self.fb.op.norm2(xi)
+
+    def calcH(self):
+        self.h_numer.mult(self.v1, self.psf)      # (A^dag A)^(1/4) psf
+        self.h_denom.mult(self.v2, self.v1)       # (B^dag B)^(-1/2)
+        return self.fb.op.dot(self.v1, self.v2)
+
+    def force_udiv(self, acc):
+        """acc += force_udiv of the rational ratio on the smeared links.  The
+        numerator's four mixed terms per pole (force_udiv1 in modes H and Hdag
+        with eta1_i and zeta_i swapped) are the cross term of the quadratic
+        force_udiv, taken by polarisation:
+            sum = (force_udiv(s eta1 + zeta/s) - force_udiv(s eta1 - zeta/s)) / 2,
+        s^2 = |zeta| / |eta1| balancing the two vectors."""
+        L = lib()
+        fa, fb = self.fa.sync(), self.fb.sync()
+        rn, rd = self.md_numer.r, self.md_denom.r
+        self.md_numer.mult(self.v1, self.psf)          # phi2, eta1_i in md_numer.xs
+        self.md_denom.mult(self.v2, self.v1)           # xi, eta2_i in md_denom.xs
+        zetas = self.md_numer2.shifts(self.v2)         # zeta_i
+        for bi, e2 in zip(rd.b, self.md_denom.xs):
+            check(L.b200_dwf_force_acc(fb.handle, b"DdagD", _p(acc), e2.ptr, None, bi, None))
+        for bi, e1, z in zip(rn.b, self.md_numer.xs, zetas):
+            ne, nz = fa.norm2(e1), fa.norm2(z)
+            if ne == 0.0 or nz == 0.0:
+                continue
+            s = (nz / ne) ** 0.25
+            fa.axpby(self.t1, s, e1, 0.0)
+            fa.axpby(self.t1, 1.0 / s, z, 1.0)
+            fa.axpby(self.t2, s, e1, 0.0)
+            fa.axpby(self.t2, -1.0 / s, z, 1.0)
+            check(L.b200_dwf_force_acc(fa.handle, b"DdagD", _p(acc), self.t1.ptr, None, 0.5 * bi, None))
+            check(L.b200_dwf_force_acc(fa.handle, b"DdagD", _p(acc), self.t2.ptr, None, -0.5 * bi, None))
+
+
+class ActionGRectangle:
+    """Action_G_Rectangle with Force_G_Rectangle (src/lib/Action/Gauge/
+    action_G_Rectangle.cpp:97-200, src/lib/Force/Gauge/force_G_Rectangle.cpp)."""
+
+    def __init__(self, lattice, beta, c_plaq=3.648, c_rect=-0.331):
+        self._L = (ctypes.c_int * 4)(*lattice)
+        self.beta, self.c_plaq, self.c_rect = beta, c_plaq, c_rect
+        self.fermion = False
+        self.u = None
+        self.label = "gauge"
+
+    def langevin(self, _xi=None):
+        return self.calcH()
+
+    def calcH(self):
+        h = ctypes.c_double()
+        check(lib().b200_gauge_action_rect(self._L, self.beta, self.c_plaq, self.c_rect,
+                                           _p(self.u), ctypes.byref(h), None))
+        return h.value
+
+    def force(self, out):
+        check(lib().b200_gauge_force_rect(self._L, self.beta, self.c_plaq, self.c_rect,
+                                          _p(out), _p(self.u), None))
+
+
+class UpdateP:
+    """Integrator_UpdateP (src/lib/HMC/integrator_UpdateP.cpp:44-66): the
+    level's summed force, cached until the links change.  The fermion
+    actions of a level share one smeared-force Jacobian and one
+    mult_generator (both are linear)."""
+
+    def __init__(self, hmc, actions):
+        import torch
+        self.hmc, self.actions = hmc, list(actions)
+        n = 18 * 4 * hmc.nvol
+        self.force = torch.zeros(n, dtype=torch.float64, device="cuda")
+        self.valid = False
+        self.evaluations = 0
+
+    def evolve(self, step, ip, u):
+        if not self.valid:
+            self.hmc.level_force(self.actions, u, self.force)
+            self.valid = True
+            self.evaluations += 1
+        check(lib().b200_momentum_update(self.hmc._L, step, _p(self.force), _p(ip), None))
+
+
+class UpdateU:
+    """Integrator_UpdateU (src/lib/HMC/integrator_UpdateU.cpp:79-98):
+    U <- exp(step iP) U, then every force cache and the director are told."""
+
+    def __init__(self, hmc, nprec):
+        self.hmc, self.nprec = hmc, nprec
+        self.clients = []
+
+    def evolve(self, step, ip, u):
+        check(lib().b200_link_update(self.hmc._L, step, _p(ip), _p(u), self.nprec, None))
+        for c in self.clients:
+            c.valid = False
+        self.hmc.director.notify_linkv()
+
+
+class Omelyan:
+    """Integrator_Omelyan::evolve (src/lib/HMC/integrator_Omelyan.cpp:
+    85-117): P(l e) [U(e/2) P((1-2l) e) U(e/2) P(2 l e)]... P(l e), the
+    inner 'U' being the next level's integrator."""
+
+    def __init__(self, update_p, inner, nstep, lam):
+        self.p, self.u, self.nstep, self.lam = update_p, inner, nstep, lam
+
+    def evolve(self, step, ip, u):
+        if self.nstep <= 0:
+            return
+        e = step / self.nstep
+        self.p.evolve(e * self.lam, ip, u)
+        for k in range(1, self.nstep + 1):
+            self.u.evolve(0.5 * e, ip, u)
+            self.p.evolve(e * (1.0 - 2.0 * self.lam), ip, u)
+            self.u.evolve(0.5 * e, ip, u)
+            if k < self.nstep:
+                self.p.evolve(2.0 * e * self.lam, ip, u)
+        self.p.evolve(e * self.lam, ip, u)
+
+
+class Leapfrog:
+    """Integrator_Leapfrog::evolve (src/lib/HMC/integrator_Leapfrog.cpp)."""
+
+    def __init__(self, update_p, inner, nstep):
+        self.p, self.u, self.nstep = update_p, inner, nstep
+
+    def evolve(self, step, ip, u):
+        if self.nstep <= 0:
+            return
+        e = step / self.nstep
+        self.p.evolve(0.5 * e, ip, u)
+        for k in range(1, self.nstep + 1):
+            self.u.evolve(e, ip, u)
+            if k < self.nstep:
+                self.p.evolve(e, ip, u)
+        self.p.evolve(0.5 * e, ip, u)
+
+
+# Gell-Mann basis: i lambda_a as (row, col, re, im) entries
+_ILAMBDA = (
+    ((0, 1, 0, 1), (1, 0, 0, 1)),
+    ((0, 1, 1, 0), (1, 0, -1, 0)),
+    ((0, 0, 0, 1), (1, 1, 0, -1)),
+    ((0, 2, 0, 1), (2, 0, 0, 1)),
+    ((0, 2, 1, 0), (2, 0, -1, 0)),
+    ((1, 2, 0, 1), (2, 1, 0, 1)),
+    ((1, 2, 1, 0), (2, 1, -1, 0)),
+    ((0, 0, 0, 3 ** -0.5), (1, 1, 0, 3 ** -0.5), (2, 2, 0, -2 * 3 ** -0.5)),
+)
+
+
+class DeviceNoise:
+    """Gaussian heatbath fields drawn on the device (torch's Philox stream):
+    momenta iP = i sum_a h_a lambda_a with <h_a^2> = 1/2, so that
+    P(iP) ~ exp(-|iP|^2/2) as Langevin_Momentum::set_iP
+    (src/lib/HMC/langevin_Momentum.cpp:86-140), and pseudofermion noise with
+    variance 1/2 per real component (RandomNumbers::gauss,
+    src/lib/Tools/randomNumbers.cpp:64-75).  Every component is iid, so the
+    noise is drawn straight in the device field layout."""
+
+    def __init__(self, seed):
+        import torch
+        self.g = torch.Generator(device="cuda")
+        self.g.manual_seed(int(seed))
+        m = torch.zeros(8, 18, dtype=torch.float64)
+        for a, entries in enumerate(_ILAMBDA):
+            for r, c, re, im in entries:
+                m[a, 2 * (c + 3 * r)] = re
+                m[a, 2 * (c + 3 * r) + 1] = im
+        self.m = m.cuda()
+
+    def momentum(self, ip):
+        import torch
+        h = torch.empty(ip.numel() // 18, 8, dtype=torch.float64, device="cuda")
+        h.normal_(0.0, 0.5 ** 0.5, generator=self.g)
+        ip.view(-1, 18).copy_(h @ self.m)
+
+    def fermion(self, field):
+        field.buf.view(dtype=__import__("torch").float64).normal_(0.0, 0.5 ** 0.5, generator=self.g)
+
+
+class HostNoise:
+    """Heatbath fields handed in from outside (for instance recorded from the
+    reference's own random-number generator): momenta in the lexical
+    Field_G layout, pseudofermion noise as even-site corelib spinors."""
+
+    def __init__(self, ip_lex, xis):
+        self.ip, self.xis = ip_lex, list(xis)
+        self.k = 0
+
+    def momentum(self, ip):
+        import torch
+        ip.copy_(torch.from_numpy(np.ascontiguousarray(self.ip, np.float64)))
+
+    def fermion(self, field):
+        field.op.convert(field, self.xis[self.k])
+        self.k += 1
+
+
+class HMCGeneral:
+    """HMC_General (src/lib/HMC/hmc_General.cpp:166-356) over device fields:
+    langevin (momenta + every action's heatbath), the nested integrator
+    built as Builder_Integrator::build_omelyan does
+    (src/lib/HMC/builder_Integrator.cpp:226-255), the Hamiltonian and the
+    Metropolis test.  actions: list of (level, action) in the reference's
+    registration order; nstep: steps per level (level 0 outermost)."""
+
+    def __init__(self, lattice, actions, director, nstep, tau=1.0, lam=0.1931833275,
+                 nprec=8, integrator="Omelyan"):
+        import torch
+        self.lattice = list(lattice)
+        self.nvol = int(np.prod(lattice))
+        self._L = (ctypes.c_int * 4)(*lattice)
+        self.actions = [a for _, a in actions]
+        self.director = director
+        self.tau = tau
+        n = 18 * 4 * self.nvol
+        self.fbuf = torch.zeros(n, dtype=torch.float64, device="cuda")
+        self.gbuf = torch.zeros(n, dtype=torch.float64, device="cuda")
+        self.update_u = UpdateU(self, nprec)
+        inner = self.update_u
+        self.update_ps = []
+        for lv in range(len(nstep) - 1, -1, -1):
+            up = UpdateP(self, [a for l, a in actions if l == lv])
+            self.update_u.clients.append(up)
+            self.update_ps.append(up)
+            inner = (Omelyan(up, inner, nstep[lv], lam) if integrator == "Omelyan"
+                     else Leapfrog(up, inner, nstep[lv]))
+        self.integrator = inner
+        self.u = None
+
+    def set_config(self, u):
+        self.u = u
+        self.director.set_config(u)
+        for a in self.actions:
+            if not a.fermion:
+                a.u = u
+
+    def level_force(self, actions, u, out):
+        """Integrator_UpdateP's summed force of one level into out."""
+        out.zero_()
+        ferm = [a for a in actions if a.fermion]
+        if ferm:
+            self.fbuf.zero_()
+            for a in ferm:
+                a.force_udiv(self.fbuf)
+            self.director.jacobian(self.fbuf)
+            check(lib().b200_force_mult_generator(self._L, _p(self.fbuf), _p(u), None))
+            out.add_(self.fbuf)
+        for a in actions:
+            if not a.fermion:
+                a.force(self.gbuf)
+                out.add_(self.gbuf)
+
+    def momentum_energy(self, ip):
+        h = ctypes.c_double()
+        check(lib().b200_momentum_energy(self._L, _p(ip), ctypes.byref(h), None))
+        return h.value
+
+    def langevin(self, ip, noise):
+        """HMC_General::langevin: returns (H_total, per-action values)."""
+        from . import Field
+        for up in self.update_ps:
+            up.valid = False
+        self.director.notify_linkv()
+        noise.momentum(ip)
+        parts = [self.momentum_energy(ip)]
+        for a in self.actions:
+            if a.fermion:
+                xi = getattr(a, "_xi", None)
+                if xi is None:
+                    xi = a._xi = Field(a.f.op if hasattr(a, "f") else a.fb.op)
+                noise.fermion(xi)
+                parts.append(a.langevin(xi))
+            else:
+                parts.append(a.langevin())
+        return sum(parts), parts
+
+    def calc_hamiltonian(self, ip):
+        parts = [self.momentum_energy(ip)] + [a.calcH() for a in self.actions]
+        return sum(parts), parts
+
+    def trajectory(self, u, noise):
+        """One trajectory from links u (device, modified in place): returns
+        a dict with H0, H1, dH and the per-action parts."""
+        import torch
+        self.set_config(u)
+        ip = torch.zeros_like(u)
+        h0, p0 = self.langevin(ip, noise)
+        self.integrator.evolve(self.tau, ip, u)
+        h1, p1 = self.calc_hamiltonian(ip)
+        return dict(H0=h0, H1=h1, dH=h1 - h0, parts0=p0, parts1=p1, ip=ip)
+
+    def update(self, u, noise, rng):
+        """HMC_General::update: trajectory + Metropolis (FP64, host uniform
+        number from rng); u keeps the accepted links."""
+        u_old = u.clone()
+        r = self.trajectory(u, noise)
+        accept = rng.random() <= np.exp(-r["dH"])
+        if not accept:
+            u.copy_(u_old)
+        r["accepted"] = bool(accept)
+        return r
+
+    @property
+    def force_evaluations(self):
+        return {len(self.update_ps) - 1 - i: up.evaluations for i, up in enumerate(self.update_ps)}
+
+
+def build_dwf_nf2p1(lattice, Ls, M0, masses, beta, c_plaq=3.648, c_rect=-0.331, rho=0.1,
+                    nsmear=2, nstep=(2, 1, 3), level=(0, 0, 1, 2), tau=1.0,
+                    lam=0.1931833275, nprec=8, np_md=16, np_h=24, rat_bounds=(1e-2, 3.16227766),
+                    tol2_md=1e-20, tol2_h=1e-20, solvers=None, b=1.0, c=0.0,
+                    bc=(1, 1, 1, -1), integrator="Omelyan"):
+    """The benchmark driver's action set (hmc_dwf_eo.cpp:155-352) on the
+    device.  masses: dict l (light), h (Hasenbusch), s (strange), pv.
+    solvers: dict of Solver objects 'l_md', 'l_h', 'h_md', 'h_h', 'pv_h'
+    (default FP64 CG at tol2_md / tol2_h)."""
+    from . import DomainWall
+    from .rational import Rational
+    dr = DirectorSmear(lattice, rho, nsmear)
+
+    def fopr(m):
+        return FoprSmeared(DomainWall(lattice, Ls, m, M0, b=b, c=c, bc=bc), dr)
+
+    lo, hi = rat_bounds
+    rats = dict(md_numer=Rational(np_md, 1, 4, lo, hi), md_denom=Rational(np_md, -1, 2, lo, hi),
+                h_numer=Rational(np_h, 1, 4, lo, hi), h_denom=Rational(np_h, -1, 2, lo, hi),
+                psf_denom=Rational(np_h, 1, 4, lo, hi), psf_numer=Rational(np_h, -1, 4, lo, hi))
+    # one operator per distinct mass: the Pauli-Villars operator serves the
+    # rational ratio and the outer Hasenbusch ratio alike
+    f_s, f_l, f_h, f_pv = (fopr(masses[k]) for k in ("s", "l", "h", "pv"))
+    f_pv1 = f_pv
+    sv = dict(solvers or {})
+    for k, t in (("l_md", tol2_md), ("h_md", tol2_md), ("l_h", tol2_h), ("h_h", tol2_h),
+                 ("pv_h", tol2_h)):
+        sv.setdefault(k, Solver("cg", t))
+    nf1 = ActionFRationalRatio(f_pv1, f_s, rats, tol2_md, tol2_h, "Nf1")
+    nf2 = ActionFRatio(f_h, f_l, sv["l_md"], sv["l_h"], sv["h_h"], "Nf2")
+    nf2p = ActionFRatio(f_pv, f_h, sv["h_md"], sv["h_h"], sv["pv_h"], "Nf2_prec")
+    gauge = ActionGRectangle(lattice, beta, c_plaq, c_rect)
+    acts = list(zip(level, (nf1, nf2, nf2p, gauge)))
+    hmc = HMCGeneral(lattice, acts, dr, list(nstep), tau, lam, nprec, integrator)
+    hmc.solvers = sv
+    hmc.fermions = dict(nf1=nf1, nf2=nf2, nf2p=nf2p)
+    return hmc

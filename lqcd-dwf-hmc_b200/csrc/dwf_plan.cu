@@ -1170,50 +1170,54 @@ static ForceParams force_base(const b200_dwf_t* op, double* force, int ieo) {
   return f;
 }
 
-int b200_dwf_force_udiv1(b200_dwf_t* op, const char* mode, double* force, const void* a,
-                         const void* b, void* stream) {
-  if (!op || !mode || !force || !a || !b) return fail(B200_EINVAL, "invalid argument");
-  if (misaligned(a) || misaligned(b)) return fail(B200_EINVAL, "field pointers must be 16-byte aligned");
+// force = beta * force + scale * force_udiv1 (mode "H"/"Hdag", reference
+// argument order) or force_udiv (mode "DdagD", a = eta, b unused).
+static int force_impl(b200_dwf_t* op, const char* mode, double* force, const void* a,
+                      const void* b, double scale, double beta, cudaStream_t st) {
+  if (!op || !mode || !force || !a) return fail(B200_EINVAL, "invalid argument");
   if (op->k.alpha != 1.0)
     return fail(B200_EINVAL, "force with parameter_alpha != 1 is not available (as in the reference)");
   const std::string m = mode;
-  if (m != "H" && m != "Hdag") return fail(B200_EINVAL, "%s: unknown mode %s", "Force_F_Domainwall_eo", mode);
-  cudaStream_t st = (cudaStream_t)stream;
+  const bool udiv = (m == "DdagD");
+  if (!udiv && m != "H" && m != "Hdag")
+    return fail(B200_EINVAL, "%s: unknown mode %s", "Force_F_Domainwall_eo", mode);
+  if (!udiv && !b) return fail(B200_EINVAL, "invalid argument");
+  if (misaligned(a) || (b && misaligned(b)))
+    return fail(B200_EINVAL, "field pointers must be 16-byte aligned");
   const bool hdag = (m == "Hdag");
-  const void* eta = hdag ? a : b;     // reference argument order
-  const void* zeta = hdag ? b : a;
+  const void* eta = udiv ? a : (hdag ? a : b);
+  const void* zeta = udiv ? nullptr : (hdag ? b : a);
   int rc;
-  if ((rc = force_fields(op, eta, zeta, false, st))) return rc;
+  if ((rc = force_fields(op, eta, zeta, udiv, st))) return rc;
   void* ye = op->work[0][PREC_F64];
   void* yo = op->work[1][PREC_F64];
   void* ae = op->work[2][PREC_F64];
   void* ao = op->work[3][PREC_F64];
   ForceParams fe = force_base(op, force, 0), fo = force_base(op, force, 1);
-  if (!hdag) { fe.y1 = yo; fe.z1 = ae; fo.y1 = ye; fo.z1 = ao; }
-  else { fe.y2 = ao; fe.z2 = ye; fo.y2 = ae; fo.z2 = yo; }
+  fe.coef *= scale; fo.coef *= scale;
+  fe.beta = beta; fo.beta = beta;
+  if (udiv || !hdag) { fe.y1 = yo; fe.z1 = ae; fo.y1 = ye; fo.z1 = ao; }
+  if (udiv || hdag) { fe.y2 = ao; fe.z2 = ye; fo.y2 = ae; fo.z2 = yo; }
   B200_CHECK_CUDA(launch_force(fe, st));
   B200_CHECK_CUDA(launch_force(fo, st));
   return 0;
 }
 
+int b200_dwf_force_udiv1(b200_dwf_t* op, const char* mode, double* force, const void* a,
+                         const void* b, void* stream) {
+  if (mode && std::string(mode) == "DdagD")
+    return fail(B200_EINVAL, "%s: unknown mode %s", "Force_F_Domainwall_eo", mode);
+  if (!b) return fail(B200_EINVAL, "invalid argument");
+  return force_impl(op, mode, force, a, b, 1.0, 0.0, (cudaStream_t)stream);
+}
+
 int b200_dwf_force_udiv(b200_dwf_t* op, double* force, const void* eta, void* stream) {
-  if (!op || !force || !eta) return fail(B200_EINVAL, "invalid argument");
-  if (misaligned(eta)) return fail(B200_EINVAL, "field pointers must be 16-byte aligned");
-  if (op->k.alpha != 1.0)
-    return fail(B200_EINVAL, "force with parameter_alpha != 1 is not available (as in the reference)");
-  cudaStream_t st = (cudaStream_t)stream;
-  int rc;
-  if ((rc = force_fields(op, eta, nullptr, true, st))) return rc;
-  void* ye = op->work[0][PREC_F64];
-  void* yo = op->work[1][PREC_F64];
-  void* ae = op->work[2][PREC_F64];
-  void* ao = op->work[3][PREC_F64];
-  ForceParams fe = force_base(op, force, 0), fo = force_base(op, force, 1);
-  fe.y1 = yo; fe.z1 = ae; fe.y2 = ao; fe.z2 = ye;
-  fo.y1 = ye; fo.z1 = ao; fo.y2 = ae; fo.z2 = yo;
-  B200_CHECK_CUDA(launch_force(fe, st));
-  B200_CHECK_CUDA(launch_force(fo, st));
-  return 0;
+  return force_impl(op, "DdagD", force, eta, nullptr, 1.0, 0.0, (cudaStream_t)stream);
+}
+
+int b200_dwf_force_acc(b200_dwf_t* op, const char* mode, double* force, const void* a,
+                       const void* b, double scale, void* stream) {
+  return force_impl(op, mode, force, a, b, scale, 1.0, (cudaStream_t)stream);
 }
 
 int b200_tuning_table(char* buf, size_t n) {

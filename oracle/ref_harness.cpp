@@ -37,6 +37,20 @@
 //             (src/lib/Smear/forceSmear_APE.cpp, projection_Stout_SU3.cpp
 //             force_recursive) applied to in_dir/sigma.bin from the top
 //             level down to the thin links: jacobian.bin.
+//   traj    : one 2+1-flavour HMC trajectory with the action set, smearing
+//             and nested integrator of the reference's benchmark driver
+//             (benchmark_hmc_dwf_corelib/hmc_dwf_eo.cpp:155-352): rational
+//             ratio (PV / strange) and two Hasenbusch ratios (prec / light,
+//             PV / prec), all on stout-smeared links, plus the rectangle
+//             gauge action, under Builder_Integrator (Omelyan or Leapfrog)
+//             and HMC_General::langevin / calc_Hamiltonian.  The Gaussian
+//             fields the random-number generator hands out are recorded:
+//             mom.bin (iP after the momentum heatbath), xi_<k>.bin (the
+//             even-site noise of the k-th fermion action, Field(24, Nvol/2,
+//             Ls)); the end links and momenta go to u_end.bin / mom_end.bin
+//             and the Hamiltonians to traj.txt; force_<i>.bin holds each
+//             action's force at the start links.  The rational coefficient
+//             files (Math_Rational format) are read from in_dir.
 
 #include <cstdio>
 #include <cstdlib>
@@ -66,6 +80,18 @@
 #include "Force/Gauge/force_G_Rectangle.h"
 #include "Action/Gauge/action_G_Rectangle.h"
 #include "IO/bridgeIO.h"
+#include "Field/index_eo.h"
+#include "Fopr/fopr_Smeared_eo.h"
+#include "Force/Fermion/force_F_Smeared.h"
+#include "Force/Fermion/force_F_Rational_Ratio.h"
+#include "Action/Fermion/action_F_Ratio_eo.h"
+#include "Action/Fermion/action_F_Rational_Ratio_eo.h"
+#include "Measurements/Fermion/fprop_Standard_eo.h"
+#include "HMC/action_list.h"
+#include "HMC/builder_Integrator.h"
+#include "HMC/hmc_General.h"
+#include "Tools/randomNumbers_Mseries.h"
+#include <unistd.h>
 
 using Bridge::vout;
 
@@ -146,12 +172,199 @@ Parameters dwf_params(const Kv& kv)
   return p;
 }
 
+// M-series generator that keeps a copy of every Gaussian field it hands out,
+// so the same momenta and pseudofermion noise can drive another
+// implementation of the trajectory.
+class RecordingMseries : public RandomNumbers_Mseries {
+ public:
+  explicit RecordingMseries(int seed) : RandomNumbers_Mseries(seed) {}
+  void gauss_lex_global(Field& f) {
+    RandomNumbers::gauss_lex_global(f);
+    record.push_back(f);
+  }
+  std::vector<Field> record;
+};
+
+Parameters rational_params(const Kv& kv, int np, int n_exp, int d_exp, double tol)
+{
+  Parameters p;
+  p.set_int("number_of_poles", np);
+  p.set_int("exponent_numerator", n_exp);
+  p.set_int("exponent_denominator", d_exp);
+  p.set_double("lower_bound", getd(kv, "rat_lo", 1e-2));
+  p.set_double("upper_bound", getd(kv, "rat_hi", 3.16227766));
+  p.set_int("maximum_number_of_iteration", geti(kv, "rat_maxiter", 10000));
+  p.set_double("convergence_criterion_squared", tol);
+  p.set_string("verbose_level", "Crucial");
+  return p;
+}
+
+Parameters dwf_mass(const Kv& kv, const char *key)
+{
+  Parameters p = dwf_params(kv);
+  p.set_double("quark_mass", getd(kv, key, 0.01));
+  return p;
+}
+
+int run_traj(const Kv& kv, const std::string& in_dir, const std::string& out_dir, Field_G& Uorg)
+{
+  const int Nvol = CommonParameters::Nvol();
+  const int Ls = geti(kv, "Ls", 8);
+  const int np_md = geti(kv, "np_md", 16), np_h = geti(kv, "np_h", 24);
+  const double tol_md = getd(kv, "tol_md", 1e-24), tol_h = getd(kv, "tol_h", 1e-24);
+  const int cg_iter = geti(kv, "cg_maxiter", 100), cg_restart = geti(kv, "cg_restart", 100);
+
+  // Math_Rational opens its coefficient files relative to the working directory
+  std::string abs_out = out_dir;
+  if (abs_out[0] != '/') {
+    char cwd[4096];
+    if (getcwd(cwd, sizeof(cwd))) abs_out = std::string(cwd) + "/" + out_dir;
+  }
+  if (chdir(in_dir.c_str()) != 0) { fprintf(stderr, "cannot chdir %s\n", in_dir.c_str()); return 2; }
+
+  // through Parameters, as Action::New does in the driver: only this form
+  // also configures the action's Force_G_Rectangle
+  Parameters pg;
+  pg.set_double("beta", getd(kv, "beta", 2.13));
+  pg.set_double("c_plaq", getd(kv, "c_plaq", 3.648));
+  pg.set_double("c_rect", getd(kv, "c_rect", -0.331));
+  pg.set_string("verbose_level", "Crucial");
+  Action_G_Rectangle action_G(pg);
+
+  Projection_Stout_SU3 proj;
+  Smear_APE smear(&proj);
+  smear.set_parameters(getd(kv, "rho", 0.1));
+  ForceSmear_APE force_smear(&proj);
+  force_smear.set_parameters(getd(kv, "rho", 0.1));
+  Director_Smear dr_smear(&smear);
+  dr_smear.set_parameters(geti(kv, "nsmear", 2));
+
+  // one flavour: rational ratio det[(B^dag B)^(1/2) / (A^dag A)^(1/2)],
+  // B = strange domain wall, A = Pauli-Villars (mass mq_pv)
+  Fopr_Domainwall_eo fopr_nf1(dwf_mass(kv, "mq_s"));
+  Force_F_Domainwall_eo force_nf1(dwf_mass(kv, "mq_s"));
+  Fopr_Domainwall_eo fopr_nf1_pv(dwf_mass(kv, "mq_pv"));
+  Force_F_Domainwall_eo force_nf1_pv(dwf_mass(kv, "mq_pv"));
+  Parameters prat_md;
+  prat_md.set_Parameters("Fopr_Rational_numerator_MD", rational_params(kv, np_md, 1, 4, tol_md));
+  prat_md.set_Parameters("Fopr_Rational_denominator_MD", rational_params(kv, np_md, -1, 2, tol_md));
+  Force_F_Rational_Ratio force_rat(&fopr_nf1_pv, &force_nf1_pv, &fopr_nf1, &force_nf1, prat_md);
+  Fopr_Smeared_eo fopr_nf1_smr(&fopr_nf1, &dr_smear);
+  Fopr_Smeared_eo fopr_nf1_pv_smr(&fopr_nf1_pv, &dr_smear);
+  Force_F_Smeared force_rat_smr(&force_rat, &force_smear, &dr_smear);
+  Parameters prat_h;
+  prat_h.set_Parameters("Fopr_Rational_numerator_calcH", rational_params(kv, np_h, 1, 4, tol_h));
+  prat_h.set_Parameters("Fopr_Rational_denominator_calcH", rational_params(kv, np_h, -1, 2, tol_h));
+  Action_F_Rational_Ratio_eo action_nf1(&fopr_nf1_pv_smr, &fopr_nf1_smr, &force_rat_smr, prat_h);
+
+  // two flavours: Hasenbusch ratios prec/light and PV/prec
+  Fopr_Domainwall_eo fopr_l(dwf_mass(kv, "mq_l"));
+  Force_F_Domainwall_eo force_l(dwf_mass(kv, "mq_l"));
+  Fopr_Domainwall_eo fopr_h(dwf_mass(kv, "mq_h"));
+  Force_F_Domainwall_eo force_h(dwf_mass(kv, "mq_h"));
+  Fopr_Domainwall_eo fopr_pv(dwf_mass(kv, "mq_pv"));
+  Force_F_Domainwall_eo force_pv(dwf_mass(kv, "mq_pv"));
+  Fopr_Smeared_eo fopr_l_smr(&fopr_l, &dr_smear);
+  Fopr_Smeared_eo fopr_h_smr(&fopr_h, &dr_smear);
+  Fopr_Smeared_eo fopr_pv_smr(&fopr_pv, &dr_smear);
+  Force_F_Smeared force_l_smr(&force_l, &force_smear, &dr_smear);
+  Force_F_Smeared force_h_smr(&force_h, &force_smear, &dr_smear);
+  Force_F_Smeared force_pv_smr(&force_pv, &force_smear, &dr_smear);
+  Solver_CG solver_l_md(&fopr_l_smr), solver_h_md(&fopr_h_smr);
+  Solver_CG solver_l_h(&fopr_l_smr), solver_h_h(&fopr_h_smr), solver_pv_h(&fopr_pv_smr);
+  solver_l_md.set_parameters(cg_iter, cg_restart, tol_md, false);
+  solver_h_md.set_parameters(cg_iter, cg_restart, tol_md, false);
+  solver_l_h.set_parameters(cg_iter, cg_restart, tol_h, false);
+  solver_h_h.set_parameters(cg_iter, cg_restart, tol_h, false);
+  solver_pv_h.set_parameters(cg_iter, cg_restart, tol_h, false);
+  Fprop_Standard_eo fprop_l_md(&solver_l_md), fprop_h_md(&solver_h_md);
+  Fprop_Standard_eo fprop_l_h(&solver_l_h), fprop_h_h(&solver_h_h), fprop_pv_h(&solver_pv_h);
+  Action_F_Ratio_eo action_nf2(&fopr_h_smr, &force_h_smr, &fopr_l_smr, &force_l_smr,
+                               &fprop_h_h, &fprop_l_md, &fprop_l_h);
+  Action_F_Ratio_eo action_nf2_prec(&fopr_pv_smr, &force_pv_smr, &fopr_h_smr, &force_h_smr,
+                                    &fprop_pv_h, &fprop_h_md, &fprop_h_h);
+
+  std::vector<int> level = getiv(kv, "level");
+  std::vector<int> nstep = getiv(kv, "nstep");
+  if (level.size() != 4 || nstep.empty()) { fprintf(stderr, "level/nstep missing\n"); return 2; }
+  ActionList actions(int(nstep.size()));
+  actions.append(level[0], &action_nf1);
+  actions.append(level[1], &action_nf2);
+  actions.append(level[2], &action_nf2_prec);
+  actions.append(level[3], &action_G);
+  std::vector<Director *> directors(1, &dr_smear);
+
+  Parameters pint;
+  Kv::const_iterator iit = kv.find("integrator");
+  pint.set_string("integrator", iit == kv.end() ? std::string("Omelyan") : iit->second[0]);
+  pint.set_int("number_of_levels", int(nstep.size()));
+  pint.set_int_vector("level_of_actions", level);
+  pint.set_int_vector("number_of_steps", nstep);
+  pint.set_int("order_of_exp_iP", geti(kv, "nprec", 8));
+  pint.set_double("lambda_Omelyan", getd(kv, "lambda", 0.1931833275));
+  pint.set_string("verbose_level", "Crucial");
+  Builder_Integrator builder(actions, directors, pint);
+  Integrator *integrator = builder.build();
+
+  RecordingMseries rand(geti(kv, "seed", 1234567));
+  Parameters phmc;
+  phmc.set_double("trajectory_length", getd(kv, "tau", 1.0));
+  phmc.set_string("Metropolis_test", "false");
+  phmc.set_string("verbose_level", "Crucial");
+  HMC_General hmc(actions, directors, integrator, &rand, phmc);
+
+  // HMC_General::update (src/lib/HMC/hmc_General.cpp) without the Metropolis
+  // step, with the random fields and both Hamiltonians kept
+  Field_G U(Uorg);
+  ActionSet all = actions.get_actions();
+  for (size_t i = 0; i < all.size(); ++i) all[i]->set_config(&U);
+  Field_G iP(Nvol, 4);
+  const double H0 = hmc.langevin(iP, U);
+  const size_t ng = size_t(18) * Nvol * 4;
+  write_bin(abs_out + "/mom.bin", iP.ptr(0), ng);
+  Index_eo index;
+  int k = 0;
+  for (size_t r = 0; r < rand.record.size(); ++r) {
+    if (rand.record[r].nin() != 24) continue;     // the momentum draw (8 reals per link)
+    Field xi(24, Nvol / 2, Ls);
+    index.convertField(xi, rand.record[r], 0);
+    char name[64];
+    snprintf(name, sizeof(name), "/xi_%d.bin", k++);
+    write_bin(abs_out + name, xi.ptr(0), size_t(24) * (Nvol / 2) * Ls);
+  }
+  std::vector<double> h_start(all.size());
+  for (size_t i = 0; i < all.size(); ++i) h_start[i] = all[i]->calcH();
+  // each action's force (Action::force, after mult_generator) at the start
+  for (size_t i = 0; i < all.size(); ++i) {
+    Field_G F(Nvol, 4);
+    all[i]->force(F);
+    char name[64];
+    snprintf(name, sizeof(name), "/force_%zu.bin", i);
+    write_bin(abs_out + name, F.ptr(0), ng);
+  }
+  integrator->evolve(getd(kv, "tau", 1.0), iP, U);
+  const double H1 = hmc.calc_Hamiltonian(iP, U);
+  std::vector<double> h_end(all.size());
+  for (size_t i = 0; i < all.size(); ++i) h_end[i] = all[i]->calcH();
+  write_bin(abs_out + "/u_end.bin", U.ptr(0), ng);
+  write_bin(abs_out + "/mom_end.bin", iP.ptr(0), ng);
+  FILE *f = fopen((abs_out + "/traj.txt").c_str(), "w");
+  fprintf(f, "H0 %.17e\nH1 %.17e\ndH %.17e\n", H0, H1, H1 - H0);
+  fprintf(f, "h_start");
+  for (size_t i = 0; i < all.size(); ++i) fprintf(f, " %.17e", h_start[i]);
+  fprintf(f, "\nh_end");
+  for (size_t i = 0; i < all.size(); ++i) fprintf(f, " %.17e", h_end[i]);
+  fprintf(f, "\n");
+  fclose(f);
+  return 0;
+}
+
 }  // namespace
 
 int main(int argc, char **argv)
 {
   if (argc < 5) {
-    fprintf(stderr, "usage: %s <modes|cg|shiftcg|time|force|smear|gauge> params.txt in_dir out_dir\n", argv[0]);
+    fprintf(stderr, "usage: %s <modes|cg|shiftcg|time|force|smear|gauge|traj> params.txt in_dir out_dir\n", argv[0]);
     return 2;
   }
   const std::string cmd = argv[1];
@@ -179,6 +392,8 @@ int main(int argc, char **argv)
   Parameters pf = dwf_params(kv);
   Fopr_Domainwall_eo fopr(pf);
   fopr.set_config(&U);
+
+  if (cmd == "traj") return run_traj(kv, in_dir, out_dir, U);
 
   const size_t nsp = size_t(24) * Nvol2 * Ls;
   Field src(24, Nvol2, Ls), out(24, Nvol2, Ls);

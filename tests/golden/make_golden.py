@@ -51,6 +51,18 @@ GAUGE = dict(lattice=[4, 6, 4, 8], Ls=4, mq=0.01, M0=1.8, b=1.0, c=0.0, alpha=1.
 # force: Moebius (alpha must be 1 for Force_F_Domainwall_eo), antiperiodic t
 FORCE = dict(lattice=[4, 4, 4, 4], Ls=4, mq=0.02, M0=1.4, b=1.5, c=0.5, alpha=1.0,
              bc=[1, 1, 1, -1], gauge=("near", 31), src=32, src2=33)
+# one 2+1-flavour trajectory of the benchmark driver's action set on the
+# 4^3x8 Ls=8 Shamir hot start: light 0.01 over Hasenbusch 0.1 over PV 1.0,
+# strange 0.04 as a PV rational ratio with 10-pole approximations, Iwasaki
+# beta 2.13, 2 stout levels rho 0.1, Omelyan [2,1,3], length 1.  The momenta
+# and pseudofermion noise of the reference's M-series generator (seed
+# 1234567) are stored with the results.
+TRAJ = dict(lattice=[4, 4, 4, 8], Ls=8, mq=0.01, M0=1.8, b=1.0, c=0.0, alpha=1.0,
+            bc=[1, 1, 1, -1], gauge=("hot", 101), src=102,
+            mq_l=0.01, mq_h=0.1, mq_s=0.04, mq_pv=1.0, beta=2.13, c_plaq=3.648,
+            c_rect=-0.331, rho=0.1, nsmear=2, tau=1.0, nstep=[2, 1, 3], level=[0, 0, 1, 2],
+            integrator="Omelyan", lambda_=0.1931833275, nprec=8, np_md=10, np_h=10,
+            rat_lo=0.01, rat_hi=3.16227766, tol_md=1e-24, tol_h=1e-24, seed=1234567)
 
 
 def write_params(path, case, extra=None):
@@ -82,7 +94,32 @@ def run(cmd, case, extra, tmp):
                    check=True, stdout=subprocess.DEVNULL)
 
 
+def traj():
+    import shutil
+    from b200dwf.rational import TABLE_DIR
+    keys = ("mq_l", "mq_h", "mq_s", "mq_pv", "beta", "c_plaq", "c_rect", "rho", "nsmear",
+            "tau", "nstep", "level", "integrator", "nprec", "np_md", "np_h", "rat_lo",
+            "rat_hi", "tol_md", "tol_h", "seed")
+    extra = {k: TRAJ[k] for k in keys}
+    extra["lambda"] = TRAJ["lambda_"]
+    with tempfile.TemporaryDirectory() as tmp:
+        for name in os.listdir(TABLE_DIR):
+            shutil.copy(os.path.join(TABLE_DIR, name), tmp)
+        run("traj", TRAJ, extra, tmp)
+        out = {k: np.fromfile(os.path.join(tmp, k + ".bin"))
+               for k in ("mom", "xi_0", "xi_1", "xi_2", "u_end", "mom_end",
+                         "force_0", "force_1", "force_2", "force_3")}
+        for line in open(os.path.join(tmp, "traj.txt")):
+            key, *vals = line.split()
+            out[key] = np.array([float(v) for v in vals])
+    np.savez_compressed(os.path.join(HERE, "traj_nf2p1.npz"), meta=json.dumps(TRAJ), **out)
+    print("wrote traj_nf2p1.npz: H0 %.10f dH %.10f" % (out["H0"][0], out["dH"][0]))
+
+
 def main():
+    if sys.argv[1:] == ["traj"]:
+        traj()
+        return
     for name, case in CASES.items():
         with tempfile.TemporaryDirectory() as tmp:
             run("modes", case, {"modes": " ".join(case["modes"])}, tmp)
@@ -138,6 +175,7 @@ def main():
                         **{"shift_%d" % i: v for i, v in enumerate(xs)})
     print("wrote solve_shamir.npz", info.strip().replace("\n", " "),
           sinfo.strip().replace("\n", " "))
+    traj()
 
 
 if __name__ == "__main__":
