@@ -19,6 +19,7 @@ reference corelib CPU path timed on this host as the CPU baseline.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 """
 import argparse
+import gc
 import json
 import os
 import subprocess
@@ -63,13 +64,14 @@ def parse():
     ap.add_argument("--learned-epochs", type=int, default=2)
     ap.add_argument("--no-trajectory", action="store_true",
                     help="skip the molecular-dynamics trajectory timing")
-    ap.add_argument("--traj-steps", type=int, default=5)
-    ap.add_argument("--traj-flavours", default="2+1", choices=["2", "2+1"],
-                    help="light two-flavour DWF only, or plus an RHMC strange quark")
-    ap.add_argument("--traj-length", type=float, default=0.05)
-    ap.add_argument("--traj-lattice", type=int, nargs=4, default=None,
-                    help="lattice of the trajectory timing (default: the Dslash workload's); "
-                         "e.g. 24 24 24 48 for the batched-RHMC configuration's volume")
+    ap.add_argument("--traj-nstep", type=int, nargs=3, default=[2, 1, 3],
+                    help="Omelyan steps per level (rational + light ratio, Hasenbusch, gauge)")
+    ap.add_argument("--traj-length", type=float, default=0.1,
+                    help="trajectory length (0.1 as in the reference's published runs)")
+    ap.add_argument("--traj-all-forms", action="store_true",
+                    help="also time FP64 CG with the windowed multishift")
+    ap.add_argument("--traj-lattice", type=int, nargs=4, default=[24, 24, 24, 48],
+                    help="lattice of the 2+1-flavour trajectory timing")
     return ap.parse_args()
 
 
@@ -291,77 +293,87 @@ def learned_section(op, lattice, w, u_workload, args):
 
 
 # ------------------------------------------------------------------ trajectory
+TRAJ_MASSES = dict(l=MQ, h=0.1, s=MS, pv=1.0)
+
+
 def trajectory_section(op, lattice, u_workload, args, lp=None):
-    if args.traj_lattice and list(args.traj_lattice) != list(lattice):
-        # another volume: its own operator and configuration (near-unit links +
-        # 2 stout steps, smeared on the device); the trained network's weights
-        # are volume independent and are carried over
-        import b200dwf
-        from b200dwf import synth
-        lattice = list(args.traj_lattice)
-        sm = b200dwf.StoutSmear(lattice, 0.1, 2)
-        sm.set_config(synth.gauge_field(lattice, SEED_U + 3, "near", 0.3))
-        u_workload = sm.config(2)
-        op = b200dwf.DomainWall(lattice, LS, MQ, M0, 1.0, 0.0, 1.0, (1, 1, 1, -1))
-        op.set_config(u_workload)
-        if lp is not None:
-            lp2 = b200dwf.LearnedPrecond(op, hidden=lp.hidden, seed=1)
-            lp2.set_weights(lp.weights(deployed=False))
-            lp = lp2
-    return _trajectory(op, lattice, u_workload, args, lp)
-
-
-def _trajectory(op, lattice, u_workload, args, lp):
-    """One leapfrog molecular-dynamics trajectory of 2+1-flavour domain-wall
-    fermions (light: two-flavour action with the workload's operator; strange:
-    one-flavour RHMC over the multishift solver) + the Iwasaki gauge action
-    (beta 2.13), every operator, solve, force and update on the device,
-    timed with each light-quark solver to |r|/|b| < 1e-10: plain FP64 CG,
-    mixed-precision Richardson (f16 storage, FP32 inner, FP64 outer) and,
-    when a trained network is given, the learned flexible CG."""
+    """One 2+1-flavour HMC trajectory with the reference benchmark driver's
+    action set (benchmark_hmc_dwf_corelib/hmc_dwf_eo.cpp): strange quark as
+    a rational ratio over Pauli-Villars (16 poles in the force, 24 in the
+    heatbath and Hamiltonian, FP64 multishift), the light pair as two
+    Hasenbusch ratios (light 0.01 / 0.1 / PV 1.0), Iwasaki beta 2.13, stout
+    smeared fermion links (2 x rho 0.1), nested Omelyan [2,1,3], length 0.1,
+    momenta and pseudofermion noise from the device generator (the same
+    seed for every form).  Timed per form, all solves to |r|/|b| < 1e-10:
+    plain = FP64 CG and the multishift updating every shift every iteration;
+    batched = the multishift's windowed shift updates, with mixed-precision
+    Richardson (f16 storage, FP32 inner, FP64 outer) for the light,
+    Hasenbusch and PV solves and, when a trained network is given, the
+    learned flexible CG for the light solves."""
     import torch
     import b200dwf
     from b200dwf import synth
-    from b200dwf.hmc import GaugeMD, TwoFlavour, Rational
-    from b200dwf.rational import inv_sqrt_partial_fractions
-    ip = synth.algebra_field(lattice, SEED_U + 7, 1.0)
-    xi = op.new_field(0)
-    op.convert(xi, synth.spinor_field(lattice, LS, SEED_B + 7))
-    psi = op.new_field(0)
-    op.set_config(u_workload)
-    op.mult_dag(psi, xi, "D")                 # heatbath: psi = D^+ xi
-    # strange quark: one-flavour RHMC, 16 poles on [1e-4, 10], FP64 multishift
-    ops = b200dwf.DomainWall(lattice, LS, MS, M0, 1.0, 0.0, 1.0, (1, 1, 1, -1))
-    ops.set_config(u_workload)
-    phi = ops.new_field(0)
-    ops.convert(phi, synth.spinor_field(lattice, LS, SEED_B + 8))
-    ra0, rb, rc = inv_sqrt_partial_fractions(1e-4, 10.0, 16)
-    solvers = [("fp64_cg", "cg"), ("mixed_f16", "mixed")]
+    from b200dwf.hmc import build_dwf_nf2p1, DeviceNoise, Solver
+    lattice = list(args.traj_lattice or lattice)
+    sm = b200dwf.StoutSmear(lattice, 0.1, 2)
+    sm.set_config(synth.gauge_field(lattice, SEED_U + 3, "near", 0.3))
+    u0 = sm.config(2)
+    del sm
+    cg = {k: "cg" for k in ("l_md", "l_h", "h_md", "h_h", "pv_h")}
+    mixed = {k: "mixed" for k in ("l_md", "l_h", "h_md", "h_h", "pv_h")}
+    # (name, solver kinds, multishift window): the plain form is FP64 CG with
+    # every shift updated every iteration; the optimised forms use the
+    # mixed-precision solves and the windowed (batched) multishift
+    forms = [("fp64_plain", cg, 0)]
+    if args.traj_all_forms:
+        forms.append(("fp64_batched", cg, 8))
+    forms.append(("mixed_batched", mixed, 8))
     if lp is not None:
-        solvers.append(("learned_fcg", "learned"))
+        forms.append(("mixed_batched_learned",
+                      dict({k: "mixed" for k in ("h_md", "h_h", "pv_h")}, l_md="learned",
+                           l_h="learned"), 8))
+    tol2 = 1e-20
     res = {}
-    for name, solver in solvers:
-        two = TwoFlavour(op, psi, 1e-20, solver, None, lp)
-        acts = [two] if args.traj_flavours == "2" else [two, Rational(ops, phi, ra0, rb, rc, 1e-20)]
-        md = GaugeMD(lattice, 2.13, fermions=acts)
-        md.trajectory_dh(u_workload, ip, args.traj_length, 1)   # untimed warm-up
-        md.iterations = 0
+    for name, kinds, window in forms:
+        gc.collect()
+        torch.cuda.empty_cache()
+        sv = {k: Solver(v, tol2) for k, v in kinds.items()}
+        hmc = build_dwf_nf2p1(lattice, LS, M0, TRAJ_MASSES, 2.13, nstep=args.traj_nstep,
+                              tau=args.traj_length, np_md=16, np_h=24, tol2_md=tol2, tol2_h=tol2,
+                              solvers=sv, shift_window=window)
+        if "learned" in kinds.values():
+            # the trained weights are volume independent; the network runs on
+            # the light operator's own (smeared) links
+            lp_form = b200dwf.LearnedPrecond(hmc.fermions["nf2"].f.op, hidden=lp.hidden, seed=1)
+            lp_form.set_weights(lp.weights(deployed=False))
+            for v in sv.values():
+                v.lp = lp_form
+        ud = torch.from_numpy(u0.copy()).cuda()
+        hmc.set_config(ud)
+        hmc.warmup()
+        for v in sv.values():
+            v.iterations, v.seconds, v.calls = 0, 0.0, 0
+        for r in hmc.fermions["nf1"].rationals.values():
+            r.iterations, r.seconds, r.calls = 0, 0.0, 0
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        dh, _ = md.trajectory_dh(u_workload, ip, args.traj_length, args.traj_steps)
+        r = hmc.trajectory(ud, DeviceNoise(SEED_U + 11))
         torch.cuda.synchronize()
-        res[name] = {"sec_per_trajectory": time.perf_counter() - t0, "dH": dh,
-                     "light_solver_iterations": two.iterations,
-                     "strange_multishift_iterations": md.iterations - two.iterations}
-    op.set_config(u_workload)
-    out = {"lattice": lattice, "Ls": LS, "mq": MQ, "flavours": args.traj_flavours,
-           "strange": None if args.traj_flavours == "2" else
-           {"mq": MS, "rational": "16 poles, x^-1/2 on [1e-4, 10]", "solver": "FP64 multishift CG"},
-           "gauge": "Iwasaki beta 2.13",
-           "integrator": "leapfrog", "length": args.traj_length, "steps": args.traj_steps,
-           "solver_tol_rel_residual": 1e-10, **res}
+        res[name] = {"sec_per_trajectory": time.perf_counter() - t0, "dH": r["dH"],
+                     "H0": r["H0"], "multishift_window": window, **hmc.stats()}
+        del hmc, ud, r, sv
+    gc.collect()
+    torch.cuda.empty_cache()
+    out = {"lattice": lattice, "Ls": LS, "M0": M0, "masses": TRAJ_MASSES,
+           "actions": "rational ratio (strange / PV, 16|24 poles, FP64 multishift), "
+                      "Hasenbusch ratios light/0.1 and 0.1/PV, Iwasaki beta 2.13, "
+                      "2 stout rho 0.1 on the fermion links",
+           "integrator": "Omelyan %s, lambda 0.1931833275" % list(args.traj_nstep),
+           "length": args.traj_length, "solver_tol_rel_residual": 1e-10,
+           "links": "near-unit exp(i*0.3*H) + 2 stout rho=0.1 (seed %d)" % (SEED_U + 3), **res}
     for name in res:
-        out["speedup_" + name] = res["fp64_cg"]["sec_per_trajectory"] / res[name]["sec_per_trajectory"]
+        out["speedup_" + name] = (res["fp64_plain"]["sec_per_trajectory"]
+                                  / res[name]["sec_per_trajectory"])
     return out
 
 
@@ -485,15 +497,24 @@ def b200_arm(args, rank, world, local_rank):
             del x
         sigma = list(np.logspace(-4, np.log10(64.0), 16))
         xs = [op.new_field(0) for _ in sigma]
-        op.shiftcg(xs, sigma, w, 1e-20, 3)                # untimed warm-up
-        torch.cuda.synchronize()
-        c0 = time.perf_counter()
-        n, diff, rc = op.shiftcg(xs, sigma, w, 1e-20, 20000)
-        torch.cuda.synchronize()
-        c1 = time.perf_counter()
-        solvers["multishift"] = {"shifts": len(sigma), "iterations": n, "max_true_rel_residual": diff,
-                                 "seconds": c1 - c0, "ms_per_iteration": (c1 - c0) * 1e3 / max(n, 1),
-                                 "converged": rc == 0}
+        ms = {}
+        for window in (0, 8, 16):
+            # window 0: every shift's x_i, p_i updated every iteration (the
+            # reference's form); 8 / 16: deferred updates from stored residuals
+            op.set_shift_window(window)
+            op.shiftcg(xs, sigma, w, 1e-20, 20)               # untimed warm-up
+            torch.cuda.synchronize()
+            c0 = time.perf_counter()
+            n, diff, rc = op.shiftcg(xs, sigma, w, 1e-20, 20000)
+            torch.cuda.synchronize()
+            c1 = time.perf_counter()
+            ms["window_%d" % window] = {"iterations": n, "max_true_rel_residual": diff,
+                                        "seconds": c1 - c0,
+                                        "ms_per_iteration": (c1 - c0) * 1e3 / max(n, 1),
+                                        "converged": rc == 0}
+        op.set_shift_window(8)
+        solvers["multishift"] = {"shifts": len(sigma), "sigma": "log-spaced 1e-4..64",
+                                 **ms["window_8"], "by_window": ms}
         del xs
 
     learned, lp = None, None

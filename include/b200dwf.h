@@ -124,6 +124,12 @@ int b200_cg_solve(b200_dwf_t *op, int prec, void *x, const void *b, int maxiter,
 int b200_shiftcg_solve(b200_dwf_t *op, void *const *x, const double *sigma, int nshift,
                        const void *b, int maxiter, double tol2, int *nconv, double *diff,
                        void *stream);
+/* Window m of the multishift solver's deferred shift updates (default 8):
+ * the residuals of m iterations stay in HBM (m extra fields) and every shift's
+ * x_i, p_i are updated once per window; 0 updates every shift every
+ * iteration, as AShiftsolver_CG::solve_step does
+ * (src/lib/Solver/ashiftsolver_CG-tmpl.h:216-286).  m <= 16. */
+int b200_shiftcg_set_window(b200_dwf_t *op, int window);
 
 /* Fprop_alt_Standard_eo_Richardson::invert_DdagD_even
  * (src/lib_alt/Measurements/Fermion/fprop_alt_Standard_eo_Richardson-tmpl.h:

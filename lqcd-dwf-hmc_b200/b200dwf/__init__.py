@@ -66,6 +66,7 @@ def lib():
                                         ctypes.c_int, ctypes.c_double, ip, ip, dp, vp]
     L.b200_dwf_force_udiv1.argtypes = [vp, ctypes.c_char_p, vp, vp, vp, vp]
     L.b200_dwf_force_udiv.argtypes = [vp, vp, vp, vp]
+    L.b200_shiftcg_set_window.argtypes = [vp, ctypes.c_int]
     L.b200_dwf_force_acc.argtypes = [vp, ctypes.c_char_p, vp, vp, vp, ctypes.c_double, vp]
     L.b200_smear_create.argtypes = [ctypes.POINTER(vp), ip, ctypes.c_double, ctypes.c_int]
     L.b200_smear_destroy.argtypes = [vp]
@@ -249,6 +250,10 @@ class DomainWall:
         if rc not in (0, -4):
             check(rc)
         return n.value, d.value, rc
+
+    def set_shift_window(self, window):
+        """Residual window of the multishift solver (0: per-iteration updates)."""
+        check(lib().b200_shiftcg_set_window(self.handle, int(window)))
 
     def richardson(self, x, b, inner_prec, tol2, maxiter=100, tol2_inner=1e-8, maxiter_inner=10000):
         """Mixed-precision Richardson (FP64 outer, inner CG in inner_prec)."""

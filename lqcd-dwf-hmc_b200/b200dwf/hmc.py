@@ -20,6 +20,7 @@ kernels, and the fermion actions' solves and forces.  Actions:
 The leapfrog trajectory conserves H = |iP|^2/2 + sum S up to O(eps^2).
 """
 import ctypes
+import time
 
 import numpy as np
 
@@ -277,8 +278,17 @@ class Solver:
         self.inner_prec = F16 if inner_prec is None else inner_prec
         self.lp = lp
         self.iterations = 0
+        self.seconds = 0.0
+        self.calls = 0
 
     def solve(self, op, x, b):
+        t0 = time.perf_counter()
+        n = self._solve(op, x, b)
+        self.seconds += time.perf_counter() - t0   # the solvers end with a host read
+        self.calls += 1
+        return n
+
+    def _solve(self, op, x, b):
         if self.kind == "cg":
             n, _, rc = op.cg(x, b, self.tol2, self.maxiter)
         elif self.kind == "mixed":
@@ -304,6 +314,8 @@ class FoprRational:
         self.tol2, self.maxiter = tol2, maxiter
         self.xs = None
         self.iterations = 0
+        self.seconds = 0.0
+        self.calls = 0
 
     def shifts(self, b):
         """x_i = (DdagD + c_i)^-1 b (kept in self.xs)."""
@@ -311,7 +323,10 @@ class FoprRational:
         op = self.fopr.sync()
         if self.xs is None:
             self.xs = [Field(op) for _ in self.r.c]
+        t0 = time.perf_counter()
         n, _, rc = op.shiftcg(self.xs, self.r.c, b, self.tol2, self.maxiter)
+        self.seconds += time.perf_counter() - t0
+        self.calls += 1
         if rc != 0:
             raise RuntimeError("multishift solve did not converge")
         self.iterations += n
@@ -394,11 +409,29 @@ class ActionFRationalRatio:
         self.psf, self.v1, self.v2 = Field(op), Field(op), Field(op)
         self.t1, self.t2 = Field(op), Field(op)
         self.fermion = True
+        # one pool of solution vectors: eta1_i in the first np_md slots, eta2_i
+        # and later zeta_i in the next np_md (the denominator's forces are
+        # taken before zeta overwrites eta2), and the heatbath / Hamiltonian
+        # rationals, which only need their sums, in the first np_h slots
+        nmd, nh = len(rats["md_numer"].c), len(rats["h_numer"].c)
+        if len(rats["md_denom"].c) != nmd:
+            raise ValueError("numerator and denominator MD rationals need equal pole counts")
+        self.pool = [Field(op) for _ in range(max(2 * nmd, nh))]
+        self.md_numer.xs = self.pool[:nmd]
+        self.md_denom.xs = self.pool[nmd:2 * nmd]
+        self.md_numer2.xs = self.pool[nmd:2 * nmd]
+        for r in (self.h_numer, self.h_denom, self.psf_denom, self.psf_numer):
+            r.xs = self.pool[:len(r.r.c)]
+
+    @property
+    def rationals(self):
+        return dict(md_numer=self.md_numer, md_denom=self.md_denom, md_numer2=self.md_numer2,
+                    h_numer=self.h_numer, h_denom=self.h_denom, psf_denom=self.psf_denom,
+                    psf_numer=self.psf_numer)
 
     @property
     def iterations(self):
-        return sum(r.iterations for r in (self.md_numer, self.md_denom, self.md_numer2, self.h_numer,
-                                          self.h_denom, self.psf_denom, self.psf_numer))
+        return sum(r.iterations for r in self.rationals.values())
 
     def langevin(self, xi):
         self.psf_denom.mult(self.v1, xi)          # (B^dag B)^(1/4) xi
@@ -422,9 +455,9 @@ class ActionFRationalRatio:
         rn, rd = self.md_numer.r, self.md_denom.r
         self.md_numer.mult(self.v1, self.psf)          # phi2, eta1_i in md_numer.xs
         self.md_denom.mult(self.v2, self.v1)           # xi, eta2_i in md_denom.xs
-        zetas = self.md_numer2.shifts(self.v2)         # zeta_i
         for bi, e2 in zip(rd.b, self.md_denom.xs):
             check(L.b200_dwf_force_acc(fb.handle, b"DdagD", _p(acc), e2.ptr, None, bi, None))
+        zetas = self.md_numer2.shifts(self.v2)         # zeta_i, over the eta2_i slots
         for bi, e1, z in zip(rn.b, self.md_numer.xs, zetas):
             ne, nz = fa.norm2(e1), fa.norm2(z)
             if ne == 0.0 or nz == 0.0:
@@ -710,22 +743,80 @@ class HMCGeneral:
     def force_evaluations(self):
         return {len(self.update_ps) - 1 - i: up.evaluations for i, up in enumerate(self.update_ps)}
 
+    def stats(self):
+        """Iterations, calls and host-side seconds of every solver and
+        multishift of the action set (the solvers end with a host read, so
+        their wall times are device times plus launch overhead)."""
+        out = {}
+        for name, sv in getattr(self, "solvers", {}).items():
+            out["solver_" + name] = dict(kind=sv.kind, iterations=sv.iterations, calls=sv.calls,
+                                         seconds=sv.seconds)
+        nf1 = getattr(self, "fermions", {}).get("nf1")
+        if nf1 is not None:
+            for name, r in nf1.rationals.items():
+                out["multishift_" + name] = dict(poles=len(r.r.c), iterations=r.iterations,
+                                                 calls=r.calls, seconds=r.seconds)
+        out["force_evaluations"] = self.force_evaluations
+        return out
+
+    def warmup(self):
+        """Untimed first use of every operator, solver, multishift pole set
+        and force path (autotuning, work buffers, multishift graph capture)."""
+        import torch
+        from . import Field
+        ops = {}
+        for a in self.actions:
+            for fo in (getattr(a, "fp", None), getattr(a, "f", None), getattr(a, "fa", None),
+                       getattr(a, "fb", None)):
+                if fo is not None:
+                    ops[id(fo)] = fo
+        scratch = torch.zeros_like(self.fbuf)
+        for fo in ops.values():
+            op = fo.sync()
+            b = Field(op)
+            DeviceNoise(1).fermion(b)
+            x = Field(op)
+            op.cg(x, b, 1e-30, 5)
+            for sv in getattr(self, "solvers", {}).values():
+                if sv.kind == "mixed":
+                    op.richardson(x, b, sv.inner_prec, 1e-30, 1, 1e-4, 5)
+                elif sv.kind == "learned":
+                    op.fcg(x, b, sv.lp, 1.0, 5, 2)
+            check(lib().b200_dwf_force_acc(op.handle, b"DdagD", _p(scratch), b.ptr, None, 0.0, None))
+            check(lib().b200_dwf_force_acc(op.handle, b"H", _p(scratch), b.ptr, x.ptr, 0.0, None))
+        nf1 = getattr(self, "fermions", {}).get("nf1")
+        if nf1 is not None:
+            for r in nf1.rationals.values():
+                op = r.fopr.sync()
+                if r.xs is None:
+                    r.xs = [Field(op) for _ in r.r.c]
+                b = Field(op)
+                DeviceNoise(2).fermion(b)
+                op.shiftcg(r.xs, r.r.c, b, 1e-30, 40)
+        self.director.jacobian(scratch)
+        torch.cuda.synchronize()
+
 
 def build_dwf_nf2p1(lattice, Ls, M0, masses, beta, c_plaq=3.648, c_rect=-0.331, rho=0.1,
                     nsmear=2, nstep=(2, 1, 3), level=(0, 0, 1, 2), tau=1.0,
                     lam=0.1931833275, nprec=8, np_md=16, np_h=24, rat_bounds=(1e-2, 3.16227766),
                     tol2_md=1e-20, tol2_h=1e-20, solvers=None, b=1.0, c=0.0,
-                    bc=(1, 1, 1, -1), integrator="Omelyan"):
+                    bc=(1, 1, 1, -1), integrator="Omelyan", shift_window=None):
     """The benchmark driver's action set (hmc_dwf_eo.cpp:155-352) on the
     device.  masses: dict l (light), h (Hasenbusch), s (strange), pv.
     solvers: dict of Solver objects 'l_md', 'l_h', 'h_md', 'h_h', 'pv_h'
-    (default FP64 CG at tol2_md / tol2_h)."""
+    (default FP64 CG at tol2_md / tol2_h).  shift_window: residual window of
+    the multishift solves (None keeps the library default, 0 updates every
+    shift every iteration)."""
     from . import DomainWall
     from .rational import Rational
     dr = DirectorSmear(lattice, rho, nsmear)
 
     def fopr(m):
-        return FoprSmeared(DomainWall(lattice, Ls, m, M0, b=b, c=c, bc=bc), dr)
+        op = DomainWall(lattice, Ls, m, M0, b=b, c=c, bc=bc)
+        if shift_window is not None:
+            op.set_shift_window(shift_window)
+        return FoprSmeared(op, dr)
 
     lo, hi = rat_bounds
     rats = dict(md_numer=Rational(np_md, 1, 4, lo, hi), md_denom=Rational(np_md, -1, 2, lo, hi),

@@ -69,11 +69,22 @@ enum MsScalar {
   MS_DONE,      // 0 while iterating; 1 converged, 2 NaN, 3 iteration cap (set by MSS_PRUNE)
   MS_ITER,      // iterations completed (counted on the device)
   MS_MAXITER,
-  MS_N = 16
+  MS_WIN,       // windowed mode: residuals stored in the current window
+  MS_NACTW,     // windowed mode: active shifts when the window opened
+  MS_WSIZE,     // window length m (0: every shift updated every iteration)
+  MS_N = 18
 };
 // per-shift arrays follow the scalars: [MS_N + a*kMaxShift + i]
 enum MsArray { MSA_ZETA1 = 0, MSA_ZETA2, MSA_CSH2, MSA_BETAS, MSA_ALPHAS, MSA_ZETA, MSA_PP, MSA_COUNT };
-constexpr int kMsStateSize = MS_N + MSA_COUNT * kMaxShift;
+// Windowed mode ("deferred shift updates"): the residuals r_0..r_(m-1) of m
+// iterations are kept, and each shift carries coefficient vectors so that
+//   p_i = PC[0] p_i(window start) + sum_l PC[1+l] r_l
+//   x_i = x_i(window start) + XC[0] p_i(window start) + sum_l XC[1+l] r_l;
+// the fields are touched once per window instead of once per iteration.
+constexpr int kMaxWin = 16;
+constexpr int kMsCoef = MS_N + MSA_COUNT * kMaxShift;                 // PC[i][0..m]
+constexpr int kMsXCoef = kMsCoef + kMaxShift * (kMaxWin + 1);         // XC[i][0..m]
+constexpr int kMsStateSize = kMsXCoef + kMaxShift * (kMaxWin + 1);
 
 struct MsUpdParams {
   void* const* xs;       // device array [nshift] of solution fields
@@ -84,8 +95,14 @@ struct MsUpdParams {
   double* red;           // partials [kMaxShift][nblocks] of |p_i|^2
   int nblocks;
   Geom g;
+  void* const* win;      // windowed mode: device array [kMaxWin] of residual slots (else null)
 };
 cudaError_t launch_ms_update(int prec, const MsUpdParams& p, const ChainCoefs& c, cudaStream_t st);
+// Windowed mode: once the window is full (or the solve is over) apply the
+// stored residuals to every shift that was active in the window (FP64), then
+// reset the window (single-block kernel).
+cudaError_t launch_ms_flush(const MsUpdParams& p, cudaStream_t st);
+cudaError_t launch_ms_window_reset(double* st, cudaStream_t stream);
 enum MsStep { MSS_BETA = 0, MSS_ALPHA = 1, MSS_PRUNE = 2 };
 // scalar steps: MSS_BETA sums the K2 partials (pq) -> beta; MSS_ALPHA sums
 // the K4 partials (rr_new) -> alpha and the per-shift zeta recurrence;

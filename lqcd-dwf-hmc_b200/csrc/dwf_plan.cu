@@ -116,6 +116,9 @@ struct b200_dwf {
   double* ms_red = nullptr;     // multishift per-shift partials
   void** ms_ptrs = nullptr;     // device arrays of x_i and p_i pointers
   std::vector<void*> ms_p;      // multishift search directions p_1..p_(n-1)
+  int ms_window = 8;            // multishift residual window (0: per-iteration shift updates)
+  std::vector<void*> ms_win;    // multishift residual window slots
+  void** ms_win_ptrs = nullptr; // device array of the window slots
   std::vector<void*> fcg_buf;   // flexible-CG fields (FP64 ring of directions)
   void* fcg_part = nullptr;     // complex reduction partials
   void* fcg_sc = nullptr;       // complex device scalars
@@ -514,6 +517,8 @@ int b200_dwf_destroy(b200_dwf_t* op) {
   cudaFree(op->ms_red);
   cudaFree(op->ms_ptrs);
   for (void* q : op->ms_p) cudaFree(q);
+  for (void* q : op->ms_win) cudaFree(q);
+  cudaFree(op->ms_win_ptrs);
   for (void* q : op->fcg_buf) cudaFree(q);
   cudaFree(op->fcg_part);
   cudaFree(op->fcg_sc);
@@ -747,9 +752,15 @@ int b200_cg_solve(b200_dwf_t* op, int prec, void* x, const void* b, int maxiter,
 }
 
 // AShiftsolver_CG (src/lib/Solver/ashiftsolver_CG-tmpl.h:89-329) on
-// DdagD + sigma_i, FP64.  One iteration = the four fused DdagD hops, one fused
-// update of every active shift, and three single-block scalar steps; the host
-// reads |r|^2 once per iteration.
+// DdagD + sigma_i, FP64.  One iteration = the four fused DdagD hops, the base
+// system's update and three single-block scalar steps.  The shifted systems
+// are updated either every iteration (window 0: one fused pass over every
+// active x_i, p_i) or, by default, once per window of m iterations from the
+// stored residuals and device-side coefficient recurrences (the same
+// recurrences regrouped; |p_i|^2 for the pruning test follows from
+// |p_i|^2 = zeta_i^2 |r|^2 + alpha_i^2 |p_i|^2 since r is orthogonal to the
+// earlier directions).  The iterations replay as captured CUDA graphs and the
+// device decides when the solve is over.
 int b200_shiftcg_solve(b200_dwf_t* op, void* const* x, const double* sigma, int nshift,
                        const void* b, int maxiter, double tol2, int* nconv, double* diff,
                        void* stream) {
@@ -782,6 +793,20 @@ int b200_shiftcg_solve(b200_dwf_t* op, void* const* x, const double* sigma, int 
         cudaMalloc(&op->ms_p[i - 1], field_bytes(prec, g.vh, g.ls)) != cudaSuccess)
       return fail(B200_ENOMEM, "cudaMalloc for multishift direction %d failed", i);
     ps[i] = op->ms_p[i - 1];
+  }
+  // windowed mode: m residual slots (allocated on first use)
+  const int window = op->ms_window;
+  if (window > 0) {
+    if (!op->ms_win_ptrs && cudaMalloc(&op->ms_win_ptrs, kMaxWin * sizeof(void*)) != cudaSuccess)
+      return fail(B200_ENOMEM, "cudaMalloc for multishift window pointers failed");
+    if (op->ms_win.size() < (size_t)window) op->ms_win.resize(window, nullptr);
+    for (int l = 0; l < window; ++l)
+      if (!op->ms_win[l] && cudaMalloc(&op->ms_win[l], field_bytes(prec, g.vh, g.ls)) != cudaSuccess)
+        return fail(B200_ENOMEM, "cudaMalloc for multishift window slot %d failed", l);
+    std::vector<void*> wp(kMaxWin, nullptr);
+    for (int l = 0; l < window; ++l) wp[l] = op->ms_win[l];
+    B200_CHECK_CUDA(cudaMemcpyAsync(op->ms_win_ptrs, wp.data(), kMaxWin * sizeof(void*),
+                                    cudaMemcpyHostToDevice, st));
   }
   void* y0 = op->work[0][prec];
   void* y1 = op->work[1][prec];
@@ -817,6 +842,13 @@ int b200_shiftcg_solve(b200_dwf_t* op, void* const* x, const double* sigma, int 
   h[MS_DONE] = 0.0;
   h[MS_ITER] = 0.0;
   h[MS_MAXITER] = (double)maxiter;
+  h[MS_WIN] = 0.0;
+  h[MS_NACTW] = nshift;
+  h[MS_WSIZE] = window;
+  for (int i = 0; i < kMaxShift; ++i) {
+    h[kMsCoef + i * (kMaxWin + 1)] = 1.0;
+    h[MS_N + MSA_PP * kMaxShift + i] = 1.0;     // |p_i|^2 / |b|^2 with p_i = b
+  }
   for (int i = 0; i < nshift; ++i) {
     h[MS_N + MSA_ZETA1 * kMaxShift + i] = 1.0;
     h[MS_N + MSA_ZETA2 * kMaxShift + i] = 1.0;
@@ -858,8 +890,13 @@ int b200_shiftcg_solve(b200_dwf_t* op, void* const* x, const double* sigma, int 
     MsUpdParams mu;
     mu.xs = op->ms_ptrs; mu.ps = op->ms_ptrs + kMaxShift; mu.r = r; mu.y0 = y0;
     mu.st = S; mu.red = op->ms_red; mu.nblocks = nb_hop; mu.g = g;
+    mu.win = window > 0 ? op->ms_win_ptrs : nullptr;
     B200_CHECK_CUDA(launch_ms_update(prec, mu, op->coefs, s));
     B200_CHECK_CUDA(launch_ms_scalar(MSS_PRUNE, op->ms_red, nb_hop, S, nshift, s));
+    if (window > 0) {
+      B200_CHECK_CUDA(launch_ms_flush(mu, s));
+      B200_CHECK_CUDA(launch_ms_window_reset(S, s));
+    }
     return 0;
   };
   // host view of S[MS_RR .. MS_MAXITER]
@@ -920,6 +957,13 @@ int b200_shiftcg_solve(b200_dwf_t* op, void* const* x, const double* sigma, int 
   if (diff) *diff = dmax;
   if (nconv) *nconv = it_conv < 0 ? maxiter : it_conv;
   if (it_conv < 0) return fail(B200_ENOCONV, "multishift CG not converged in %d iterations", maxiter);
+  return 0;
+}
+
+int b200_shiftcg_set_window(b200_dwf_t* op, int window) {
+  if (!op || window < 0 || window > kMaxWin)
+    return fail(B200_EINVAL, "window must be in [0, %d]", kMaxWin);
+  op->ms_window = window;
   return 0;
 }
 

@@ -366,6 +366,11 @@ ms_update_kernel(MsUpdParams p, const __grid_constant__ ChainCoef<typename Store
     St::store(p.y0, vh, LS, site, s, o);
   }
   block_reduce_store(nrm, p.red);
+  if (p.win) {
+    // windowed mode: keep this iteration's residual; the shifts follow later
+    if (active) St::store(p.win[(int)p.st[MS_WIN]], vh, LS, site, s, rv);
+    return;
+  }
   for (int ish = 1; ish < nact; ++ish) {
     __syncthreads();
     const R bs = (R)p.st[MS_N + MSA_BETAS * kMaxShift + ish];
@@ -480,13 +485,32 @@ __global__ void ms_scalar_kernel(int step, const double* partials, int n, double
         zeta2[i] = zeta1[i];
         zeta1[i] = z;
       }
+      if (st[MS_WSIZE] > 0.0) {
+        // deferred form of x_i -= beta_i p_i ; p_i = alpha_i p_i + zeta_i r_w,
+        // and |p_i|^2 by its recurrence (the new residual is orthogonal to
+        // every earlier direction): pp_i = zeta_i^2 |r|^2 + alpha_i^2 pp_i
+        const int w = (int)st[MS_WIN];
+        const double rrn = rr * st[MS_SNORM];
+        for (int i = 1; i < nact; ++i) {
+          double* pc = st + kMsCoef + i * (kMaxWin + 1);
+          double* xc = st + kMsXCoef + i * (kMaxWin + 1);
+          const double bs = betas[i], as = alphas[i], zt = zeta[i];
+          for (int j = 0; j <= w; ++j) {
+            xc[j] -= bs * pc[j];
+            pc[j] *= as;
+          }
+          pc[1 + w] = zt;
+          pp[i] = zt * zt * rrn + as * as * pp[i];
+        }
+      }
       st[MS_ALPHA_P] = alpha;
       st[MS_BETA_P] = beta;
       st[MS_RR] = rr;
     }
   } else {  // MSS_PRUNE
+    const bool windowed = st[MS_WSIZE] > 0.0;
     const int nact = (int)st[MS_NACT];
-    for (int i = 0; i < nact; ++i) {
+    for (int i = 0; i < (windowed ? 1 : nact); ++i) {
       const double v = block_sum_partials(partials + (size_t)i * n, n);
       if (threadIdx.x == 0) {
         if (i == 0) st[MS_PP0] = v;
@@ -499,6 +523,7 @@ __global__ void ms_scalar_kernel(int step, const double* partials, int n, double
         if (pp[i] > st[MS_TOL2]) { ish1 = i + 1; break; }
       }
       st[MS_NACT] = (double)ish1;
+      if (windowed) st[MS_WIN] = st[MS_WIN] + 1.0;
       // end of an iteration: count it and decide on the device whether the
       // solve is over, so that iterations can be replayed without the host
       const double it = st[MS_ITER] + 1.0;
@@ -514,6 +539,76 @@ __global__ void ms_scalar_kernel(int step, const double* partials, int n, double
 cudaError_t launch_ms_scalar(int step, const double* partials, int n, double* st, int nshift,
                              cudaStream_t stream) {
   ms_scalar_kernel<<<1, 1024, 0, stream>>>(step, partials, n, st, nshift);
+  return cudaGetLastError();
+}
+
+// Windowed multishift: the window is applied when it is full or when the
+// solve has ended with residuals still pending.
+__device__ __forceinline__ bool ms_window_due(const double* st) {
+  const double w = st[MS_WIN];
+  return w > 0.0 && (w >= st[MS_WSIZE] || st[MS_DONE] != 0.0);
+}
+
+// p_i = PC0 p_i + sum_l PC_l r_l ; x_i += XC0 p_i(old) + sum_l XC_l r_l for
+// every shift active in the window; flat over the FP64 field as double2.
+__global__ void __launch_bounds__(256) ms_flush_kernel(MsUpdParams p, long n2) {
+  const double* st = p.st;
+  if (!ms_window_due(st)) return;
+  __shared__ double cs[2 * kMaxShift * (kMaxWin + 1)];
+  const int w = (int)st[MS_WIN];
+  const int nsh = (int)st[MS_NACTW];
+  for (int i = threadIdx.x; i < 2 * kMaxShift * (kMaxWin + 1); i += blockDim.x) cs[i] = st[kMsCoef + i];
+  __syncthreads();
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < n2; e += (long)gridDim.x * blockDim.x) {
+    double2 rv[kMaxWin];
+#pragma unroll
+    for (int l = 0; l < kMaxWin; ++l)
+      if (l < w) rv[l] = __ldcs(reinterpret_cast<const double2*>(p.win[l]) + e);
+    for (int i = 1; i < nsh; ++i) {
+      const double* pc = cs + i * (kMaxWin + 1);
+      const double* xc = cs + kMaxShift * (kMaxWin + 1) + i * (kMaxWin + 1);
+      double2* pp = reinterpret_cast<double2*>(p.ps[i]) + e;
+      double2* xp = reinterpret_cast<double2*>(p.xs[i]) + e;
+      const double2 p0 = *pp;
+      double2 x = *xp;
+      double2 q;
+      q.x = pc[0] * p0.x; q.y = pc[0] * p0.y;
+      x.x = fma(xc[0], p0.x, x.x); x.y = fma(xc[0], p0.y, x.y);
+#pragma unroll
+      for (int l = 0; l < kMaxWin; ++l) {
+        if (l < w) {
+          q.x = fma(pc[1 + l], rv[l].x, q.x); q.y = fma(pc[1 + l], rv[l].y, q.y);
+          x.x = fma(xc[1 + l], rv[l].x, x.x); x.y = fma(xc[1 + l], rv[l].y, x.y);
+        }
+      }
+      *pp = q;
+      *xp = x;
+    }
+  }
+}
+
+__global__ void ms_window_reset_kernel(double* st) {
+  if (threadIdx.x != 0 || !ms_window_due(st)) return;
+  for (int i = 0; i < kMaxShift; ++i) {
+    double* pc = st + kMsCoef + i * (kMaxWin + 1);
+    double* xc = st + kMsXCoef + i * (kMaxWin + 1);
+    for (int j = 0; j <= kMaxWin; ++j) { pc[j] = 0.0; xc[j] = 0.0; }
+    pc[0] = 1.0;
+  }
+  st[MS_WIN] = 0.0;
+  st[MS_NACTW] = st[MS_NACT];
+}
+
+cudaError_t launch_ms_flush(const MsUpdParams& p, cudaStream_t st) {
+  const long n2 = (long)12 * p.g.vh * p.g.ls;      // FP64 field as double2
+  long blocks = (n2 + 255) / 256;
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  ms_flush_kernel<<<(int)blocks, 256, 0, st>>>(p, n2);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ms_window_reset(double* st, cudaStream_t stream) {
+  ms_window_reset_kernel<<<1, 32, 0, stream>>>(st);
   return cudaGetLastError();
 }
 

@@ -25,8 +25,13 @@ def rel(a, b):
     return np.linalg.norm(a - b) / np.linalg.norm(b)
 
 
-def test_multishift_matches_oracle():
+@pytest.mark.parametrize("window", [0, 3, 8, 16])
+def test_multishift_matches_oracle(window):
+    """Per-iteration shift updates (window 0) and deferred updates from a
+    window of stored residuals (the default 8; 3 exercises windows that end
+    mid-solve and shifts pruned inside a window) against the oracle."""
     ora, dev = make()
+    dev.set_shift_window(window)
     b = synth.spinor_field(LAT, LS, 9)
     sigma = [0.005, 0.05, 0.5, 5.0]
     fb = dev.new_field(0)
@@ -40,6 +45,32 @@ def test_multishift_matches_oracle():
     assert diff < 1e-9
     for i in range(len(sigma)):
         assert rel(dev.reverse(xs[i]), xr[i]) < 1e-9, i
+
+
+def test_multishift_window_agrees_with_per_iteration_updates():
+    """Sixteen shifts spanning 1e-4..64 (the rational poles' range): the
+    windowed solver reproduces the per-iteration one to rounding, iteration
+    count included, and rejects windows outside [0, 16]."""
+    import b200dwf
+    _, dev = make(7)
+    b = synth.spinor_field(LAT, LS, 11)
+    fb = dev.new_field(0)
+    dev.convert(fb, b)
+    sigma = list(np.logspace(-4, np.log10(64.0), 16))
+    out = {}
+    for window in (0, 8, 16):
+        dev.set_shift_window(window)
+        xs = [dev.new_field(0) for _ in sigma]
+        n, diff, rc = dev.shiftcg(xs, sigma, fb, 1e-22, 3000)
+        assert rc == 0 and diff < 1e-9
+        out[window] = (n, [dev.reverse(x) for x in xs])
+    for window in (8, 16):
+        assert abs(out[window][0] - out[0][0]) <= 1
+        for i in range(len(sigma)):
+            assert rel(out[window][1][i], out[0][1][i]) < 1e-10, (window, i)
+    for bad in (-1, 17):
+        with pytest.raises(b200dwf.B200Error):
+            dev.set_shift_window(bad)
 
 
 @pytest.mark.parametrize("inner", [1, 2, 3])
