@@ -335,33 +335,10 @@ def trajectory_section(op, lattice, u_workload, args, lp=None):
     tol2 = 1e-20
     res = {}
     for name, kinds, window in forms:
-        gc.collect()
-        torch.cuda.empty_cache()
-        sv = {k: Solver(v, tol2) for k, v in kinds.items()}
-        hmc = build_dwf_nf2p1(lattice, LS, M0, TRAJ_MASSES, 2.13, nstep=args.traj_nstep,
-                              tau=args.traj_length, np_md=16, np_h=24, tol2_md=tol2, tol2_h=tol2,
-                              solvers=sv, shift_window=window)
-        if "learned" in kinds.values():
-            # the trained weights are volume independent; the network runs on
-            # the light operator's own (smeared) links
-            lp_form = b200dwf.LearnedPrecond(hmc.fermions["nf2"].f.op, hidden=lp.hidden, seed=1)
-            lp_form.set_weights(lp.weights(deployed=False))
-            for v in sv.values():
-                v.lp = lp_form
-        ud = torch.from_numpy(u0.copy()).cuda()
-        hmc.set_config(ud)
-        hmc.warmup()
-        for v in sv.values():
-            v.iterations, v.seconds, v.calls = 0, 0.0, 0
-        for r in hmc.fermions["nf1"].rationals.values():
-            r.iterations, r.seconds, r.calls = 0, 0.0, 0
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        r = hmc.trajectory(ud, DeviceNoise(SEED_U + 11))
-        torch.cuda.synchronize()
-        res[name] = {"sec_per_trajectory": time.perf_counter() - t0, "dH": r["dH"],
-                     "H0": r["H0"], "multishift_window": window, **hmc.stats()}
-        del hmc, ud, r, sv
+        try:
+            res[name] = _trajectory_form(lattice, u0, args, lp, kinds, window, tol2)
+        except Exception as e:  # noqa: BLE001  (one form's failure keeps the others)
+            res[name] = {"error": str(e)}
     gc.collect()
     torch.cuda.empty_cache()
     out = {"lattice": lattice, "Ls": LS, "M0": M0, "masses": TRAJ_MASSES,
@@ -372,8 +349,45 @@ def trajectory_section(op, lattice, u_workload, args, lp=None):
            "length": args.traj_length, "solver_tol_rel_residual": 1e-10,
            "links": "near-unit exp(i*0.3*H) + 2 stout rho=0.1 (seed %d)" % (SEED_U + 3), **res}
     for name in res:
-        out["speedup_" + name] = (res["fp64_plain"]["sec_per_trajectory"]
-                                  / res[name]["sec_per_trajectory"])
+        if "sec_per_trajectory" in res[name] and "sec_per_trajectory" in res.get("fp64_plain", {}):
+            out["speedup_" + name] = (res["fp64_plain"]["sec_per_trajectory"]
+                                      / res[name]["sec_per_trajectory"])
+    return out
+
+
+def _trajectory_form(lattice, u0, args, lp, kinds, window, tol2):
+    import torch
+    import b200dwf
+    from b200dwf.hmc import build_dwf_nf2p1, DeviceNoise, Solver
+    gc.collect()
+    torch.cuda.empty_cache()
+    sv = {k: Solver(v, tol2) for k, v in kinds.items()}
+    hmc = build_dwf_nf2p1(lattice, LS, M0, TRAJ_MASSES, 2.13, nstep=args.traj_nstep,
+                          tau=args.traj_length, np_md=16, np_h=24, tol2_md=tol2, tol2_h=tol2,
+                          solvers=sv, shift_window=window)
+    if "learned" in kinds.values():
+        # the trained weights are volume independent; the network runs on
+        # the light operator's own (smeared) links
+        lp_form = b200dwf.LearnedPrecond(hmc.fermions["nf2"].f.op, hidden=lp.hidden, seed=1)
+        lp_form.set_weights(lp.weights(deployed=False))
+        for v in sv.values():
+            v.lp = lp_form
+    ud = torch.from_numpy(u0.copy()).cuda()
+    hmc.set_config(ud)
+    hmc.warmup()
+    for v in sv.values():
+        v.iterations, v.seconds, v.calls = 0, 0.0, 0
+    for r in hmc.fermions["nf1"].rationals.values():
+        r.iterations, r.seconds, r.calls = 0, 0.0, 0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    r = hmc.trajectory(ud, DeviceNoise(SEED_U + 11))
+    torch.cuda.synchronize()
+    out = {"sec_per_trajectory": time.perf_counter() - t0, "dH": r["dH"],
+           "H0": r["H0"], "multishift_window": window, **hmc.stats()}
+    del hmc, ud, r, sv
+    gc.collect()
+    torch.cuda.empty_cache()
     return out
 
 

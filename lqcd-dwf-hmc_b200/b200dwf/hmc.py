@@ -780,7 +780,7 @@ class HMCGeneral:
             for sv in getattr(self, "solvers", {}).values():
                 if sv.kind == "mixed":
                     op.richardson(x, b, sv.inner_prec, 1e-30, 1, 1e-4, 5)
-                elif sv.kind == "learned":
+                elif sv.kind == "learned" and sv.lp is not None and sv.lp.op is op:
                     op.fcg(x, b, sv.lp, 1.0, 5, 2)
             check(lib().b200_dwf_force_acc(op.handle, b"DdagD", _p(scratch), b.ptr, None, 0.0, None))
             check(lib().b200_dwf_force_acc(op.handle, b"H", _p(scratch), b.ptr, x.ptr, 0.0, None))

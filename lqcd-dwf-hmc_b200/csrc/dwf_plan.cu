@@ -94,6 +94,50 @@ void set_precond(DwfCoef& k) {
 }  // namespace
 
 // ------------------------------------------------------------ plan
+// The multishift solver's shifted search directions and residual window are
+// pure per-call workspace (1 GB each at 24^3x48 Ls=16, up to 23 + 16 of them):
+// plans of one device and field size share one pool instead of holding a copy
+// each, so the operators of an action set (strange, Pauli-Villars, ...) do not
+// multiply it.  Consequence: two plans of one geometry must not run multishift
+// solves concurrently on different streams.
+struct MsPool {
+  std::vector<void*> p;         // directions p_1..p_(n-1)
+  std::vector<void*> win;       // residual window slots
+  int users = 0;
+};
+static std::mutex g_ms_pool_mu;
+static std::map<std::pair<int, size_t>, MsPool*> g_ms_pools;
+
+static MsPool* ms_pool_acquire(size_t bytes) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(g_ms_pool_mu);
+  MsPool*& pool = g_ms_pools[std::make_pair(dev, bytes)];
+  if (!pool) pool = new MsPool();
+  ++pool->users;
+  return pool;
+}
+
+static void ms_pool_release(MsPool* pool) {
+  if (!pool) return;
+  std::lock_guard<std::mutex> lock(g_ms_pool_mu);
+  if (--pool->users > 0) return;
+  for (void* q : pool->p) cudaFree(q);
+  for (void* q : pool->win) cudaFree(q);
+  for (auto it = g_ms_pools.begin(); it != g_ms_pools.end(); ++it)
+    if (it->second == pool) { g_ms_pools.erase(it); break; }
+  delete pool;
+}
+
+// slot i of a pool vector, allocated on first use
+static int ms_pool_slot(std::vector<void*>& v, size_t i, size_t bytes, void** out) {
+  std::lock_guard<std::mutex> lock(g_ms_pool_mu);
+  if (v.size() <= i) v.resize(i + 1, nullptr);
+  if (!v[i] && cudaMalloc(&v[i], bytes) != cudaSuccess) { v[i] = nullptr; return 1; }
+  *out = v[i];
+  return 0;
+}
+
 struct b200_dwf {
   int L[4];
   DwfCoef k;
@@ -115,9 +159,8 @@ struct b200_dwf {
   double* ms_state = nullptr;   // multishift scalar state (device)
   double* ms_red = nullptr;     // multishift per-shift partials
   void** ms_ptrs = nullptr;     // device arrays of x_i and p_i pointers
-  std::vector<void*> ms_p;      // multishift search directions p_1..p_(n-1)
+  struct MsPool* ms_pool = nullptr;  // shared multishift directions / window slots
   int ms_window = 8;            // multishift residual window (0: per-iteration shift updates)
-  std::vector<void*> ms_win;    // multishift residual window slots
   void** ms_win_ptrs = nullptr; // device array of the window slots
   std::vector<void*> fcg_buf;   // flexible-CG fields (FP64 ring of directions)
   void* fcg_part = nullptr;     // complex reduction partials
@@ -516,8 +559,7 @@ int b200_dwf_destroy(b200_dwf_t* op) {
   cudaFree(op->ms_state);
   cudaFree(op->ms_red);
   cudaFree(op->ms_ptrs);
-  for (void* q : op->ms_p) cudaFree(q);
-  for (void* q : op->ms_win) cudaFree(q);
+  ms_pool_release(op->ms_pool);
   cudaFree(op->ms_win_ptrs);
   for (void* q : op->fcg_buf) cudaFree(q);
   cudaFree(op->fcg_part);
@@ -784,27 +826,25 @@ int b200_shiftcg_solve(b200_dwf_t* op, void* const* x, const double* sigma, int 
     return fail(B200_ENOMEM, "cudaMalloc for multishift partials failed");
   if (!op->ms_ptrs && cudaMalloc(&op->ms_ptrs, 2 * kMaxShift * sizeof(void*)) != cudaSuccess)
     return fail(B200_ENOMEM, "cudaMalloc for multishift pointers failed");
-  // search directions p_i: work slots 8.. are allocated per shift on demand
+  // search directions p_i: p_0 is a work slot, the others come from the
+  // multishift pool shared by every plan of this field size
+  const size_t fbytes = field_bytes(prec, g.vh, g.ls);
+  if (!op->ms_pool) op->ms_pool = ms_pool_acquire(fbytes);
   std::vector<void*> ps(nshift);
   for (int i = 0; i < nshift; ++i) {
     if (i == 0) { ps[0] = op->work[6][prec]; continue; }
-    if (op->ms_p.size() < (size_t)i) op->ms_p.resize(i, nullptr);
-    if (!op->ms_p[i - 1] &&
-        cudaMalloc(&op->ms_p[i - 1], field_bytes(prec, g.vh, g.ls)) != cudaSuccess)
+    if (ms_pool_slot(op->ms_pool->p, i - 1, fbytes, &ps[i]))
       return fail(B200_ENOMEM, "cudaMalloc for multishift direction %d failed", i);
-    ps[i] = op->ms_p[i - 1];
   }
   // windowed mode: m residual slots (allocated on first use)
   const int window = op->ms_window;
   if (window > 0) {
     if (!op->ms_win_ptrs && cudaMalloc(&op->ms_win_ptrs, kMaxWin * sizeof(void*)) != cudaSuccess)
       return fail(B200_ENOMEM, "cudaMalloc for multishift window pointers failed");
-    if (op->ms_win.size() < (size_t)window) op->ms_win.resize(window, nullptr);
-    for (int l = 0; l < window; ++l)
-      if (!op->ms_win[l] && cudaMalloc(&op->ms_win[l], field_bytes(prec, g.vh, g.ls)) != cudaSuccess)
-        return fail(B200_ENOMEM, "cudaMalloc for multishift window slot %d failed", l);
     std::vector<void*> wp(kMaxWin, nullptr);
-    for (int l = 0; l < window; ++l) wp[l] = op->ms_win[l];
+    for (int l = 0; l < window; ++l)
+      if (ms_pool_slot(op->ms_pool->win, l, fbytes, &wp[l]))
+        return fail(B200_ENOMEM, "cudaMalloc for multishift window slot %d failed", l);
     B200_CHECK_CUDA(cudaMemcpyAsync(op->ms_win_ptrs, wp.data(), kMaxWin * sizeof(void*),
                                     cudaMemcpyHostToDevice, st));
   }
