@@ -326,12 +326,12 @@ def trajectory_section(op, lattice, u_workload, args, lp=None):
     # mixed-precision solves and the windowed (batched) multishift
     forms = [("fp64_plain", cg, 0)]
     if args.traj_all_forms:
-        forms.append(("fp64_batched", cg, 8))
-    forms.append(("mixed_batched", mixed, 8))
+        forms.append(("fp64_batched", cg, 16))
+    forms.append(("mixed_batched", mixed, 16))
     if lp is not None:
         forms.append(("mixed_batched_learned",
                       dict({k: "mixed" for k in ("h_md", "h_h", "pv_h")}, l_md="learned",
-                           l_h="learned"), 8))
+                           l_h="learned"), 16))
     tol2 = 1e-20
     res = {}
     for name, kinds, window in forms:
@@ -526,9 +526,9 @@ def b200_arm(args, rank, world, local_rank):
                                         "seconds": c1 - c0,
                                         "ms_per_iteration": (c1 - c0) * 1e3 / max(n, 1),
                                         "converged": rc == 0}
-        op.set_shift_window(8)
+        op.set_shift_window(16)
         solvers["multishift"] = {"shifts": len(sigma), "sigma": "log-spaced 1e-4..64",
-                                 **ms["window_8"], "by_window": ms}
+                                 **ms["window_16"], "by_window": ms}
         del xs
 
     learned, lp = None, None

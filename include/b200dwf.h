@@ -127,7 +127,7 @@ int b200_shiftcg_solve(b200_dwf_t *op, void *const *x, const double *sigma, int 
 /* The shifted directions and the residual window are workspace shared by all
  * plans of one device and field size: plans of one geometry must not run
  * multishift solves concurrently on different streams.
- * Window m of the multishift solver's deferred shift updates (default 8):
+ * Window m of the multishift solver's deferred shift updates (default 16):
  * the residuals of m iterations stay in HBM (m extra fields) and every shift's
  * x_i, p_i are updated once per window; 0 updates every shift every
  * iteration, as AShiftsolver_CG::solve_step does

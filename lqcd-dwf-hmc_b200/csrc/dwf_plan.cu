@@ -160,7 +160,7 @@ struct b200_dwf {
   double* ms_red = nullptr;     // multishift per-shift partials
   void** ms_ptrs = nullptr;     // device arrays of x_i and p_i pointers
   struct MsPool* ms_pool = nullptr;  // shared multishift directions / window slots
-  int ms_window = 8;            // multishift residual window (0: per-iteration shift updates)
+  int ms_window = 16;           // multishift residual window (0: per-iteration shift updates)
   void** ms_win_ptrs = nullptr; // device array of the window slots
   std::vector<void*> fcg_buf;   // flexible-CG fields (FP64 ring of directions)
   void* fcg_part = nullptr;     // complex reduction partials

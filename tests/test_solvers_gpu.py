@@ -28,7 +28,7 @@ def rel(a, b):
 @pytest.mark.parametrize("window", [0, 3, 8, 16])
 def test_multishift_matches_oracle(window):
     """Per-iteration shift updates (window 0) and deferred updates from a
-    window of stored residuals (the default 8; 3 exercises windows that end
+    window of stored residuals (8, the default 16; 3 exercises windows that end
     mid-solve and shifts pruned inside a window) against the oracle."""
     ora, dev = make()
     dev.set_shift_window(window)
