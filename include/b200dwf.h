@@ -124,9 +124,9 @@ int b200_cg_solve(b200_dwf_t *op, int prec, void *x, const void *b, int maxiter,
 int b200_shiftcg_solve(b200_dwf_t *op, void *const *x, const double *sigma, int nshift,
                        const void *b, int maxiter, double tol2, int *nconv, double *diff,
                        void *stream);
-/* The shifted directions and the residual window are workspace shared by all
- * plans of one device and field size: plans of one geometry must not run
- * multishift solves concurrently on different streams.
+/* Work fields, the shifted directions and the residual window are per-call
+ * workspace shared by all plans of one device and geometry (vh, Ls): plans of
+ * one geometry must not run calls concurrently on different streams.
  * Window m of the multishift solver's deferred shift updates (default 16):
  * the residuals of m iterations stay in HBM (m extra fields) and every shift's
  * x_i, p_i are updated once per window; 0 updates every shift every

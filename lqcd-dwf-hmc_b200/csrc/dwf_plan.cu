@@ -94,44 +94,49 @@ void set_precond(DwfCoef& k) {
 }  // namespace
 
 // ------------------------------------------------------------ plan
-// The multishift solver's shifted search directions and residual window are
-// pure per-call workspace (1 GB each at 24^3x48 Ls=16, up to 23 + 16 of them):
-// plans of one device and field size share one pool instead of holding a copy
-// each, so the operators of an action set (strange, Pauli-Villars, ...) do not
-// multiply it.  Consequence: two plans of one geometry must not run multishift
-// solves concurrently on different streams.
-struct MsPool {
-  std::vector<void*> p;         // directions p_1..p_(n-1)
-  std::vector<void*> win;       // residual window slots
+// Per-call device workspace shared by every plan of one device and geometry
+// (vh, Ls): the work fields of the operator modes, solvers and forces, and the
+// multishift solver's shifted directions and residual window.  At 24^3x48
+// Ls=16 a field is 1 GB and a plan touches up to ~40 of them, so the several
+// operators of an action set (light, Hasenbusch, strange, Pauli-Villars)
+// share one copy instead of holding one each.  Every entry point uses these
+// fields only for the duration of one call, so the one rule is: plans of one
+// geometry must not run calls concurrently on different streams.
+struct Workspace {
+  void* work[12][4] = {};       // work fields per slot and storage precision
+  std::vector<void*> p;         // multishift directions p_1..p_(n-1)
+  std::vector<void*> win;       // multishift residual window slots
   int users = 0;
 };
-static std::mutex g_ms_pool_mu;
-static std::map<std::pair<int, size_t>, MsPool*> g_ms_pools;
+static std::mutex g_ws_mu;
+static std::map<std::tuple<int, int, int>, Workspace*> g_workspaces;
 
-static MsPool* ms_pool_acquire(size_t bytes) {
+static Workspace* workspace_acquire(int vh, int ls) {
   int dev = 0;
   cudaGetDevice(&dev);
-  std::lock_guard<std::mutex> lock(g_ms_pool_mu);
-  MsPool*& pool = g_ms_pools[std::make_pair(dev, bytes)];
-  if (!pool) pool = new MsPool();
-  ++pool->users;
-  return pool;
+  std::lock_guard<std::mutex> lock(g_ws_mu);
+  Workspace*& ws = g_workspaces[std::make_tuple(dev, vh, ls)];
+  if (!ws) ws = new Workspace();
+  ++ws->users;
+  return ws;
 }
 
-static void ms_pool_release(MsPool* pool) {
-  if (!pool) return;
-  std::lock_guard<std::mutex> lock(g_ms_pool_mu);
-  if (--pool->users > 0) return;
-  for (void* q : pool->p) cudaFree(q);
-  for (void* q : pool->win) cudaFree(q);
-  for (auto it = g_ms_pools.begin(); it != g_ms_pools.end(); ++it)
-    if (it->second == pool) { g_ms_pools.erase(it); break; }
-  delete pool;
+static void workspace_release(Workspace* ws) {
+  if (!ws) return;
+  std::lock_guard<std::mutex> lock(g_ws_mu);
+  if (--ws->users > 0) return;
+  for (int i = 0; i < 12; ++i)
+    for (int p = 0; p < 4; ++p) cudaFree(ws->work[i][p]);
+  for (void* q : ws->p) cudaFree(q);
+  for (void* q : ws->win) cudaFree(q);
+  for (auto it = g_workspaces.begin(); it != g_workspaces.end(); ++it)
+    if (it->second == ws) { g_workspaces.erase(it); break; }
+  delete ws;
 }
 
-// slot i of a pool vector, allocated on first use
+// slot i of a workspace vector, allocated on first use
 static int ms_pool_slot(std::vector<void*>& v, size_t i, size_t bytes, void** out) {
-  std::lock_guard<std::mutex> lock(g_ms_pool_mu);
+  std::lock_guard<std::mutex> lock(g_ws_mu);
   if (v.size() <= i) v.resize(i + 1, nullptr);
   if (!v[i] && cudaMalloc(&v[i], bytes) != cudaSuccess) { v[i] = nullptr; return 1; }
   *out = v[i];
@@ -153,13 +158,13 @@ struct b200_dwf {
   double* sc_host = nullptr;    // pinned mirror (also of the multishift scalars)
   int* err_host = nullptr;      // pinned mirror of err
   double* stage = nullptr;      // device f64 staging for convert/reverse
-  void* work[12][4] = {};       // work fields per precision
+  Workspace* ws = nullptr;      // shared per-call workspace of this geometry
+  void* (*work)[4] = nullptr;   // = ws->work: work fields per slot and precision
   void* tune_out[2][4] = {};    // autotuner scratch outputs per precision
   ChainCoefs coefs;             // fifth-dimension chain coefficients
   double* ms_state = nullptr;   // multishift scalar state (device)
   double* ms_red = nullptr;     // multishift per-shift partials
   void** ms_ptrs = nullptr;     // device arrays of x_i and p_i pointers
-  struct MsPool* ms_pool = nullptr;  // shared multishift directions / window slots
   int ms_window = 16;           // multishift residual window (0: per-iteration shift updates)
   void** ms_win_ptrs = nullptr; // device array of the window slots
   std::vector<void*> fcg_buf;   // flexible-CG fields (FP64 ring of directions)
@@ -171,10 +176,13 @@ struct b200_dwf {
 namespace {
 
 int ensure_work(b200_dwf* op, int prec, int i) {
+  std::lock_guard<std::mutex> lock(g_ws_mu);
   if (!op->work[i][prec]) {
     const size_t bytes = field_bytes(prec, op->g.vh, op->g.ls);
-    if (cudaMalloc(&op->work[i][prec], bytes) != cudaSuccess)
+    if (cudaMalloc(&op->work[i][prec], bytes) != cudaSuccess) {
+      op->work[i][prec] = nullptr;
       return fail(B200_ENOMEM, "cudaMalloc of %zu bytes for a work field failed", bytes);
+    }
   }
   return 0;
 }
@@ -485,6 +493,8 @@ int b200_dwf_create(b200_dwf_t** out, const int lattice[4], int Ls, double mq, d
   const long vol = (long)lattice[0] * lattice[1] * lattice[2] * lattice[3];
   op->g.nx2 = lattice[0] / 2; op->g.ny = lattice[1]; op->g.nz = lattice[2]; op->g.nt = lattice[3];
   op->g.ls = Ls; op->g.vh = (int)(vol / 2);
+  op->ws = workspace_acquire(op->g.vh, Ls);
+  op->work = op->ws->work;
 
   // fifth-dimension chain coefficients (both arithmetic types)
   {
@@ -554,12 +564,10 @@ int b200_dwf_destroy(b200_dwf_t* op) {
   if (op->sc_host) cudaFreeHost(op->sc_host);
   if (op->err_host) cudaFreeHost(op->err_host);
   cudaFree(op->stage);
-  for (int i = 0; i < 12; ++i)
-    for (int p = 0; p < 4; ++p) cudaFree(op->work[i][p]);
   cudaFree(op->ms_state);
   cudaFree(op->ms_red);
   cudaFree(op->ms_ptrs);
-  ms_pool_release(op->ms_pool);
+  workspace_release(op->ws);
   cudaFree(op->ms_win_ptrs);
   for (void* q : op->fcg_buf) cudaFree(q);
   cudaFree(op->fcg_part);
@@ -829,11 +837,10 @@ int b200_shiftcg_solve(b200_dwf_t* op, void* const* x, const double* sigma, int 
   // search directions p_i: p_0 is a work slot, the others come from the
   // multishift pool shared by every plan of this field size
   const size_t fbytes = field_bytes(prec, g.vh, g.ls);
-  if (!op->ms_pool) op->ms_pool = ms_pool_acquire(fbytes);
   std::vector<void*> ps(nshift);
   for (int i = 0; i < nshift; ++i) {
     if (i == 0) { ps[0] = op->work[6][prec]; continue; }
-    if (ms_pool_slot(op->ms_pool->p, i - 1, fbytes, &ps[i]))
+    if (ms_pool_slot(op->ws->p, i - 1, fbytes, &ps[i]))
       return fail(B200_ENOMEM, "cudaMalloc for multishift direction %d failed", i);
   }
   // windowed mode: m residual slots (allocated on first use)
@@ -843,7 +850,7 @@ int b200_shiftcg_solve(b200_dwf_t* op, void* const* x, const double* sigma, int 
       return fail(B200_ENOMEM, "cudaMalloc for multishift window pointers failed");
     std::vector<void*> wp(kMaxWin, nullptr);
     for (int l = 0; l < window; ++l)
-      if (ms_pool_slot(op->ms_pool->win, l, fbytes, &wp[l]))
+      if (ms_pool_slot(op->ws->win, l, fbytes, &wp[l]))
         return fail(B200_ENOMEM, "cudaMalloc for multishift window slot %d failed", l);
     B200_CHECK_CUDA(cudaMemcpyAsync(op->ms_win_ptrs, wp.data(), kMaxWin * sizeof(void*),
                                     cudaMemcpyHostToDevice, st));

@@ -90,8 +90,11 @@ def _hmc_from_meta(meta, solvers=None):
 @pytest.mark.gpu
 def test_trajectory_matches_reference():
     """One device trajectory driven by the reference's recorded momenta and
-    noise: H_total(init) to 1e-12, every action's start value to the solver
-    tolerance, H(diff) and the end links to what the reference produced."""
+    noise (solvers at |r|^2/|b|^2 < 1e-24 on both sides): H_total(init),
+    every action's Hamiltonian and force at the start, H(diff) and the end
+    links and momenta against what the reference produced.  Measured on a
+    B200: H0 to 2e-15, actions to 2e-13, forces to 2e-10, |dH - dH_ref|
+    8e-9 (dH = 44.5), end links to 4e-11, end momenta to 1.3e-10."""
     import torch
     from b200dwf.hmc import HostNoise
     meta, u, z = golden()
@@ -101,9 +104,9 @@ def test_trajectory_matches_reference():
     ip = torch.zeros_like(ud)
     noise = HostNoise(z["mom"], [z["xi_0"], z["xi_1"], z["xi_2"]])
     h0, parts0 = hmc.langevin(ip, noise)
-    assert h0 == pytest.approx(float(z["H0"][0]), rel=1e-12)
+    assert h0 == pytest.approx(float(z["H0"][0]), rel=1e-13)
     hs = [a.calcH() for a in hmc.actions]
-    np.testing.assert_allclose(hs, z["h_start"], rtol=1e-9)
+    np.testing.assert_allclose(hs, z["h_start"], rtol=1e-11)
     # every action's force at the start links (Action::force after
     # mult_generator, smeared-force Jacobian included)
     F = torch.zeros_like(ud)
@@ -111,14 +114,14 @@ def test_trajectory_matches_reference():
         hmc.level_force([a], ud, F)
         ref = z["force_%d" % i]
         err = np.linalg.norm(F.cpu().numpy() - ref) / np.linalg.norm(ref)
-        assert err < 1e-9, (i, err)
+        assert err < 2e-9, (i, err)
     hmc.integrator.evolve(meta["tau"], ip, ud)
     h1, parts1 = hmc.calc_hamiltonian(ip)
     dh = h1 - h0
-    np.testing.assert_allclose(parts1[1:], z["h_end"], rtol=1e-7)
-    assert abs(dh - float(z["dH"][0])) < 1e-5, (dh, float(z["dH"][0]))
-    assert np.max(np.abs(ud.cpu().numpy() - z["u_end"])) < 1e-7
-    assert np.max(np.abs(ip.cpu().numpy() - z["mom_end"])) < 1e-5
+    np.testing.assert_allclose(parts1[1:], z["h_end"], rtol=1e-10)
+    assert abs(dh - float(z["dH"][0])) < 1e-7, (dh, float(z["dH"][0]))
+    assert np.max(np.abs(ud.cpu().numpy() - z["u_end"])) < 1e-9
+    assert np.max(np.abs(ip.cpu().numpy() - z["mom_end"])) < 1e-8
     # the nested Omelyan [2,1,3] with cached forces evaluates 5 / 9 / 49
     # forces on levels 0 / 1 / 2
     assert hmc.force_evaluations == {0: 5, 1: 9, 2: 49}
