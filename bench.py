@@ -201,6 +201,79 @@ def run_reference_cpu(lattice, ls, steps, warmup, budget_s=60.0, threads=None):
     return gbs, t_step, reps, threads
 
 
+# The configuration the reference runs on its CPU path (4^3x8, Ls=8 Shamir
+# M0=1.8, hot start, light 0.01 / Hasenbusch 0.1 / strange 0.04 / PV 1.0,
+# Iwasaki beta 2.13, 2 stout rho 0.1, Omelyan [2,1,3], length 1, 10-pole
+# rationals, solves to |r|^2/|b|^2 < 1e-24).
+SMALL_TRAJ = dict(lattice=[4, 4, 4, 8], Ls=8, M0=1.8, gauge_seed=101, mq_l=0.01, mq_h=0.1,
+                  mq_s=0.04, mq_pv=1.0, beta=2.13, c_plaq=3.648, c_rect=-0.331, rho=0.1,
+                  nsmear=2, tau=1.0, nstep=[2, 1, 3], level=[0, 0, 1, 2],
+                  lam=0.1931833275, nprec=8, np_md=10, np_h=10, rat_lo=0.01,
+                  rat_hi=3.16227766, tol=1e-24, seed=1234567)
+
+
+def small_trajectory_beside_reference(threads=None):
+    """One 2+1-flavour trajectory of the reference corelib (oracle/_ref
+    ref_harness traj, built from the reference sources) on this host's cores,
+    and the same trajectory on the device driven by the momenta and noise the
+    reference's generator handed out: both times and both H(diff)."""
+    import shutil
+    import torch
+    from b200dwf import synth
+    from b200dwf.hmc import build_dwf_nf2p1, HostNoise
+    from b200dwf.rational import TABLE_DIR
+    if not os.path.exists(REF_HARNESS):
+        return {"unavailable": "oracle/_ref/ref_harness not built"}
+    c = SMALL_TRAJ
+    threads = threads or os.cpu_count() or 1
+    u = synth.gauge_field(c["lattice"], c["gauge_seed"], "hot")
+    with tempfile.TemporaryDirectory() as d:
+        for name in os.listdir(TABLE_DIR):
+            shutil.copy(os.path.join(TABLE_DIR, name), d)
+        u.tofile(os.path.join(d, "gauge.bin"))
+        with open(os.path.join(d, "params.txt"), "w") as f:
+            f.write("lattice %s\nLs %d\nM0 %r\nb 1.0\nc 0.0\nalpha 1.0\nbc 1 1 1 -1\n"
+                    % (" ".join(map(str, c["lattice"])), c["Ls"], c["M0"]))
+            for k in ("mq_l", "mq_h", "mq_s", "mq_pv", "beta", "c_plaq", "c_rect", "rho",
+                      "nsmear", "tau", "nprec", "np_md", "np_h", "rat_lo", "rat_hi", "seed"):
+                f.write("%s %r\n" % (k, c[k]))
+            f.write("nstep %s\nlevel %s\nlambda %r\ntol_md %r\ntol_h %r\nthreads %d\n"
+                    % (" ".join(map(str, c["nstep"])), " ".join(map(str, c["level"])), c["lam"],
+                       c["tol"], c["tol"], threads))
+        t0 = time.perf_counter()
+        subprocess.run([REF_HARNESS, "traj", os.path.join(d, "params.txt"), d, d],
+                       capture_output=True, text=True, check=True)
+        t_ref = time.perf_counter() - t0
+        mom = np.fromfile(os.path.join(d, "mom.bin"))
+        xis = [np.fromfile(os.path.join(d, "xi_%d.bin" % k)) for k in range(3)]
+        ref = {}
+        for line in open(os.path.join(d, "traj.txt")):
+            key, *vals = line.split()
+            ref[key] = [float(v) for v in vals]
+
+    def device_run():
+        hmc = build_dwf_nf2p1(c["lattice"], c["Ls"], c["M0"],
+                              dict(l=c["mq_l"], h=c["mq_h"], s=c["mq_s"], pv=c["mq_pv"]),
+                              c["beta"], c["c_plaq"], c["c_rect"], c["rho"], c["nsmear"],
+                              c["nstep"], c["level"], c["tau"], c["lam"], c["nprec"], c["np_md"],
+                              c["np_h"], (c["rat_lo"], c["rat_hi"]), c["tol"], c["tol"])
+        ud = torch.from_numpy(u.copy()).cuda()
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        r = hmc.trajectory(ud, HostNoise(mom, xis))
+        torch.cuda.synchronize()
+        return time.perf_counter() - t, r["dH"]
+
+    device_run()                     # untimed: autotuning and workspace
+    t_dev, dh = device_run()
+    return {"config": "4^3x8 Ls=8 Shamir M0=1.8, hot start, masses 0.01/0.1/0.04/PV 1.0, "
+                      "Iwasaki 2.13, 2 stout, Omelyan [2,1,3], length 1, 10 poles, tol2 1e-24",
+            "reference_cpu_sec": t_ref, "reference_cpu_cores": threads,
+            "device_sec": t_dev, "dH_reference": ref["dH"][0], "dH_device": dh,
+            "dH_abs_diff": abs(dh - ref["dH"][0]),
+            "noise": "the reference's recorded M-series momenta and pseudofermion noise"}
+
+
 def reference_arm(args, rank, world):
     if rank != 0:
         return
@@ -308,8 +381,9 @@ def trajectory_section(op, lattice, u_workload, args, lp=None):
     plain = FP64 CG and the multishift updating every shift every iteration;
     batched = the multishift's windowed shift updates, with mixed-precision
     Richardson (f16 storage, FP32 inner, FP64 outer) for the light,
-    Hasenbusch and PV solves and, when a trained network is given, the
-    learned flexible CG for the light solves."""
+    Hasenbusch and PV solves, each MD solve starting from the action's
+    previous solution (use_initial_guess) and, when a trained network is
+    given, the learned flexible CG for the light solves."""
     import torch
     import b200dwf
     from b200dwf import synth
@@ -320,7 +394,7 @@ def trajectory_section(op, lattice, u_workload, args, lp=None):
     u0 = sm.config(2)
     del sm
     cg = {k: "cg" for k in ("l_md", "l_h", "h_md", "h_h", "pv_h")}
-    mixed = {k: "mixed" for k in ("l_md", "l_h", "h_md", "h_h", "pv_h")}
+    mixed = {k: "mixed+" for k in ("l_md", "l_h", "h_md", "h_h", "pv_h")}
     # (name, solver kinds, multishift window): the plain form is FP64 CG with
     # every shift updated every iteration; the optimised forms use the
     # mixed-precision solves and the windowed (batched) multishift
@@ -330,7 +404,7 @@ def trajectory_section(op, lattice, u_workload, args, lp=None):
     forms.append(("mixed_batched", mixed, 16))
     if lp is not None:
         forms.append(("mixed_batched_learned",
-                      dict({k: "mixed" for k in ("h_md", "h_h", "pv_h")}, l_md="learned",
+                      dict({k: "mixed+" for k in ("h_md", "h_h", "pv_h")}, l_md="learned",
                            l_h="learned"), 16))
     tol2 = 1e-20
     res = {}
@@ -361,7 +435,9 @@ def _trajectory_form(lattice, u0, args, lp, kinds, window, tol2):
     from b200dwf.hmc import build_dwf_nf2p1, DeviceNoise, Solver
     gc.collect()
     torch.cuda.empty_cache()
-    sv = {k: Solver(v, tol2) for k, v in kinds.items()}
+    # "mixed+": mixed-precision Richardson whose MD solves start from the
+    # action's previous solution (use_initial_guess)
+    sv = {k: Solver(v.rstrip("+"), tol2, chrono=v.endswith("+")) for k, v in kinds.items()}
     hmc = build_dwf_nf2p1(lattice, LS, M0, TRAJ_MASSES, 2.13, nstep=args.traj_nstep,
                           tau=args.traj_length, np_md=16, np_h=24, tol2_md=tol2, tol2_h=tol2,
                           solvers=sv, shift_window=window)
@@ -538,6 +614,12 @@ def b200_arm(args, rank, world, local_rank):
     if not args.no_trajectory:
         trajectory = trajectory_section(op, lattice, u, args, lp)
 
+    small = None
+    if world == 1 and not args.no_cpu and not args.no_trajectory:
+        try:
+            small = small_trajectory_beside_reference()
+        except Exception as e:  # noqa: BLE001
+            small = {"unavailable": str(e)}
     if rank != 0:
         return
     cpu = None
@@ -570,6 +652,7 @@ def b200_arm(args, rank, world, local_rank):
         "solvers": solvers,
         "learned_preconditioner": learned,
         "trajectory": trajectory,
+        "trajectory_4x4x4x8_beside_reference": small,
         "autotune": b200dwf.tuning_table().strip().splitlines(),
         "cpu_baseline": cpu,
     }

@@ -146,6 +146,13 @@ int b200_shiftcg_set_window(b200_dwf_t *op, int window);
 int b200_richardson_solve(b200_dwf_t *op, int inner_prec, void *x, const void *b,
                           int maxiter, double tol2, int maxiter_inner, double tol2_inner,
                           int *nconv, int *nconv_inner, double *diff, void *stream);
+/* use_initial_guess of the reference's solvers (Solver_CG::set_parameters,
+ * src/lib/Solver/solver_CG.cpp; ASolver_Richardson, src/lib_alt/Solver/
+ * asolver_Richardson-tmpl.h:131-213): when set, b200_cg_solve and
+ * b200_richardson_solve start from the x passed in instead of zero (CG runs on
+ * the residual equation and adds the correction).  The stopping rule stays
+ * |b - DdagD x|^2 / |b|^2 < tol2.  Default 0, as in the reference's inputs. */
+int b200_solver_set_initial_guess(b200_dwf_t *op, int use);
 
 /* Allocation-free |x|^2 for callers that cannot allocate device memory: code
  * inside a CUDA graph capture, code running under a host framework that owns

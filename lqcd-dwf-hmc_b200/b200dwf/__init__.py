@@ -67,6 +67,7 @@ def lib():
     L.b200_dwf_force_udiv1.argtypes = [vp, ctypes.c_char_p, vp, vp, vp, vp]
     L.b200_dwf_force_udiv.argtypes = [vp, vp, vp, vp]
     L.b200_shiftcg_set_window.argtypes = [vp, ctypes.c_int]
+    L.b200_solver_set_initial_guess.argtypes = [vp, ctypes.c_int]
     L.b200_dwf_force_acc.argtypes = [vp, ctypes.c_char_p, vp, vp, vp, ctypes.c_double, vp]
     L.b200_smear_create.argtypes = [ctypes.POINTER(vp), ip, ctypes.c_double, ctypes.c_int]
     L.b200_smear_destroy.argtypes = [vp]
@@ -250,6 +251,10 @@ class DomainWall:
         if rc not in (0, -4):
             check(rc)
         return n.value, d.value, rc
+
+    def set_initial_guess(self, use):
+        """use_initial_guess for cg / richardson: start from the x passed in."""
+        check(lib().b200_solver_set_initial_guess(self.handle, int(bool(use))))
 
     def set_shift_window(self, window):
         """Residual window of the multishift solver (0: per-iteration updates)."""

@@ -270,20 +270,34 @@ class FoprSmeared:
 
 class Solver:
     """Fprop 'DdagD_even' with a chosen method: FP64 CG (the reference's
-    Solver_CG), mixed-precision Richardson, or the learned flexible CG."""
+    Solver_CG), mixed-precision Richardson, or the learned flexible CG.
+    chrono: the MD solves of an action start from that action's previous
+    solution (the reference's use_initial_guess; CG and Richardson only)."""
 
-    def __init__(self, kind="cg", tol2=1e-20, maxiter=100000, inner_prec=None, lp=None):
+    def __init__(self, kind="cg", tol2=1e-20, maxiter=100000, inner_prec=None, lp=None,
+                 chrono=False):
         from . import F16
         self.kind, self.tol2, self.maxiter = kind, tol2, maxiter
+        self.chrono = chrono
         self.inner_prec = F16 if inner_prec is None else inner_prec
         self.lp = lp
         self.iterations = 0
         self.seconds = 0.0
         self.calls = 0
 
-    def solve(self, op, x, b):
+    def solve(self, op, x, b, guess=False):
+        """x = (DdagD)^-1 b; with guess (and chrono) x on entry is the start."""
         t0 = time.perf_counter()
-        n = self._solve(op, x, b)
+        use = bool(guess and self.chrono and self.kind in ("cg", "mixed"))
+        if use:
+            op.set_initial_guess(True)
+        else:
+            x.buf.zero_()
+        try:
+            n = self._solve(op, x, b)
+        finally:
+            if use:
+                op.set_initial_guess(False)
         self.seconds += time.perf_counter() - t0   # the solvers end with a host read
         self.calls += 1
         return n
@@ -356,20 +370,21 @@ class ActionFRatio:
         op = fopr.op
         self.psf, self.v1, self.v2 = Field(op), Field(op), Field(op)
         self.fermion = True
+        self._guess = False       # v2 holds a solution of the current psf
 
     def langevin(self, xi):
         f, fp = self.f.sync(), self.fp.sync()
         f.mult_dag(self.v2, xi, "H")
-        self.v1.buf.zero_()
         self.solver_h_prec.solve(fp, self.v1, self.v2)
         fp.mult(self.psf, self.v1, "H")
+        self._guess = False
         return f.norm2(xi)
 
     def calcH(self):
         f, fp = self.f.sync(), self.fp.sync()
         fp.mult_dag(self.v1, self.psf, "H")
-        self.v2.buf.zero_()
-        self.solver_h.solve(f, self.v2, self.v1)
+        self.solver_h.solve(f, self.v2, self.v1, self._guess)
+        self._guess = True
         return f.dot(self.v1, self.v2)
 
     def force_udiv(self, acc):
@@ -377,8 +392,8 @@ class ActionFRatio:
         (action_F_Ratio_eo.cpp:171-205 before mult_generator)."""
         f, fp = self.f.sync(), self.fp.sync()
         fp.mult_dag(self.v1, self.psf, "H")
-        self.v2.buf.zero_()
-        self.solver_md.solve(f, self.v2, self.v1)
+        self.solver_md.solve(f, self.v2, self.v1, self._guess)
+        self._guess = True
         L = lib()
         check(L.b200_dwf_force_acc(f.handle, b"DdagD", _p(acc), self.v2.ptr, None, 1.0, None))
         check(L.b200_dwf_force_acc(fp.handle, b"Hdag", _p(acc), self.v2.ptr, self.psf.ptr, -1.0, None))

@@ -166,6 +166,7 @@ struct b200_dwf {
   double* ms_red = nullptr;     // multishift per-shift partials
   void** ms_ptrs = nullptr;     // device arrays of x_i and p_i pointers
   int ms_window = 16;           // multishift residual window (0: per-iteration shift updates)
+  bool init_guess = false;      // CG / Richardson start from the x passed in
   void** ms_win_ptrs = nullptr; // device array of the window slots
   std::vector<void*> fcg_buf;   // flexible-CG fields (FP64 ring of directions)
   void* fcg_part = nullptr;     // complex reduction partials
@@ -789,7 +790,31 @@ int b200_cg_solve(b200_dwf_t* op, int prec, void* x, const void* b, int maxiter,
   cudaStream_t st = (cudaStream_t)stream;
   int n = 0;
   double rel2 = 0.0;
-  const int rc = cg_core(op, prec, x, b, maxiter, tol2, &n, &rel2, st);
+  int rc;
+  if (op->init_guess) {
+    // use_initial_guess: CG on the residual equation DdagD e = b - DdagD x
+    // from e = 0, stopped at the same |b - DdagD x|^2 / |b|^2, then x += e
+    if ((rc = ensure_work(op, prec, 8)) || (rc = ensure_work(op, prec, 9))) return rc;
+    void* r0 = op->work[8][prec];
+    void* e = op->work[9][prec];
+    double bn2 = 0.0, rn2 = 0.0;
+    if ((rc = field_norm2_dev(op, prec, b, op->sc + SC_RR_NEW, st)) ||
+        (rc = host_scalar(op, SC_RR_NEW, &bn2, st)))
+      return rc;
+    if ((rc = apply_DdagD(op, prec, r0, x, st))) return rc;
+    B200_CHECK_CUDA(launch_axpby(prec, op->g, r0, b, 1.0, nullptr, -1.0, nullptr, st));
+    if ((rc = field_norm2_dev(op, prec, r0, op->sc + SC_RR_NEW, st)) ||
+        (rc = host_scalar(op, SC_RR_NEW, &rn2, st)))
+      return rc;
+    rc = 0;
+    if (rn2 > tol2 * bn2) {
+      rc = cg_core(op, prec, e, r0, maxiter, tol2 * bn2 / rn2, &n, &rel2, st);
+      if (rc && rc != B200_ENOCONV) return rc;
+      B200_CHECK_CUDA(launch_axpby(prec, op->g, x, e, 1.0, nullptr, 1.0, nullptr, st));
+    }
+  } else {
+    rc = cg_core(op, prec, x, b, maxiter, tol2, &n, &rel2, st);
+  }
   if (rc && rc != B200_ENOCONV) return rc;
   const std::string msg = g_err;
   double d = 0.0;
@@ -1007,6 +1032,12 @@ int b200_shiftcg_solve(b200_dwf_t* op, void* const* x, const double* sigma, int 
   return 0;
 }
 
+int b200_solver_set_initial_guess(b200_dwf_t* op, int use) {
+  if (!op) return fail(B200_EINVAL, "invalid argument");
+  op->init_guess = use != 0;
+  return 0;
+}
+
 int b200_shiftcg_set_window(b200_dwf_t* op, int window) {
   if (!op || window < 0 || window > kMaxWin)
     return fail(B200_EINVAL, "window must be in [0, %d]", kMaxWin);
@@ -1039,16 +1070,25 @@ int b200_richardson_solve(b200_dwf_t* op, int inner_prec, void* x, const void* b
   if ((rc = field_norm2_dev(op, P64, b, op->sc + SC_RR_NEW, st))) return rc;
   double bnorm2 = 0.0;
   if ((rc = host_scalar(op, SC_RR_NEW, &bnorm2, st))) return rc;
-  B200_CHECK_CUDA(launch_axpby(P64, g, x, nullptr, 0.0, nullptr, 0.0, nullptr, st));
+  if (!op->init_guess) B200_CHECK_CUDA(launch_axpby(P64, g, x, nullptr, 0.0, nullptr, 0.0, nullptr, st));
   int total_inner = 0;
   if (!(bnorm2 > 0.0)) {
+    B200_CHECK_CUDA(launch_axpby(P64, g, x, nullptr, 0.0, nullptr, 0.0, nullptr, st));
     if (nconv) *nconv = 0;
     if (nconv_inner) *nconv_inner = 0;
     if (diff) *diff = 0.0;
     return 0;
   }
-  B200_CHECK_CUDA(launch_axpby(P64, g, r, b, -1.0, nullptr, 0.0, nullptr, st));
   double r2 = bnorm2;
+  if (op->init_guess) {
+    // use_initial_guess: start from the residual of the x passed in
+    if ((rc = apply_DdagD(op, P64, r, x, st))) return rc;
+    B200_CHECK_CUDA(launch_axpby(P64, g, r, b, -1.0, nullptr, 1.0, nullptr, st));
+    if ((rc = field_norm2_dev(op, P64, r, op->sc + SC_RR_NEW, st))) return rc;
+    if ((rc = host_scalar(op, SC_RR_NEW, &r2, st))) return rc;
+  } else {
+    B200_CHECK_CUDA(launch_axpby(P64, g, r, b, -1.0, nullptr, 0.0, nullptr, st));
+  }
   int conv = -1;
   for (int it = 0; it < maxiter; ++it) {
     if (r2 < bnorm2 * tol2) { conv = it; break; }

@@ -212,3 +212,26 @@ def test_mixed_precision_solvers_reproduce_the_fp64_trajectory():
         out[kind] = (h1 - h0, ud.cpu().numpy())
     assert abs(out["mixed"][0] - out["cg"][0]) < 1e-8
     assert np.max(np.abs(out["mixed"][1] - out["cg"][1])) < 1e-10
+
+
+@pytest.mark.gpu
+def test_chronological_guess_keeps_the_trajectory_and_saves_iterations():
+    """The MD solves of the ratio actions starting from the previous solution
+    (use_initial_guess, CG and Richardson): the same dH and end links to the
+    solver tolerance, and fewer solver iterations."""
+    from b200dwf.hmc import Solver
+    out = {}
+    for chrono in (False, True):
+        for kind in ("cg", "mixed"):
+            sv = {k: Solver(kind, 1e-24, chrono=chrono) for k in ("l_md", "h_md", "l_h", "h_h", "pv_h")}
+            hmc, u, ud, ip = _small_hmc(151, solvers=sv)
+            h0, _ = hmc.calc_hamiltonian(ip)
+            hmc.integrator.evolve(0.2, ip, ud)
+            h1, _ = hmc.calc_hamiltonian(ip)
+            its = sum(sv[k].iterations for k in ("l_md", "h_md"))
+            out[(chrono, kind)] = (h1 - h0, ud.cpu().numpy(), its)
+    for kind in ("cg", "mixed"):
+        a, b = out[(False, kind)], out[(True, kind)]
+        assert abs(a[0] - b[0]) < 1e-8, kind
+        assert np.max(np.abs(a[1] - b[1])) < 1e-10, kind
+        assert b[2] < a[2], (kind, a[2], b[2])
