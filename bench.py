@@ -571,7 +571,7 @@ def b200_arm(args, rank, world, local_rank):
     # mixed-precision Richardson (FP64 outer, inner CG in f32/f16/bf16) and the
     # 16-pole multishift CG (shifts log-spaced 1e-4..64), same lattice and RHS
     solvers = None
-    if not args.no_solvers:
+    if not args.no_solvers and world == 1:
         solvers = {"richardson": {}, "multishift": None}
         for name, prec, tin in (("f32", 1, 1e-8), ("f16", 2, 1e-4), ("bf16", 3, 1e-4)):
             x = op.new_field(0)
@@ -608,10 +608,12 @@ def b200_arm(args, rank, world, local_rank):
         del xs
 
     learned, lp = None, None
-    if not args.no_learned:
+    # the solver, learned-network and trajectory sections are one-GPU
+    # workloads; under torchrun (replicas) only the Dslash metric is timed
+    if not args.no_learned and world == 1:
         learned, lp = learned_section(op, lattice, w, u, args)
     trajectory = None
-    if not args.no_trajectory:
+    if not args.no_trajectory and world == 1:
         trajectory = trajectory_section(op, lattice, u, args, lp)
 
     small = None
