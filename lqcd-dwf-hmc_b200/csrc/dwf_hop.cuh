@@ -28,9 +28,14 @@ enum LinkFmt { LINK_F64_18 = 0, LINK_F64_12 = 1, LINK_F32_12 = 2, LINK_F16_12 = 
 
 template <int LF> struct LinkLoad;
 
+// kPhased: the plan stores this format with the boundary phase bc[mu]
+// already multiplied into the links of the last slice along mu (full
+// 3x3 records only: a reconstructed third row would not carry the phase), so
+// the hop kernels skip the per-direction phase factor.
 template <> struct LinkLoad<LINK_F64_18> {
   using R = double;
   static constexpr int kChunks = 9;
+  static constexpr bool kPhased = true;
   __device__ static void load_plain(const void* rec, double* u) {
     const double2* p = reinterpret_cast<const double2*>(rec);
 #pragma unroll
@@ -45,6 +50,7 @@ template <> struct LinkLoad<LINK_F64_18> {
 template <> struct LinkLoad<LINK_F64_12> {
   using R = double;
   static constexpr int kChunks = 6;
+  static constexpr bool kPhased = false;
   __device__ static void load_plain(const void* rec, double* u) {
     const double2* p = reinterpret_cast<const double2*>(rec);
 #pragma unroll
@@ -61,6 +67,7 @@ template <> struct LinkLoad<LINK_F64_12> {
 template <> struct LinkLoad<LINK_F32_12> {
   using R = float;
   static constexpr int kChunks = 3;
+  static constexpr bool kPhased = false;
   __device__ static void load_plain(const void* rec, float* u) {
     const float4* p = reinterpret_cast<const float4*>(rec);
 #pragma unroll
@@ -83,6 +90,7 @@ template <> struct LinkLoad<LINK_F32_12> {
 template <> struct LinkLoad<LINK_F16_12> {
   using R = float;
   static constexpr int kChunks = 2;
+  static constexpr bool kPhased = false;
   __device__ static void load_plain(const void* rec, float* u) {
     const uint4* p = reinterpret_cast<const uint4*>(rec);
     uint4 a = p[0], b = p[1];
@@ -165,12 +173,14 @@ __device__ __forceinline__ void project(const R* w, R* h) {
   }
 }
 
-template <typename R, int MU, int SIGN>
+// kUnit: the phase is 1 (phased links), no multiplication is issued.
+template <typename R, int MU, int SIGN, bool kUnit = false>
 __device__ __forceinline__ void reconstruct_acc(R* acc, const R* o, R ph) {
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    const R a0r = ph * o[2 * c], a0i = ph * o[2 * c + 1];
-    const R a1r = ph * o[6 + 2 * c], a1i = ph * o[6 + 2 * c + 1];
+    const R a0r = kUnit ? o[2 * c] : ph * o[2 * c], a0i = kUnit ? o[2 * c + 1] : ph * o[2 * c + 1];
+    const R a1r = kUnit ? o[6 + 2 * c] : ph * o[6 + 2 * c];
+    const R a1i = kUnit ? o[6 + 2 * c + 1] : ph * o[6 + 2 * c + 1];
     R* r0 = acc + 2 * c;
     R* r1 = acc + 2 * (c + 3);
     R* r2 = acc + 2 * (c + 6);
@@ -396,6 +406,7 @@ dwf_hop_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename Sto
   using St = Store<P>;
   using R = typename St::R;
   constexpr bool kDagHop = EpiIsDag<EPI>::v;
+  constexpr bool kPh = LinkLoad<LF>::kPhased;
   constexpr int G = 32 / LS;              // sites per warp
   constexpr int WARPS = 4;
   constexpr bool kTile = (EPI != EPI_HALF) || (FK != F_NONE);
@@ -434,7 +445,7 @@ dwf_hop_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename Sto
     {                                                                                \
       R w[24], h[12], o[12], u[18];                                                  \
       {                                                                              \
-        const R ph = (COORD == EXT - 1) ? (R)p.bc[MU] : R(1);                        \
+        const R ph = (kPh || COORD != EXT - 1) ? R(1) : (R)p.bc[MU];                 \
         const int nb = NBP;                                                          \
         St::load(p.in, vh, LS, nb, s, w);                                            \
         if (kDagHop) {                                                               \
@@ -444,10 +455,10 @@ dwf_hop_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename Sto
         project<R, MU, 1>(w, h);                                                     \
         LinkLoad<LF>::load(p.links, (size_t)(ieo + 2 * MU) * strideMu + site, u);    \
         su3_mult_half<R, false>(u, h, o);                                            \
-        reconstruct_acc<R, MU, 1>(acc, o, ph);                                       \
+        reconstruct_acc<R, MU, 1, kPh>(acc, o, ph);                                  \
       }                                                                              \
       {                                                                              \
-        const R ph = (COORD == 0) ? (R)p.bc[MU] : R(1);                              \
+        const R ph = (kPh || COORD != 0) ? R(1) : (R)p.bc[MU];                       \
         const int nb = NBM;                                                          \
         St::load(p.in, vh, LS, nb, s, w);                                            \
         if (kDagHop) {                                                               \
@@ -457,7 +468,7 @@ dwf_hop_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename Sto
         project<R, MU, -1>(w, h);                                                    \
         LinkLoad<LF>::load(p.links, (size_t)(1 - ieo + 2 * MU) * strideMu + nb, u);  \
         su3_mult_half<R, true>(u, h, o);                                             \
-        reconstruct_acc<R, MU, -1>(acc, o, ph);                                      \
+        reconstruct_acc<R, MU, -1, kPh>(acc, o, ph);                                 \
       }                                                                              \
     }
 
@@ -870,6 +881,8 @@ dwf_hop_tma_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename
   using R = typename St::R;
   using TG = TmaGeom<LS, P, LF>;
   constexpr bool kDagHop = EpiIsDag<EPI>::v;
+  constexpr bool kPh = LinkLoad<LF>::kPhased;
+  constexpr int NPH = kPh ? 1 : 8;        // edge phases kept in registers
   constexpr int G = TG::G;
   constexpr int WARPS = 4;
   constexpr int WB = TG::template warp_bytes<S>();
@@ -899,7 +912,9 @@ dwf_hop_tma_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename
 
   // neighbour sites and edge phases of the 8 directions (x+, x-, y+, ..., t-)
   int nb[8];
-  R ph[8];
+  R ph[NPH];
+#pragma unroll
+  for (int d = 0; d < NPH; ++d) ph[d] = R(1);
   if (active) {
     const int ix2 = site % p.nx2;
     const int iyzt = site / p.nx2;
@@ -912,24 +927,26 @@ dwf_hop_tma_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename
     const int row = p.nx2 * iyzt;
     nb[0] = row + ((ix2 + keo == p.nx2) ? 0 : ix2 + keo);
     nb[1] = row + ((ix2 - 1 + keo < 0) ? p.nx2 - 1 : ix2 - 1 + keo);
-    ph[0] = (x == 2 * p.nx2 - 1) ? (R)p.bc[0] : R(1);
-    ph[1] = (x == 0) ? (R)p.bc[0] : R(1);
     const int sy = p.nx2, sz = p.nx2 * p.ny, st4 = p.nx2 * p.ny * p.nz;
     nb[2] = (y == p.ny - 1) ? site - (p.ny - 1) * sy : site + sy;
     nb[3] = (y == 0) ? site + (p.ny - 1) * sy : site - sy;
-    ph[2] = (y == p.ny - 1) ? (R)p.bc[1] : R(1);
-    ph[3] = (y == 0) ? (R)p.bc[1] : R(1);
     nb[4] = (z == p.nz - 1) ? site - (p.nz - 1) * sz : site + sz;
     nb[5] = (z == 0) ? site + (p.nz - 1) * sz : site - sz;
-    ph[4] = (z == p.nz - 1) ? (R)p.bc[2] : R(1);
-    ph[5] = (z == 0) ? (R)p.bc[2] : R(1);
     nb[6] = (t == p.nt - 1) ? site - (p.nt - 1) * st4 : site + st4;
     nb[7] = (t == 0) ? site + (p.nt - 1) * st4 : site - st4;
-    ph[6] = (t == p.nt - 1) ? (R)p.bc[3] : R(1);
-    ph[7] = (t == 0) ? (R)p.bc[3] : R(1);
+    if constexpr (!kPh) {
+      ph[0 % NPH] = (x == 2 * p.nx2 - 1) ? (R)p.bc[0] : R(1);
+      ph[1 % NPH] = (x == 0) ? (R)p.bc[0] : R(1);
+      ph[2 % NPH] = (y == p.ny - 1) ? (R)p.bc[1] : R(1);
+      ph[3 % NPH] = (y == 0) ? (R)p.bc[1] : R(1);
+      ph[4 % NPH] = (z == p.nz - 1) ? (R)p.bc[2] : R(1);
+      ph[5 % NPH] = (z == 0) ? (R)p.bc[2] : R(1);
+      ph[6 % NPH] = (t == p.nt - 1) ? (R)p.bc[3] : R(1);
+      ph[7 % NPH] = (t == 0) ? (R)p.bc[3] : R(1);
+    }
   } else {
 #pragma unroll
-    for (int d = 0; d < 8; ++d) { nb[d] = 0; ph[d] = R(0); }
+    for (int d = 0; d < 8; ++d) nb[d] = 0;
   }
 
   auto col_ptr = [&](int st) { return wbase + (size_t)(st * G + g) * TG::SLOT; };
@@ -980,7 +997,7 @@ dwf_hop_tma_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename
       project<R, MU, SIGN>(w, h);                                                    \
       LinkLoad<LF>::load_plain(c + TG::COL, u);                                      \
       su3_mult_half<R, (SIGN < 0)>(u, h, o);                                         \
-      reconstruct_acc<R, MU, SIGN>(acc, o, ph[D]);                                   \
+      reconstruct_acc<R, MU, SIGN, kPh>(acc, o, ph[(D) % NPH]);                      \
     }                                                                                \
     __syncwarp();                                                                    \
     if ((D) + S < 8 && ok) {                                                         \

@@ -46,7 +46,7 @@ struct CgUpdParams {
   void* x;
   void* p;
   const void* r;
-  void* y;
+  void* y;               // M5pre(p) for the next hop; null when M5pre is the identity
   const double* alpha;
   const double* beta;
   Geom g;
@@ -90,7 +90,7 @@ struct MsUpdParams {
   void* const* xs;       // device array [nshift] of solution fields
   void* const* ps;       // device array [nshift] of search directions
   const void* r;
-  void* y0;              // M5pre(p_0) for the next hop
+  void* y0;              // M5pre(p_0) for the next hop (null: M5pre is the identity)
   const double* st;      // multishift state (MS_*, MSA_*)
   double* red;           // partials [kMaxShift][nblocks] of |p_i|^2
   int nblocks;
@@ -152,8 +152,9 @@ cudaError_t launch_from_corelib(int prec, void* out, const double* in_dev, const
 cudaError_t launch_to_corelib(int prec, double* out_dev, const void* in, const Geom& g,
                               cudaStream_t st);
 // lexical links (corelib Field_G layout) -> even/odd links in link format lf
+// (LINK_F64_18 with the boundary phases bc multiplied into the edge links)
 cudaError_t launch_links_from_lex(int lf, void* out, const double* u_lex_dev, const Geom& g,
-                                  cudaStream_t st);
+                                  const int bc[4], cudaStream_t st);
 
 // out[0] = sum(partials[0..n)); op selects a solver scalar update afterwards:
 enum FinalizeOp {

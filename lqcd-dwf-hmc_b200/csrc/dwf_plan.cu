@@ -162,6 +162,7 @@ struct b200_dwf {
   void* (*work)[4] = nullptr;   // = ws->work: work fields per slot and precision
   void* tune_out[2][4] = {};    // autotuner scratch outputs per precision
   ChainCoefs coefs;             // fifth-dimension chain coefficients
+  bool m5pre_id = false;        // D_eo pre-factor is the identity (b = 1, c = 0, alpha = 1)
   double* ms_state = nullptr;   // multishift scalar state (device)
   double* ms_red = nullptr;     // multishift per-shift partials
   void** ms_ptrs = nullptr;     // device arrays of x_i and p_i pointers
@@ -198,7 +199,7 @@ int ensure_links(b200_dwf* op, int prec, cudaStream_t st) {
   if (!op->links[lf]) {
     if (cudaMalloc(&op->links[lf], link_bytes(lf, op->g.vh)) != cudaSuccess)
       return fail(B200_ENOMEM, "cudaMalloc for links failed");
-    B200_CHECK_CUDA(launch_links_from_lex(lf, op->links[lf], op->u_lex, op->g, st));
+    B200_CHECK_CUDA(launch_links_from_lex(lf, op->links[lf], op->u_lex, op->g, op->bc, st));
   }
   return 0;
 }
@@ -338,9 +339,9 @@ int apply_D(b200_dwf* op, int prec, void* v, const void* w, int fk, void* v2, do
   if ((rc = ensure_work(op, prec, 0)) || (rc = ensure_work(op, prec, 1))) return rc;
   void* t0 = op->work[0][prec];
   void* y1 = op->work[1][prec];
-  if ((rc = apply_sop(op, prec, t0, w, SOP_M5PRE, st))) return rc;
+  if (!op->m5pre_id && (rc = apply_sop(op, prec, t0, w, SOP_M5PRE, st))) return rc;
   HopParams p1 = hop_base(op, prec, 1, EPI_K1);
-  p1.in = t0; p1.out1 = y1;
+  p1.in = op->m5pre_id ? w : t0; p1.out1 = y1;
   if ((rc = run_hop(op, prec, p1, st))) return rc;
   HopParams p2 = hop_base(op, prec, 0, EPI_K2N, fk);
   p2.in = y1; p2.out1 = v;
@@ -413,11 +414,14 @@ int apply_mode(b200_dwf* op, int prec, void* v, const void* w, const std::string
       p.in = w; p.out1 = v;
       return run_hop(op, prec, p, st);
     }
-    if ((rc = ensure_work(op, prec, 0))) return rc;
-    void* t0 = op->work[0][prec];
-    if ((rc = apply_sop(op, prec, t0, w, SOP_M5PRE, st))) return rc;
     HopParams p = hop_base(op, prec, out_par, EPI_HALF);
-    p.in = t0; p.out1 = v;
+    p.in = w; p.out1 = v;
+    if (!op->m5pre_id || v == w) {
+      if ((rc = ensure_work(op, prec, 0))) return rc;
+      void* t0 = op->work[0][prec];
+      if ((rc = apply_sop(op, prec, t0, w, SOP_M5PRE, st))) return rc;
+      p.in = t0;
+    }
     return run_hop(op, prec, p, st);
   }
   if (mode == "Dee" || mode == "Doo") return apply_sop(op, prec, v, w, dag ? SOP_DEE_T : SOP_DEE, st);
@@ -491,6 +495,12 @@ int b200_dwf_create(b200_dwf_t** out, const int lattice[4], int Ls, double mq, d
   if (b) op->k.b.assign(b, b + Ls);
   if (c) op->k.c.assign(c, c + Ls);
   set_precond(op->k);
+  // Shamir kernel at alpha = 1: M5pre = b_s Wf + c_s(...) is the identity, so
+  // the pre-factor pass before each D_eo hop (and the M5pre p field of the
+  // solvers) is skipped and the hop reads its input directly.
+  op->m5pre_id = (alpha == 1.0);
+  for (int s = 0; s < Ls; ++s)
+    if (op->k.b[s] != 1.0 || op->k.c[s] != 0.0) op->m5pre_id = false;
   const long vol = (long)lattice[0] * lattice[1] * lattice[2] * lattice[3];
   op->g.nx2 = lattice[0] / 2; op->g.ny = lattice[1]; op->g.nz = lattice[2]; op->g.nt = lattice[3];
   op->g.ls = Ls; op->g.vh = (int)(vol / 2);
@@ -596,7 +606,7 @@ static int set_config_common(b200_dwf_t* op, const double* u, cudaMemcpyKind kin
   B200_CHECK_CUDA(cudaMemcpyAsync(op->u_lex, u, n * sizeof(double), kind, st));
   op->have_links = true;
   for (int lf = 0; lf < 4; ++lf)
-    if (op->links[lf]) B200_CHECK_CUDA(launch_links_from_lex(lf, op->links[lf], op->u_lex, op->g, st));
+    if (op->links[lf]) B200_CHECK_CUDA(launch_links_from_lex(lf, op->links[lf], op->u_lex, op->g, op->bc, st));
   B200_CHECK_CUDA(cudaStreamSynchronize(st));
   return 0;
 }
@@ -714,7 +724,8 @@ static int cg_core(b200_dwf_t* op, int prec, void* x, const void* b, int maxiter
   *nconv = 0;
   *rel2 = 0.0;
   if (!(bnorm2 > 0.0)) return 0;
-  if ((rc = apply_sop(op, prec, yp, p, SOP_M5PRE, st))) return rc;
+  if (op->m5pre_id) yp = p;
+  else if ((rc = apply_sop(op, prec, yp, p, SOP_M5PRE, st))) return rc;
 
   double rr = bnorm2;
   for (int it = 0; it < maxiter; ++it) {
@@ -744,7 +755,7 @@ static int cg_core(b200_dwf_t* op, int prec, void* x, const void* b, int maxiter
     if ((rc = reduce_to(op, nb_hop, op->sc, FIN_CG_BETA, st))) return rc;
 
     CgUpdParams pu;
-    pu.x = x; pu.p = p; pu.r = r; pu.y = yp;
+    pu.x = x; pu.p = p; pu.r = r; pu.y = op->m5pre_id ? nullptr : yp;
     pu.alpha = op->sc + SC_ALPHA; pu.beta = op->sc + SC_BETA; pu.g = g;
     B200_CHECK_CUDA(launch_cg_update(prec, pu, op->coefs, st));
     if (snap)
@@ -930,7 +941,8 @@ int b200_shiftcg_solve(b200_dwf_t* op, void* const* x, const double* sigma, int 
   for (int i = 0; i < nshift; ++i) { hp[i] = x[i]; hp[kMaxShift + i] = ps[i]; }
   B200_CHECK_CUDA(cudaMemcpyAsync(op->ms_state, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, st));
   B200_CHECK_CUDA(cudaMemcpyAsync(op->ms_ptrs, hp.data(), hp.size() * sizeof(void*), cudaMemcpyHostToDevice, st));
-  if ((rc = apply_sop(op, prec, y0, p0, SOP_M5PRE, st))) return rc;
+  if (op->m5pre_id) y0 = p0;
+  else if ((rc = apply_sop(op, prec, y0, p0, SOP_M5PRE, st))) return rc;
   double* S = op->ms_state;
 
   // One iteration: the four fused DdagD hops, the scalar steps and the fused
@@ -960,7 +972,7 @@ int b200_shiftcg_solve(b200_dwf_t* op, void* const* x, const double* sigma, int 
     if ((rc2 = run_hop(op, prec, p4, s))) return rc2;
     B200_CHECK_CUDA(launch_ms_scalar(MSS_ALPHA, op->red, nb_hop, S, nshift, s));
     MsUpdParams mu;
-    mu.xs = op->ms_ptrs; mu.ps = op->ms_ptrs + kMaxShift; mu.r = r; mu.y0 = y0;
+    mu.xs = op->ms_ptrs; mu.ps = op->ms_ptrs + kMaxShift; mu.r = r; mu.y0 = op->m5pre_id ? nullptr : y0;
     mu.st = S; mu.red = op->ms_red; mu.nblocks = nb_hop; mu.g = g;
     mu.win = window > 0 ? op->ms_win_ptrs : nullptr;
     B200_CHECK_CUDA(launch_ms_update(prec, mu, op->coefs, s));
@@ -1265,11 +1277,11 @@ static int force_fields(b200_dwf_t* op, const void* eta, const void* zeta, bool 
   if ((rc = ensure_links(op, prec, st))) return rc;
   for (int i = 0; i < 5; ++i)
     if ((rc = ensure_work(op, prec, i))) return rc;
-  void* ye = op->work[0][prec];
+  const void* ye = op->m5pre_id ? eta : op->work[0][prec];
   void* yo = op->work[1][prec];
   void* ae = op->work[2][prec];
   void* ao = op->work[3][prec];
-  if ((rc = apply_sop(op, prec, ye, eta, SOP_M5PRE, st))) return rc;
+  if (!op->m5pre_id && (rc = apply_sop(op, prec, op->work[0][prec], eta, SOP_M5PRE, st))) return rc;
   HopParams p1 = hop_base(op, prec, 1, EPI_K1);
   p1.in = ye; p1.out1 = yo;
   if ((rc = run_hop(op, prec, p1, st))) return rc;
@@ -1320,7 +1332,7 @@ static int force_impl(b200_dwf_t* op, const char* mode, double* force, const voi
   const void* zeta = udiv ? nullptr : (hdag ? b : a);
   int rc;
   if ((rc = force_fields(op, eta, zeta, udiv, st))) return rc;
-  void* ye = op->work[0][PREC_F64];
+  const void* ye = op->m5pre_id ? eta : op->work[0][PREC_F64];
   void* yo = op->work[1][PREC_F64];
   void* ae = op->work[2][PREC_F64];
   void* ao = op->work[3][PREC_F64];

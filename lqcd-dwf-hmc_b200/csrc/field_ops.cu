@@ -254,6 +254,7 @@ cg_update_kernel(CgUpdParams p, const __grid_constant__ ChainCoef<typename Store
     St::store(p.x, vh, LS, site, s, xv);
     St::store(p.p, vh, LS, site, s, pv);
   }
+  if (!p.y) return;   // identity pre-factor: the next hop reads p itself
   if (g < G) {
     tile_put(tile_row<R, LS>(tile, g, s), pv);
   }
@@ -351,19 +352,21 @@ ms_update_kernel(MsUpdParams p, const __grid_constant__ ChainCoef<typename Store
     St::store(p.xs[0], vh, LS, site, s, xv);
     St::store(p.ps[0], vh, LS, site, s, pv);
   }
-  if (g < G) {
-    tile_put(tile_row<R, LS>(tile, g, s), pv);
-  }
-  __syncwarp();
-  tile_chiral<R, LS, G>(tile, lane, [&](R* xp, R* xm) {
-    chain_m5pre<R, LS, 0>(k, xp);
-    chain_m5pre<R, LS, 1>(k, xm);
-  });
-  __syncwarp();
-  if (active) {
-    R o[24];
-    tile_get(tile_row<R, LS>(tile, g, s), o);
-    St::store(p.y0, vh, LS, site, s, o);
+  if (p.y0) {         // null: identity pre-factor, the next hop reads p_0
+    if (g < G) {
+      tile_put(tile_row<R, LS>(tile, g, s), pv);
+    }
+    __syncwarp();
+    tile_chiral<R, LS, G>(tile, lane, [&](R* xp, R* xm) {
+      chain_m5pre<R, LS, 0>(k, xp);
+      chain_m5pre<R, LS, 1>(k, xm);
+    });
+    __syncwarp();
+    if (active) {
+      R o[24];
+      tile_get(tile_row<R, LS>(tile, g, s), o);
+      St::store(p.y0, vh, LS, site, s, o);
+    }
   }
   block_reduce_store(nrm, p.red);
   if (p.win) {
@@ -700,9 +703,16 @@ __global__ void to_corelib_kernel(Geom g, double* out, const void* in) {
 }
 
 // links: out index (ieo + 2*mu)*Vh + site_eo  (reference m_Ueo ordering,
-// src/lib_alt_Accel/Fopr/afopr_Domainwall_5din_eo-tmpl.h:140-141)
+// src/lib_alt_Accel/Fopr/afopr_Domainwall_5din_eo-tmpl.h:140-141).
+// The full-record FP64 format (LINK_F64_18, LinkLoad::kPhased) carries the
+// boundary phase: links U_mu(x) with x_mu = L_mu - 1 are stored times
+// bc[mu], which is the factor the reference applies to both hops across that
+// edge (forward from x, backward from x + mu), so the hop kernels need no
+// per-direction phase.  Real phases only (bc is an integer vector).
+struct LinkPhase { double bc[4]; };
+
 template <int LF>
-__global__ void links_kernel(Geom g, void* out, const double* u) {
+__global__ void links_kernel(Geom g, void* out, const double* u, LinkPhase ph) {
   const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (long)8 * g.vh) return;
   const int site = (int)(idx % g.vh);
@@ -719,8 +729,11 @@ __global__ void links_kernel(Geom g, void* out, const double* u) {
   const size_t vol = (size_t)2 * g.vh;
   const double* m = u + 18 * (lex + vol * mu);
   if (LF == LINK_F64_18) {
+    const int c = (mu == 0) ? x : (mu == 1) ? y : (mu == 2) ? z : t;
+    const int ext = (mu == 0) ? nx : (mu == 1) ? g.ny : (mu == 2) ? g.nz : g.nt;
+    const double f = (c == ext - 1) ? ph.bc[mu] : 1.0;
     double2* o = reinterpret_cast<double2*>(out) + idx * 9;
-    for (int j = 0; j < 9; ++j) o[j] = make_double2(m[2 * j], m[2 * j + 1]);
+    for (int j = 0; j < 9; ++j) o[j] = make_double2(f * m[2 * j], f * m[2 * j + 1]);
   } else if (LF == LINK_F64_12) {
     double2* o = reinterpret_cast<double2*>(out) + idx * 6;
     for (int j = 0; j < 6; ++j) o[j] = make_double2(m[2 * j], m[2 * j + 1]);
@@ -837,14 +850,16 @@ cudaError_t launch_to_corelib(int prec, double* out_dev, const void* in, const G
 }
 
 cudaError_t launch_links_from_lex(int lf, void* out, const double* u_lex_dev, const Geom& g,
-                                  cudaStream_t st) {
+                                  const int bc[4], cudaStream_t st) {
   const long n = 8L * g.vh;
   const int grid = (int)((n + 127) / 128);
+  LinkPhase ph;
+  for (int mu = 0; mu < 4; ++mu) ph.bc[mu] = (double)bc[mu];
   switch (lf) {
-    case LINK_F64_18: links_kernel<LINK_F64_18><<<grid, 128, 0, st>>>(g, out, u_lex_dev); break;
-    case LINK_F64_12: links_kernel<LINK_F64_12><<<grid, 128, 0, st>>>(g, out, u_lex_dev); break;
-    case LINK_F32_12: links_kernel<LINK_F32_12><<<grid, 128, 0, st>>>(g, out, u_lex_dev); break;
-    case LINK_F16_12: links_kernel<LINK_F16_12><<<grid, 128, 0, st>>>(g, out, u_lex_dev); break;
+    case LINK_F64_18: links_kernel<LINK_F64_18><<<grid, 128, 0, st>>>(g, out, u_lex_dev, ph); break;
+    case LINK_F64_12: links_kernel<LINK_F64_12><<<grid, 128, 0, st>>>(g, out, u_lex_dev, ph); break;
+    case LINK_F32_12: links_kernel<LINK_F32_12><<<grid, 128, 0, st>>>(g, out, u_lex_dev, ph); break;
+    case LINK_F16_12: links_kernel<LINK_F16_12><<<grid, 128, 0, st>>>(g, out, u_lex_dev, ph); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
