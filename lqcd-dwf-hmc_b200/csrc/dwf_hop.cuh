@@ -24,7 +24,10 @@
 
 namespace b200 {
 
-enum LinkFmt { LINK_F64_18 = 0, LINK_F64_12 = 1, LINK_F32_12 = 2, LINK_F16_12 = 3 };
+enum LinkFmt {
+  LINK_F64_18 = 0, LINK_F64_12 = 1, LINK_F32_12 = 2, LINK_F16_12 = 3, LINK_F32_18 = 4, LINK_F16_18 = 5,
+  LINK_NFMT = 6
+};
 
 template <int LF> struct LinkLoad;
 
@@ -115,6 +118,56 @@ template <> struct LinkLoad<LINK_F16_12> {
   }
 };
 
+// Full 3x3 records in FP32 (18 floats padded to 5 float4) and in FP16 (18
+// halves padded to 3 uint4): no third-row rebuild in the hop (the lanes of a
+// site would each repeat it), boundary phase folded in like LINK_F64_18.
+template <> struct LinkLoad<LINK_F32_18> {
+  using R = float;
+  static constexpr int kChunks = 5;
+  static constexpr bool kPhased = true;
+  __device__ static void load_plain(const void* rec, float* u) {
+    const float4* p = reinterpret_cast<const float4*>(rec);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      float4 c = p[j];
+      u[4 * j] = c.x; u[4 * j + 1] = c.y; u[4 * j + 2] = c.z; u[4 * j + 3] = c.w;
+    }
+    const float2 c = reinterpret_cast<const float2*>(p + 4)[0];
+    u[16] = c.x; u[17] = c.y;
+  }
+  __device__ static void load(const void* base, size_t idx, float* u) {
+    const float4* p = reinterpret_cast<const float4*>(base) + idx * 5;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      float4 c = __ldg(p + j);
+      u[4 * j] = c.x; u[4 * j + 1] = c.y; u[4 * j + 2] = c.z; u[4 * j + 3] = c.w;
+    }
+    const float2 c = __ldg(reinterpret_cast<const float2*>(p + 4));
+    u[16] = c.x; u[17] = c.y;
+  }
+};
+template <> struct LinkLoad<LINK_F16_18> {
+  using R = float;
+  static constexpr int kChunks = 3;
+  static constexpr bool kPhased = true;
+  __device__ static void decode(uint4 a, uint4 b, uint4 c, float* u) {
+    const unsigned int w[9] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x};
+#pragma unroll
+    for (int j = 0; j < 9; ++j) {
+      float2 f = HalfOps<__half>::to2(w[j]);
+      u[2 * j] = f.x; u[2 * j + 1] = f.y;
+    }
+  }
+  __device__ static void load_plain(const void* rec, float* u) {
+    const uint4* p = reinterpret_cast<const uint4*>(rec);
+    decode(p[0], p[1], p[2], u);
+  }
+  __device__ static void load(const void* base, size_t idx, float* u) {
+    const uint4* p = reinterpret_cast<const uint4*>(base) + idx * 3;
+    decode(__ldg(p), __ldg(p + 1), __ldg(p + 2), u);
+  }
+};
+
 // ------------------------------------------------------------ complex helpers
 template <typename R>
 __device__ __forceinline__ void cmul_acc(R& ore, R& oim, R ar, R ai, R br, R bi) {
@@ -199,6 +252,62 @@ __device__ __forceinline__ void reconstruct_acc(R* acc, const R* o, R ph) {
       r2[0] -= SIGN * a1r; r2[1] -= SIGN * a1i;
       r3[0] += SIGN * a0r; r3[1] += SIGN * a0i;
     } else {              // MU==2: rows 2,3 = -+ i h0, +- i h1
+      r2[0] += SIGN * a0i; r2[1] -= SIGN * a0r;
+      r3[0] -= SIGN * a1i; r3[1] += SIGN * a1r;
+    }
+  }
+}
+
+// One hop direction for full (18-real) FP64 link records read from shared
+// memory, colour by colour: for output colour i only the three link entries
+// it needs (row i of U, or column i for U^+) are loaded, multiplied into both
+// projected spins and reconstructed into acc, so the live state is the
+// accumulator, the projected half spinor and one link row (instead of the
+// whole link and the whole product).  Phased links (no edge factor).
+template <int MU, int SIGN>
+__device__ __forceinline__ void hop_dir_rows_f64(const double2* urec, const double* h, double* acc) {
+  constexpr bool kDag = SIGN < 0;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    double2 uc[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) uc[j] = urec[kDag ? (3 * j + i) : (3 * i + j)];
+    double o[12];
+#pragma unroll
+    for (int q = 0; q < 12; ++q) o[q] = 0.0;
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {
+      double re = 0.0, im = 0.0;
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const double ur = uc[j].x;
+        const double ui = kDag ? -uc[j].y : uc[j].y;
+        cmul_acc(re, im, ur, ui, h[6 * a + 2 * j], h[6 * a + 2 * j + 1]);
+      }
+      o[6 * a + 2 * i] = re;
+      o[6 * a + 2 * i + 1] = im;
+    }
+    // reconstruct colour i only (reconstruct_acc's colour loop body)
+    const double a0r = o[2 * i], a0i = o[2 * i + 1];
+    const double a1r = o[6 + 2 * i], a1i = o[6 + 2 * i + 1];
+    double* r0 = acc + 2 * i;
+    double* r1 = acc + 2 * (i + 3);
+    double* r2 = acc + 2 * (i + 6);
+    double* r3 = acc + 2 * (i + 9);
+    if (MU == 3) {
+      if (SIGN > 0) { r2[0] += a0r; r2[1] += a0i; r3[0] += a1r; r3[1] += a1i; }
+      else          { r0[0] += a0r; r0[1] += a0i; r1[0] += a1r; r1[1] += a1i; }
+      continue;
+    }
+    r0[0] += a0r; r0[1] += a0i;
+    r1[0] += a1r; r1[1] += a1i;
+    if (MU == 0) {
+      r2[0] += SIGN * a1i; r2[1] -= SIGN * a1r;
+      r3[0] += SIGN * a0i; r3[1] -= SIGN * a0r;
+    } else if (MU == 1) {
+      r2[0] -= SIGN * a1r; r2[1] -= SIGN * a1i;
+      r3[0] += SIGN * a0r; r3[1] += SIGN * a0i;
+    } else {
       r2[0] += SIGN * a0i; r2[1] -= SIGN * a0r;
       r3[0] -= SIGN * a1i; r3[1] += SIGN * a1r;
     }
@@ -580,6 +689,7 @@ dwf_hop_pair_kernel(const HopParams p, const __grid_constant__ ChainCoef<typenam
   static_assert(sizeof(R) == 4, "packed kernel is for FP32 arithmetic");
   static_assert(32 % LS == 0 && LS % 2 == 0, "packed kernel needs Ls | 32");
   constexpr bool kDagHop = EpiIsDag<EPI>::v;
+  constexpr bool kPh = LinkLoad<LF>::kPhased;
   constexpr int H = LS / 2;               // lanes per site
   constexpr int G = 32 / H;               // sites per warp
   constexpr int WARPS = 4;
@@ -641,10 +751,10 @@ dwf_hop_pair_kernel(const HopParams p, const __grid_constant__ ChainCoef<typenam
 #define B200_PAIR_DIR(MU, COORD, EXT, NBP, NBM)                                      \
     {                                                                                \
       const int nbp = NBP;                                                           \
-      const float php = (COORD == EXT - 1) ? (float)p.bc[MU] : 1.f;                  \
+      const float php = (kPh || COORD != EXT - 1) ? 1.f : (float)p.bc[MU];           \
       B200_PAIR_HALF(MU, 1, nbp, php, (size_t)(ieo + 2 * MU) * vh + site)            \
       const int nbm = NBM;                                                           \
-      const float phm = (COORD == 0) ? (float)p.bc[MU] : 1.f;                        \
+      const float phm = (kPh || COORD != 0) ? 1.f : (float)p.bc[MU];                 \
       B200_PAIR_HALF(MU, -1, nbm, phm, (size_t)(1 - ieo + 2 * MU) * vh + nbm)        \
     }
 
@@ -684,7 +794,7 @@ template <int P>
 struct PairRaw {
   uint4 c0[3], c1[3];   // stored chunks of slices s0 and s1
   float sc0, sc1;       // their scales
-  uint4 l0, l1;         // link record (two rows, 12 halves)
+  uint4 l0, l1, l2;     // link record (LINK_F16_18: full 3x3, 18 halves, phase folded in)
 };
 
 template <int LS, int P>
@@ -701,9 +811,10 @@ __device__ __forceinline__ void pair_fetch(const HopParams& p, int nb, size_t li
   const float* scp = reinterpret_cast<const float*>(c + 3 * LS);
   r.sc0 = __ldg(scp + s0);
   r.sc1 = __ldg(scp + s1);
-  const uint4* lp = reinterpret_cast<const uint4*>(p.links) + lidx * 2;
+  const uint4* lp = reinterpret_cast<const uint4*>(p.links) + lidx * 3;
   r.l0 = __ldg(lp);
   r.l1 = __ldg(lp + 1);
+  r.l2 = __ldg(lp + 2);
 }
 
 template <int P>
@@ -735,15 +846,7 @@ __device__ __forceinline__ void pair_compute(const PairRaw<P>& r, float ph, floa
   const float2 sc = make_float2(r.sc0, r.sc1);
 #pragma unroll
   for (int q = 0; q < 12; ++q) h[q] = __fmul2_rn(make_float2(h0[q], h1[q]), sc);
-  {
-    const unsigned int wl[6] = {r.l0.x, r.l0.y, r.l0.z, r.l0.w, r.l1.x, r.l1.y};
-#pragma unroll
-    for (int q = 0; q < 6; ++q) {
-      const float2 f = HalfOps<__half>::to2(wl[q]);
-      u[2 * q] = f.x; u[2 * q + 1] = f.y;
-    }
-    su3_reconstruct(u);
-  }
+  LinkLoad<LINK_F16_18>::decode(r.l0, r.l1, r.l2, u);
   su3_mult_half2<(SIGN < 0)>(u, h, o);
   reconstruct_acc2<MU, SIGN>(acc, o, ph);
 }
@@ -794,21 +897,21 @@ dwf_hop_pair_pf_kernel(const HopParams p, const __grid_constant__ ChainCoef<type
     const int row = p.nx2 * iyzt;
     nb[0] = row + ((ix2 + keo == p.nx2) ? 0 : ix2 + keo);
     nb[1] = row + ((ix2 - 1 + keo < 0) ? p.nx2 - 1 : ix2 - 1 + keo);
-    ph[0] = (x == 2 * p.nx2 - 1) ? (float)p.bc[0] : 1.f;
-    ph[1] = (x == 0) ? (float)p.bc[0] : 1.f;
+    ph[0] = 1.f;
+    ph[1] = 1.f;
     const int sy = p.nx2, sz = p.nx2 * p.ny, st4 = p.nx2 * p.ny * p.nz;
     nb[2] = (y == p.ny - 1) ? site - (p.ny - 1) * sy : site + sy;
     nb[3] = (y == 0) ? site + (p.ny - 1) * sy : site - sy;
-    ph[2] = (y == p.ny - 1) ? (float)p.bc[1] : 1.f;
-    ph[3] = (y == 0) ? (float)p.bc[1] : 1.f;
+    ph[2] = 1.f;
+    ph[3] = 1.f;
     nb[4] = (z == p.nz - 1) ? site - (p.nz - 1) * sz : site + sz;
     nb[5] = (z == 0) ? site + (p.nz - 1) * sz : site - sz;
-    ph[4] = (z == p.nz - 1) ? (float)p.bc[2] : 1.f;
-    ph[5] = (z == 0) ? (float)p.bc[2] : 1.f;
+    ph[4] = 1.f;
+    ph[5] = 1.f;
     nb[6] = (t == p.nt - 1) ? site - (p.nt - 1) * st4 : site + st4;
     nb[7] = (t == 0) ? site + (p.nt - 1) * st4 : site - st4;
-    ph[6] = (t == p.nt - 1) ? (float)p.bc[3] : 1.f;
-    ph[7] = (t == 0) ? (float)p.bc[3] : 1.f;
+    ph[6] = 1.f;
+    ph[7] = 1.f;
     auto lidx = [&](int d) -> size_t {
       const int mu = d >> 1;
       return (d & 1) ? (size_t)(1 - ieo + 2 * mu) * vh + nb[d] : (size_t)(ieo + 2 * mu) * vh + site;
@@ -995,9 +1098,15 @@ dwf_hop_tma_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename
           R tmp = w[q]; w[q] = w[q + 12]; w[q + 12] = tmp; }                         \
       }                                                                              \
       project<R, MU, SIGN>(w, h);                                                    \
-      LinkLoad<LF>::load_plain(c + TG::COL, u);                                      \
-      su3_mult_half<R, (SIGN < 0)>(u, h, o);                                         \
-      reconstruct_acc<R, MU, SIGN, kPh>(acc, o, ph[(D) % NPH]);                      \
+      if constexpr (LF == LINK_F64_18) {                                             \
+        hop_dir_rows_f64<MU, SIGN>(reinterpret_cast<const double2*>(c + TG::COL),    \
+                                   reinterpret_cast<const double*>(h),               \
+                                   reinterpret_cast<double*>(acc));                  \
+      } else {                                                                       \
+        LinkLoad<LF>::load_plain(c + TG::COL, u);                                    \
+        su3_mult_half<R, (SIGN < 0)>(u, h, o);                                       \
+        reconstruct_acc<R, MU, SIGN, kPh>(acc, o, ph[(D) % NPH]);                    \
+      }                                                                              \
     }                                                                                \
     __syncwarp();                                                                    \
     if ((D) + S < 8 && ok) {                                                         \
@@ -1043,6 +1152,7 @@ dwf_hop_tma_pair_kernel(const HopParams p, const __grid_constant__ ChainCoef<typ
   constexpr int G = 32 / H;
   using TG = TmaGeom<LS, P, LF, G>;
   constexpr bool kDagHop = EpiIsDag<EPI>::v;
+  constexpr bool kPh = LinkLoad<LF>::kPhased;
   constexpr int WARPS = 4;
   constexpr int WB = TG::template warp_bytes<S>();
   constexpr int WBA = (WB + 127) / 128 * 128;
@@ -1084,21 +1194,21 @@ dwf_hop_tma_pair_kernel(const HopParams p, const __grid_constant__ ChainCoef<typ
     const int row = p.nx2 * iyzt;
     nb[0] = row + ((ix2 + keo == p.nx2) ? 0 : ix2 + keo);
     nb[1] = row + ((ix2 - 1 + keo < 0) ? p.nx2 - 1 : ix2 - 1 + keo);
-    ph[0] = (x == 2 * p.nx2 - 1) ? (float)p.bc[0] : 1.f;
-    ph[1] = (x == 0) ? (float)p.bc[0] : 1.f;
+    ph[0] = (!kPh && (x == 2 * p.nx2 - 1)) ? (float)p.bc[0] : 1.f;
+    ph[1] = (!kPh && (x == 0)) ? (float)p.bc[0] : 1.f;
     const int sy = p.nx2, sz = p.nx2 * p.ny, st4 = p.nx2 * p.ny * p.nz;
     nb[2] = (y == p.ny - 1) ? site - (p.ny - 1) * sy : site + sy;
     nb[3] = (y == 0) ? site + (p.ny - 1) * sy : site - sy;
-    ph[2] = (y == p.ny - 1) ? (float)p.bc[1] : 1.f;
-    ph[3] = (y == 0) ? (float)p.bc[1] : 1.f;
+    ph[2] = (!kPh && (y == p.ny - 1)) ? (float)p.bc[1] : 1.f;
+    ph[3] = (!kPh && (y == 0)) ? (float)p.bc[1] : 1.f;
     nb[4] = (z == p.nz - 1) ? site - (p.nz - 1) * sz : site + sz;
     nb[5] = (z == 0) ? site + (p.nz - 1) * sz : site - sz;
-    ph[4] = (z == p.nz - 1) ? (float)p.bc[2] : 1.f;
-    ph[5] = (z == 0) ? (float)p.bc[2] : 1.f;
+    ph[4] = (!kPh && (z == p.nz - 1)) ? (float)p.bc[2] : 1.f;
+    ph[5] = (!kPh && (z == 0)) ? (float)p.bc[2] : 1.f;
     nb[6] = (t == p.nt - 1) ? site - (p.nt - 1) * st4 : site + st4;
     nb[7] = (t == 0) ? site + (p.nt - 1) * st4 : site - st4;
-    ph[6] = (t == p.nt - 1) ? (float)p.bc[3] : 1.f;
-    ph[7] = (t == 0) ? (float)p.bc[3] : 1.f;
+    ph[6] = (!kPh && (t == p.nt - 1)) ? (float)p.bc[3] : 1.f;
+    ph[7] = (!kPh && (t == 0)) ? (float)p.bc[3] : 1.f;
   } else {
 #pragma unroll
     for (int d = 0; d < 8; ++d) { nb[d] = 0; ph[d] = 0.f; }

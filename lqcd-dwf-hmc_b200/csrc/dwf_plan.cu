@@ -148,7 +148,7 @@ struct b200_dwf {
   DwfCoef k;
   int bc[4];
   Geom g;
-  void* links[4] = {nullptr, nullptr, nullptr, nullptr};
+  void* links[LINK_NFMT] = {};
   double* u_lex = nullptr;      // device copy of the lexical links
   bool have_links = false;
   double* red = nullptr;        // reduction partials
@@ -189,19 +189,24 @@ int ensure_work(b200_dwf* op, int prec, int i) {
   return 0;
 }
 
+// link format read by the hop kernels of each storage precision: full 3x3
+// records with the boundary phase folded in
 int link_format_for(int prec) {
-  return prec == PREC_F64 ? LINK_F64_18 : (prec == PREC_F32 ? LINK_F32_12 : LINK_F16_12);
+  return prec == PREC_F64 ? LINK_F64_18 : (prec == PREC_F32 ? LINK_F32_18 : LINK_F16_18);
 }
 
-int ensure_links(b200_dwf* op, int prec, cudaStream_t st) {
+int ensure_link_format(b200_dwf* op, int lf, cudaStream_t st) {
   if (!op->have_links) return fail(B200_EINVAL, "set_config has not been called on this operator");
-  const int lf = link_format_for(prec);
   if (!op->links[lf]) {
     if (cudaMalloc(&op->links[lf], link_bytes(lf, op->g.vh)) != cudaSuccess)
       return fail(B200_ENOMEM, "cudaMalloc for links failed");
     B200_CHECK_CUDA(launch_links_from_lex(lf, op->links[lf], op->u_lex, op->g, op->bc, st));
   }
   return 0;
+}
+
+int ensure_links(b200_dwf* op, int prec, cudaStream_t st) {
+  return ensure_link_format(op, link_format_for(prec), st);
 }
 
 HopParams hop_base(const b200_dwf* op, int prec, int ieo, int epi, int fk = F_NONE) {
@@ -244,6 +249,9 @@ bool variant_supported(int prec, int ls, int v) {
   if (v < 5) return true;
   if (v == 7 && prec == PREC_F64) return true;
   if (v == 9 && (prec == PREC_F64 || prec == PREC_F32)) return false;
+  // 8 stages of 16 sites x (f32 column + 80-byte link record) per warp would
+  // need 232 KB of shared memory per block, above the 227 KB limit
+  if (v == 8 && ls == 4 && prec == PREC_F32) return false;
   return prec != PREC_F64 && 32 % ls == 0;
 }
 std::map<TuneKey, std::pair<int, float> > g_tune;
@@ -567,7 +575,7 @@ int b200_dwf_create(b200_dwf_t** out, const int lattice[4], int Ls, double mq, d
 
 int b200_dwf_destroy(b200_dwf_t* op) {
   if (!op) return 0;
-  for (int i = 0; i < 4; ++i) cudaFree(op->links[i]);
+  for (int i = 0; i < LINK_NFMT; ++i) cudaFree(op->links[i]);
   cudaFree(op->u_lex);
   cudaFree(op->red);
   cudaFree(op->sc);
@@ -605,7 +613,7 @@ static int set_config_common(b200_dwf_t* op, const double* u, cudaMemcpyKind kin
     return fail(B200_ENOMEM, "cudaMalloc for lexical links failed");
   B200_CHECK_CUDA(cudaMemcpyAsync(op->u_lex, u, n * sizeof(double), kind, st));
   op->have_links = true;
-  for (int lf = 0; lf < 4; ++lf)
+  for (int lf = 0; lf < LINK_NFMT; ++lf)
     if (op->links[lf]) B200_CHECK_CUDA(launch_links_from_lex(lf, op->links[lf], op->u_lex, op->g, op->bc, st));
   B200_CHECK_CUDA(cudaStreamSynchronize(st));
   return 0;
@@ -1392,7 +1400,7 @@ int plan_apply_ddagd(b200_dwf* op, void* v, const void* w, cudaStream_t st) {
   return apply_mode(op, PREC_F32, v, w, "DdagD", 0, st);
 }
 int plan_links_f32(b200_dwf* op, const void** links, cudaStream_t st) {
-  const int rc = ensure_links(op, PREC_F32, st);
+  const int rc = ensure_link_format(op, LINK_F32_12, st);
   if (rc) return rc;
   *links = op->links[LINK_F32_12];
   return 0;

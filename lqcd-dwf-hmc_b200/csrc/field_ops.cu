@@ -704,8 +704,8 @@ __global__ void to_corelib_kernel(Geom g, double* out, const void* in) {
 
 // links: out index (ieo + 2*mu)*Vh + site_eo  (reference m_Ueo ordering,
 // src/lib_alt_Accel/Fopr/afopr_Domainwall_5din_eo-tmpl.h:140-141).
-// The full-record FP64 format (LINK_F64_18, LinkLoad::kPhased) carries the
-// boundary phase: links U_mu(x) with x_mu = L_mu - 1 are stored times
+// The full-record formats (LINK_F64_18, LINK_F32_18, LINK_F16_18:
+// LinkLoad::kPhased) carry the boundary phase: links U_mu(x) with x_mu = L_mu - 1 are stored times
 // bc[mu], which is the factor the reference applies to both hops across that
 // edge (forward from x, backward from x + mu), so the hop kernels need no
 // per-direction phase.  Real phases only (bc is an integer vector).
@@ -728,12 +728,24 @@ __global__ void links_kernel(Geom g, void* out, const double* u, LinkPhase ph) {
   const size_t lex = x + (size_t)nx * (y + (size_t)g.ny * (z + (size_t)g.nz * t));
   const size_t vol = (size_t)2 * g.vh;
   const double* m = u + 18 * (lex + vol * mu);
+  const int cmu = (mu == 0) ? x : (mu == 1) ? y : (mu == 2) ? z : t;
+  const int ext = (mu == 0) ? nx : (mu == 1) ? g.ny : (mu == 2) ? g.nz : g.nt;
+  const double f = (cmu == ext - 1) ? ph.bc[mu] : 1.0;   // phased formats only
   if (LF == LINK_F64_18) {
-    const int c = (mu == 0) ? x : (mu == 1) ? y : (mu == 2) ? z : t;
-    const int ext = (mu == 0) ? nx : (mu == 1) ? g.ny : (mu == 2) ? g.nz : g.nt;
-    const double f = (c == ext - 1) ? ph.bc[mu] : 1.0;
     double2* o = reinterpret_cast<double2*>(out) + idx * 9;
     for (int j = 0; j < 9; ++j) o[j] = make_double2(f * m[2 * j], f * m[2 * j + 1]);
+  } else if (LF == LINK_F32_18) {
+    float* o = reinterpret_cast<float*>(reinterpret_cast<float4*>(out) + idx * 5);
+    for (int j = 0; j < 18; ++j) o[j] = (float)(f * m[j]);
+    o[18] = 0.f; o[19] = 0.f;
+  } else if (LF == LINK_F16_18) {
+    uint4* o = reinterpret_cast<uint4*>(out) + idx * 3;
+    unsigned int w[12];
+    for (int j = 0; j < 9; ++j) w[j] = HalfOps<__half>::from2((float)(f * m[2 * j]), (float)(f * m[2 * j + 1]));
+    w[9] = 0u; w[10] = 0u; w[11] = 0u;
+    o[0] = make_uint4(w[0], w[1], w[2], w[3]);
+    o[1] = make_uint4(w[4], w[5], w[6], w[7]);
+    o[2] = make_uint4(w[8], w[9], w[10], w[11]);
   } else if (LF == LINK_F64_12) {
     double2* o = reinterpret_cast<double2*>(out) + idx * 6;
     for (int j = 0; j < 6; ++j) o[j] = make_double2(m[2 * j], m[2 * j + 1]);
@@ -757,6 +769,8 @@ size_t link_bytes(int lf, size_t vh) {
     case LINK_F64_18: return n * 9 * 16;
     case LINK_F64_12: return n * 6 * 16;
     case LINK_F32_12: return n * 3 * 16;
+    case LINK_F32_18: return n * 5 * 16;
+    case LINK_F16_18: return n * 3 * 16;
     default: return n * 2 * 16;
   }
 }
@@ -860,6 +874,8 @@ cudaError_t launch_links_from_lex(int lf, void* out, const double* u_lex_dev, co
     case LINK_F64_12: links_kernel<LINK_F64_12><<<grid, 128, 0, st>>>(g, out, u_lex_dev, ph); break;
     case LINK_F32_12: links_kernel<LINK_F32_12><<<grid, 128, 0, st>>>(g, out, u_lex_dev, ph); break;
     case LINK_F16_12: links_kernel<LINK_F16_12><<<grid, 128, 0, st>>>(g, out, u_lex_dev, ph); break;
+    case LINK_F32_18: links_kernel<LINK_F32_18><<<grid, 128, 0, st>>>(g, out, u_lex_dev, ph); break;
+    case LINK_F16_18: links_kernel<LINK_F16_18><<<grid, 128, 0, st>>>(g, out, u_lex_dev, ph); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();

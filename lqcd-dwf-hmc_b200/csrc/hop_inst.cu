@@ -13,9 +13,9 @@ namespace b200 {
 
 template <int P> struct DefaultLink;
 template <> struct DefaultLink<PREC_F64> { static constexpr int v = LINK_F64_18; };
-template <> struct DefaultLink<PREC_F32> { static constexpr int v = LINK_F32_12; };
-template <> struct DefaultLink<PREC_F16> { static constexpr int v = LINK_F16_12; };
-template <> struct DefaultLink<PREC_BF16> { static constexpr int v = LINK_F16_12; };
+template <> struct DefaultLink<PREC_F32> { static constexpr int v = LINK_F32_18; };
+template <> struct DefaultLink<PREC_F16> { static constexpr int v = LINK_F16_18; };
+template <> struct DefaultLink<PREC_BF16> { static constexpr int v = LINK_F16_18; };
 
 namespace {
 

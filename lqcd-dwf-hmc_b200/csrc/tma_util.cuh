@@ -31,6 +31,7 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
+// One try (blocks for at most a hardware-defined time slice).
 __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
@@ -43,13 +44,24 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait for the phase with the given parity: gives up after a fixed
-// number of tries (each try itself blocks for at most a hardware time slice)
-// and reports false instead of spinning forever.
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Bounded wait for the phase with the given parity: gives up after 2 s of
+// global time or 2^22 tries, whichever comes first, and reports false
+// instead of waiting forever.  The clock is read only after a failed try.
 __device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
+  if (mbar_try_wait(bar, parity)) return true;
   constexpr int kMaxTries = 1 << 22;
-  for (int i = 0; i < kMaxTries; ++i)
+  constexpr uint64_t kMaxNs = 2000000000ull;
+  const uint64_t t0 = global_ns();
+  for (int i = 0; i < kMaxTries; ++i) {
     if (mbar_try_wait(bar, parity)) return true;
+    if (global_ns() - t0 > kMaxNs) return false;
+  }
   return false;
 }
 
