@@ -31,14 +31,16 @@ enum LinkFmt {
 
 template <int LF> struct LinkLoad;
 
-// kPhased: the plan stores this format with the boundary phase bc[mu]
-// already multiplied into the links of the last slice along mu (full
-// 3x3 records only: a reconstructed third row would not carry the phase), so
-// the hop kernels skip the per-direction phase factor.
+// kFolded: the plan stores this format with two constant factors of the hop
+// already multiplied into the links: the boundary phase bc[mu] on the links
+// of the last slice along mu, and the factor 2 of the (1 -+ gamma_4)
+// projection on every t link (full 3x3 records only: a reconstructed third
+// row would carry neither).  The hop kernels then skip the per-direction
+// phase and the doubling of the t projection.
 template <> struct LinkLoad<LINK_F64_18> {
   using R = double;
   static constexpr int kChunks = 9;
-  static constexpr bool kPhased = true;
+  static constexpr bool kFolded = true;
   __device__ static void load_plain(const void* rec, double* u) {
     const double2* p = reinterpret_cast<const double2*>(rec);
 #pragma unroll
@@ -53,7 +55,7 @@ template <> struct LinkLoad<LINK_F64_18> {
 template <> struct LinkLoad<LINK_F64_12> {
   using R = double;
   static constexpr int kChunks = 6;
-  static constexpr bool kPhased = false;
+  static constexpr bool kFolded = false;
   __device__ static void load_plain(const void* rec, double* u) {
     const double2* p = reinterpret_cast<const double2*>(rec);
 #pragma unroll
@@ -70,7 +72,7 @@ template <> struct LinkLoad<LINK_F64_12> {
 template <> struct LinkLoad<LINK_F32_12> {
   using R = float;
   static constexpr int kChunks = 3;
-  static constexpr bool kPhased = false;
+  static constexpr bool kFolded = false;
   __device__ static void load_plain(const void* rec, float* u) {
     const float4* p = reinterpret_cast<const float4*>(rec);
 #pragma unroll
@@ -93,7 +95,7 @@ template <> struct LinkLoad<LINK_F32_12> {
 template <> struct LinkLoad<LINK_F16_12> {
   using R = float;
   static constexpr int kChunks = 2;
-  static constexpr bool kPhased = false;
+  static constexpr bool kFolded = false;
   __device__ static void load_plain(const void* rec, float* u) {
     const uint4* p = reinterpret_cast<const uint4*>(rec);
     uint4 a = p[0], b = p[1];
@@ -120,11 +122,11 @@ template <> struct LinkLoad<LINK_F16_12> {
 
 // Full 3x3 records in FP32 (18 floats padded to 5 float4) and in FP16 (18
 // halves padded to 3 uint4): no third-row rebuild in the hop (the lanes of a
-// site would each repeat it), boundary phase folded in like LINK_F64_18.
+// site would each repeat it), phase and t factor folded in like LINK_F64_18.
 template <> struct LinkLoad<LINK_F32_18> {
   using R = float;
   static constexpr int kChunks = 5;
-  static constexpr bool kPhased = true;
+  static constexpr bool kFolded = true;
   __device__ static void load_plain(const void* rec, float* u) {
     const float4* p = reinterpret_cast<const float4*>(rec);
 #pragma unroll
@@ -149,7 +151,7 @@ template <> struct LinkLoad<LINK_F32_18> {
 template <> struct LinkLoad<LINK_F16_18> {
   using R = float;
   static constexpr int kChunks = 3;
-  static constexpr bool kPhased = true;
+  static constexpr bool kFolded = true;
   __device__ static void decode(uint4 a, uint4 b, uint4 c, float* u) {
     const unsigned int w[9] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x};
 #pragma unroll
@@ -199,7 +201,8 @@ __device__ __forceinline__ void su3_mult_half(const R* u, const R* h, R* o) {
 // and reconstruction acc += ph * (1 - sign*gamma_mu)-shaped result from uh.
 // Dirac basis (reference src/lib/Tools/gammaMatrixSet_Dirac.cpp:31-60).
 // w index: ri + 2*(c + 3*sp).  sign = +1 forward (1-g), -1 backward (1+g).
-template <typename R, int MU, int SIGN>
+// kT2 = false: the t links carry the projection's factor 2 (kFolded formats).
+template <typename R, int MU, int SIGN, bool kT2 = true>
 __device__ __forceinline__ void project(const R* w, R* h) {
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
@@ -218,8 +221,9 @@ __device__ __forceinline__ void project(const R* w, R* h) {
       h0r = w0r - SIGN * w2i; h0i = w0i + SIGN * w2r;
       h1r = w1r + SIGN * w3i; h1i = w1i - SIGN * w3r;
     } else {              // (1 - g4) keeps lower spins, (1 + g4) upper, x2
-      if (SIGN > 0) { h0r = 2 * w2r; h0i = 2 * w2i; h1r = 2 * w3r; h1i = 2 * w3i; }
-      else          { h0r = 2 * w0r; h0i = 2 * w0i; h1r = 2 * w1r; h1i = 2 * w1i; }
+      const R two = kT2 ? R(2) : R(1);
+      if (SIGN > 0) { h0r = two * w2r; h0i = two * w2i; h1r = two * w3r; h1i = two * w3i; }
+      else          { h0r = two * w0r; h0i = two * w0i; h1r = two * w1r; h1i = two * w1i; }
     }
     h[2 * c] = h0r; h[2 * c + 1] = h0i;
     h[6 + 2 * c] = h1r; h[6 + 2 * c + 1] = h1i;
@@ -335,6 +339,7 @@ struct HopParams {
   const double* c_x3_dev;
   double* red;           // per-block partials of |o1|^2 (nullable)
   int* err;              // device error word: set when a bounded wait gives up
+  unsigned int wait_ns;  // suspend-time hint of the TMA kernels' mbarrier tries (0: none)
   const double* skip;    // when non-null and *skip != 0 the launch does nothing
                          // (lets a captured solver iteration replay as a no-op)
   int vh, nx2, ny, nz, nt, ls;
@@ -360,11 +365,17 @@ __device__ __forceinline__ void hop_epilogue_rows(const HopParams& p,
   constexpr int WARPS = 4;
   const size_t vh = p.vh;
   R o1[NR][24];
+  // ce is uniform over the launch: folded into the constant factor of
+  // EPI_HALF, and skipped when it is 1 (both exact, so results are unchanged)
+  const R ce = (R)(p.ce * (p.ce_dev ? *p.ce_dev : 1.0));
+  bool ce_done = (ce == R(1));
   if (EPI == EPI_HALF) {
+    const R c = R(-0.5) * ce;
 #pragma unroll
     for (int r = 0; r < NR; ++r)
 #pragma unroll
-      for (int i = 0; i < 24; ++i) o1[r][i] = R(-0.5) * acc[r][i];
+      for (int i = 0; i < 24; ++i) o1[r][i] = c * acc[r][i];
+    ce_done = true;
   } else if (NR == 1 && (EPI == EPI_DDAGEO || EPI == EPI_K4N)) {
     // c * M5^+ g5 acc (c = -1/2 or +1/2): in the chiral basis M5^+ couples s
     // only to s+1 (x+) or s-1 (x-) of the same site, whose values sit in the
@@ -413,7 +424,6 @@ __device__ __forceinline__ void hop_epilogue_rows(const HopParams& p,
 
   double nrm = 0.0;
   if (active) {
-    const R ce = (R)(p.ce * (p.ce_dev ? *p.ce_dev : 1.0));
     const R c1 = (R)(p.c_x1 * (p.c_x1_dev ? *p.c_x1_dev : 1.0));
     const R c2 = (R)(p.c_x2 * (p.c_x2_dev ? *p.c_x2_dev : 1.0));
     const R c3 = (R)(p.c_x3 * (p.c_x3_dev ? *p.c_x3_dev : 1.0));
@@ -421,7 +431,9 @@ __device__ __forceinline__ void hop_epilogue_rows(const HopParams& p,
     for (int r = 0; r < NR; ++r) {
       const int s = srow[r];
 #pragma unroll
-      for (int i = 0; i < 24; ++i) o1[r][i] *= ce;
+      if (!ce_done)
+#pragma unroll
+        for (int i = 0; i < 24; ++i) o1[r][i] *= ce;
       if (p.x1) {
         R xv[24];
         St::load(p.x1, vh, LS, site, s, xv);
@@ -515,7 +527,7 @@ dwf_hop_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename Sto
   using St = Store<P>;
   using R = typename St::R;
   constexpr bool kDagHop = EpiIsDag<EPI>::v;
-  constexpr bool kPh = LinkLoad<LF>::kPhased;
+  constexpr bool kPh = LinkLoad<LF>::kFolded;
   constexpr int G = 32 / LS;              // sites per warp
   constexpr int WARPS = 4;
   constexpr bool kTile = (EPI != EPI_HALF) || (FK != F_NONE);
@@ -561,7 +573,7 @@ dwf_hop_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename Sto
           _Pragma("unroll") for (int q = 0; q < 12; ++q) {                           \
             R tmp = w[q]; w[q] = w[q + 12]; w[q + 12] = tmp; }                       \
         }                                                                            \
-        project<R, MU, 1>(w, h);                                                     \
+        project<R, MU, 1, !kPh>(w, h);                                               \
         LinkLoad<LF>::load(p.links, (size_t)(ieo + 2 * MU) * strideMu + site, u);    \
         su3_mult_half<R, false>(u, h, o);                                            \
         reconstruct_acc<R, MU, 1, kPh>(acc, o, ph);                                  \
@@ -574,7 +586,7 @@ dwf_hop_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename Sto
           _Pragma("unroll") for (int q = 0; q < 12; ++q) {                           \
             R tmp = w[q]; w[q] = w[q + 12]; w[q + 12] = tmp; }                       \
         }                                                                            \
-        project<R, MU, -1>(w, h);                                                    \
+        project<R, MU, -1, !kPh>(w, h);                                              \
         LinkLoad<LF>::load(p.links, (size_t)(1 - ieo + 2 * MU) * strideMu + nb, u);  \
         su3_mult_half<R, true>(u, h, o);                                             \
         reconstruct_acc<R, MU, -1, kPh>(acc, o, ph);                                 \
@@ -689,7 +701,7 @@ dwf_hop_pair_kernel(const HopParams p, const __grid_constant__ ChainCoef<typenam
   static_assert(sizeof(R) == 4, "packed kernel is for FP32 arithmetic");
   static_assert(32 % LS == 0 && LS % 2 == 0, "packed kernel needs Ls | 32");
   constexpr bool kDagHop = EpiIsDag<EPI>::v;
-  constexpr bool kPh = LinkLoad<LF>::kPhased;
+  constexpr bool kPh = LinkLoad<LF>::kFolded;
   constexpr int H = LS / 2;               // lanes per site
   constexpr int G = 32 / H;               // sites per warp
   constexpr int WARPS = 4;
@@ -735,8 +747,8 @@ dwf_hop_pair_kernel(const HopParams p, const __grid_constant__ ChainCoef<typenam
           float t0 = w0[q]; w0[q] = w0[q + 12]; w0[q + 12] = t0;                     \
           float t1 = w1[q]; w1[q] = w1[q + 12]; w1[q + 12] = t1; }                   \
       }                                                                              \
-      project<float, MU, SIGN>(w0, h0);                                              \
-      project<float, MU, SIGN>(w1, h1);                                              \
+      project<float, MU, SIGN, !kPh>(w0, h0);                                        \
+      project<float, MU, SIGN, !kPh>(w1, h1);                                        \
       float2 h[12], o[12];                                                           \
       _Pragma("unroll") for (int q = 0; q < 12; ++q) h[q] = make_float2(h0[q], h1[q]); \
       if (St::kScaled) {                                                             \
@@ -840,8 +852,8 @@ __device__ __forceinline__ void pair_compute(const PairRaw<P>& r, float ph, floa
       float t1 = w1[q]; w1[q] = w1[q + 12]; w1[q + 12] = t1;
     }
   }
-  project<float, MU, SIGN>(w0, h0);
-  project<float, MU, SIGN>(w1, h1);
+  project<float, MU, SIGN, false>(w0, h0);   // LINK_F16_18: t factor in the links
+  project<float, MU, SIGN, false>(w1, h1);
   float2 h[12], o[12];
   const float2 sc = make_float2(r.sc0, r.sc1);
 #pragma unroll
@@ -984,7 +996,7 @@ dwf_hop_tma_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename
   using R = typename St::R;
   using TG = TmaGeom<LS, P, LF>;
   constexpr bool kDagHop = EpiIsDag<EPI>::v;
-  constexpr bool kPh = LinkLoad<LF>::kPhased;
+  constexpr bool kPh = LinkLoad<LF>::kFolded;
   constexpr int NPH = kPh ? 1 : 8;        // edge phases kept in registers
   constexpr int G = TG::G;
   constexpr int WARPS = 4;
@@ -1084,7 +1096,7 @@ dwf_hop_tma_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename
     constexpr int st = (D) % S;                                                      \
     const uint32_t parity = ((D) / S) & 1;                                           \
     if (ok) {                                                                        \
-      const bool got = mbar_wait_bounded(smem_u32(&bars[warp][st]), parity);         \
+      const bool got = mbar_wait_bounded(smem_u32(&bars[warp][st]), parity, p.wait_ns); \
       ok = __all_sync(0xffffffffu, got);                                             \
       if (ok) ndone = (D) + 1;                                                       \
       else if (lane == 0 && p.err) atomicExch(p.err, 1);                             \
@@ -1097,7 +1109,7 @@ dwf_hop_tma_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename
         _Pragma("unroll") for (int q = 0; q < 12; ++q) {                             \
           R tmp = w[q]; w[q] = w[q + 12]; w[q + 12] = tmp; }                         \
       }                                                                              \
-      project<R, MU, SIGN>(w, h);                                                    \
+      project<R, MU, SIGN, !kPh>(w, h);                                              \
       if constexpr (LF == LINK_F64_18) {                                             \
         hop_dir_rows_f64<MU, SIGN>(reinterpret_cast<const double2*>(c + TG::COL),    \
                                    reinterpret_cast<const double*>(h),               \
@@ -1129,7 +1141,8 @@ dwf_hop_tma_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename
   // flight, then the whole CTA returns without touching its outputs; the host
   // sees p.err.
   if (!ok) {
-    for (int d = ndone; d < nissued; ++d) mbar_wait_bounded(smem_u32(&bars[warp][d % S]), (d / S) & 1);
+    for (int d = ndone; d < nissued; ++d)
+      mbar_wait_bounded(smem_u32(&bars[warp][d % S]), (d / S) & 1, p.wait_ns);
   }
   if (!__syncthreads_and(ok ? 1 : 0)) return;
   hop_epilogue<LS, P, EPI, FK>(p, k, acc, reinterpret_cast<R*>(wbase), red_warp, tid, lane, warp, g, s,
@@ -1152,7 +1165,7 @@ dwf_hop_tma_pair_kernel(const HopParams p, const __grid_constant__ ChainCoef<typ
   constexpr int G = 32 / H;
   using TG = TmaGeom<LS, P, LF, G>;
   constexpr bool kDagHop = EpiIsDag<EPI>::v;
-  constexpr bool kPh = LinkLoad<LF>::kPhased;
+  constexpr bool kPh = LinkLoad<LF>::kFolded;
   constexpr int WARPS = 4;
   constexpr int WB = TG::template warp_bytes<S>();
   constexpr int WBA = (WB + 127) / 128 * 128;
@@ -1246,7 +1259,7 @@ dwf_hop_tma_pair_kernel(const HopParams p, const __grid_constant__ ChainCoef<typ
     constexpr int st = (D) % S;                                                      \
     const uint32_t parity = ((D) / S) & 1;                                           \
     if (ok) {                                                                        \
-      const bool got = mbar_wait_bounded(smem_u32(&bars[warp][st]), parity);         \
+      const bool got = mbar_wait_bounded(smem_u32(&bars[warp][st]), parity, p.wait_ns); \
       ok = __all_sync(0xffffffffu, got);                                             \
       if (ok) ndone = (D) + 1;                                                       \
       else if (lane == 0 && p.err) atomicExch(p.err, 1);                             \
@@ -1262,8 +1275,8 @@ dwf_hop_tma_pair_kernel(const HopParams p, const __grid_constant__ ChainCoef<typ
           float t0 = w0[q]; w0[q] = w0[q + 12]; w0[q + 12] = t0;                     \
           float t1 = w1[q]; w1[q] = w1[q + 12]; w1[q + 12] = t1; }                   \
       }                                                                              \
-      project<float, MU, SIGN>(w0, h0);                                              \
-      project<float, MU, SIGN>(w1, h1);                                              \
+      project<float, MU, SIGN, !kPh>(w0, h0);                                        \
+      project<float, MU, SIGN, !kPh>(w1, h1);                                        \
       float2 h[12], o[12];                                                           \
       _Pragma("unroll") for (int q = 0; q < 12; ++q) h[q] = make_float2(h0[q], h1[q]); \
       if (St::kScaled) {                                                             \
@@ -1292,7 +1305,8 @@ dwf_hop_tma_pair_kernel(const HopParams p, const __grid_constant__ ChainCoef<typ
 #undef B200_TMAP_STEP
 
   if (!ok) {
-    for (int d = ndone; d < nissued; ++d) mbar_wait_bounded(smem_u32(&bars[warp][d % S]), (d / S) & 1);
+    for (int d = ndone; d < nissued; ++d)
+      mbar_wait_bounded(smem_u32(&bars[warp][d % S]), (d / S) & 1, p.wait_ns);
   }
   if (!__syncthreads_and(ok ? 1 : 0)) return;
   float rows[2][24];

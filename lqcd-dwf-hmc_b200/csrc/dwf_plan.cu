@@ -209,6 +209,16 @@ int ensure_links(b200_dwf* op, int prec, cudaStream_t st) {
   return ensure_link_format(op, link_format_for(prec), st);
 }
 
+// Suspend-time hint of the TMA hop kernels' barrier waits (B200_WAIT_NS,
+// default 0: plain tries).
+unsigned int wait_hint_ns() {
+  static const unsigned int v = [] {
+    const char* e = getenv("B200_WAIT_NS");
+    return (e && e[0]) ? (unsigned int)strtoul(e, nullptr, 10) : 0u;
+  }();
+  return v;
+}
+
 HopParams hop_base(const b200_dwf* op, int prec, int ieo, int epi, int fk = F_NONE) {
   HopParams p;
   memset(&p, 0, sizeof(p));
@@ -220,6 +230,7 @@ HopParams hop_base(const b200_dwf* op, int prec, int ieo, int epi, int fk = F_NO
   p.ieo = ieo;
   p.ce = 1.0;
   p.err = op->err;
+  p.wait_ns = wait_hint_ns();
   for (int mu = 0; mu < 4; ++mu) p.bc[mu] = op->bc[mu];
   return p;
 }

@@ -705,10 +705,11 @@ __global__ void to_corelib_kernel(Geom g, double* out, const void* in) {
 // links: out index (ieo + 2*mu)*Vh + site_eo  (reference m_Ueo ordering,
 // src/lib_alt_Accel/Fopr/afopr_Domainwall_5din_eo-tmpl.h:140-141).
 // The full-record formats (LINK_F64_18, LINK_F32_18, LINK_F16_18:
-// LinkLoad::kPhased) carry the boundary phase: links U_mu(x) with x_mu = L_mu - 1 are stored times
-// bc[mu], which is the factor the reference applies to both hops across that
-// edge (forward from x, backward from x + mu), so the hop kernels need no
-// per-direction phase.  Real phases only (bc is an integer vector).
+// LinkLoad::kFolded) carry two constant factors of the hop: 2 on every t link
+// (the (1 -+ gamma_4) projection), and the boundary phase: links U_mu(x) with
+// x_mu = L_mu - 1 are stored times bc[mu], which is the factor the reference
+// applies to both hops across that edge (forward from x, backward from
+// x + mu).  Real phases only (bc is an integer vector).
 struct LinkPhase { double bc[4]; };
 
 template <int LF>
@@ -730,7 +731,8 @@ __global__ void links_kernel(Geom g, void* out, const double* u, LinkPhase ph) {
   const double* m = u + 18 * (lex + vol * mu);
   const int cmu = (mu == 0) ? x : (mu == 1) ? y : (mu == 2) ? z : t;
   const int ext = (mu == 0) ? nx : (mu == 1) ? g.ny : (mu == 2) ? g.nz : g.nt;
-  const double f = (cmu == ext - 1) ? ph.bc[mu] : 1.0;   // phased formats only
+  // folded formats only: boundary phase, and the factor 2 of the t projection
+  const double f = ((cmu == ext - 1) ? ph.bc[mu] : 1.0) * (mu == 3 ? 2.0 : 1.0);
   if (LF == LINK_F64_18) {
     double2* o = reinterpret_cast<double2*>(out) + idx * 9;
     for (int j = 0; j < 9; ++j) o[j] = make_double2(f * m[2 * j], f * m[2 * j + 1]);

@@ -31,16 +31,29 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
-// One try (blocks for at most a hardware-defined time slice).
-__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+// One try.  hint_ns = 0: blocks for at most a hardware-defined time slice;
+// otherwise the thread may be suspended until the phase completes or at most
+// hint_ns nanoseconds have passed (the PTX suspend-time hint), instead of
+// re-issuing the test.
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity, uint32_t hint_ns = 0) {
   uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(bar), "r"(parity)
-      : "memory");
+  if (hint_ns == 0) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+  } else {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity), "r"(hint_ns)
+        : "memory");
+  }
   return ok != 0;
 }
 
@@ -53,13 +66,13 @@ __device__ __forceinline__ uint64_t global_ns() {
 // Bounded wait for the phase with the given parity: gives up after 2 s of
 // global time or 2^22 tries, whichever comes first, and reports false
 // instead of waiting forever.  The clock is read only after a failed try.
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
-  if (mbar_try_wait(bar, parity)) return true;
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity, uint32_t hint_ns = 0) {
+  if (mbar_try_wait(bar, parity, hint_ns)) return true;
   constexpr int kMaxTries = 1 << 22;
   constexpr uint64_t kMaxNs = 2000000000ull;
   const uint64_t t0 = global_ns();
   for (int i = 0; i < kMaxTries; ++i) {
-    if (mbar_try_wait(bar, parity)) return true;
+    if (mbar_try_wait(bar, parity, hint_ns)) return true;
     if (global_ns() - t0 > kMaxNs) return false;
   }
   return false;
