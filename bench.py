@@ -645,7 +645,8 @@ def b200_arm(args, rank, world, local_rank):
         # Shamir b=1, c=0, alpha=1: the D_eo pre-factor is the identity, so a
         # step is two hop launches (mult Deo, mult_dag Deo)
         "gpu_launches": 2 * args.steps,
-        "roofline": {"kernel": "dwf_hop_kernel<16,f64,dag> (mult_dag Deo)", "bound": "hbm",
+        "roofline": {"kernel": "dwf_hop_tma_kernel<16,f64,EPI_DDAGEO> (mult_dag Deo, autotuned variant)",
+                     "bound": "hbm",
                      "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "algorithmic_bytes_per_launch": BYTES_PER_HALF_SITE * vh,
