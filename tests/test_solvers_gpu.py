@@ -96,3 +96,39 @@ def test_zero_rhs_and_nonconvergence_status():
     dev.convert(fb, b)
     n, diff, rc = dev.cg(fx, fb, 1e-30, 3)   # cannot converge in 3 iterations
     assert rc == -4 and n == 3 and diff > 1e-6
+
+
+@pytest.mark.parametrize("alpha", [1.0, 1.3])
+def test_solvers_with_nontrivial_prefactor(alpha):
+    """Moebius kernel (b = 1.5, c = 0.5) and, with alpha = 1.3, a pre-factor
+    that differs per chirality: the D_eo pre-factor is not the identity, so
+    CG, multishift (per-iteration and windowed) and Richardson carry the
+    M5pre p field that the Shamir runs above skip.  All against the oracle."""
+    import b200dwf
+    from oracle.oracle import OracleDWF
+    lat, ls = [4, 4, 4, 8], 8
+    u = synth.gauge_field(lat, 21, "near", eps=0.3)
+    ora = OracleDWF(lat, ls, 0.02, 1.0, 1.5, 0.5, alpha)
+    ora.set_links(u)
+    dev = b200dwf.DomainWall(lat, ls, 0.02, 1.0, 1.5, 0.5, alpha)
+    dev.set_config(u)
+    b = synth.spinor_field(lat, ls, 22)
+    fb, fx = dev.new_field(0), dev.new_field(0)
+    dev.convert(fb, b)
+    n, diff, rc = dev.cg(fx, fb, 1e-22, 3000)
+    xr, nr, _, rcr = ora.cg(b, 1e-22, 3000)
+    assert rc == 0 and rcr == 0 and abs(n - nr) <= 1
+    assert rel(dev.reverse(fx), xr) < 1e-9
+    sigma = [0.005, 0.05, 0.5, 5.0]
+    xsr, nsr, _, _ = ora.shiftcg(b, sigma, 1e-22, 3000)
+    for window in (0, 16):
+        dev.set_shift_window(window)
+        xs = [dev.new_field(0) for _ in sigma]
+        n, diff, rc = dev.shiftcg(xs, sigma, fb, 1e-22, 3000)
+        assert rc == 0 and abs(n - nsr) <= 1 and diff < 1e-9
+        for i in range(len(sigma)):
+            assert rel(dev.reverse(xs[i]), xsr[i]) < 1e-9, (window, i)
+    fx2 = dev.new_field(0)
+    nout, nin, diff, rc = dev.richardson(fx2, fb, 1, 1e-20, 60, 1e-8, 5000)
+    assert rc == 0 and diff < 1e-10
+    assert rel(dev.reverse(fx2), xr) < 1e-8
