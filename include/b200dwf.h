@@ -85,6 +85,11 @@ int b200_field_convert(b200_dwf_t *op, int prec, void *v_dev, const double *w_ho
                        void *stream);
 int b200_field_reverse(b200_dwf_t *op, int prec, double *v_host, const void *w_dev,
                        void *stream);
+/* convert() from a field already on the device (w_dev: reference layout,
+ * 24 * Nvol/2 * Ls doubles), asynchronous on `stream`: the heatbath noise
+ * drawn by b200_rng_gauss_lex goes to the operator without a host copy. */
+int b200_field_convert_device(b200_dwf_t *op, int prec, void *v_dev, const double *w_dev,
+                              void *stream);
 
 /* mult / mult_dag (afopr_Domainwall_5din_eo-tmpl.h:634-767).  mode is one of
  *   "D" "Ddag" "DdagD" "H" "Hdag" "Deo" "Doe" "Dee" "Doo" "Dee_inv" "Doo_inv"
@@ -294,6 +299,29 @@ int b200_cg_snapshots(b200_dwf_t *op, int prec, void *x, const void *b, int maxi
 int b200_fcg_solve(b200_dwf_t *op, b200_lp_t *lp, void *x, const void *b, int maxiter,
                    double tol2, int mtrunc, int *nconv, int *nconv_fallback, double *diff,
                    void *stream);
+
+/* ---------------------------------------------------------------- heatbath noise
+ * The benchmark driver's random numbers on the device (random_number_type
+ * Mseries_parallel): RandomNumbers_parallel<RandomNumbers_Mseries>
+ * (src/lib/Tools/randomNumbers_parallel-tmpl.h:160-300 init_2d,
+ * set_lex_global_2d, gauss_lex_global, uniform_lex_global; streams
+ * src/lib/Tools/randomNumbers_Mseries.cpp:32-150; Gaussian pairs
+ * src/lib/Tools/randomNumbers.cpp:53-75).  One M-series stream per (z, t)
+ * plane of the global lattice, each advancing across calls as in the
+ * reference.  Fields are device buffers of nin * Nvol * nex doubles in the
+ * corelib Field layout (component fastest, then lexical site, then extra
+ * index).  The uniform numbers are the reference's bit for bit; the
+ * Gaussians agree to the last bits of the device's log/sqrt/sin/cos.
+ * create/reset compute the streams' start states on the host (the
+ * reference's seeding and 1000 discarded numbers) and wait for the device. */
+typedef struct b200_rng b200_rng_t;
+int b200_rng_create(b200_rng_t **out, const int lattice[4], unsigned long seed);
+int b200_rng_reset(b200_rng_t *rng, unsigned long seed);   /* RandomNumbers::reset */
+/* gauss_lex_global(Field(nin, Nvol, nex)); nin even */
+int b200_rng_gauss_lex(b200_rng_t *rng, double *v, int nin, int nex, void *stream);
+/* uniform_lex_global: one number per site in component 0, the others 0 */
+int b200_rng_uniform_lex(b200_rng_t *rng, double *v, int nin, int nex, void *stream);
+int b200_rng_destroy(b200_rng_t *rng);
 
 /* ---------------------------------------------------------------- tuning
  * Text table of the autotuner's choices (one line per geometry, precision and

@@ -55,6 +55,7 @@ def lib():
     L.b200_dwf_field_nreal.restype = ctypes.c_size_t
     L.b200_field_convert.argtypes = [vp, ctypes.c_int, vp, dp, vp]
     L.b200_field_reverse.argtypes = [vp, ctypes.c_int, dp, vp, vp]
+    L.b200_field_convert_device.argtypes = [vp, ctypes.c_int, vp, vp, vp]
     L.b200_dwf_mult.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_char_p, ctypes.c_int, vp]
     L.b200_field_axpby.argtypes = [vp, ctypes.c_int, vp, ctypes.c_double, vp, ctypes.c_double, vp]
     L.b200_field_norm2.argtypes = [vp, ctypes.c_int, vp, dp, vp]
@@ -78,6 +79,11 @@ def lib():
     L.b200_smear_get_config.argtypes = [vp, ctypes.c_int, dp, vp]
     L.b200_force_mult_generator.argtypes = [ip, vp, vp, vp]
     L.b200_field_norm2_noalloc.argtypes = [ctypes.c_int, vp, ctypes.c_long, ctypes.c_int, dp, vp]
+    L.b200_rng_create.argtypes = [ctypes.POINTER(vp), ip, ctypes.c_ulong]
+    L.b200_rng_reset.argtypes = [vp, ctypes.c_ulong]
+    L.b200_rng_gauss_lex.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, vp]
+    L.b200_rng_uniform_lex.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, vp]
+    L.b200_rng_destroy.argtypes = [vp]
     L.b200_tuning_table.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
     L.b200_cg_solve.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_double,
                                 ip, dp, vp]
@@ -189,6 +195,16 @@ class DomainWall:
     def convert(self, v, w_host):
         w = np.ascontiguousarray(w_host, np.float64)
         check(lib().b200_field_convert(self.handle, v.prec, v.ptr, _dp(w), None))
+
+    def convert_device(self, v, w_dev):
+        """convert() from a float64 CUDA tensor in the reference layout."""
+        import torch
+        if w_dev.numel() != self.nreal or w_dev.dtype != torch.float64 or not w_dev.is_cuda:
+            raise B200Error("convert_device needs a float64 CUDA tensor of %d elements" % self.nreal)
+        w_dev = w_dev.contiguous()
+        check(lib().b200_field_convert_device(self.handle, v.prec, v.ptr,
+                                              ctypes.c_void_p(w_dev.data_ptr()),
+                                              ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
 
     def reverse(self, w, out=None):
         if out is None:
@@ -488,3 +504,45 @@ def mult_generator(lattice, force_lex, u_lex):
     check(lib().b200_force_mult_generator((ctypes.c_int * 4)(*lattice), ctypes.c_void_p(f.data_ptr()),
                                           ctypes.c_void_p(u.data_ptr()), None))
     return f.cpu().numpy()
+
+
+class MseriesParallel:
+    """RandomNumbers_parallel<RandomNumbers_Mseries> on the device (the
+    benchmark driver's random_number_type Mseries_parallel): one M-series
+    stream per (z, t) plane, advancing across calls as in the reference
+    (src/lib/Tools/randomNumbers_parallel-tmpl.h:160-300).  Draws fill torch
+    float64 CUDA tensors in the corelib Field(nin, Nvol, nex) layout."""
+
+    def __init__(self, lattice, seed):
+        self.lattice = list(lattice)
+        self.nvol = int(np.prod(lattice))
+        h = ctypes.c_void_p()
+        check(lib().b200_rng_create(ctypes.byref(h), (ctypes.c_int * 4)(*lattice), int(seed)))
+        self.handle = h
+
+    def reset(self, seed):
+        check(lib().b200_rng_reset(self.handle, int(seed)))
+
+    def _draw(self, fn, nin, nex, out):
+        import torch
+        n = nin * self.nvol * nex
+        if out is None:
+            out = torch.empty(n, dtype=torch.float64, device="cuda")
+        if out.numel() != n or out.dtype != torch.float64 or not out.is_cuda or not out.is_contiguous():
+            raise B200Error("output must be a contiguous float64 CUDA tensor of %d elements" % n)
+        check(fn(self.handle, ctypes.c_void_p(out.data_ptr()), int(nin), int(nex),
+                 ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+        return out
+
+    def gauss_lex_global(self, nin, nex, out=None):
+        """Field(nin, Nvol, nex) of Gaussians with variance 1/2 (nin even)."""
+        return self._draw(lib().b200_rng_gauss_lex, nin, nex, out)
+
+    def uniform_lex_global(self, nin, nex, out=None):
+        """One uniform number per site in component 0 (the others 0)."""
+        return self._draw(lib().b200_rng_uniform_lex, nin, nex, out)
+
+    def __del__(self):
+        if getattr(self, "handle", None) and _lib is not None:
+            _lib.b200_rng_destroy(self.handle)
+            self.handle = None

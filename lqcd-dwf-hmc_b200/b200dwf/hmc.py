@@ -631,6 +631,56 @@ class DeviceNoise:
         field.buf.view(dtype=__import__("torch").float64).normal_(0.0, 0.5 ** 0.5, generator=self.g)
 
 
+class MseriesNoise:
+    """The benchmark driver's heatbath draws on the device: the parallel
+    M-series generator (random_number_type Mseries_parallel, b200_rng_*)
+    hands out, in the reference's order, Field(8, Nvol, 4) Gaussians for the
+    momenta, turned into iP = i sum_a h_a lambda_a (Gell-Mann order) as
+    Langevin_Momentum::set_iP_SU3 does
+    (src/lib/HMC/langevin_Momentum.cpp:150-210), and for each fermion action a
+    lexical Field(24, Nvol, Ls) whose even sites are the noise xi
+    (Index_eo::convertField(xi, xi_lexical, 0),
+    src/lib/Action/Fermion/action_F_Ratio_eo.cpp:70-78,
+    action_F_Rational_Ratio_eo.cpp:95-99).  reset(seed) is the driver's
+    rand->reset(i_conf + traj) before each trajectory
+    (benchmark_hmc_dwf_corelib/hmc_dwf_eo.cpp:347)."""
+
+    def __init__(self, lattice, seed):
+        import torch
+        from . import MseriesParallel
+        self.lattice = list(lattice)
+        self.nvol = int(np.prod(lattice))
+        self.rng = MseriesParallel(lattice, seed)
+        sq3r = 1.0 / np.sqrt(3.0)          # the reference's constant
+        m = torch.zeros(8, 18, dtype=torch.float64)
+        for a, entries in enumerate(_ILAMBDA):
+            for r, c, re, im in entries:
+                m[a, 2 * (c + 3 * r)] = re
+                m[a, 2 * (c + 3 * r) + 1] = im
+        m[7, 2 * 0 + 1], m[7, 2 * 4 + 1], m[7, 2 * 8 + 1] = sq3r, sq3r, -2.0 * sq3r
+        self.m = m.cuda()
+        # lexical index of every even site in the reference's even/odd order
+        nx, ny, nz, nt = self.lattice
+        e = np.arange(self.nvol // 2)
+        ix2 = e % (nx // 2)
+        yzt = e // (nx // 2)
+        y, z, t = yzt % ny, (yzt // ny) % nz, yzt // (ny * nz)
+        x = 2 * ix2 + ((y + z + t) & 1)
+        self.even = torch.from_numpy(x + nx * (y + ny * (z + nz * t))).cuda()
+
+    def reset(self, seed):
+        self.rng.reset(seed)
+
+    def momentum(self, ip):
+        h = self.rng.gauss_lex_global(8, 4)
+        ip.view(-1, 18).copy_(h.view(-1, 8) @ self.m)
+
+    def fermion(self, field):
+        ls = field.op.Ls
+        lex = self.rng.gauss_lex_global(24, ls).view(ls, self.nvol, 24)
+        field.op.convert_device(field, lex.index_select(1, self.even).reshape(-1))
+
+
 class HostNoise:
     """Heatbath fields handed in from outside (for instance recorded from the
     reference's own random-number generator): momenta in the lexical

@@ -652,6 +652,12 @@ int b200_field_convert(b200_dwf_t* op, int prec, void* v, const double* w_host, 
   return 0;
 }
 
+int b200_field_convert_device(b200_dwf_t* op, int prec, void* v, const double* w_dev, void* stream) {
+  if (!op || !v || !w_dev || prec < 0 || prec > 3) return fail(B200_EINVAL, "invalid argument");
+  B200_CHECK_CUDA(launch_from_corelib(prec, v, w_dev, op->g, (cudaStream_t)stream));
+  return 0;
+}
+
 int b200_field_reverse(b200_dwf_t* op, int prec, double* v_host, const void* w, void* stream) {
   if (!op || !v_host || !w || prec < 0 || prec > 3) return fail(B200_EINVAL, "invalid argument");
   cudaStream_t st = (cudaStream_t)stream;

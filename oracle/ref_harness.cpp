@@ -81,6 +81,8 @@
 #include "Action/Gauge/action_G_Rectangle.h"
 #include "IO/bridgeIO.h"
 #include "Field/index_eo.h"
+#include "Tools/randomNumbers_parallel.h"
+#include "Tools/randomNumbers_Mseries.h"
 #include "Fopr/fopr_Smeared_eo.h"
 #include "Force/Fermion/force_F_Smeared.h"
 #include "Force/Fermion/force_F_Rational_Ratio.h"
@@ -361,10 +363,36 @@ int run_traj(const Kv& kv, const std::string& in_dir, const std::string& out_dir
 
 }  // namespace
 
+// The benchmark driver's generator (random_number_type Mseries_parallel:
+// RandomNumbers_parallel<RandomNumbers_Mseries>, one M-series stream per
+// (z, t) plane): a fixed sequence of draws in the corelib Field layout, so a
+// restatement of the generator can be checked stream against stream.
+//   u.bin  uniform Field(2, Nvol, 1)          h.bin  gauss Field(8, Nvol, 4)
+//   x.bin  gauss Field(24, Nvol, Ls)          h2.bin gauss Field(8, Nvol, 4)
+//   after reset(seed + 1)
+int run_rng(const Kv& kv, const std::string& out_dir)
+{
+  const int Nvol = CommonParameters::Nvol();
+  const int Ls = geti(kv, "Ls", 8);
+  const unsigned long seed = (unsigned long)geti(kv, "seed", 1234567);
+  RandomNumbers_parallel<RandomNumbers_Mseries> rnd(seed);
+  Field u(2, Nvol, 1), h(8, Nvol, 4), x(24, Nvol, Ls), h2(8, Nvol, 4);
+  rnd.uniform_lex_global(u);
+  rnd.gauss_lex_global(h);
+  rnd.gauss_lex_global(x);
+  rnd.reset(seed + 1);
+  rnd.gauss_lex_global(h2);
+  write_bin(out_dir + "/u.bin", u.ptr(0), size_t(2) * Nvol);
+  write_bin(out_dir + "/h.bin", h.ptr(0), size_t(8) * Nvol * 4);
+  write_bin(out_dir + "/x.bin", x.ptr(0), size_t(24) * Nvol * Ls);
+  write_bin(out_dir + "/h2.bin", h2.ptr(0), size_t(8) * Nvol * 4);
+  return 0;
+}
+
 int main(int argc, char **argv)
 {
   if (argc < 5) {
-    fprintf(stderr, "usage: %s <modes|cg|shiftcg|time|force|smear|gauge|traj> params.txt in_dir out_dir\n", argv[0]);
+    fprintf(stderr, "usage: %s <modes|cg|shiftcg|time|force|smear|gauge|traj|rng> params.txt in_dir out_dir\n", argv[0]);
     return 2;
   }
   const std::string cmd = argv[1];
@@ -381,6 +409,8 @@ int main(int argc, char **argv)
   char **fake_argv = &fake_argv0;
   bridge_initialize(&one, &fake_argv);
   bridge_setup(lat, grid, nthreads, 3, "stdout", "Crucial");
+
+  if (cmd == "rng") return run_rng(kv, out_dir);
 
   const int Nvol = CommonParameters::Nvol();
   const int Nvol2 = Nvol / 2;

@@ -5,7 +5,9 @@ built from the reference sources by ``make -f oracle/Makefile.ref``) on seeded
 synthetic inputs and stores its outputs.  Inputs are not stored: they are
 regenerated bit-for-bit from the recorded seeds by ``b200dwf.synth``.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # operator, solver, force ...
+    python tests/golden/make_golden.py traj       # one 2+1-flavour trajectory
+    python tests/golden/make_golden.py rng        # the Mseries_parallel generator
 
 Needs the reference tree (to build the harness); the committed .npz files are
 what the tests read, so the tests themselves run without it.
@@ -116,9 +118,29 @@ def traj():
     print("wrote traj_nf2p1.npz: H0 %.10f dH %.10f" % (out["H0"][0], out["dH"][0]))
 
 
+# the benchmark driver's generator (Mseries_parallel): a non-cubic lattice so
+# that x, y, z and t cannot be confused
+RNG = dict(lattice=[4, 6, 2, 4], Ls=4, seed=1234567)
+
+
+def mseries_rng():
+    with tempfile.TemporaryDirectory() as tmp:
+        with open(os.path.join(tmp, "params.txt"), "w") as f:
+            f.write("lattice %s\nLs %d\nseed %d\n"
+                    % (" ".join(map(str, RNG["lattice"])), RNG["Ls"], RNG["seed"]))
+        subprocess.run([HARNESS, "rng", os.path.join(tmp, "params.txt"), tmp, tmp],
+                       check=True, stdout=subprocess.DEVNULL)
+        out = {k: np.fromfile(os.path.join(tmp, k + ".bin")) for k in ("u", "h", "x", "h2")}
+    np.savez_compressed(os.path.join(HERE, "mseries_parallel.npz"), meta=json.dumps(RNG), **out)
+    print("wrote mseries_parallel.npz")
+
+
 def main():
     if sys.argv[1:] == ["traj"]:
         traj()
+        return
+    if sys.argv[1:] == ["rng"]:
+        mseries_rng()
         return
     for name, case in CASES.items():
         with tempfile.TemporaryDirectory() as tmp:
