@@ -376,8 +376,8 @@ def trajectory_section(op, lattice, u_workload, args, lp=None):
     heatbath and Hamiltonian, FP64 multishift), the light pair as two
     Hasenbusch ratios (light 0.01 / 0.1 / PV 1.0), Iwasaki beta 2.13, stout
     smeared fermion links (2 x rho 0.1), nested Omelyan [2,1,3], length 0.1,
-    momenta and pseudofermion noise from the device generator (the same
-    seed for every form).  Timed per form, all solves to |r|/|b| < 1e-10:
+    momenta and pseudofermion noise from the reference driver's generator
+    (Mseries_parallel) run on the device, the same seed for every form.  Timed per form, all solves to |r|/|b| < 1e-10:
     plain = FP64 CG and the multishift updating every shift every iteration;
     batched = the multishift's windowed shift updates, with mixed-precision
     Richardson (f16 storage, FP32 inner, FP64 outer) for the light,
@@ -387,7 +387,7 @@ def trajectory_section(op, lattice, u_workload, args, lp=None):
     import torch
     import b200dwf
     from b200dwf import synth
-    from b200dwf.hmc import build_dwf_nf2p1, DeviceNoise, Solver
+    from b200dwf.hmc import build_dwf_nf2p1, Solver
     lattice = list(args.traj_lattice or lattice)
     sm = b200dwf.StoutSmear(lattice, 0.1, 2)
     sm.set_config(synth.gauge_field(lattice, SEED_U + 3, "near", 0.3))
@@ -432,7 +432,7 @@ def trajectory_section(op, lattice, u_workload, args, lp=None):
 def _trajectory_form(lattice, u0, args, lp, kinds, window, tol2):
     import torch
     import b200dwf
-    from b200dwf.hmc import build_dwf_nf2p1, DeviceNoise, Solver
+    from b200dwf.hmc import build_dwf_nf2p1, MseriesNoise, Solver
     gc.collect()
     torch.cuda.empty_cache()
     # "mixed+": mixed-precision Richardson whose MD solves start from the
@@ -455,9 +455,12 @@ def _trajectory_form(lattice, u0, args, lp, kinds, window, tol2):
         v.iterations, v.seconds, v.calls = 0, 0.0, 0
     for r in hmc.fermions["nf1"].rationals.values():
         r.iterations, r.seconds, r.calls = 0, 0.0, 0
+    # the benchmark driver's generator (Mseries_parallel) on the device; its
+    # streams are seeded here, outside the timed trajectory
+    noise = MseriesNoise(lattice, SEED_U + 11)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    r = hmc.trajectory(ud, DeviceNoise(SEED_U + 11))
+    r = hmc.trajectory(ud, noise)
     torch.cuda.synchronize()
     out = {"sec_per_trajectory": time.perf_counter() - t0, "dH": r["dH"],
            "H0": r["H0"], "multishift_window": window, **hmc.stats()}

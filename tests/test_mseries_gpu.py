@@ -102,3 +102,40 @@ def test_mseries_noise_heatbath_fields():
                     ev.append(2 * ix2 + ((y + z + t) & 1) + nx * (y + ny * (z + nz * t)))
     ref = lex[:, ev, :].reshape(-1)
     assert np.abs(op.reverse(f) - ref).max() < TOL
+
+
+def test_trajectory_with_the_drivers_generator():
+    """A device 2+1-flavour trajectory drawing its heatbath from the device
+    generator equals the same trajectory fed, through HostNoise, with the
+    fields the CPU restatement of the generator produces (momentum first,
+    then each fermion action in registration order, as the reference's
+    HMC_General::langevin consumes them)."""
+    import torch
+    from b200dwf.hmc import HostNoise, MseriesNoise
+    from oracle.mseries import MseriesParallel as Oracle
+    from test_hmc_nf2p1 import _hmc_from_meta, golden
+    meta, u, _ = golden()
+    lat, ls, seed = meta["lattice"], meta["Ls"], 4242
+    nvol = int(np.prod(lat))
+    ora = Oracle(lat, seed)
+    ip_ref = _set_ip_su3(ora.gauss_lex_global(8, 4), nvol)
+    nx, ny, nz, nt = lat
+    e = np.arange(nvol // 2)
+    ix2, yzt = e % (nx // 2), e // (nx // 2)
+    y, z, t = yzt % ny, (yzt // ny) % nz, yzt // (ny * nz)
+    even = 2 * ix2 + ((y + z + t) & 1) + nx * (y + ny * (z + nz * t))
+    xis = [ora.gauss_lex_global(24, ls).reshape(ls, nvol, 24)[:, even, :].reshape(-1)
+           for _ in range(3)]
+    out = []
+    for noise in (MseriesNoise(lat, seed), HostNoise(ip_ref, xis)):
+        hmc = _hmc_from_meta(meta)
+        ud = torch.from_numpy(u.copy()).cuda()
+        hmc.set_config(ud)
+        ip = torch.zeros_like(ud)
+        h0, _ = hmc.langevin(ip, noise)
+        hmc.integrator.evolve(meta["tau"], ip, ud)
+        h1, _ = hmc.calc_hamiltonian(ip)
+        out.append((h0, h1 - h0, ud.cpu().numpy()))
+    assert out[0][0] == pytest.approx(out[1][0], rel=1e-13)
+    assert abs(out[0][1] - out[1][1]) < 1e-8
+    assert np.max(np.abs(out[0][2] - out[1][2])) < 1e-10
