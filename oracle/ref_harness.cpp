@@ -82,6 +82,7 @@
 #include "IO/bridgeIO.h"
 #include "Field/index_eo.h"
 #include "Tools/randomNumbers_parallel.h"
+#include "IO/gaugeConfig.h"
 #include "Tools/randomNumbers_Mseries.h"
 #include "Fopr/fopr_Smeared_eo.h"
 #include "Force/Fermion/force_F_Smeared.h"
@@ -389,10 +390,27 @@ int run_rng(const Kv& kv, const std::string& out_dir)
   return 0;
 }
 
+// Gauge-configuration files through the reference's own readers/writers:
+// in_dir/conf.txt (Text_4x4x4x8) is read onto the run's lattice and dumped
+// (text_read.bin, native doubles), written as Binary (conf.bin) and read
+// back (bin_read.bin).
+int run_io(const std::string& in_dir, const std::string& out_dir)
+{
+  const int Nvol = CommonParameters::Nvol();
+  const size_t ng = size_t(18) * Nvol * 4;
+  Field_G U(Nvol, 4), V(Nvol, 4);
+  GaugeConfig("Text_4x4x4x8").read(U, in_dir + "/conf.txt");
+  write_bin(out_dir + "/text_read.bin", U.ptr(0), ng);
+  GaugeConfig("Binary").write_file(U, out_dir + "/conf.bin");
+  GaugeConfig("Binary").read(V, out_dir + "/conf.bin");
+  write_bin(out_dir + "/bin_read.bin", V.ptr(0), ng);
+  return 0;
+}
+
 int main(int argc, char **argv)
 {
   if (argc < 5) {
-    fprintf(stderr, "usage: %s <modes|cg|shiftcg|time|force|smear|gauge|traj|rng> params.txt in_dir out_dir\n", argv[0]);
+    fprintf(stderr, "usage: %s <modes|cg|shiftcg|time|force|smear|gauge|traj|rng|io> params.txt in_dir out_dir\n", argv[0]);
     return 2;
   }
   const std::string cmd = argv[1];
@@ -411,6 +429,7 @@ int main(int argc, char **argv)
   bridge_setup(lat, grid, nthreads, 3, "stdout", "Crucial");
 
   if (cmd == "rng") return run_rng(kv, out_dir);
+  if (cmd == "io") return run_io(in_dir, out_dir);
 
   const int Nvol = CommonParameters::Nvol();
   const int Nvol2 = Nvol / 2;

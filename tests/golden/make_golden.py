@@ -8,6 +8,7 @@ regenerated bit-for-bit from the recorded seeds by ``b200dwf.synth``.
     python tests/golden/make_golden.py            # operator, solver, force ...
     python tests/golden/make_golden.py traj       # one 2+1-flavour trajectory
     python tests/golden/make_golden.py rng        # the Mseries_parallel generator
+    python tests/golden/make_golden.py io         # gauge-configuration files
 
 Needs the reference tree (to build the harness); the committed .npz files are
 what the tests read, so the tests themselves run without it.
@@ -135,7 +136,42 @@ def mseries_rng():
     print("wrote mseries_parallel.npz")
 
 
+# gauge-configuration files: a synthetic 4x4x4x8 text configuration (hot
+# links, seed 77, one "%.14e" number per line as the reference's
+# conf_04040408.txt) read by the reference onto 8x4x4x8 and written as Binary
+IO = dict(text_lattice=[4, 4, 4, 8], lattice=[8, 4, 4, 8], gauge=("hot", 77), fmt="%.14e")
+
+
+def io_text(case):
+    kind, seed = case["gauge"]
+    u = synth.gauge_field(case["text_lattice"], seed, kind)
+    n = int(np.prod(case["text_lattice"]))
+    t = u.reshape(4, n, 18).transpose(1, 0, 2).reshape(-1)
+    return "".join((case["fmt"] + "\n") % v for v in t)
+
+
+def gauge_io():
+    import hashlib
+    with tempfile.TemporaryDirectory() as tmp:
+        with open(os.path.join(tmp, "conf.txt"), "w") as f:
+            f.write(io_text(IO))
+        with open(os.path.join(tmp, "params.txt"), "w") as f:
+            f.write("lattice %s\n" % " ".join(map(str, IO["lattice"])))
+        subprocess.run([HARNESS, "io", os.path.join(tmp, "params.txt"), tmp, tmp],
+                       check=True, stdout=subprocess.DEVNULL)
+        digest = {}
+        for name in ("text_read.bin", "conf.bin", "bin_read.bin"):
+            with open(os.path.join(tmp, name), "rb") as f:
+                digest[name] = hashlib.sha256(f.read()).hexdigest()
+    np.savez_compressed(os.path.join(HERE, "gauge_io.npz"), meta=json.dumps(IO),
+                        digest=json.dumps(digest))
+    print("wrote gauge_io.npz")
+
+
 def main():
+    if sys.argv[1:] == ["io"]:
+        gauge_io()
+        return
     if sys.argv[1:] == ["traj"]:
         traj()
         return
