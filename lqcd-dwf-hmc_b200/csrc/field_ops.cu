@@ -567,13 +567,24 @@ __global__ void __launch_bounds__(256) ms_flush_kernel(MsUpdParams p, long n2) {
 #pragma unroll
     for (int l = 0; l < kMaxWin; ++l)
       if (l < w) rv[l] = __ldcs(reinterpret_cast<const double2*>(p.win[l]) + e);
+    // the next shift's p_i, x_i are loaded while this shift is combined, so
+    // every thread keeps two shifts' loads in flight
+    double2 pn = make_double2(0.0, 0.0), xn = pn;
+    if (nsh > 1) {
+      pn = __ldcs(reinterpret_cast<const double2*>(p.ps[1]) + e);
+      xn = __ldcs(reinterpret_cast<const double2*>(p.xs[1]) + e);
+    }
     for (int i = 1; i < nsh; ++i) {
       const double* pc = cs + i * (kMaxWin + 1);
       const double* xc = cs + kMaxShift * (kMaxWin + 1) + i * (kMaxWin + 1);
       double2* pp = reinterpret_cast<double2*>(p.ps[i]) + e;
       double2* xp = reinterpret_cast<double2*>(p.xs[i]) + e;
-      const double2 p0 = *pp;
-      double2 x = *xp;
+      const double2 p0 = pn;
+      double2 x = xn;
+      if (i + 1 < nsh) {
+        pn = __ldcs(reinterpret_cast<const double2*>(p.ps[i + 1]) + e);
+        xn = __ldcs(reinterpret_cast<const double2*>(p.xs[i + 1]) + e);
+      }
       double2 q;
       q.x = pc[0] * p0.x; q.y = pc[0] * p0.y;
       x.x = fma(xc[0], p0.x, x.x); x.y = fma(xc[0], p0.y, x.y);
@@ -584,8 +595,8 @@ __global__ void __launch_bounds__(256) ms_flush_kernel(MsUpdParams p, long n2) {
           x.x = fma(xc[1 + l], rv[l].x, x.x); x.y = fma(xc[1 + l], rv[l].y, x.y);
         }
       }
-      *pp = q;
-      *xp = x;
+      __stcs(pp, q);
+      __stcs(xp, x);
     }
   }
 }
