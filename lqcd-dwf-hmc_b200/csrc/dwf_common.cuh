@@ -10,10 +10,13 @@
 //     f32 : 2 complex  (float4),  K = 6
 //     f16/bf16 : 4 complex (8 halves in uint4), K = 3, values scaled by a
 //       per-(site, s) float stored after the site's chunks (padded to 16 B).
-// Link layout (one plan, both parities):
-//   f64 : [parity][mu][site] x 9 double2 (full 3x3), or 6 double2 (two rows)
-//   f32 : [parity][mu][site] x 3 float4  (two rows, third reconstructed)
-//   f16 : [parity][mu][site] x 2 uint4   (two rows as 12 halves + padding)
+// Link layout (one plan, both parities), record (ieo + 2*mu)*Vh + site:
+//   f64 : 9 double2 (full 3x3; LINK_F64_18, read by the FP64 hops)
+//   f32 : 5 float4  (full 3x3, 18 floats + padding; LINK_F32_18, FP32 hops)
+//         or 3 float4 (two rows, third rebuilt; LINK_F32_12, learned network)
+//   f16 : 3 uint4   (full 3x3 as 18 halves + padding; LINK_F16_18)
+// The hop formats carry the boundary phase and the t projection's factor 2
+// (dwf_hop.cuh, LinkLoad::kFolded).
 #pragma once
 
 #include <cuda_runtime.h>
