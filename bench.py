@@ -1,20 +1,24 @@
 #!/usr/bin/env python
 """Benchmark of the B200 even/odd domain-wall hot path.
 
-Workload (the operator/solver configuration the Dslash GB/s metric is quoted
-on): 16^3x32 lattice, Ls=16, Shamir DWF M0=1.8, m=0.01, seeded near-unit SU(3)
-links exp(i*0.3*H) followed by 2 stout steps rho=0.1, Gaussian RHS, FP64.
+Workload (the lattice the metric is quoted on): 24^3x48, Ls=16, Shamir DWF
+M0=1.8, m=0.01, seeded near-unit SU(3) links exp(i*0.3*H) followed by 2 stout
+steps rho=0.1 (smeared on the device by the library's stout kernels), Gaussian
+RHS, FP64.
 
 A step is one even/odd Dslash apply and its dagger through the reference
 operator interface: mult(v, w, "Deo") then mult_dag(v', w, "Deo").  Its
 algorithmic traffic is the fused D_eo byte count per 4D half-site
     B = Ls*24*(8 + 8) + 8*18*8 = 7296 bytes  (Ls=16, FP64, 18-real links)
-counted once per apply (two applies per step).
+counted once per apply (two applies per step); one apply at 24^3x48
+(Vh = 331,776) is 2.42 GB, more than L2.
 
 The JSON line also carries the dominant kernel's roofline (the fused hop
 kernel timed alone with CUDA events), an end-to-end number through the C ABI
-with host buffers, the FP64 CG time-to-solution at |r|/|b| < 1e-10 and the
-reference corelib CPU path timed on this host as the CPU baseline.
+with host buffers, the 2+1-flavour trajectory on the same lattice in its
+three forms (plain FP64, mixed+batched, mixed+batched+learned) as short
+top-level keys, the solver timings, and the reference corelib CPU path timed
+on this host as the CPU baseline.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 """
@@ -33,15 +37,17 @@ import numpy as np
 REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(REPO, "lqcd-dwf-hmc_b200"))
 
-LATTICE = [16, 16, 16, 32]
+LATTICE = [24, 24, 24, 48]
+LEARN_LATTICE = [16, 16, 16, 32]   # the learned preconditioner's configuration
 LS = 16
 MQ, M0 = 0.01, 1.8
 MS = 0.04                   # strange-quark mass of the 2+1-flavour trajectory
 SEED_U, SEED_B = 1234567, 7654321
 BYTES_PER_HALF_SITE = LS * 24 * (8 + 8) + 8 * 18 * 8
 REF_HARNESS = os.path.join(REPO, "oracle", "_ref", "ref_harness")
-WORKLOAD = "dwf_eo_dslash_16x16x16x32_Ls16_f64"
-METRIC = "Dslash HBM GB/s (D_eo + D_eo^dag, 16^3x32 Ls=16 FP64)"
+WORKLOAD = "dwf_eo_dslash_24x24x24x48_Ls16_f64"
+METRIC = "sec/trajectory 24^3x48 Ls=16: mixed+learned vs plain FP64 on B200; Dslash GB/s"
+VALUE_IS = "Dslash HBM GB/s: D_eo + D_eo^dag, FP64, algorithmic bytes / device time"
 
 
 def parse():
@@ -75,10 +81,21 @@ def parse():
     return ap.parse_args()
 
 
-def workload_inputs(lattice, ls):
+def workload_inputs(lattice, ls, device_smear=False):
+    """Seeded links exp(i*0.3*H) smeared by 2 stout steps rho=0.1, and the
+    Gaussian RHS.  device_smear: the smearing runs in the library's stout
+    kernels (equal to the numpy restatement to ~1e-14; used where the numpy
+    form would take most of a minute, 24^3x48)."""
     from b200dwf import synth
     u = synth.gauge_field(lattice, SEED_U, "near", eps=0.3)
-    u = synth.stout_smear(u, lattice, 0.1, 2)
+    if device_smear:
+        import b200dwf
+        sm = b200dwf.StoutSmear(lattice, 0.1, 2)
+        sm.set_config(u)
+        u = np.ascontiguousarray(sm.config(2))
+        del sm
+    else:
+        u = synth.stout_smear(u, lattice, 0.1, 2)
     b = synth.spinor_field(lattice, ls, SEED_B)
     return u, b
 
@@ -97,16 +114,26 @@ def read_peaks():
         return 6650.0, "fallback"
 
 
-def read_traffic():
-    """DRAM bytes per launch of the hop kernel from the committed ncu summary."""
-    path = os.path.join(REPO, "profiles", "hop_kernel_f64_16x16x16x32_Ls16.md")
+TRAFFIC_PROFILE = os.path.join(REPO, "profiles", "hop_kernel_f64_16x16x16x32_Ls16.md")
+
+
+def read_traffic(vh):
+    """DRAM bytes per launch of the FP64 hop kernel: the committed ncu
+    summary's capture (a 16^3x32 launch, small enough for a full capture),
+    scaled to vh sites.  Each site reads its column, its 8 neighbours'
+    columns (7 of them shared with other sites of the launch) and 8 links,
+    and writes its column, so the traffic grows in proportion to the sites."""
+    got = {}
     try:
-        for line in open(path):
-            if line.startswith("dram_bytes_per_launch:"):
-                return float(line.split(":")[1])
+        for line in open(TRAFFIC_PROFILE):
+            for key in ("dram_bytes_per_launch:", "vh_per_launch:"):
+                if line.startswith(key):
+                    got[key] = float(line.split(":")[1])
     except OSError:
-        pass
-    return None
+        return None
+    if len(got) < 2:
+        return None
+    return got["dram_bytes_per_launch:"] * vh / got["vh_per_launch:"]
 
 
 # ------------------------------------------------------------------ clocks
@@ -166,16 +193,19 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------ reference (CPU) arm
-def run_reference_cpu(lattice, ls, steps, warmup, budget_s=60.0, threads=None):
+def run_reference_cpu(lattice, ls, steps, warmup, budget_s=60.0, threads=None, inputs=None,
+                      ddagd=False):
     """Time the reference corelib Fopr_Domainwall_eo (oracle/_ref, built from
     the reference sources) on this host: one step = mult(v,w,"Deo") +
-    mult_dag(v,w,"Deo") on the same workload.  Returns (GB/s, seconds/step,
-    reps, threads)."""
+    mult_dag(v,w,"Deo") on the same workload (inputs = (u, b) when the caller
+    has them).  Returns a dict: GB/s, seconds/step, reps, threads, and with
+    ddagd the seconds of one mult(v,w,"DdagD")."""
     if not os.path.exists(REF_HARNESS):
         raise RuntimeError("oracle/_ref/ref_harness not built")
     threads = threads or os.cpu_count() or 1
-    u, b = workload_inputs(lattice, ls)
+    u, b = inputs if inputs is not None else workload_inputs(lattice, ls)
     vh = vh_of(lattice)
+    modes = "Deo dag_Deo" + (" DdagD" if ddagd else "")
     with tempfile.TemporaryDirectory() as d:
         u.tofile(os.path.join(d, "gauge.bin"))
         b.tofile(os.path.join(d, "src.bin"))
@@ -183,22 +213,27 @@ def run_reference_cpu(lattice, ls, steps, warmup, budget_s=60.0, threads=None):
         def timed(reps, warm):
             with open(os.path.join(d, "params.txt"), "w") as f:
                 f.write("lattice %s\nLs %d\nmq %r\nM0 %r\nthreads %d\nreps %d\nwarmup %d\n"
-                        "modes Deo dag_Deo\n"
-                        % (" ".join(map(str, lattice)), ls, MQ, M0, threads, reps, warm))
+                        "modes %s\n"
+                        % (" ".join(map(str, lattice)), ls, MQ, M0, threads, reps, warm, modes))
             r = subprocess.run([REF_HARNESS, "time", os.path.join(d, "params.txt"), d, d],
                                capture_output=True, text=True, check=True)
             t = {}
             for line in r.stdout.splitlines():
                 p = line.split()
-                if len(p) == 2 and p[0] in ("Deo", "dag_Deo"):
+                if len(p) == 2 and p[0] in ("Deo", "dag_Deo", "DdagD"):
                     t[p[0]] = float(p[1])
-            return t["Deo"] + t["dag_Deo"]
+            return t
 
-        probe = timed(1, 1)
-        reps = int(max(1, min(steps, budget_s / max(probe, 1e-6))))
-        t_step = timed(reps, max(1, warmup))
-    gbs = 2 * BYTES_PER_HALF_SITE * vh / t_step / 1e9
-    return gbs, t_step, reps, threads
+        probe = timed(1, 0)
+        per_rep = sum(probe.values())
+        reps = int(max(1, min(steps, budget_s / max(per_rep, 1e-6))))
+        t = timed(reps, max(0, min(warmup, 1)))
+    t_step = t["Deo"] + t["dag_Deo"]
+    out = {"gbs": 2 * BYTES_PER_HALF_SITE * vh / t_step / 1e9, "t_step": t_step, "reps": reps,
+           "threads": threads}
+    if ddagd:
+        out["t_ddagd"] = t["DdagD"]
+    return out
 
 
 # The configuration the reference runs on its CPU path (4^3x8, Ls=8 Shamir
@@ -278,12 +313,14 @@ def reference_arm(args, rank, world):
     if rank != 0:
         return
     try:
-        gbs, t_step, reps, threads = run_reference_cpu(args.lattice, LS, args.steps, args.warmup)
+        r = run_reference_cpu(args.lattice, LS, args.steps, args.warmup, budget_s=60.0)
+        gbs, t_step, reps, threads = r["gbs"], r["t_step"], r["reps"], r["threads"]
     except Exception as e:  # noqa: BLE001
         print(json.dumps({"impl": "reference", "unavailable": "reference corelib harness failed: %s" % e}))
         return
     line = {
-        "impl": "reference", "metric": METRIC, "value": gbs, "unit": "GB/s", "n_gpus": args.gpus,
+        "impl": "reference", "metric": METRIC, "value_is": VALUE_IS, "value": gbs, "unit": "GB/s",
+        "n_gpus": args.gpus,
         "steps": reps, "warmup": max(1, args.warmup), "ms_per_step": t_step * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "lattice": args.lattice, "Ls": LS, "M0": M0, "mq": MQ,
@@ -297,14 +334,21 @@ def reference_arm(args, rank, world):
 
 
 # ------------------------------------------------------------------ learned preconditioner
-def learned_section(op, lattice, w, u_workload, args):
-    """Train the gauge-covariant network on CG (residual, error) pairs of
-    seeded configurations (near-unit links + 2 stout steps, other seeds than
-    the workload's) and compare flexible CG with it against plain FP64 CG on
-    the workload configuration and RHS, both to |r|/|b| < 1e-10."""
+def learned_section(args):
+    """On the learned preconditioner's configuration (16^3x32, Ls=16,
+    m=0.01): train the gauge-covariant network on CG (residual, error) pairs
+    of seeded configurations (near-unit links + 2 stout steps, other seeds
+    than the evaluation's) and compare flexible CG with it against plain FP64
+    CG on the evaluation configuration and RHS, both to |r|/|b| < 1e-10."""
     import torch
     import b200dwf
     from b200dwf import synth
+    lattice = list(LEARN_LATTICE)
+    u_workload, b_host = workload_inputs(lattice, LS, device_smear=True)
+    op = b200dwf.DomainWall(lattice, LS, MQ, M0, 1.0, 0.0, 1.0, (1, 1, 1, -1))
+    op.set_config(u_workload)
+    w = op.new_field(0)
+    op.convert(w, b_host)
     lp = b200dwf.LearnedPrecond(op, hidden=8, seed=11)
     sm = b200dwf.StoutSmear(lattice, 0.1, 2)
     losses = []
@@ -356,7 +400,7 @@ def learned_section(op, lattice, w, u_workload, args):
                          "true_rel_residual": out[2], "seconds": c1 - c0, "converged": out[3] == 0,
                          "orthogonalised_against": 8 if name == "fcg_learned" else 2}
     return {"network": "3 layers, 4->8->4 channels per color, 11 paths, BF16 weights, FP32 accumulate",
-            "train_configs": args.learned_configs, "train_pairs": npairs,
+            "lattice": lattice, "train_configs": args.learned_configs, "train_pairs": npairs,
             "epochs_per_config": args.learned_epochs,
             "loss_first_last_per_config": losses, "train_seconds": t_train,
             "apply_ms": t_apply * 1e3, "tol_rel_residual": 1e-10, **res,
@@ -481,7 +525,7 @@ def b200_arm(args, rank, world, local_rank):
     b200dwf.check(b200dwf.lib().b200_init(local_rank, 0))
     lattice = args.lattice
     vh = vh_of(lattice)
-    u, b = workload_inputs(lattice, LS)
+    u, b = workload_inputs(lattice, LS, device_smear=True)
     op = b200dwf.DomainWall(lattice, LS, MQ, M0, 1.0, 0.0, 1.0, (1, 1, 1, -1))
     op.set_config(u)
     w = op.new_field(0)
@@ -489,6 +533,9 @@ def b200_arm(args, rank, world, local_rank):
     v2 = op.new_field(0)
     op.convert(w, b)
     step_bytes = 2 * BYTES_PER_HALF_SITE * vh
+    # the timed loops queue their launches without a host round trip per call;
+    # the plan's error word is checked after each loop
+    op.set_async(True)
 
     def step():
         op.mult(v1, w, "Deo")
@@ -501,6 +548,7 @@ def b200_arm(args, rank, world, local_rank):
 
     for _ in range(args.warmup):
         step()
+    op.check_error()
     torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
@@ -511,14 +559,15 @@ def b200_arm(args, rank, world, local_rank):
             step()
         e1.record()
         torch.cuda.synchronize()
+    op.check_error()
     barrier()
     torch.cuda.synchronize()
     t_total = replicas.max_over_ranks(e0.elapsed_time(e1) / 1e3, dist, "cuda")
     value = replicas.whole_job_rate(step_bytes * args.steps, t_total, world) / 1e9
 
     # dominant kernel: mult_dag("Deo") is exactly one launch of the fused hop kernel
-    nk = max(50, min(args.steps, 500))
-    for _ in range(10):
+    nk = max(20, min(args.steps, 200))
+    for _ in range(5):
         op.mult_dag(v2, w, "Deo")
     torch.cuda.synchronize()
     k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -527,17 +576,19 @@ def b200_arm(args, rank, world, local_rank):
         op.mult_dag(v2, w, "Deo")
     k1.record()
     torch.cuda.synchronize()
+    op.check_error()
     t_hop = k0.elapsed_time(k1) / 1e3 / nk
     peak, peak_kind = read_peaks()
     achieved = BYTES_PER_HALF_SITE * vh / t_hop / 1e9
-    traffic = read_traffic()
+    traffic = read_traffic(vh)
+    op.set_async(False)
 
     # end to end through the C ABI with pinned host buffers
     nbytes = 24 * vh * LS * 8
     h_in = torch.from_numpy(b).pin_memory()
     h_out1 = torch.empty(24 * vh * LS, dtype=torch.float64).pin_memory()
     h_out2 = torch.empty(24 * vh * LS, dtype=torch.float64).pin_memory()
-    ne = max(3, min(args.steps, 20))
+    ne = max(3, min(args.steps, 10))
 
     def e2e_step():
         op.convert(w, h_in.numpy())
@@ -556,6 +607,7 @@ def b200_arm(args, rank, world, local_rank):
     torch.cuda.synchronize()
     t_e2e = replicas.max_over_ranks(q0.elapsed_time(q1) / 1e3, dist, "cuda")
     e2e_value = replicas.whole_job_rate(step_bytes * ne, t_e2e, world) / 1e9
+    del h_in, h_out1, h_out2
 
     # FP64 CG time to solution, |r|/|b| < 1e-10
     cg = None
@@ -614,7 +666,7 @@ def b200_arm(args, rank, world, local_rank):
     # the solver, learned-network and trajectory sections are one-GPU
     # workloads; under torchrun (replicas) only the Dslash metric is timed
     if not args.no_learned and world == 1:
-        learned, lp = learned_section(op, lattice, w, u, args)
+        learned, lp = learned_section(args)
     trajectory = None
     if not args.no_trajectory and world == 1:
         trajectory = trajectory_section(op, lattice, u, args, lp)
@@ -627,20 +679,32 @@ def b200_arm(args, rank, world, local_rank):
             small = {"unavailable": str(e)}
     if rank != 0:
         return
-    cpu = None
+    cpu, cpu_traj = None, None
     if world == 1 and not args.no_cpu:
         try:
-            gbs, t_step, reps, threads = run_reference_cpu(lattice, LS, 100, 1, budget_s=20.0)
-            cpu = {"value": gbs, "unit": "GB/s", "cores": threads, "kind": "reference",
-                   "sample": "%d steps (Deo + Ddag_eo) of the reference corelib Fopr_Domainwall_eo "
-                             "on the full workload lattice, bounded to ~20 s" % reps}
+            r = run_reference_cpu(lattice, LS, 100, 1, budget_s=20.0, inputs=(u, b), ddagd=True)
+            cpu = {"value": r["gbs"], "unit": "GB/s", "cores": r["threads"], "kind": "reference",
+                   "sample": "%d steps (Deo + Ddag_eo, plus one DdagD each) of the reference corelib "
+                             "Fopr_Domainwall_eo on the full %s Ls=16 workload, bounded to ~20 s"
+                             % (r["reps"], "x".join(map(str, lattice))),
+                   "ddagd_seconds": r["t_ddagd"]}
+            plain = (trajectory or {}).get("fp64_plain", {})
+            n_ddagd = sum(v.get("iterations", 0) for k, v in plain.items()
+                          if isinstance(v, dict) and (k.startswith("solver_") or k.startswith("multishift_")))
+            if n_ddagd:
+                cpu_traj = {"sec_per_trajectory": n_ddagd * r["t_ddagd"], "kind": "extrapolated",
+                            "how": "reference corelib DdagD seconds on %d host cores x the %d DdagD "
+                                   "applications (CG + multishift iterations) of the plain FP64 "
+                                   "device trajectory; a lower bound (forces, smearing and vector "
+                                   "updates left out)" % (r["threads"], n_ddagd)}
         except Exception as e:  # noqa: BLE001
             cpu = {"value": None, "unit": "GB/s", "cores": 0, "kind": "reference",
                    "sample": "unavailable: %s" % e}
     line = {
-        "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": t_total * 1e3 / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "metric": METRIC, "value_is": VALUE_IS, "value": value, "unit": "GB/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_total * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
         "config": {"workload": WORKLOAD, "lattice": lattice, "Ls": LS, "M0": M0, "mq": MQ,
                    "links": "near-unit exp(i*0.3*H) + 2 stout rho=0.1", "parallelism": "replicas",
                    "l2": "inputs larger than L2 (%.0f MB per field)" % (nbytes / 1e6)},
@@ -652,18 +716,34 @@ def b200_arm(args, rank, world, local_rank):
                      "bound": "hbm",
                      "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
+                     "traffic_note": "ncu DRAM bytes of a 16^3x32 launch scaled by sites",
                      "algorithmic_bytes_per_launch": BYTES_PER_HALF_SITE * vh,
-                     "launch_us": t_hop * 1e6},
+                     "launch_us": t_hop * 1e6, "target_frac": 0.7},
         "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": nbytes,
                 "d2h_bytes_per_step": 2 * nbytes},
+    }
+    # the trajectory's headline numbers as short top-level keys
+    if trajectory:
+        for form in ("fp64_plain", "mixed_batched", "mixed_batched_learned"):
+            f = trajectory.get(form, {})
+            if "sec_per_trajectory" in f:
+                line["sec_traj_" + form] = round(f["sec_per_trajectory"], 3)
+                line["dH_" + form] = f.get("dH")
+            if "speedup_" + form in trajectory:
+                line["speedup_" + form] = round(trajectory["speedup_" + form], 3)
+        line["speedup_target"] = 3.0
+    if cpu_traj:
+        line["sec_traj_cpu_reference_extrapolated"] = round(cpu_traj["sec_per_trajectory"], 1)
+    line.update({
+        "cpu_baseline": cpu,
+        "cpu_trajectory": cpu_traj,
         "cg_f64": cg,
         "solvers": solvers,
         "learned_preconditioner": learned,
         "trajectory": trajectory,
         "trajectory_4x4x4x8_beside_reference": small,
         "autotune": b200dwf.tuning_table().strip().splitlines(),
-        "cpu_baseline": cpu,
-    }
+    })
     print(json.dumps(line))
 
 

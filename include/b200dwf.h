@@ -84,7 +84,7 @@ size_t b200_dwf_field_nreal(const b200_dwf_t *op);
 int b200_field_convert(b200_dwf_t *op, int prec, void *v_dev, const double *w_host,
                        void *stream);
 int b200_field_reverse(b200_dwf_t *op, int prec, double *v_host, const void *w_dev,
-                       void *stream);
+                       void *stream);   /* also reports the plan's error word */
 /* convert() from a field already on the device (w_dev: reference layout,
  * 24 * Nvol/2 * Ls doubles), asynchronous on `stream`: the heatbath noise
  * drawn by b200_rng_gauss_lex goes to the operator without a host copy. */
@@ -94,9 +94,32 @@ int b200_field_convert_device(b200_dwf_t *op, int prec, void *v_dev, const doubl
 /* mult / mult_dag (afopr_Domainwall_5din_eo-tmpl.h:634-767).  mode is one of
  *   "D" "Ddag" "DdagD" "H" "Hdag" "Deo" "Doe" "Dee" "Doo" "Dee_inv" "Doo_inv"
  *   "gm5R" "R"
- * dag != 0 selects mult_dag.  v and w are distinct fields of precision prec. */
+ * dag != 0 selects mult_dag.  v and w are distinct fields of precision prec.
+ * Synchronous by default, like the reference's mult (its OpenACC launches
+ * return after the kernels, mult_Domainwall_5din_eo_openacc-inc.h): the call
+ * waits for its kernels and reports a bulk-copy wait that gave up as
+ * B200_ECUDA (the output is then not written); see b200_dwf_set_async. */
 int b200_dwf_mult(b200_dwf_t *op, int prec, void *v, const void *w,
                   const char *mode, int dag, void *stream);
+
+/* Asynchronous calls (async != 0): b200_dwf_mult and the b200_dwf_force_*
+ * entry points return once their kernels are queued on `stream`.  A hop that
+ * gave up waiting for its bulk copies then surfaces at the next synchronising
+ * call on this plan (b200_field_reverse, norm2/dot, the solvers) or at
+ * b200_dwf_check_error.  No reference counterpart: the reference's launches
+ * are synchronous.  Default 0. */
+int b200_dwf_set_async(b200_dwf_t *op, int async_calls);
+/* Waits for `stream`, then reports (B200_ECUDA) and clears the plan's device
+ * error word of the hop kernels' bounded waits; 0 when it is clear. */
+int b200_dwf_check_error(b200_dwf_t *op, void *stream);
+/* Test hook of the failure path (host-set; no reference counterpart): every
+ * bulk-copy (TMA-fed) hop launched by this plan treats its wait for hop
+ * direction `direction` (0..7 = x+, x-, y+, y-, z+, z-, t+, t-) as if its
+ * bound had run out: it sets the error word, still waits (with the long
+ * drain bound) for the copies it has in flight, and returns without writing
+ * its outputs.  Hops fed by plain loads have no waits and are unaffected.
+ * -1 switches it off (the default). */
+int b200_dwf_inject_wait_failure(b200_dwf_t *op, int direction);
 
 /* ---------------------------------------------------------------- fields
  * AField<REAL, ACCEL> BLAS (src/lib_alt_Accel/Field/afield-tmpl.h:637-720 ->
@@ -160,9 +183,10 @@ int b200_richardson_solve(b200_dwf_t *op, int inner_prec, void *x, const void *b
 int b200_solver_set_initial_guess(b200_dwf_t *op, int use);
 
 /* Allocation-free |x|^2 for callers that cannot allocate device memory: code
- * inside a CUDA graph capture, code running under a host framework that owns
- * all device memory through its own pool, or a caller on a GPU whose memory is
- * already committed.  It needs no operator plan (a plan owns its reduction
+ * running under a host framework that owns all device memory through its own
+ * pool (an allocation behind its back can fail or exhaust what the pool
+ * planned for), or a caller on a GPU whose memory is already committed to
+ * resident fields.  It needs no operator plan (a plan owns its reduction
  * scratch): pass the field x (precision prec, nsite 4D half-lattice sites,
  * Ls = ls) and a host pointer for the result.  No counterpart in the
  * reference (its norm2 always runs on fields that an operator allocated).
@@ -199,6 +223,8 @@ int b200_dwf_force_udiv(b200_dwf_t *op, double *force, const void *eta, void *st
  * src/lib/Action/Fermion/action_F_Ratio_eo.cpp:171-205). */
 int b200_dwf_force_acc(b200_dwf_t *op, const char *mode, double *force, const void *a,
                        const void *b, double scale, void *stream);
+/* The force entry points are synchronous like b200_dwf_mult (and report the
+ * error word) unless the plan is switched to asynchronous calls. */
 
 /* ---------------------------------------------------------------- stout
  * Stout smearing levels and the smeared-force Jacobian, on the device.

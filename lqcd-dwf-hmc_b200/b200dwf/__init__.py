@@ -57,6 +57,9 @@ def lib():
     L.b200_field_reverse.argtypes = [vp, ctypes.c_int, dp, vp, vp]
     L.b200_field_convert_device.argtypes = [vp, ctypes.c_int, vp, vp, vp]
     L.b200_dwf_mult.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_char_p, ctypes.c_int, vp]
+    L.b200_dwf_set_async.argtypes = [vp, ctypes.c_int]
+    L.b200_dwf_check_error.argtypes = [vp, vp]
+    L.b200_dwf_inject_wait_failure.argtypes = [vp, ctypes.c_int]
     L.b200_field_axpby.argtypes = [vp, ctypes.c_int, vp, ctypes.c_double, vp, ctypes.c_double, vp]
     L.b200_field_norm2.argtypes = [vp, ctypes.c_int, vp, dp, vp]
     L.b200_field_dot.argtypes = [vp, ctypes.c_int, vp, vp, dp, vp]
@@ -219,6 +222,21 @@ class DomainWall:
     def mult_dag(self, v, w, mode=None):
         check(lib().b200_dwf_mult(self.handle, w.prec, v.ptr, w.ptr,
                                   (mode or self.mode).encode(), 1, None))
+
+    def set_async(self, flag):
+        """Asynchronous mult/force calls (errors surface at the next
+        synchronising call or check_error); default synchronous."""
+        check(lib().b200_dwf_set_async(self.handle, int(bool(flag))))
+
+    def check_error(self):
+        """Wait for the work queued so far and raise if a hop kernel gave up
+        waiting for its bulk copies."""
+        check(lib().b200_dwf_check_error(self.handle, None))
+
+    def inject_wait_failure(self, direction):
+        """Test hook: TMA-fed hops treat their wait for hop direction
+        `direction` (0..7) as timed out; -1 switches it off."""
+        check(lib().b200_dwf_inject_wait_failure(self.handle, int(direction)))
 
     # AField BLAS -------------------------------------------------------
     def axpby(self, y, a, x, b):

@@ -338,7 +338,10 @@ struct HopParams {
   const double* c_x2_dev;
   const double* c_x3_dev;
   double* red;           // per-block partials of |o1|^2 (nullable)
-  int* err;              // device error word: set when a bounded wait gives up
+  int* err;              // device error word: 1 when a bounded wait gave up, 2 when the
+                         // drain of the copies still in flight gave up as well
+  int fail_dir;          // host-set test hook: the wait for this hop direction (0..7)
+                         // reports failure as if its bound had run out (-1: none)
   unsigned int wait_ns;  // suspend-time hint of the TMA kernels' mbarrier tries (0: none)
   const double* skip;    // when non-null and *skip != 0 the launch does nothing
                          // (lets a captured solver iteration replay as a no-op)
@@ -974,6 +977,17 @@ inline int hop_pair_grid(int ls, int vh) {
 // flight, without holding registers.  Stage buffers are reused after the
 // warp's lanes have finished reading them (__syncwarp + proxy fence).
 // All waits are bounded; on timeout the kernel sets p.err and skips its work.
+// After a failed wait: wait for the stages this warp issued but has not seen
+// complete (directions ndone .. nissued-1), each with the drain bound; if even
+// that runs out, the error word says so (2).
+template <int S>
+__device__ __forceinline__ void drain_copies(uint64_t* bars, int ndone, int nissued, int lane, int* err) {
+  bool all = true;
+  for (int d = ndone; d < nissued; ++d)
+    all = mbar_wait_drain(smem_u32(&bars[d % S]), (d / S) & 1) && all;
+  if (!__all_sync(0xffffffffu, all) && lane == 0 && err) atomicExch(err, 2);
+}
+
 template <int LS, int P, int LF, int GS = 32 / LS> struct TmaGeom {
   static constexpr int G = GS;              // sites per warp
   static constexpr int COL = (int)Store<P>::col_bytes(LS);
@@ -1096,7 +1110,8 @@ dwf_hop_tma_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename
     constexpr int st = (D) % S;                                                      \
     const uint32_t parity = ((D) / S) & 1;                                           \
     if (ok) {                                                                        \
-      const bool got = mbar_wait_bounded(smem_u32(&bars[warp][st]), parity, p.wait_ns); \
+      const bool got = ((D) != p.fail_dir) &&                                      \
+                       mbar_wait_bounded(smem_u32(&bars[warp][st]), parity, p.wait_ns); \
       ok = __all_sync(0xffffffffu, got);                                             \
       if (ok) ndone = (D) + 1;                                                       \
       else if (lane == 0 && p.err) atomicExch(p.err, 1);                             \
@@ -1137,13 +1152,11 @@ dwf_hop_tma_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename
   B200_TMA_STEP(7, 3, -1)
 #undef B200_TMA_STEP
 
-  // A warp that gave up waits (again bounded) for the copies it still has in
-  // flight, then the whole CTA returns without touching its outputs; the host
-  // sees p.err.
-  if (!ok) {
-    for (int d = ndone; d < nissued; ++d)
-      mbar_wait_bounded(smem_u32(&bars[warp][d % S]), (d / S) & 1, p.wait_ns);
-  }
+  // A warp that gave up waits for the copies it still has in flight (with a
+  // bound far longer than the first wait's, so that no bulk copy is left
+  // writing into shared memory when the CTA exits), then the whole CTA
+  // returns without touching its outputs; the host sees p.err.
+  if (!ok) drain_copies<S>(&bars[warp][0], ndone, nissued, lane, p.err);
   if (!__syncthreads_and(ok ? 1 : 0)) return;
   hop_epilogue<LS, P, EPI, FK>(p, k, acc, reinterpret_cast<R*>(wbase), red_warp, tid, lane, warp, g, s,
                                site, active);
@@ -1259,7 +1272,8 @@ dwf_hop_tma_pair_kernel(const HopParams p, const __grid_constant__ ChainCoef<typ
     constexpr int st = (D) % S;                                                      \
     const uint32_t parity = ((D) / S) & 1;                                           \
     if (ok) {                                                                        \
-      const bool got = mbar_wait_bounded(smem_u32(&bars[warp][st]), parity, p.wait_ns); \
+      const bool got = ((D) != p.fail_dir) &&                                      \
+                       mbar_wait_bounded(smem_u32(&bars[warp][st]), parity, p.wait_ns); \
       ok = __all_sync(0xffffffffu, got);                                             \
       if (ok) ndone = (D) + 1;                                                       \
       else if (lane == 0 && p.err) atomicExch(p.err, 1);                             \
@@ -1304,10 +1318,7 @@ dwf_hop_tma_pair_kernel(const HopParams p, const __grid_constant__ ChainCoef<typ
   B200_TMAP_STEP(7, 3, -1)
 #undef B200_TMAP_STEP
 
-  if (!ok) {
-    for (int d = ndone; d < nissued; ++d)
-      mbar_wait_bounded(smem_u32(&bars[warp][d % S]), (d / S) & 1, p.wait_ns);
-  }
+  if (!ok) drain_copies<S>(&bars[warp][0], ndone, nissued, lane, p.err);
   if (!__syncthreads_and(ok ? 1 : 0)) return;
   float rows[2][24];
 #pragma unroll

@@ -157,6 +157,8 @@ struct b200_dwf {
   double* sc = nullptr;         // solver scalars (device)
   double* sc_host = nullptr;    // pinned mirror (also of the multishift scalars)
   int* err_host = nullptr;      // pinned mirror of err
+  bool async_calls = false;     // mult / force return without synchronising (b200_dwf_set_async)
+  int inject_dir = -1;          // hop direction whose bulk-copy wait reports failure (-1: none)
   double* stage = nullptr;      // device f64 staging for convert/reverse
   Workspace* ws = nullptr;      // shared per-call workspace of this geometry
   void* (*work)[4] = nullptr;   // = ws->work: work fields per slot and precision
@@ -230,6 +232,7 @@ HopParams hop_base(const b200_dwf* op, int prec, int ieo, int epi, int fk = F_NO
   p.ieo = ieo;
   p.ce = 1.0;
   p.err = op->err;
+  p.fail_dir = op->inject_dir;
   p.wait_ns = wait_hint_ns();
   for (int mu = 0; mu < 4; ++mu) p.bc[mu] = op->bc[mu];
   return p;
@@ -281,6 +284,7 @@ int tune_hop(b200_dwf* op, int prec, const HopParams& p0, cudaStream_t st, int* 
         return fail(B200_ENOMEM, "cudaMalloc for autotuner scratch failed");
     }
   HopParams p = p0;
+  p.fail_dir = -1;   // the trials time real launches
   if (p.out1) p.out1 = op->tune_out[0][prec];
   if (p.out2) p.out2 = op->tune_out[1][prec];
   cudaEvent_t a, b;
@@ -460,15 +464,45 @@ int reduce_to(b200_dwf* op, int nblocks, double* out_dev, int fin_op, cudaStream
   return 0;
 }
 
+// The device error word of the bounded bulk-copy waits, after the stream has
+// been synchronised with err_host's copy in it: report a set word as
+// B200_ECUDA and clear it, so that the next call starts clean.  The hop that
+// gave up returned without writing its outputs.
+int report_err(b200_dwf* op, cudaStream_t st) {
+  const int code = *op->err_host;
+  if (code == 0) return 0;
+  *op->err_host = 0;
+  B200_CHECK_CUDA(cudaMemsetAsync(op->err, 0, sizeof(int), st));
+  B200_CHECK_CUDA(cudaStreamSynchronize(st));
+  return fail(B200_ECUDA,
+              "a hop kernel gave up waiting for its bulk copies (device error word %d); "
+              "its outputs were not written",
+              code);
+}
+
+// Synchronises the stream, then reads, reports and clears the error word.
+int check_err(b200_dwf* op, cudaStream_t st) {
+  B200_CHECK_CUDA(cudaMemcpyAsync(op->err_host, op->err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  B200_CHECK_CUDA(cudaStreamSynchronize(st));
+  return report_err(op, st);
+}
+
+// The end of a call that launched hops: synchronous plans (the reference's
+// behaviour, the default) wait for the work and report the error word; plans
+// switched to asynchronous calls leave that to the next synchronising call.
+int finish_call(b200_dwf* op, int rc, cudaStream_t st) {
+  if (rc || op->async_calls) return rc;
+  return check_err(op, st);
+}
+
 // Reads one solver scalar (and the device error word) back to the host.
 int host_scalar(b200_dwf* op, int idx, double* out, cudaStream_t st) {
   B200_CHECK_CUDA(cudaMemcpyAsync(op->sc_host + idx, op->sc + idx, sizeof(double),
                                   cudaMemcpyDeviceToHost, st));
   B200_CHECK_CUDA(cudaMemcpyAsync(op->err_host, op->err, sizeof(int), cudaMemcpyDeviceToHost, st));
   B200_CHECK_CUDA(cudaStreamSynchronize(st));
-  if (*op->err_host != 0)
-    return fail(B200_ECUDA, "a kernel gave up waiting for its bulk copies (device error word %d)",
-                *op->err_host);
+  int rc = report_err(op, st);
+  if (rc) return rc;
   *out = op->sc_host[idx];
   return 0;
 }
@@ -666,8 +700,11 @@ int b200_field_reverse(b200_dwf_t* op, int prec, double* v_host, const void* w, 
     return fail(B200_ENOMEM, "cudaMalloc for the staging field failed");
   B200_CHECK_CUDA(launch_to_corelib(prec, op->stage, w, op->g, st));
   B200_CHECK_CUDA(cudaMemcpyAsync(v_host, op->stage, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+  // the field read back may come from asynchronous hop calls on this plan:
+  // their error word is reported here
+  B200_CHECK_CUDA(cudaMemcpyAsync(op->err_host, op->err, sizeof(int), cudaMemcpyDeviceToHost, st));
   B200_CHECK_CUDA(cudaStreamSynchronize(st));
-  return 0;
+  return report_err(op, st);
 }
 
 int b200_dwf_mult(b200_dwf_t* op, int prec, void* v, const void* w, const char* mode, int dag,
@@ -675,7 +712,26 @@ int b200_dwf_mult(b200_dwf_t* op, int prec, void* v, const void* w, const char* 
   if (!op || !v || !w || !mode || prec < 0 || prec > 3) return fail(B200_EINVAL, "invalid argument");
   if (v == w) return fail(B200_EINVAL, "mult: input and output fields must differ");
   if (misaligned(v) || misaligned(w)) return fail(B200_EINVAL, "mult: field pointers must be 16-byte aligned");
-  return apply_mode(op, prec, v, w, mode, dag, (cudaStream_t)stream);
+  cudaStream_t st = (cudaStream_t)stream;
+  return finish_call(op, apply_mode(op, prec, v, w, mode, dag, st), st);
+}
+
+int b200_dwf_set_async(b200_dwf_t* op, int async_calls) {
+  if (!op) return fail(B200_EINVAL, "null operator");
+  op->async_calls = async_calls != 0;
+  return 0;
+}
+
+int b200_dwf_check_error(b200_dwf_t* op, void* stream) {
+  if (!op) return fail(B200_EINVAL, "null operator");
+  return check_err(op, (cudaStream_t)stream);
+}
+
+int b200_dwf_inject_wait_failure(b200_dwf_t* op, int direction) {
+  if (!op) return fail(B200_EINVAL, "null operator");
+  if (direction < -1 || direction > 7) return fail(B200_EINVAL, "hop direction %d not in -1..7", direction);
+  op->inject_dir = direction;
+  return 0;
 }
 
 int b200_field_axpby(b200_dwf_t* op, int prec, void* y, double a, const void* x, double b,
@@ -1014,9 +1070,8 @@ int b200_shiftcg_solve(b200_dwf_t* op, void* const* x, const double* sigma, int 
                                     cudaMemcpyDeviceToHost, s));
     B200_CHECK_CUDA(cudaMemcpyAsync(op->err_host, op->err, sizeof(int), cudaMemcpyDeviceToHost, s));
     B200_CHECK_CUDA(cudaStreamSynchronize(s));
-    if (*op->err_host != 0)
-      return fail(B200_ECUDA, "a kernel gave up waiting for its bulk copies (device error word %d)",
-                  *op->err_host);
+    int rc_err = report_err(op, s);
+    if (rc_err) return rc_err;
     *done = op->sc_host[MS_DONE];
     *iters = op->sc_host[MS_ITER];
     *rr_out = op->sc_host[MS_RR];
@@ -1376,16 +1431,19 @@ int b200_dwf_force_udiv1(b200_dwf_t* op, const char* mode, double* force, const 
   if (mode && std::string(mode) == "DdagD")
     return fail(B200_EINVAL, "%s: unknown mode %s", "Force_F_Domainwall_eo", mode);
   if (!b) return fail(B200_EINVAL, "invalid argument");
-  return force_impl(op, mode, force, a, b, 1.0, 0.0, (cudaStream_t)stream);
+  cudaStream_t st = (cudaStream_t)stream;
+  return finish_call(op, force_impl(op, mode, force, a, b, 1.0, 0.0, st), st);
 }
 
 int b200_dwf_force_udiv(b200_dwf_t* op, double* force, const void* eta, void* stream) {
-  return force_impl(op, "DdagD", force, eta, nullptr, 1.0, 0.0, (cudaStream_t)stream);
+  cudaStream_t st = (cudaStream_t)stream;
+  return finish_call(op, force_impl(op, "DdagD", force, eta, nullptr, 1.0, 0.0, st), st);
 }
 
 int b200_dwf_force_acc(b200_dwf_t* op, const char* mode, double* force, const void* a,
                        const void* b, double scale, void* stream) {
-  return force_impl(op, mode, force, a, b, scale, 1.0, (cudaStream_t)stream);
+  cudaStream_t st = (cudaStream_t)stream;
+  return finish_call(op, force_impl(op, mode, force, a, b, scale, 1.0, st), st);
 }
 
 int b200_tuning_table(char* buf, size_t n) {

@@ -3,12 +3,13 @@
 //
 // Who needs it: code that runs where cudaMalloc is forbidden or unsafe -- a
 // host framework that owns all device memory through its own pool and counts
-// on libraries not to allocate behind its back, code that runs between the
-// begin and end of a CUDA graph capture (an allocation would break the
-// capture), or a caller on a GPU whose memory is already fully committed.
-// Such a caller cannot create an operator plan (which owns its reduction
-// scratch), so it gets this one entry point that takes only the field and its
-// size and returns the norm.
+// on libraries not to allocate behind its back (an allocation outside the pool
+// can fail, or fragment and exhaust what the pool planned for), or a caller on
+// a GPU whose memory is already fully committed to resident gauge and fermion
+// fields (at 24^3x48 Ls=16 a multishift solve alone holds ~35 GB).  Such a
+// caller cannot create an operator plan (which owns its reduction scratch), so
+// it gets this one entry point that takes only the field and its size and
+// returns the norm.
 //
 // The block partial sums live in a file-scope __device__ array of fixed size
 // (kNoallocMaxBlocks doubles + one result slot, 512 KiB), which every GPU

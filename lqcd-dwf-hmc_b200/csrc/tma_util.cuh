@@ -78,6 +78,20 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity,
   return false;
 }
 
+// The wait of the error path: copies that were issued must land before the
+// CTA exits, so this bound is far longer (2^26 tries or 20 s of global time).
+__device__ __forceinline__ bool mbar_wait_drain(uint32_t bar, uint32_t parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  constexpr int kMaxTries = 1 << 26;
+  constexpr uint64_t kMaxNs = 20000000000ull;
+  const uint64_t t0 = global_ns();
+  for (int i = 0; i < kMaxTries; ++i) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (global_ns() - t0 > kMaxNs) return false;
+  }
+  return false;
+}
+
 // Order earlier generic-proxy accesses of shared memory before later
 // asynchronous-proxy (bulk copy) writes to the same addresses.
 __device__ __forceinline__ void fence_proxy_async_smem() {

@@ -101,6 +101,39 @@ def test_cg_f64_matches_oracle():
     assert rel(dev.reverse(fx), xr) < 1e-10
 
 
+# Every FP64 hop variant the autotuner may pick (direct loads at two register
+# budgets, bulk-copy pipelines of 2 / 3 / 4 stages, 2 stages at 128
+# registers), pinned with B200_HOP_VARIANT so that the result never depends on
+# which one was fastest on the test machine.
+FP64_VARIANTS = [0, 1, 2, 3, 4, 7]
+
+
+@pytest.mark.parametrize("variant", FP64_VARIANTS)
+@pytest.mark.parametrize("ci", [1, 3, 4])          # Ls = 8, 12, 16
+def test_fp64_hop_variants_all_modes(variant, ci, monkeypatch):
+    """Each FP64 hop variant on all 13 modes x dag against the oracle at the
+    reference's 1e-13, for an Ls that divides 32 (8, 16) and one that does
+    not (12), plus one FP64 CG solve on the pinned variant."""
+    monkeypatch.setenv("B200_HOP_VARIANT", str(variant))
+    case = CASES[ci]
+    ora, dev = make(case, 20 + ci)
+    w = synth.spinor_field(case[0], case[1], 31 + ci)
+    fw, fv = dev.new_field(0), dev.new_field(0)
+    dev.convert(fw, w)
+    for mode in MODES:
+        for dag in (False, True):
+            (dev.mult_dag if dag else dev.mult)(fv, fw, mode)
+            ref = ora.mult(mode, w, dag)
+            err = rel(dev.reverse(fv), ref)
+            assert err < TOL[0], (variant, mode, dag, err)
+    fx = dev.new_field(0)
+    nconv, diff, rc = dev.cg(fx, fw, 1e-24, 3000)
+    assert rc == 0
+    xr, nr, _, rcr = ora.cg(w, 1e-24, 3000)
+    assert rcr == 0 and abs(nconv - nr) <= 2, (variant, nconv, nr)
+    assert rel(dev.reverse(fx), xr) < 1e-10
+
+
 @pytest.mark.parametrize("variant", [5, 6, 7, 8, 9])
 @pytest.mark.parametrize("ci", [1, 4])
 def test_packed_variants_reduced_precision(variant, ci):
