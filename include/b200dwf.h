@@ -85,6 +85,17 @@ int b200_field_convert(b200_dwf_t *op, int prec, void *v_dev, const double *w_ho
                        void *stream);
 int b200_field_reverse(b200_dwf_t *op, int prec, double *v_host, const void *w_dev,
                        void *stream);   /* also reports the plan's error word */
+/* Asynchronous convert / reverse for pipelined host transfers (no reference
+ * counterpart: the reference's convert/reverse are synchronous).  The host
+ * field must be page-locked and stay untouched until `stream` has passed the
+ * call.  Each direction has a ring of two device staging fields; a slot is
+ * reused only after its previous transfer finished (a device-side wait), so
+ * an upload on one stream and a download on another overlap on the two
+ * copy directions. */
+int b200_field_convert_async(b200_dwf_t *op, int prec, void *v_dev, const double *w_host,
+                             void *stream);
+int b200_field_reverse_async(b200_dwf_t *op, int prec, double *v_host, const void *w_dev,
+                             void *stream);
 /* convert() from a field already on the device (w_dev: reference layout,
  * 24 * Nvol/2 * Ls doubles), asynchronous on `stream`: the heatbath noise
  * drawn by b200_rng_gauss_lex goes to the operator without a host copy. */

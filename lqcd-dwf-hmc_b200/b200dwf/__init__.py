@@ -56,6 +56,8 @@ def lib():
     L.b200_field_convert.argtypes = [vp, ctypes.c_int, vp, dp, vp]
     L.b200_field_reverse.argtypes = [vp, ctypes.c_int, dp, vp, vp]
     L.b200_field_convert_device.argtypes = [vp, ctypes.c_int, vp, vp, vp]
+    L.b200_field_convert_async.argtypes = [vp, ctypes.c_int, vp, vp, vp]
+    L.b200_field_reverse_async.argtypes = [vp, ctypes.c_int, vp, vp, vp]
     L.b200_dwf_mult.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_char_p, ctypes.c_int, vp]
     L.b200_dwf_set_async.argtypes = [vp, ctypes.c_int]
     L.b200_dwf_check_error.argtypes = [vp, vp]
@@ -132,6 +134,11 @@ def tuning_table():
 
 def _dp(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _stream(s):
+    """ctypes handle of a torch.cuda.Stream (None: the legacy default stream)."""
+    return None if s is None else ctypes.c_void_p(s.cuda_stream)
 
 
 class Field:
@@ -215,13 +222,28 @@ class DomainWall:
         check(lib().b200_field_reverse(self.handle, w.prec, _dp(out), w.ptr, None))
         return out
 
-    def mult(self, v, w, mode=None):
+    def mult(self, v, w, mode=None, stream=None):
         check(lib().b200_dwf_mult(self.handle, w.prec, v.ptr, w.ptr,
-                                  (mode or self.mode).encode(), 0, None))
+                                  (mode or self.mode).encode(), 0, _stream(stream)))
 
-    def mult_dag(self, v, w, mode=None):
+    def mult_dag(self, v, w, mode=None, stream=None):
         check(lib().b200_dwf_mult(self.handle, w.prec, v.ptr, w.ptr,
-                                  (mode or self.mode).encode(), 1, None))
+                                  (mode or self.mode).encode(), 1, _stream(stream)))
+
+    def convert_async(self, v, w_pinned, stream=None):
+        """convert() from a page-locked host array (numpy view of a pinned
+        torch tensor), queued on `stream` (torch.cuda.Stream or None)."""
+        if w_pinned.size != self.nreal or w_pinned.dtype != np.float64:
+            raise B200Error("convert_async needs %d float64 values" % self.nreal)
+        check(lib().b200_field_convert_async(self.handle, v.prec, v.ptr,
+                                             ctypes.c_void_p(w_pinned.ctypes.data), _stream(stream)))
+
+    def reverse_async(self, w, out_pinned, stream=None):
+        """reverse() into a page-locked host array, queued on `stream`."""
+        if out_pinned.size != self.nreal or out_pinned.dtype != np.float64:
+            raise B200Error("reverse_async needs %d float64 values" % self.nreal)
+        check(lib().b200_field_reverse_async(self.handle, w.prec, ctypes.c_void_p(out_pinned.ctypes.data),
+                                             w.ptr, _stream(stream)))
 
     def set_async(self, flag):
         """Asynchronous mult/force calls (errors surface at the next

@@ -32,12 +32,18 @@ def _check_lattice(lattice):
 
 def read_text_4x4x4x8(path, lattice):
     """GaugeConfig("Text_4x4x4x8").read: the 4x4x4x8 file tiled onto lattice."""
+    return tile_text_4x4x4x8(np.loadtxt(path, dtype=np.float64, ndmin=1), lattice, path)
+
+
+def tile_text_4x4x4x8(vals, lattice, name="configuration"):
+    """The numbers of a Text_4x4x4x8 file (site-major [t][z][y][x][mu][18])
+    tiled periodically onto lattice, as the lexical Field_G(Nvol, 4)."""
     lx, ly, lz, lt = _check_lattice(lattice)
     nf = int(np.prod(TEXT_LATTICE))
-    vals = np.loadtxt(path, dtype=np.float64, ndmin=1)
+    vals = np.asarray(vals, dtype=np.float64).reshape(-1)
     if vals.size < nf * 4 * 18:
         raise ValueError("%s: %d numbers, %d needed for a 4x4x4x8 configuration"
-                         % (path, vals.size, nf * 4 * 18))
+                         % (name, vals.size, nf * 4 * 18))
     f = vals[:nf * 72].reshape(TEXT_LATTICE[3], TEXT_LATTICE[2], TEXT_LATTICE[1],
                                 TEXT_LATTICE[0], 4, 18)          # [t][z][y][x][mu][r]
     t = np.arange(lt) % TEXT_LATTICE[3]

@@ -866,15 +866,24 @@ def build_dwf_nf2p1(lattice, Ls, M0, masses, beta, c_plaq=3.648, c_rect=-0.331, 
                     nsmear=2, nstep=(2, 1, 3), level=(0, 0, 1, 2), tau=1.0,
                     lam=0.1931833275, nprec=8, np_md=16, np_h=24, rat_bounds=(1e-2, 3.16227766),
                     tol2_md=1e-20, tol2_h=1e-20, solvers=None, b=1.0, c=0.0,
-                    bc=(1, 1, 1, -1), integrator="Omelyan", shift_window=None):
+                    bc=(1, 1, 1, -1), integrator="Omelyan", shift_window=None,
+                    rational_dir=None, tol2_rat_md=None, tol2_rat_h=None):
     """The benchmark driver's action set (hmc_dwf_eo.cpp:155-352) on the
     device.  masses: dict l (light), h (Hasenbusch), s (strange), pv.
     solvers: dict of Solver objects 'l_md', 'l_h', 'h_md', 'h_h', 'pv_h'
     (default FP64 CG at tol2_md / tol2_h).  shift_window: residual window of
     the multishift solves (None keeps the library default, 0 updates every
-    shift every iteration)."""
+    shift every iteration).  rational_dir: directory of the coefficient files
+    (Math_Rational's format and names; default: this package's tables), as
+    the reference reads them from its run directory.  tol2_rat_md /
+    tol2_rat_h: the multishift tolerances of the rational operators
+    (Fopr_Nf1_Rational_MD / _calcH convergence_criterion_squared; default
+    tol2_md / tol2_h)."""
     from . import DomainWall
-    from .rational import Rational
+    from .rational import Rational, TABLE_DIR
+    tdir = rational_dir or TABLE_DIR
+    tol2_rat_md = tol2_md if tol2_rat_md is None else tol2_rat_md
+    tol2_rat_h = tol2_h if tol2_rat_h is None else tol2_rat_h
     dr = DirectorSmear(lattice, rho, nsmear)
 
     def fopr(m):
@@ -884,9 +893,11 @@ def build_dwf_nf2p1(lattice, Ls, M0, masses, beta, c_plaq=3.648, c_rect=-0.331, 
         return FoprSmeared(op, dr)
 
     lo, hi = rat_bounds
-    rats = dict(md_numer=Rational(np_md, 1, 4, lo, hi), md_denom=Rational(np_md, -1, 2, lo, hi),
-                h_numer=Rational(np_h, 1, 4, lo, hi), h_denom=Rational(np_h, -1, 2, lo, hi),
-                psf_denom=Rational(np_h, 1, 4, lo, hi), psf_numer=Rational(np_h, -1, 4, lo, hi))
+    rats = dict(md_numer=Rational(np_md, 1, 4, lo, hi, tdir),
+                md_denom=Rational(np_md, -1, 2, lo, hi, tdir),
+                h_numer=Rational(np_h, 1, 4, lo, hi, tdir), h_denom=Rational(np_h, -1, 2, lo, hi, tdir),
+                psf_denom=Rational(np_h, 1, 4, lo, hi, tdir),
+                psf_numer=Rational(np_h, -1, 4, lo, hi, tdir))
     # one operator per distinct mass: the Pauli-Villars operator serves the
     # rational ratio and the outer Hasenbusch ratio alike
     f_s, f_l, f_h, f_pv = (fopr(masses[k]) for k in ("s", "l", "h", "pv"))
@@ -895,7 +906,7 @@ def build_dwf_nf2p1(lattice, Ls, M0, masses, beta, c_plaq=3.648, c_rect=-0.331, 
     for k, t in (("l_md", tol2_md), ("h_md", tol2_md), ("l_h", tol2_h), ("h_h", tol2_h),
                  ("pv_h", tol2_h)):
         sv.setdefault(k, Solver("cg", t))
-    nf1 = ActionFRationalRatio(f_pv1, f_s, rats, tol2_md, tol2_h, "Nf1")
+    nf1 = ActionFRationalRatio(f_pv1, f_s, rats, tol2_rat_md, tol2_rat_h, "Nf1")
     nf2 = ActionFRatio(f_h, f_l, sv["l_md"], sv["l_h"], sv["h_h"], "Nf2")
     nf2p = ActionFRatio(f_pv, f_h, sv["h_md"], sv["h_h"], sv["pv_h"], "Nf2_prec")
     gauge = ActionGRectangle(lattice, beta, c_plaq, c_rect)

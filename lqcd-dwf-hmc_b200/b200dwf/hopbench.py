@@ -1,0 +1,74 @@
+"""Time one operator mode of the even/odd domain-wall operator.
+
+    python -m b200dwf.hopbench --lattice 16 16 16 32 --ls 16 --prec f16 \
+        --mode Deo --dag --reps 50 [--variant N] [--warmup 5]
+
+Builds the operator on seeded near-unit links (exp(i*0.3*H), no smearing:
+timing does not depend on it), converts a Gaussian field into the chosen
+storage precision, and times `reps` calls of mult / mult_dag with CUDA events
+on the stream they run on.  Prints one JSON line: microseconds per call, and
+for the single-hop modes (Deo, Doe) the fused hop's algorithmic bytes per
+call and GB/s,
+    B = Vh * (Ls * 2 * s_spinor + 8 * s_link)
+with s_spinor the stored bytes of one (site, s) spinor (f64 192, f32 96,
+f16/bf16 48 + a 4-byte scale) and s_link the bytes of one link record (f64
+144, f32 80, f16/bf16 48).  --variant pins the hop kernel variant
+(B200_HOP_VARIANT) instead of the autotuner's choice."""
+import argparse
+import json
+import os
+
+import numpy as np
+
+SPINOR_BYTES = {0: 192, 1: 96, 2: 52, 3: 52}
+LINK_BYTES = {0: 144, 1: 80, 2: 48, 3: 48}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--lattice", type=int, nargs=4, default=[16, 16, 16, 32])
+    ap.add_argument("--ls", type=int, default=16)
+    ap.add_argument("--prec", default="f64", choices=["f64", "f32", "f16", "bf16"])
+    ap.add_argument("--mode", default="Deo")
+    ap.add_argument("--dag", action="store_true")
+    ap.add_argument("--reps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--variant", type=int, default=None)
+    ap.add_argument("--mq", type=float, default=0.01)
+    ap.add_argument("--m0", type=float, default=1.8)
+    a = ap.parse_args(argv)
+    if a.variant is not None:
+        os.environ["B200_HOP_VARIANT"] = str(a.variant)
+    import torch
+    import b200dwf
+    from b200dwf import synth
+    prec = b200dwf.PREC_NAMES[a.prec]
+    op = b200dwf.DomainWall(a.lattice, a.ls, a.mq, a.m0)
+    op.set_config(synth.gauge_field(a.lattice, 1234567, "near", eps=0.3))
+    w, v = op.new_field(prec), op.new_field(prec)
+    op.convert(w, synth.spinor_field(a.lattice, a.ls, 7654321))
+    call = op.mult_dag if a.dag else op.mult
+    op.set_async(True)
+    for _ in range(a.warmup):
+        call(v, w, a.mode)
+    op.check_error()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.reps):
+        call(v, w, a.mode)
+    e1.record()
+    torch.cuda.synchronize()
+    op.check_error()
+    us = e0.elapsed_time(e1) * 1e3 / a.reps
+    out = {"lattice": a.lattice, "Ls": a.ls, "prec": a.prec, "mode": a.mode, "dag": a.dag,
+           "variant": a.variant, "us_per_call": us}
+    if a.mode in ("Deo", "Doe"):
+        vh = int(np.prod(a.lattice)) // 2
+        nbytes = vh * (a.ls * 2 * SPINOR_BYTES[prec] + 8 * LINK_BYTES[prec])
+        out.update(bytes_per_call=nbytes, gbs=nbytes / (us * 1e-6) / 1e9)
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

@@ -160,6 +160,11 @@ struct b200_dwf {
   bool async_calls = false;     // mult / force return without synchronising (b200_dwf_set_async)
   int inject_dir = -1;          // hop direction whose bulk-copy wait reports failure (-1: none)
   double* stage = nullptr;      // device f64 staging for convert/reverse
+  // staging rings of the asynchronous host transfers (upload, download): a
+  // slot is reused only after the event of its previous use has fired
+  double* ring_buf[2][2] = {};
+  cudaEvent_t ring_done[2][2] = {};
+  int ring_next[2] = {0, 0};
   Workspace* ws = nullptr;      // shared per-call workspace of this geometry
   void* (*work)[4] = nullptr;   // = ws->work: work fields per slot and precision
   void* tune_out[2][4] = {};    // autotuner scratch outputs per precision
@@ -628,6 +633,11 @@ int b200_dwf_destroy(b200_dwf_t* op) {
   if (op->sc_host) cudaFreeHost(op->sc_host);
   if (op->err_host) cudaFreeHost(op->err_host);
   cudaFree(op->stage);
+  for (int d = 0; d < 2; ++d)
+    for (int k = 0; k < 2; ++k) {
+      cudaFree(op->ring_buf[d][k]);
+      if (op->ring_done[d][k]) cudaEventDestroy(op->ring_done[d][k]);
+    }
   cudaFree(op->ms_state);
   cudaFree(op->ms_red);
   cudaFree(op->ms_ptrs);
@@ -683,6 +693,62 @@ int b200_field_convert(b200_dwf_t* op, int prec, void* v, const double* w_host, 
   B200_CHECK_CUDA(cudaMemcpyAsync(op->stage, w_host, n * sizeof(double), cudaMemcpyHostToDevice, st));
   B200_CHECK_CUDA(launch_from_corelib(prec, v, op->stage, op->g, st));
   B200_CHECK_CUDA(cudaStreamSynchronize(st));
+  return 0;
+}
+
+// A staging slot of ring dir (0 upload, 1 download) for `st`: allocated on
+// first use; later uses wait on the device for the slot's previous use.
+static int ring_slot(b200_dwf_t* op, int dir, cudaStream_t st, int* slot) {
+  const int k = op->ring_next[dir];
+  op->ring_next[dir] = (k + 1) % 2;
+  if (!op->ring_buf[dir][k]) {
+    const size_t bytes = b200_dwf_field_nreal(op) * sizeof(double);
+    if (cudaMalloc(&op->ring_buf[dir][k], bytes) != cudaSuccess) {
+      op->ring_buf[dir][k] = nullptr;
+      return fail(B200_ENOMEM, "cudaMalloc of %zu bytes for a transfer staging field failed", bytes);
+    }
+    B200_CHECK_CUDA(cudaEventCreateWithFlags(&op->ring_done[dir][k], cudaEventDisableTiming));
+  } else {
+    B200_CHECK_CUDA(cudaStreamWaitEvent(st, op->ring_done[dir][k], 0));
+  }
+  *slot = k;
+  return 0;
+}
+
+static bool page_locked(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+int b200_field_convert_async(b200_dwf_t* op, int prec, void* v, const double* w_host, void* stream) {
+  if (!op || !v || !w_host || prec < 0 || prec > 3) return fail(B200_EINVAL, "invalid argument");
+  if (!page_locked(w_host))
+    return fail(B200_EINVAL, "convert_async: the host field must be page-locked (cudaHostAlloc / cudaHostRegister)");
+  cudaStream_t st = (cudaStream_t)stream;
+  int k = 0, rc = ring_slot(op, 0, st, &k);
+  if (rc) return rc;
+  const size_t bytes = b200_dwf_field_nreal(op) * sizeof(double);
+  B200_CHECK_CUDA(cudaMemcpyAsync(op->ring_buf[0][k], w_host, bytes, cudaMemcpyHostToDevice, st));
+  B200_CHECK_CUDA(launch_from_corelib(prec, v, op->ring_buf[0][k], op->g, st));
+  B200_CHECK_CUDA(cudaEventRecord(op->ring_done[0][k], st));
+  return 0;
+}
+
+int b200_field_reverse_async(b200_dwf_t* op, int prec, double* v_host, const void* w, void* stream) {
+  if (!op || !v_host || !w || prec < 0 || prec > 3) return fail(B200_EINVAL, "invalid argument");
+  if (!page_locked(v_host))
+    return fail(B200_EINVAL, "reverse_async: the host field must be page-locked (cudaHostAlloc / cudaHostRegister)");
+  cudaStream_t st = (cudaStream_t)stream;
+  int k = 0, rc = ring_slot(op, 1, st, &k);
+  if (rc) return rc;
+  const size_t bytes = b200_dwf_field_nreal(op) * sizeof(double);
+  B200_CHECK_CUDA(launch_to_corelib(prec, op->ring_buf[1][k], w, op->g, st));
+  B200_CHECK_CUDA(cudaMemcpyAsync(v_host, op->ring_buf[1][k], bytes, cudaMemcpyDeviceToHost, st));
+  B200_CHECK_CUDA(cudaEventRecord(op->ring_done[1][k], st));
   return 0;
 }
 

@@ -137,33 +137,30 @@ __global__ void gauge_action_kernel(const double* u, LexGeom g, double* partial)
   if (threadIdx.x == 0) { partial[2 * blockIdx.x] = sp[0]; partial[2 * blockIdx.x + 1] = sr[0]; }
 }
 
-// Mat_SU_N::reunit_SU3: normalise row 1, orthogonalise and normalise row 2,
-// row 3 = conj(row1 x row2)
-__device__ void reunit3(M3& a) {
-  double* v = reinterpret_cast<double*>(a.m);
-  const double sn1 = 1.0 / sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2] + v[3] * v[3] + v[4] * v[4] + v[5] * v[5]);
-  double r[18];
+// Back onto SU(3) after the link update, as Mat_SU_N::reunit_SU3 does
+// (src/lib/Tools/mat_SU_N.cpp:18-88): Gram-Schmidt on the first two rows,
+// then the third row completes a unit-determinant matrix.  With rows a, b:
+//   a <- a / |a|;   b <- b - <a, b> a,  b <- b / |b|;   c = conj(a x b).
+__device__ void reunit3(M3& m) {
+  Cx* a = m.m;
+  Cx* b = m.m + 3;
+  Cx* c = m.m + 6;
+  const double ia = 1.0 / sqrt(a[0].r * a[0].r + a[0].i * a[0].i + a[1].r * a[1].r + a[1].i * a[1].i +
+                               a[2].r * a[2].r + a[2].i * a[2].i);
 #pragma unroll
-  for (int k = 0; k < 18; ++k) r[k] = v[k];
+  for (int j = 0; j < 3; ++j) a[j] = ia * a[j];
+  const Cx ab = conj(a[0]) * b[0] + conj(a[1]) * b[1] + conj(a[2]) * b[2];   // <a, b>
 #pragma unroll
-  for (int k = 0; k < 6; ++k) v[k] = r[k] * sn1;
-  const double sp1r = v[0] * r[6] + v[1] * r[7] + v[2] * r[8] + v[3] * r[9] + v[4] * r[10] + v[5] * r[11];
-  const double sp1i = v[0] * r[7] - v[1] * r[6] + v[2] * r[9] - v[3] * r[8] + v[4] * r[11] - v[5] * r[10];
-  v[6] = r[6] - sp1r * v[0] + sp1i * v[1];
-  v[7] = r[7] - sp1r * v[1] - sp1i * v[0];
-  v[8] = r[8] - sp1r * v[2] + sp1i * v[3];
-  v[9] = r[9] - sp1r * v[3] - sp1i * v[2];
-  v[10] = r[10] - sp1r * v[4] + sp1i * v[5];
-  v[11] = r[11] - sp1r * v[5] - sp1i * v[4];
-  const double sn2 = 1.0 / sqrt(v[6] * v[6] + v[7] * v[7] + v[8] * v[8] + v[9] * v[9] + v[10] * v[10] + v[11] * v[11]);
+  for (int j = 0; j < 3; ++j) b[j] = b[j] - ab * a[j];
+  const double ib = 1.0 / sqrt(b[0].r * b[0].r + b[0].i * b[0].i + b[1].r * b[1].r + b[1].i * b[1].i +
+                               b[2].r * b[2].r + b[2].i * b[2].i);
 #pragma unroll
-  for (int k = 6; k < 12; ++k) v[k] *= sn2;
-  v[12] = v[2] * v[10] - v[3] * v[11] - v[4] * v[8] + v[5] * v[9];
-  v[13] = -v[2] * v[11] - v[3] * v[10] + v[4] * v[9] + v[5] * v[8];
-  v[14] = v[4] * v[6] - v[5] * v[7] - v[0] * v[10] + v[1] * v[11];
-  v[15] = -v[4] * v[7] - v[5] * v[6] + v[0] * v[11] + v[1] * v[10];
-  v[16] = v[0] * v[8] - v[1] * v[9] - v[2] * v[6] + v[3] * v[7];
-  v[17] = -v[0] * v[9] - v[1] * v[8] + v[2] * v[7] + v[3] * v[6];
+  for (int j = 0; j < 3; ++j) b[j] = ib * b[j];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    const int k = (j + 1) % 3, l = (j + 2) % 3;
+    c[j] = conj(a[k] * b[l] - a[l] * b[k]);
+  }
 }
 
 // u <- reunit( (u + a iP (u + a/2 iP ( ... (u + a/n iP u) ...))) ), n = nprec

@@ -42,50 +42,144 @@ __device__ M3 staple_sum(const double* u, const LexGeom& g, size_t site, int mu,
   return c;
 }
 
-__device__ __forceinline__ double xi0f(double w) { return (w == 0.0) ? 1.0 : sin(w) / w; }
-__device__ __forceinline__ double xi1f(double w) {
-  if (w < 0.25) {
-    const double w2 = w * w;
-    const double c0 = -1.0 / 3.0, c1 = 1.0 / 30.0, c2 = -1.0 / 840.0, c3 = 1.0 / 45360.0,
-                 c4 = -1.0 / 3991680.0;
-    return c0 + w2 * (c1 + w2 * (c2 + w2 * (c3 + w2 * c4)));
+// ---------------------------------------------------------------------------
+// exp(iQ) of a traceless Hermitian 3x3 matrix Q by the Cayley-Hamilton
+// theorem, after C. Morningstar and M. Peardon, "Analytic smearing of SU(3)
+// link variables in lattice QCD", Phys. Rev. D 69, 054501 (2004), sec. III:
+//   exp(iQ) = f0 + f1 Q + f2 Q^2,
+// the f_j being functions of the two invariants c0 = det Q = tr(Q^3)/3 and
+// c1 = tr(Q^2)/2 only (through the eigenvalue parameters u and w).  The stout
+// force needs their derivatives, B1 = sum_j (df_j/dc1) Q^j and
+// B2 = sum_j (df_j/dc0) Q^j.  The closed forms are evaluated at |c0| (where
+// they are best conditioned) and carried to c0 < 0 by the paper's symmetry
+// f_j(-c0) = (-1)^j conj f_j(c0), whose derivative gives
+// d f_j/dc1 (-c0) = (-1)^j conj(...) and d f_j/dc0 (-c0) = (-1)^(j+1) conj(...).
+// ---------------------------------------------------------------------------
+
+// sin(w)/w
+__device__ __forceinline__ double sinc_w(double w) { return (w == 0.0) ? 1.0 : sin(w) / w; }
+
+// (cos w - sin(w)/w) / w^2 = d/dw (sin(w)/w) / w.  For small w, where the
+// closed form cancels, its Taylor series
+//   sum_m (-1)^(m+1) (2m+2) w^(2m) / (2m+3)!
+// is summed term by term (each term from the previous one).
+__device__ double dsinc_w(double w) {
+  if (w >= 0.5) return (cos(w) - sin(w) / w) / (w * w);
+  const double w2 = w * w;
+  double term = -1.0 / 3.0, sum = 0.0;
+  for (int m = 1; m < 12; ++m) {
+    sum += term;
+    term *= -w2 * (2 * m + 2) / ((double)(2 * m) * (2 * m + 2) * (2 * m + 3));
   }
-  return (w * cos(w) - sin(w)) / (w * w * w);
+  return sum + term;
 }
 
-// Cayley-Hamilton coefficients of exp(iQ) (set_uw, set_fj)
-__device__ void uw_fj(const M3& iQ2, const M3& iQ3, double& u, double& w, Cx& f0, Cx& f1, Cx& f2) {
-  const double c0 = -(iQ3.m[0].i + iQ3.m[4].i + iQ3.m[8].i) / 3.0;
-  const double c1 = -0.5 * (iQ2.m[0].r + iQ2.m[4].r + iQ2.m[8].r);
-  const double c13r = sqrt(c1 / 3.0);
-  const double c0max = 2.0 * c13r * c13r * c13r;
-  const double theta = acos(c0 / c0max);
-  u = c13r * cos(theta / 3.0);
-  w = sqrt(c1) * sin(theta / 3.0);
-  const double xi0 = xi0f(w);
-  const double u2 = u * u, w2 = w * w, cos_w = cos(w);
-  const double cos_u = cos(u), sin_u = sin(u);
-  const Cx emiu = cx(cos_u, -sin_u);
-  const Cx e2iu = cx(cos_u * cos_u - sin_u * sin_u, 2.0 * sin_u * cos_u);
-  const Cx h0 = e2iu * cx(u2 - w2, 0.0) + emiu * cx(8.0 * u2 * cos_w, 2.0 * u * (3.0 * u2 + w2) * xi0);
-  const Cx h1 = e2iu * cx(2 * u, 0.0) - emiu * cx(2.0 * u * cos_w, -(3.0 * u2 - w2) * xi0);
-  const Cx h2 = e2iu - emiu * cx(cos_w, 3.0 * u * xi0);
-  const double fden = 1.0 / (9.0 * u2 - w2);
-  f0 = fden * h0;
-  f1 = fden * h1;
-  f2 = fden * h2;
+struct ExpCoef {
+  Cx f[3];     // exp(iQ) = f0 + f1 Q + f2 Q^2
+  Cx d1[3];    // d f_j / d c1
+  Cx d0[3];    // d f_j / d c0
+};
+
+__device__ __forceinline__ Cx expi(double a) { return cx(cos(a), sin(a)); }
+__device__ __forceinline__ Cx imul(double s, Cx a) { return cx(-s * a.i, s * a.r); }   // i s a
+
+// kDeriv: also the derivatives (the force's B1, B2)
+template <bool kDeriv>
+__device__ ExpCoef expi_coef(double c0, double c1) {
+  const bool flip = c0 < 0.0;
+  const double a0 = fabs(c0);
+  const double s3 = sqrt(c1 / 3.0);
+  const double theta = acos(fmin(1.0, a0 / (2.0 * s3 * s3 * s3)));
+  const double u = s3 * cos(theta / 3.0);
+  const double w = sqrt(c1) * sin(theta / 3.0);
+  const double uu = u * u, ww = w * w;
+  const double sw = sinc_w(w), cw = cos(w);
+  const Cx p2 = expi(2.0 * u);      // e^{2iu}
+  const Cx m1 = expi(-u);           // e^{-iu}
+  const double den = 9.0 * uu - ww;
+  ExpCoef r;
+  // h_j / (9u^2 - w^2), paper eqs. (30)-(33)
+  r.f[0] = (1.0 / den) * ((uu - ww) * p2 + m1 * cx(8.0 * uu * cw, 2.0 * u * (3.0 * uu + ww) * sw));
+  r.f[1] = (1.0 / den) * ((2.0 * u) * p2 - m1 * cx(2.0 * u * cw, -(3.0 * uu - ww) * sw));
+  r.f[2] = (1.0 / den) * (p2 - m1 * cx(cw, 3.0 * u * sw));
+  if (kDeriv) {
+    const double ds = dsinc_w(w);
+    // the paper's r_j^(1), r_j^(2) (eqs. 58-60), written out per component
+    Cx ra[3], rb[3];
+    ra[0] = 2.0 * (cx(u, uu - ww) * p2) +
+            2.0 * (m1 * cx(8.0 * u * cw + u * (3.0 * uu + ww) * sw,
+                           -4.0 * uu * cw + (9.0 * uu + ww) * sw));
+    ra[1] = 2.0 * (cx(1.0, 2.0 * u) * p2) +
+            m1 * cx(-2.0 * cw + (3.0 * uu - ww) * sw, 2.0 * u * cw + 6.0 * u * sw);
+    ra[2] = imul(2.0, p2) + m1 * cx(-3.0 * u * sw, cw - 3.0 * sw);
+    rb[0] = -2.0 * p2 + m1 * cx(-8.0 * uu * sw, 2.0 * u * (cw + sw + 3.0 * uu * ds));
+    rb[1] = m1 * cx(2.0 * u * sw, -(cw + sw - 3.0 * uu * ds));
+    rb[2] = m1 * cx(sw, -3.0 * u * ds);
+    const double inv = 1.0 / (2.0 * den * den);
+    for (int j = 0; j < 3; ++j) {
+      r.d1[j] = inv * ((2.0 * u) * ra[j] + (3.0 * uu - ww) * rb[j] - (30.0 * uu + 2.0 * ww) * r.f[j]);
+      r.d0[j] = inv * (ra[j] - (3.0 * u) * rb[j] - (24.0 * u) * r.f[j]);
+    }
+  }
+  if (flip) {
+    for (int j = 0; j < 3; ++j) {
+      const double sj = (j & 1) ? -1.0 : 1.0;
+      r.f[j] = sj * conj(r.f[j]);
+      if (kDeriv) {
+        r.d1[j] = sj * conj(r.d1[j]);
+        r.d0[j] = -sj * conj(r.d0[j]);
+      }
+    }
+  }
+  return r;
 }
 
-// f0 + f1 Q + f2 Q^2 with Q = -i iQ1 and Q^2 = -iQ2
-__device__ __forceinline__ M3 ch_combine(Cx f0, Cx f1, Cx f2, const M3& iQ1, const M3& iQ2) {
+// a0 + a1 Q + a2 Q^2
+__device__ __forceinline__ M3 qpoly(const Cx* a, const M3& Q, const M3& Q2) {
   M3 e;
 #pragma unroll
   for (int k = 0; k < 9; ++k) {
-    const Cx id = (k == 0 || k == 4 || k == 8) ? cx(1, 0) : cx(0, 0);
-    e.m[k] = f0 * id + f1 * cx(iQ1.m[k].i, -iQ1.m[k].r) - f2 * iQ2.m[k];
+    const Cx id = (k % 4 == 0) ? a[0] : cx(0.0, 0.0);
+    e.m[k] = id + a[1] * Q.m[k] + a[2] * Q2.m[k];
   }
   return e;
 }
+
+// tr(A B)
+__device__ __forceinline__ Cx tr_mul(const M3& a, const M3& b) {
+  Cx t = cx(0.0, 0.0);
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) t = t + a.m[3 * i + j] * b.m[3 * j + i];
+  return t;
+}
+
+// The stout generator of one link: Q = -i TA(C U^+) (Hermitian, traceless),
+// its square, and the invariants c0, c1.
+struct StoutQ {
+  M3 Q, Q2;
+  double c0, c1;
+};
+
+__device__ __forceinline__ StoutQ stout_q(const M3& C, const M3& U) {
+  StoutQ q;
+  M3 a = mul_nd(C, U);
+  at3(a);                                    // a = i Q
+#pragma unroll
+  for (int k = 0; k < 9; ++k) q.Q.m[k] = cx(a.m[k].i, -a.m[k].r);
+  q.Q2 = mul_nn(q.Q, q.Q);
+  q.c1 = 0.5 * (q.Q2.m[0].r + q.Q2.m[4].r + q.Q2.m[8].r);
+  q.c0 = tr_mul(q.Q, q.Q2).r / 3.0;
+  return q;
+}
+
+// The reference treats a link whose generator is negligible as unsmeared:
+// exp(iQ) = 1 and no Lambda term in the force, when |iQ|^2 = tr(Q^2) = 2 c1
+// is at most 1e-10 (Projection_Stout_SU3::force_recursive / project,
+// src/lib/Smear/projection_Stout_SU3.cpp); the same cut keeps results equal
+// on (near-)cold links.
+__device__ __forceinline__ bool stout_negligible(const StoutQ& q) { return 2.0 * q.c1 <= 1.0e-10; }
 
 struct StoutParams {
   const double* u;     // links of this level (input of the smearing step)
@@ -97,30 +191,27 @@ struct StoutParams {
   LexGeom g;
 };
 
+// U' = exp(iQ) U, one thread per link
 __global__ void stout_smear_kernel(StoutParams p) {
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= 4 * p.g.vol) return;
   const int mu = (int)(idx / p.g.vol);
   const size_t site = idx % p.g.vol;
   const M3 U = load3(p.u, idx);
-  const M3 C = staple_sum(p.u, p.g, site, mu, p.rho);
-  M3 iQ1 = mul_nd(C, U);
-  at3(iQ1);
-  const M3 iQ2 = mul_nn(iQ1, iQ1);
-  const M3 iQ3 = mul_nn(iQ1, iQ2);
-  M3 e;
-  if (norm2_3(iQ1) > 1.0e-10) {
-    double u, w;
-    Cx f0, f1, f2;
-    uw_fj(iQ2, iQ3, u, w, f0, f1, f2);
-    e = ch_combine(f0, f1, f2, iQ1, iQ2);
-  } else {
-    e = unit3();
+  const StoutQ q = stout_q(staple_sum(p.u, p.g, site, mu, p.rho), U);
+  if (stout_negligible(q)) {
+    store3(p.u_out, idx, U);
+    return;
   }
-  store3(p.u_out, idx, mul_nn(e, U));
+  const ExpCoef k = expi_coef<false>(q.c0, q.c1);
+  store3(p.u_out, idx, mul_nn(qpoly(k.f, q.Q, q.Q2), U));
 }
 
-// Projection_Stout_SU3::force_recursive: Xi = Sigma' e^{iQ} + C^+ iGamma, iTheta = iGamma U
+// One backward step of the stout chain for link (x, mu): with M = U Sigma'
+//   Gamma  = tr(M B1) Q + tr(M B2) Q^2 + f1 M + f2 (Q M + M Q)
+//   iLambda = TA(i Gamma),   iTheta = iLambda U   (kept for force_each)
+//   Sigma  = Sigma' exp(iQ) + C^+ iLambda
+// (paper eqs. 69-75); the staple derivative terms follow in force_each.
 __global__ void stout_recursive_kernel(StoutParams p) {
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= 4 * p.g.vol) return;
@@ -129,62 +220,30 @@ __global__ void stout_recursive_kernel(StoutParams p) {
   const M3 U = load3(p.u, idx);
   const M3 C = staple_sum(p.u, p.g, site, mu, p.rho);
   const M3 Sp = load3(p.sigp, idx);
-  M3 iQ1 = mul_nd(C, U);
-  at3(iQ1);
-  const M3 iQ2 = mul_nn(iQ1, iQ1);
-  const M3 iQ3 = mul_nn(iQ1, iQ2);
-  M3 e, iG;
-  if (norm2_3(iQ1) > 1.0e-10) {
-    double u, w;
-    Cx f0, f1, f2;
-    uw_fj(iQ2, iQ3, u, w, f0, f1, f2);
-    e = ch_combine(f0, f1, f2, iQ1, iQ2);
-    const double xi0 = xi0f(w), xi1 = xi1f(w);
-    const double u2 = u * u, w2 = w * w, cos_w = cos(w);
-    const Cx emiu = cx(cos(u), -sin(u));
-    const Cx e2iu = cx(cos(2.0 * u), sin(2.0 * u));
-    const Cx r01 = cx(2.0 * u, 2.0 * (u2 - w2)) * e2iu +
-                   emiu * cx(16.0 * u * cos_w + 2.0 * u * (3.0 * u2 + w2) * xi0,
-                             -8.0 * u2 * cos_w + 2.0 * (9.0 * u2 + w2) * xi0);
-    const Cx r11 = cx(2.0, 4.0 * u) * e2iu +
-                   emiu * cx(-2.0 * cos_w + (3.0 * u2 - w2) * xi0, 2.0 * u * cos_w + 6.0 * u * xi0);
-    const Cx r21 = cx(0.0, 2.0) * e2iu + emiu * cx(-3.0 * u * xi0, cos_w - 3.0 * xi0);
-    const Cx r02 = cx(-2.0, 0.0) * e2iu +
-                   emiu * cx(-8.0 * u2 * xi0, 2.0 * u * (cos_w + xi0 + 3.0 * u2 * xi1));
-    const Cx r12 = emiu * cx(2.0 * u * xi0, -cos_w - xi0 + 3.0 * u2 * xi1);
-    const Cx r22 = emiu * cx(xi0, -3.0 * u * xi1);
-    const double fden = 1.0 / (2 * (9.0 * u2 - w2) * (9.0 * u2 - w2));
-    const double c2u = 2.0 * u, c3 = 3.0 * u2 - w2, c30 = 30.0 * u2 + 2.0 * w2;
-    const Cx b10 = fden * (c2u * r01 + c3 * r02 - c30 * f0);
-    const Cx b11 = fden * (c2u * r11 + c3 * r12 - c30 * f1);
-    const Cx b12 = fden * (c2u * r21 + c3 * r22 - c30 * f2);
-    const Cx b20 = fden * (r01 - (3.0 * u) * r02 - (24.0 * u) * f0);
-    const Cx b21 = fden * (r11 - (3.0 * u) * r12 - (24.0 * u) * f1);
-    const Cx b22 = fden * (r21 - (3.0 * u) * r22 - (24.0 * u) * f2);
-    const M3 B1 = ch_combine(b10, b11, b12, iQ1, iQ2);
-    const M3 B2 = ch_combine(b20, b21, b22, iQ1, iQ2);
-    const M3 US = mul_nn(U, Sp);
-    const M3 t1 = mul_nn(US, B1);
-    const M3 t2 = mul_nn(US, B2);
-    const Cx tr1 = t1.m[0] + t1.m[4] + t1.m[8];
-    const Cx tr2 = t2.m[0] + t2.m[4] + t2.m[8];
-    const M3 iQUS = mul_nn(iQ1, US);
-    const M3 iUSQ = mul_nn(US, iQ1);
-#pragma unroll
-    for (int k = 0; k < 9; ++k) {
-      const Cx qt = tr1 * cx(iQ1.m[k].i, -iQ1.m[k].r) - tr2 * iQ2.m[k] + f1 * US.m[k] +
-                    f2 * cx(iQUS.m[k].i, -iQUS.m[k].r) + f2 * cx(iUSQ.m[k].i, -iUSQ.m[k].r);
-      iG.m[k] = cx(-qt.i, qt.r);
-    }
-  } else {
-    iG = zero3();
+  const StoutQ q = stout_q(C, U);
+  M3 e, il;
+  if (stout_negligible(q)) {
     e = unit3();
+    il = zero3();
+  } else {
+    const ExpCoef k = expi_coef<true>(q.c0, q.c1);
+    e = qpoly(k.f, q.Q, q.Q2);
+    const M3 M = mul_nn(U, Sp);
+    const Cx g1 = tr_mul(M, qpoly(k.d1, q.Q, q.Q2));
+    const Cx g0 = tr_mul(M, qpoly(k.d0, q.Q, q.Q2));
+    const M3 QM = mul_nn(q.Q, M);
+    const M3 MQ = mul_nn(M, q.Q);
+#pragma unroll
+    for (int n = 0; n < 9; ++n) {
+      const Cx gam = g1 * q.Q.m[n] + g0 * q.Q2.m[n] + k.f[1] * M.m[n] + k.f[2] * (QM.m[n] + MQ.m[n]);
+      il.m[n] = imul(1.0, gam);
+    }
+    at3(il);
   }
-  at3(iG);
-  store3(p.itheta, idx, mul_nn(iG, U));
-  M3 xi = mul_nn(Sp, e);
-  add_to(xi, mul_dn(C, iG));
-  store3(p.sig, idx, xi);
+  store3(p.itheta, idx, mul_nn(il, U));
+  M3 sig = mul_nn(Sp, e);
+  add_to(sig, mul_dn(C, il));
+  store3(p.sig, idx, sig);
 }
 
 // ForceSmear_APE::force_each summed over nu != mu, times rho, added to sig

@@ -9,6 +9,7 @@ regenerated bit-for-bit from the recorded seeds by ``b200dwf.synth``.
     python tests/golden/make_golden.py traj       # one 2+1-flavour trajectory
     python tests/golden/make_golden.py rng        # the Mseries_parallel generator
     python tests/golden/make_golden.py io         # gauge-configuration files
+    python tests/golden/make_golden.py sample [REF]   # the published 8^4 trajectory
 
 Needs the reference tree (to build the harness); the committed .npz files are
 what the tests read, so the tests themselves run without it.
@@ -168,7 +169,73 @@ def gauge_io():
     print("wrote gauge_io.npz")
 
 
+# The reference's published single-GPU trajectory (sample_1gpu/): 8^4 lattice
+# from conf_04040408.txt tiled, Moebius DWF b=1.5 c=0.5 M0=1.0 Ls=12, masses
+# Nf1 0.02 (rational), Nf2 0.0005 over Nf2_prec 0.002 over PV 1.0, tree-level
+# Symanzik beta 4.17, 3 stout steps rho 0.1, Omelyan [2,1,3] on levels
+# [0,0,1,2], length 0.1, Mseries_parallel reset to i_conf = 200000, solver
+# tolerances |r|^2/|b|^2 1e-28 (CG), 1e-26 / 1e-28 (MD / calcH multishift),
+# shipped 16- and 24-pole tables on [1e-4, 10]
+# (sample_1gpu/HMC_DWF_Nf2p1_eo.yaml, main.yaml).  Stored: the configuration
+# file's numbers, the table files' text, and the published log values with
+# the log line each comes from.
+SAMPLE = dict(lattice=[8, 8, 8, 8], Ls=12, M0=1.0, b=1.5, c=0.5, mq_l=0.0005, mq_h=0.002,
+              mq_s=0.02, mq_pv=1.0, beta=4.17, c_plaq=5.0 / 3.0, c_rect=-1.0 / 12.0, rho=0.1,
+              nsmear=3, nstep=[2, 1, 3], level=[0, 0, 1, 2], tau=0.1, lam=0.1931833275, nprec=8,
+              np_md=16, np_h=24, rat_lo=1.0e-2, rat_hi=3.16227766, tol_cg=1e-28,
+              tol_ms_md=1e-26, tol_ms_h=1e-28, seed=200000)
+SAMPLE_TABLES = ["parameter_rational.%s_%d_0.00010000_010.000" % (k, n)
+                 for n in (16, 24) for k in ("1_4", "1_4inv", "1_2inv")]
+# (key, log file, label printed in the log, occurrence)
+SAMPLE_LOG = [("H_total_init", "sample_1gpu/run.log", "H_total(init)", 0),
+              ("H_Frational_init", "sample_1gpu/run.log", "H_Frational", 0),
+              ("H_Fratio_Nf2_init", "sample_1gpu/run.log", "H_Fratio", 0),
+              ("H_Fratio_Nf2prec_init", "sample_1gpu/run.log", "H_Fratio", 2),
+              ("H_Grectangle_init", "sample_1gpu/run.log", "H_Grectangle", 0),
+              ("plaq_init", "sample_1gpu/run.log", "plaq(init)", 0),
+              ("H_total_final", "sample_1gpu/run.log", "H_total(trial)", 0),
+              ("H_diff", "sample_1gpu/run.log", "H(diff)", 0),
+              ("plaq_final", "sample_1gpu/run.log", "plaq(final)", 0),
+              ("H_total_init_corelib", "sample_x86_corelib/run.log", "H_total(init)", 0),
+              ("H_total_final_corelib", "sample_x86_corelib/run.log", "H_total(trial)", 0),
+              ("H_total_init_qxs", "sample_x86/run.log", "H_total(init)", 0),
+              ("H_total_final_qxs", "sample_x86/run.log", "H_total(trial)", 0)]
+
+
+def sample(ref):
+    import re
+    vals = np.loadtxt(os.path.join(ref, "conf_04040408.txt"), dtype=np.float64)
+    tables = {}
+    for name in SAMPLE_TABLES:
+        with open(os.path.join(ref, "sample_1gpu", name)) as f:
+            tables[name] = f.read()
+    published, where = {}, {}
+    for key, log, label, nth in SAMPLE_LOG:
+        hits = []
+        with open(os.path.join(ref, log)) as f:
+            for i, line in enumerate(f, 1):
+                m = re.match(r"\s*%s\s*=\s*([-+0-9.eE]+)" % re.escape(label), line)
+                if m:
+                    hits.append((float(m.group(1)), i))
+        published[key], line_no = hits[nth]
+        where[key] = "%s:%d" % (log, line_no)
+    with open(os.path.join(ref, "sample_1gpu", "run.log")) as f:
+        for i, line in enumerate(f, 1):
+            m = re.match(r"Elapsed time: each trajectory: total\s+([0-9.]+) sec", line)
+            if m:
+                published["sec_per_trajectory"] = float(m.group(1))
+                where["sec_per_trajectory"] = "sample_1gpu/run.log:%d" % i
+    np.savez_compressed(os.path.join(HERE, "sample_8x8x8x8.npz"), meta=json.dumps(SAMPLE),
+                        conf_04040408=vals, tables=json.dumps(tables),
+                        published=json.dumps(published), where=json.dumps(where))
+    print("wrote sample_8x8x8x8.npz", published)
+
+
 def main():
+    if sys.argv[1:2] == ["sample"]:
+        ref = sys.argv[2] if len(sys.argv) > 2 else os.environ.get("B200_REFERENCE_DIR", "/root/reference")
+        sample(ref)
+        return
     if sys.argv[1:] == ["io"]:
         gauge_io()
         return

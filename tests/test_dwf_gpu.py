@@ -160,3 +160,35 @@ def test_packed_variants_reduced_precision(variant, ci):
             del os.environ["B200_HOP_VARIANT"]
         else:
             os.environ["B200_HOP_VARIANT"] = old
+
+
+def test_async_transfers_match_sync():
+    """convert_async / reverse_async on side streams (page-locked host
+    fields, staging rings) give the synchronous calls' bytes, and reject
+    pageable host memory."""
+    import torch
+    import b200dwf
+    case = CASES[1]
+    ora, dev = make(case, 9)
+    w = synth.spinor_field(case[0], case[1], 41)
+    for prec in (0, 2):
+        h_in = torch.from_numpy(w).pin_memory()
+        outs = [torch.empty(w.size, dtype=torch.float64).pin_memory() for _ in range(3)]
+        s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+        fw, fv = dev.new_field(prec), dev.new_field(prec)
+        for k in range(3):                         # wraps both staging rings
+            dev.convert_async(fw, h_in.numpy(), s1)
+            s2.wait_stream(s1)
+            dev.mult(fv, fw, "Deo", stream=s2)
+            dev.reverse_async(fv, outs[k].numpy(), s2)
+        torch.cuda.synchronize()
+        fw2, fv2 = dev.new_field(prec), dev.new_field(prec)
+        dev.convert(fw2, w)
+        dev.mult(fv2, fw2, "Deo")
+        ref = dev.reverse(fv2)
+        for k in range(3):
+            assert np.array_equal(outs[k].numpy(), ref), (prec, k)
+    with pytest.raises(b200dwf.B200Error, match="page-locked"):
+        dev.convert_async(fw, w, None)
+    with pytest.raises(b200dwf.B200Error, match="page-locked"):
+        dev.reverse_async(fv, np.empty_like(w), None)
