@@ -309,6 +309,51 @@ def small_trajectory_beside_reference(threads=None):
             "noise": "the reference's recorded M-series momenta and pseudofermion noise"}
 
 
+def published_trajectory():
+    """The reference's published single-GPU run (sample_1gpu: 8^4 from
+    conf_04040408.txt, Moebius Ls=12, 2+1 flavours, Symanzik 4.17, 3 stout,
+    the shipped rational tables, Mseries_parallel reset to 200000) on the
+    device, from the committed fixture tests/golden/sample_8x8x8x8.npz: the
+    device seconds and H(diff) beside the published 21.44 s and 0.00083995
+    (sample_1gpu/run.log:1994-2000)."""
+    import torch
+    from b200dwf.gauge_io import tile_text_4x4x4x8
+    from b200dwf.hmc import build_dwf_nf2p1, MseriesNoise
+    z = np.load(os.path.join(REPO, "tests", "golden", "sample_8x8x8x8.npz"))
+    c = json.loads(str(z["meta"]))
+    pub = json.loads(str(z["published"]))
+    tables = json.loads(str(z["tables"]))
+    with tempfile.TemporaryDirectory() as d:
+        for name, text in tables.items():
+            with open(os.path.join(d, name), "w") as f:
+                f.write(text)
+
+        def run():
+            hmc = build_dwf_nf2p1(c["lattice"], c["Ls"], c["M0"],
+                                  dict(l=c["mq_l"], h=c["mq_h"], s=c["mq_s"], pv=c["mq_pv"]),
+                                  c["beta"], c["c_plaq"], c["c_rect"], c["rho"], c["nsmear"],
+                                  c["nstep"], c["level"], c["tau"], c["lam"], c["nprec"],
+                                  c["np_md"], c["np_h"], (c["rat_lo"], c["rat_hi"]), c["tol_cg"],
+                                  c["tol_cg"], b=c["b"], c=c["c"], rational_dir=d,
+                                  tol2_rat_md=c["tol_ms_md"], tol2_rat_h=c["tol_ms_h"])
+            ud = torch.from_numpy(tile_text_4x4x4x8(z["conf_04040408"], c["lattice"])).cuda()
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            r = hmc.trajectory(ud, MseriesNoise(c["lattice"], c["seed"]))
+            torch.cuda.synchronize()
+            return time.perf_counter() - t, r
+
+        run()                            # untimed: autotuning, workspaces, graphs
+        sec, r = run()
+    return {"config": "sample_1gpu: 8^4, Moebius b=1.5 c=0.5 M0=1.0 Ls=12, masses 0.0005/0.002/"
+                      "0.02/PV 1.0, Symanzik beta 4.17, 3 stout, Omelyan [2,1,3], length 0.1, "
+                      "tol2 1e-28, the reference's rational tables, Mseries_parallel 200000",
+            "device_sec": sec, "published_sec": pub["sec_per_trajectory"],
+            "H0_device": r["H0"], "H0_published": pub["H_total_init"],
+            "dH_device": r["dH"], "dH_published": pub["H_total_final"] - pub["H_total_init"],
+            "dH_published_log": pub["H_diff"]}
+
+
 def reference_arm(args, rank, world):
     if rank != 0:
         return
@@ -720,6 +765,12 @@ def b200_arm(args, rank, world, local_rank):
     if not args.no_trajectory and world == 1:
         trajectory = trajectory_section(op, lattice, u, args, lp)
 
+    published = None
+    if world == 1 and not args.no_trajectory:
+        try:
+            published = published_trajectory()
+        except Exception as e:  # noqa: BLE001
+            published = {"unavailable": str(e)}
     small = None
     if world == 1 and not args.no_cpu and not args.no_trajectory:
         try:
@@ -786,6 +837,10 @@ def b200_arm(args, rank, world, local_rank):
         line["speedup_target"] = 3.0
     if cpu_traj:
         line["sec_traj_cpu_reference_extrapolated"] = round(cpu_traj["sec_per_trajectory"], 1)
+    if published and "device_sec" in published:
+        line["sec_traj_published_8x8x8x8_device"] = round(published["device_sec"], 3)
+        line["sec_traj_published_8x8x8x8_reference_gpu"] = published["published_sec"]
+        line["dH_published_8x8x8x8_device"] = published["dH_device"]
     line.update({
         "cpu_baseline": cpu,
         "cpu_trajectory": cpu_traj,
@@ -794,6 +849,7 @@ def b200_arm(args, rank, world, local_rank):
         "learned_preconditioner": learned,
         "trajectory": trajectory,
         "trajectory_4x4x4x8_beside_reference": small,
+        "trajectory_published_8x8x8x8": published,
         "autotune": b200dwf.tuning_table().strip().splitlines(),
     })
     print(json.dumps(line))
