@@ -477,11 +477,16 @@ def trajectory_section(op, lattice, u_workload, args, lp=None):
     import b200dwf
     from b200dwf import synth
     from b200dwf.hmc import build_dwf_nf2p1, Solver
+    from b200dwf.gauge_io import tile_text_4x4x4x8
     lattice = list(args.traj_lattice or lattice)
-    sm = b200dwf.StoutSmear(lattice, 0.1, 2)
-    sm.set_config(synth.gauge_field(lattice, SEED_U + 3, "near", 0.3))
-    u0 = sm.config(2)
-    del sm
+    # the reference benchmark's start: conf_04040408.txt tiled onto the
+    # lattice (GaugeConfig("Text_4x4x4x8"), src/lib/IO/fieldIO_Text_4x4x4x8.cpp)
+    fx = np.load(os.path.join(REPO, "tests", "golden", "sample_8x8x8x8.npz"))
+    u0 = tile_text_4x4x4x8(fx["conf_04040408"], lattice)
+    table_dir = tempfile.mkdtemp()
+    for name, text in json.loads(str(fx["tables"])).items():
+        with open(os.path.join(table_dir, name), "w") as f:
+            f.write(text)
     cg = {k: "cg" for k in ("l_md", "l_h", "h_md", "h_h", "pv_h")}
     mixed = {k: "mixed+" for k in ("l_md", "l_h", "h_md", "h_h", "pv_h")}
     # (name, solver kinds, multishift window): the plain form is FP64 CG with
@@ -499,9 +504,11 @@ def trajectory_section(op, lattice, u_workload, args, lp=None):
     res = {}
     for name, kinds, window in forms:
         try:
-            res[name] = _trajectory_form(lattice, u0, args, lp, kinds, window, tol2)
+            res[name] = _trajectory_form(lattice, u0, args, lp, kinds, window, tol2, table_dir)
         except Exception as e:  # noqa: BLE001  (one form's failure keeps the others)
             res[name] = {"error": str(e)}
+    import shutil
+    shutil.rmtree(table_dir, ignore_errors=True)
     gc.collect()
     torch.cuda.empty_cache()
     out = {"lattice": lattice, "Ls": LS, "M0": M0, "masses": TRAJ_MASSES,
@@ -510,7 +517,9 @@ def trajectory_section(op, lattice, u_workload, args, lp=None):
                       "2 stout rho 0.1 on the fermion links",
            "integrator": "Omelyan %s, lambda 0.1931833275" % list(args.traj_nstep),
            "length": args.traj_length, "solver_tol_rel_residual": 1e-10,
-           "links": "near-unit exp(i*0.3*H) + 2 stout rho=0.1 (seed %d)" % (SEED_U + 3), **res}
+           "links": "conf_04040408.txt tiled (the reference benchmark's start configuration)",
+           "rational_tables": "the reference's shipped 16-pole (MD) and 24-pole (heatbath, H) "
+                              "tables on [1e-4, 10]", **res}
     for name in res:
         if "sec_per_trajectory" in res[name] and "sec_per_trajectory" in res.get("fp64_plain", {}):
             out["speedup_" + name] = (res["fp64_plain"]["sec_per_trajectory"]
@@ -518,7 +527,7 @@ def trajectory_section(op, lattice, u_workload, args, lp=None):
     return out
 
 
-def _trajectory_form(lattice, u0, args, lp, kinds, window, tol2):
+def _trajectory_form(lattice, u0, args, lp, kinds, window, tol2, table_dir=None):
     import torch
     import b200dwf
     from b200dwf.hmc import build_dwf_nf2p1, MseriesNoise, Solver
@@ -529,7 +538,7 @@ def _trajectory_form(lattice, u0, args, lp, kinds, window, tol2):
     sv = {k: Solver(v.rstrip("+"), tol2, chrono=v.endswith("+")) for k, v in kinds.items()}
     hmc = build_dwf_nf2p1(lattice, LS, M0, TRAJ_MASSES, 2.13, nstep=args.traj_nstep,
                           tau=args.traj_length, np_md=16, np_h=24, tol2_md=tol2, tol2_h=tol2,
-                          solvers=sv, shift_window=window)
+                          solvers=sv, shift_window=window, rational_dir=table_dir)
     if "learned" in kinds.values():
         # the trained weights are volume independent; the network runs on
         # the light operator's own (smeared) links

@@ -96,6 +96,12 @@ int b200_field_convert_async(b200_dwf_t *op, int prec, void *v_dev, const double
                              void *stream);
 int b200_field_reverse_async(b200_dwf_t *op, int prec, double *v_host, const void *w_dev,
                              void *stream);
+/* The sites of parity ieo of a full-lattice lexical Field(24, Nvol, Ls) on
+ * the device into a field (Index_eo::convertField(v, w_lex, ieo),
+ * src/lib/Field/index_eo.cpp), asynchronous on `stream`: the heatbath's
+ * lexical noise (action_F_Ratio_eo.cpp:70-78) without a separate gather. */
+int b200_field_convert_lex_device(b200_dwf_t *op, int prec, void *v_dev, const double *w_lex_dev,
+                                  int ieo, void *stream);
 /* convert() from a field already on the device (w_dev: reference layout,
  * 24 * Nvol/2 * Ls doubles), asynchronous on `stream`: the heatbath noise
  * drawn by b200_rng_gauss_lex goes to the operator without a host copy. */
@@ -212,6 +218,29 @@ int b200_solver_set_initial_guess(b200_dwf_t *op, int use);
 int b200_field_norm2_noalloc(int prec, const void *x, long nsite, int ls,
                              double *result, void *stream);
 
+/* ---------------------------------------------------------------- flat vectors
+ * Plan-free vector operations on device arrays of n reals (prec 0: double,
+ * 1: float), for field containers that hold a library field as a flat
+ * array: the reference-side AField<REAL, B200> shell.  They replace the
+ * BridgeACC vector functions (src/lib_alt_Accel/BridgeOpenACC/src/
+ * afield_openacc-inc.h:14-446).  Element-wise work does not depend on the
+ * layout; complex forms act on adjacent (re, im) pairs (n even).
+ * Reductions accumulate in double and return synchronously on `stream`. */
+int b200_blas_axpby(int prec, size_t n, double a, const void *x, double b, void *y,
+                    void *stream);                         /* y = a x + b y (b = 0: y not read) */
+int b200_blas_caxpby(int prec, size_t n, double ar, double ai, const void *x, double br,
+                     double bi, void *y, void *stream);    /* complex pairs */
+int b200_blas_fill(int prec, size_t n, double value, void *y, void *stream);
+int b200_blas_dot(int prec, size_t n, const void *x, const void *y, double *result,
+                  void *stream);                           /* sum x_i y_i */
+int b200_blas_dotc(int prec, size_t n, const void *x, const void *y, double *re, double *im,
+                   void *stream);                          /* sum conj(x) y over pairs */
+/* Precision copy of a field of nsite (site, Ls) columns between storage
+ * precisions 0..3 (convert_h, afield_copy_openacc-inc.h:11-54): the storage
+ * layouts differ per precision, so this is layout-aware. */
+int b200_field_convert_prec(int prec_out, void *out, int prec_in, const void *in, long nsite,
+                            int ls, void *stream);
+
 /* ---------------------------------------------------------------- force
  * Force_F_Domainwall_eo::force_udiv1 (src/lib/Force/Fermion/
  * force_F_Domainwall_eo.cpp:170-318; Accel form AForce_F_Domainwall_5din_eo::
@@ -285,6 +314,15 @@ int b200_momentum_update(const int lattice[4], double eps, const double *force, 
                          void *stream);
 /* HMC_General::calcH_P (src/lib/HMC/hmc_General.cpp:340-346): H = |iP|^2 / 2;
  * synchronous. */
+/* iP = i sum_a h_a lambda_a on every link from Field(8, Nvol, 4) Gaussians h
+ * (Langevin_Momentum::set_iP_SU3, src/lib/HMC/langevin_Momentum.cpp:150-210);
+ * device arrays, asynchronous on `stream`. */
+int b200_momentum_from_gauss(const int lattice[4], const double *h, double *ip, void *stream);
+/* y = a x + b y over link/force fields (Field_G(Nvol, 4), 72 Nvol doubles);
+ * b = 0 overwrites y without reading it.  The force sums of
+ * Integrator_UpdateP (src/lib/HMC/integrator_UpdateP.cpp:44-66). */
+int b200_links_axpby(const int lattice[4], double a, const double *x, double b, double *y,
+                     void *stream);
 int b200_momentum_energy(const int lattice[4], const double *ip, double *H, void *stream);
 
 /* ---------------------------------------------------------------- learned preconditioner

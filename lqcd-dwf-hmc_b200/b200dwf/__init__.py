@@ -98,6 +98,9 @@ def lib():
     L.b200_link_update.argtypes = [ip, d_, vp, vp, ctypes.c_int, vp]
     L.b200_momentum_update.argtypes = [ip, d_, vp, vp, vp]
     L.b200_momentum_energy.argtypes = [ip, vp, dp, vp]
+    L.b200_momentum_from_gauss.argtypes = [ip, vp, vp, vp]
+    L.b200_links_axpby.argtypes = [ip, d_, vp, d_, vp, vp]
+    L.b200_field_convert_lex_device.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_int, vp]
     fp = ctypes.POINTER(ctypes.c_float)
     L.b200_lp_create.argtypes = [ctypes.POINTER(vp), vp, ctypes.c_int, ctypes.c_ulonglong,
                                  ctypes.c_double]

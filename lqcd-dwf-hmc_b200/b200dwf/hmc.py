@@ -588,19 +588,6 @@ class Leapfrog:
         self.p.evolve(0.5 * e, ip, u)
 
 
-# Gell-Mann basis: i lambda_a as (row, col, re, im) entries
-_ILAMBDA = (
-    ((0, 1, 0, 1), (1, 0, 0, 1)),
-    ((0, 1, 1, 0), (1, 0, -1, 0)),
-    ((0, 0, 0, 1), (1, 1, 0, -1)),
-    ((0, 2, 0, 1), (2, 0, 0, 1)),
-    ((0, 2, 1, 0), (2, 0, -1, 0)),
-    ((1, 2, 0, 1), (2, 1, 0, 1)),
-    ((1, 2, 1, 0), (2, 1, -1, 0)),
-    ((0, 0, 0, 3 ** -0.5), (1, 1, 0, 3 ** -0.5), (2, 2, 0, -2 * 3 ** -0.5)),
-)
-
-
 class DeviceNoise:
     """Gaussian heatbath fields drawn on the device (torch's Philox stream):
     momenta iP = i sum_a h_a lambda_a with <h_a^2> = 1/2, so that
@@ -614,18 +601,14 @@ class DeviceNoise:
         import torch
         self.g = torch.Generator(device="cuda")
         self.g.manual_seed(int(seed))
-        m = torch.zeros(8, 18, dtype=torch.float64)
-        for a, entries in enumerate(_ILAMBDA):
-            for r, c, re, im in entries:
-                m[a, 2 * (c + 3 * r)] = re
-                m[a, 2 * (c + 3 * r) + 1] = im
-        self.m = m.cuda()
 
     def momentum(self, ip):
         import torch
         h = torch.empty(ip.numel() // 18, 8, dtype=torch.float64, device="cuda")
         h.normal_(0.0, 0.5 ** 0.5, generator=self.g)
-        ip.view(-1, 18).copy_(h @ self.m)
+        nlink = ip.numel() // 18        # the kernel needs only the link count
+        check(lib().b200_momentum_from_gauss((ctypes.c_int * 4)(nlink // 4, 1, 1, 4), _p(h), _p(ip),
+                                             None))
 
     def fermion(self, field):
         field.buf.view(dtype=__import__("torch").float64).normal_(0.0, 0.5 ** 0.5, generator=self.g)
@@ -646,39 +629,22 @@ class MseriesNoise:
     (benchmark_hmc_dwf_corelib/hmc_dwf_eo.cpp:347)."""
 
     def __init__(self, lattice, seed):
-        import torch
         from . import MseriesParallel
         self.lattice = list(lattice)
         self.nvol = int(np.prod(lattice))
         self.rng = MseriesParallel(lattice, seed)
-        sq3r = 1.0 / np.sqrt(3.0)          # the reference's constant
-        m = torch.zeros(8, 18, dtype=torch.float64)
-        for a, entries in enumerate(_ILAMBDA):
-            for r, c, re, im in entries:
-                m[a, 2 * (c + 3 * r)] = re
-                m[a, 2 * (c + 3 * r) + 1] = im
-        m[7, 2 * 0 + 1], m[7, 2 * 4 + 1], m[7, 2 * 8 + 1] = sq3r, sq3r, -2.0 * sq3r
-        self.m = m.cuda()
-        # lexical index of every even site in the reference's even/odd order
-        nx, ny, nz, nt = self.lattice
-        e = np.arange(self.nvol // 2)
-        ix2 = e % (nx // 2)
-        yzt = e // (nx // 2)
-        y, z, t = yzt % ny, (yzt // ny) % nz, yzt // (ny * nz)
-        x = 2 * ix2 + ((y + z + t) & 1)
-        self.even = torch.from_numpy(x + nx * (y + ny * (z + nz * t))).cuda()
 
     def reset(self, seed):
         self.rng.reset(seed)
 
     def momentum(self, ip):
         h = self.rng.gauss_lex_global(8, 4)
-        ip.view(-1, 18).copy_(h.view(-1, 8) @ self.m)
+        check(lib().b200_momentum_from_gauss((ctypes.c_int * 4)(*self.lattice), _p(h), _p(ip), None))
 
     def fermion(self, field):
-        ls = field.op.Ls
-        lex = self.rng.gauss_lex_global(24, ls).view(ls, self.nvol, 24)
-        field.op.convert_device(field, lex.index_select(1, self.even).reshape(-1))
+        lex = self.rng.gauss_lex_global(24, field.op.Ls)
+        check(lib().b200_field_convert_lex_device(field.op.handle, field.prec, field.ptr, _p(lex), 0,
+                                                  None))
 
 
 class HostNoise:
@@ -739,20 +705,26 @@ class HMCGeneral:
                 a.u = u
 
     def level_force(self, actions, u, out):
-        """Integrator_UpdateP's summed force of one level into out."""
-        out.zero_()
+        """Integrator_UpdateP's summed force of one level into out (library
+        kernels: the first term overwrites out, the others add to it)."""
+        L = lib()
+        beta = 0.0
         ferm = [a for a in actions if a.fermion]
         if ferm:
-            self.fbuf.zero_()
+            check(L.b200_links_axpby(self._L, 0.0, _p(self.fbuf), 0.0, _p(self.fbuf), None))
             for a in ferm:
                 a.force_udiv(self.fbuf)
             self.director.jacobian(self.fbuf)
-            check(lib().b200_force_mult_generator(self._L, _p(self.fbuf), _p(u), None))
-            out.add_(self.fbuf)
+            check(L.b200_force_mult_generator(self._L, _p(self.fbuf), _p(u), None))
+            check(L.b200_links_axpby(self._L, 1.0, _p(self.fbuf), beta, _p(out), None))
+            beta = 1.0
         for a in actions:
             if not a.fermion:
                 a.force(self.gbuf)
-                out.add_(self.gbuf)
+                check(L.b200_links_axpby(self._L, 1.0, _p(self.gbuf), beta, _p(out), None))
+                beta = 1.0
+        if beta == 0.0:
+            check(L.b200_links_axpby(self._L, 0.0, _p(out), 0.0, _p(out), None))
 
     def momentum_energy(self, ip):
         h = ctypes.c_double()

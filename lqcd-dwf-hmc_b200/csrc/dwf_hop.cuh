@@ -276,6 +276,24 @@ __device__ __forceinline__ void hop_dir_rows_f64(const double2* urec, const doub
     double2 uc[3];
 #pragma unroll
     for (int j = 0; j < 3; ++j) uc[j] = urec[kDag ? (3 * j + i) : (3 * i + j)];
+    if (MU == 3) {
+      // the t projection keeps one spin pair, so U h lands in it unchanged:
+      // the multiply-add chains start from the accumulator itself
+#pragma unroll
+      for (int a = 0; a < 2; ++a) {
+        double* tgt = acc + 2 * (i + 3 * (a + (SIGN > 0 ? 2 : 0)));
+        double re = tgt[0], im = tgt[1];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          const double ur = uc[j].x;
+          const double ui = kDag ? -uc[j].y : uc[j].y;
+          cmul_acc(re, im, ur, ui, h[6 * a + 2 * j], h[6 * a + 2 * j + 1]);
+        }
+        tgt[0] = re;
+        tgt[1] = im;
+      }
+      continue;
+    }
     double o[12];
 #pragma unroll
     for (int q = 0; q < 12; ++q) o[q] = 0.0;
@@ -298,11 +316,6 @@ __device__ __forceinline__ void hop_dir_rows_f64(const double2* urec, const doub
     double* r1 = acc + 2 * (i + 3);
     double* r2 = acc + 2 * (i + 6);
     double* r3 = acc + 2 * (i + 9);
-    if (MU == 3) {
-      if (SIGN > 0) { r2[0] += a0r; r2[1] += a0i; r3[0] += a1r; r3[1] += a1i; }
-      else          { r0[0] += a0r; r0[1] += a0i; r1[0] += a1r; r1[1] += a1i; }
-      continue;
-    }
     r0[0] += a0r; r0[1] += a0i;
     r1[0] += a1r; r1[1] += a1i;
     if (MU == 0) {
@@ -655,13 +668,16 @@ __device__ __forceinline__ void su3_mult_half2(const float* u, const float2* h, 
   }
 }
 
-// acc (pairs) += ph * (1 - sign*gamma_mu)-shaped result; same algebra as
-// reconstruct_acc, the factor i only selects the re/im pair.
+// acc (pairs) += m * (1 - sign*gamma_mu)-shaped result, m a per-slice
+// multiplier (the edge phase and, for f16/bf16 storage, the neighbour's
+// per-(site, s) scale: U (sc h) = sc (U h), so the scale rides on the
+// reconstruction's multiply-adds instead of costing its own multiplies);
+// same algebra as reconstruct_acc, the factor i only selects the re/im pair.
 template <int MU, int SIGN>
-__device__ __forceinline__ void reconstruct_acc2(float2* acc, const float2* o, float ph) {
-  const float2 pp = f2(ph);
-  const float2 sp = f2(SIGN > 0 ? ph : -ph);
-  const float2 sm = f2(SIGN > 0 ? -ph : ph);
+__device__ __forceinline__ void reconstruct_acc2(float2* acc, const float2* o, float2 m) {
+  const float2 pp = m;
+  const float2 sp = SIGN > 0 ? m : make_float2(-m.x, -m.y);
+  const float2 sm = SIGN > 0 ? make_float2(-m.x, -m.y) : m;
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     const float2 a0r = o[2 * c], a0i = o[2 * c + 1];
@@ -754,13 +770,10 @@ dwf_hop_pair_kernel(const HopParams p, const __grid_constant__ ChainCoef<typenam
       project<float, MU, SIGN, !kPh>(w1, h1);                                        \
       float2 h[12], o[12];                                                           \
       _Pragma("unroll") for (int q = 0; q < 12; ++q) h[q] = make_float2(h0[q], h1[q]); \
-      if (St::kScaled) {                                                             \
-        const float2 sc = make_float2(sc0, sc1);                                     \
-        _Pragma("unroll") for (int q = 0; q < 12; ++q) h[q] = __fmul2_rn(h[q], sc);  \
-      }                                                                              \
+      const float2 mul = St::kScaled ? make_float2(sc0 * (PH), sc1 * (PH)) : f2(PH); \
       LinkLoad<LF>::load(p.links, LIDX, u);                                          \
       su3_mult_half2<(SIGN < 0)>(u, h, o);                                           \
-      reconstruct_acc2<MU, SIGN>(acc, o, PH);                                        \
+      reconstruct_acc2<MU, SIGN>(acc, o, mul);                                       \
     }
 
 #define B200_PAIR_DIR(MU, COORD, EXT, NBP, NBM)                                      \
@@ -858,12 +871,11 @@ __device__ __forceinline__ void pair_compute(const PairRaw<P>& r, float ph, floa
   project<float, MU, SIGN, false>(w0, h0);   // LINK_F16_18: t factor in the links
   project<float, MU, SIGN, false>(w1, h1);
   float2 h[12], o[12];
-  const float2 sc = make_float2(r.sc0, r.sc1);
 #pragma unroll
-  for (int q = 0; q < 12; ++q) h[q] = __fmul2_rn(make_float2(h0[q], h1[q]), sc);
+  for (int q = 0; q < 12; ++q) h[q] = make_float2(h0[q], h1[q]);
   LinkLoad<LINK_F16_18>::decode(r.l0, r.l1, r.l2, u);
   su3_mult_half2<(SIGN < 0)>(u, h, o);
-  reconstruct_acc2<MU, SIGN>(acc, o, ph);
+  reconstruct_acc2<MU, SIGN>(acc, o, make_float2(r.sc0 * ph, r.sc1 * ph));
 }
 
 template <int LS, int P, int EPI, int FK, int MB>
@@ -1293,13 +1305,10 @@ dwf_hop_tma_pair_kernel(const HopParams p, const __grid_constant__ ChainCoef<typ
       project<float, MU, SIGN, !kPh>(w1, h1);                                        \
       float2 h[12], o[12];                                                           \
       _Pragma("unroll") for (int q = 0; q < 12; ++q) h[q] = make_float2(h0[q], h1[q]); \
-      if (St::kScaled) {                                                             \
-        const float2 sc = make_float2(sc0, sc1);                                     \
-        _Pragma("unroll") for (int q = 0; q < 12; ++q) h[q] = __fmul2_rn(h[q], sc);  \
-      }                                                                              \
+      const float2 mul = St::kScaled ? make_float2(sc0 * ph[D], sc1 * ph[D]) : f2(ph[D]); \
       LinkLoad<LF>::load_plain(c + TG::COL, u);                                      \
       su3_mult_half2<(SIGN < 0)>(u, h, o);                                           \
-      reconstruct_acc2<MU, SIGN>(acc, o, ph[D]);                                     \
+      reconstruct_acc2<MU, SIGN>(acc, o, mul);                                       \
     }                                                                                \
     __syncwarp();                                                                    \
     if ((D) + S < 8 && ok) {                                                         \

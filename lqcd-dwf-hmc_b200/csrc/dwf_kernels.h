@@ -149,6 +149,9 @@ cudaError_t launch_convert(int pout, void* out, int pin, const void* in, const G
                            cudaStream_t st);
 cudaError_t launch_from_corelib(int prec, void* out, const double* in_dev, const Geom& g,
                                 cudaStream_t st);
+// parity ieo of a full-lattice lexical Field(24, Nvol, Ls) on the device
+cudaError_t launch_from_lex_parity(int prec, void* out, const double* lex_dev, int ieo, const Geom& g,
+                                  cudaStream_t st);
 cudaError_t launch_to_corelib(int prec, double* out_dev, const void* in, const Geom& g,
                               cudaStream_t st);
 // lexical links (corelib Field_G layout) -> even/odd links in link format lf

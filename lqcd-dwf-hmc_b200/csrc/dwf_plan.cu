@@ -752,6 +752,14 @@ int b200_field_reverse_async(b200_dwf_t* op, int prec, double* v_host, const voi
   return 0;
 }
 
+int b200_field_convert_lex_device(b200_dwf_t* op, int prec, void* v, const double* w_lex_dev, int ieo,
+                                  void* stream) {
+  if (!op || !v || !w_lex_dev || prec < 0 || prec > 3 || (ieo != 0 && ieo != 1))
+    return fail(B200_EINVAL, "invalid argument");
+  B200_CHECK_CUDA(launch_from_lex_parity(prec, v, w_lex_dev, ieo, op->g, (cudaStream_t)stream));
+  return 0;
+}
+
 int b200_field_convert_device(b200_dwf_t* op, int prec, void* v, const double* w_dev, void* stream) {
   if (!op || !v || !w_dev || prec < 0 || prec > 3) return fail(B200_EINVAL, "invalid argument");
   B200_CHECK_CUDA(launch_from_corelib(prec, v, w_dev, op->g, (cudaStream_t)stream));

@@ -701,6 +701,26 @@ __global__ void from_corelib_kernel(Geom g, void* out, const double* in) {
   Store<P>::store(out, g.vh, g.ls, site, s, v);
 }
 
+// Parity ieo of a full-lattice lexical spinor Field(24, Nvol, Ls), index
+// in + 24*(x + Nx*(y + Ny*(z + Nz*t)) + Nvol*s), into the device layout of the
+// half lattice (Index_eo::convertField, src/lib/Field/index_eo.cpp).
+template <int P>
+__global__ void from_lex_parity_kernel(Geom g, void* out, const double* lex, int ieo) {
+  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long)g.vh * g.ls) return;
+  const int site = (int)(idx / g.ls), s = (int)(idx % g.ls);
+  const int ix2 = site % g.nx2;
+  const int yzt = site / g.nx2;
+  const int y = yzt % g.ny, z = (yzt / g.ny) % g.nz, t = yzt / (g.ny * g.nz);
+  const int x = 2 * ix2 + ((ieo + y + z + t) & 1);
+  const size_t lexsite = x + (size_t)(2 * g.nx2) * (y + (size_t)g.ny * (z + (size_t)g.nz * t));
+  const double* src = lex + 24 * (lexsite + (size_t)2 * g.vh * s);
+  typename Store<P>::R v[24];
+#pragma unroll
+  for (int i = 0; i < 24; ++i) v[i] = (typename Store<P>::R)src[i];
+  Store<P>::store(out, g.vh, g.ls, site, s, v);
+}
+
 template <int P>
 __global__ void to_corelib_kernel(Geom g, double* out, const void* in) {
   const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -862,6 +882,15 @@ cudaError_t launch_from_corelib(int prec, void* out, const double* in_dev, const
                                 cudaStream_t st) {
   const int grid = site_s_grid(g.ls, g.vh);
 #define L(PP) from_corelib_kernel<PP><<<grid, kSiteSBlock, 0, st>>>(g, out, in_dev)
+  B200_PREC_SWITCH(prec, L)
+#undef L
+  return cudaGetLastError();
+}
+
+cudaError_t launch_from_lex_parity(int prec, void* out, const double* lex_dev, int ieo, const Geom& g,
+                                  cudaStream_t st) {
+  const int grid = site_s_grid(g.ls, g.vh);
+#define L(PP) from_lex_parity_kernel<PP><<<grid, kSiteSBlock, 0, st>>>(g, out, lex_dev, ieo)
   B200_PREC_SWITCH(prec, L)
 #undef L
   return cudaGetLastError();

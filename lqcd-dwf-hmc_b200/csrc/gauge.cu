@@ -185,6 +185,38 @@ __global__ void axpy_links_kernel(double* y, const double* x, size_t n, double a
     y[i] = fma(a, x[i], y[i]);
 }
 
+// y = a x + b y over link fields (b = 0: y = a x, y not read)
+__global__ void axpby_links_kernel(double* y, const double* x, size_t n, double a, double b) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    y[i] = (b == 0.0) ? a * x[i] : fma(a, x[i], b * y[i]);
+}
+
+// iP = i sum_a h_a lambda_a on every link (Langevin_Momentum::set_iP_SU3,
+// src/lib/HMC/langevin_Momentum.cpp:150-210) from h = Field(8, Nvol, 4) of
+// Gaussians, written into the Field_G layout entry by entry: the Gell-Mann
+// matrices lambda_1..8 have at most two non-zero entries per position, and
+// lambda_8's 1/sqrt(3) is passed in (s).  Diagonal: i (h_3 +- s h_8) and
+// -2 i s h_8; off-diagonal (r, c) / (c, r): i h for the symmetric lambdas,
+// +-h for the antisymmetric ones.
+__global__ void momentum_from_gauss_kernel(const double* h, double* ip, size_t nlink, double s) {
+  const size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (idx >= nlink) return;
+  double a[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) a[k] = h[8 * idx + k];
+  double* o = ip + 18 * idx;
+  const double d8 = __dmul_rn(s, a[7]);
+  o[0] = 0.0;    o[1] = __dadd_rn(a[2], d8);               // (0,0)
+  o[2] = a[1];   o[3] = a[0];                               // (0,1)
+  o[4] = a[4];   o[5] = a[3];                               // (0,2)
+  o[6] = -a[1];  o[7] = a[0];                               // (1,0)
+  o[8] = 0.0;    o[9] = __dadd_rn(-a[2], d8);              // (1,1)
+  o[10] = a[6];  o[11] = a[5];                              // (1,2)
+  o[12] = -a[4]; o[13] = a[3];                              // (2,0)
+  o[14] = -a[6]; o[15] = a[5];                              // (2,1)
+  o[16] = 0.0;   o[17] = __dmul_rn(-2.0 * s, a[7]);        // (2,2)
+}
+
 __global__ void norm2_links_kernel(const double* x, size_t n, double* partial) {
   __shared__ double sh[256];
   double acc = 0.0;
@@ -301,6 +333,24 @@ int b200_momentum_energy(const int lattice[4], const double* ip, double* H, void
   double s = 0.0;
   for (int b = 0; b < nb; ++b) s += h[b];
   *H = 0.5 * s;
+  return 0;
+}
+
+int b200_links_axpby(const int lattice[4], double a, const double* x, double b, double* y, void* stream) {
+  LexGeom g;
+  if (!geom_ok(lattice, &g) || !x || !y) return fail_code(B200_EINVAL, "invalid argument");
+  axpby_links_kernel<<<592, 256, 0, (cudaStream_t)stream>>>(y, x, 18 * 4 * g.vol, a, b);
+  G_CHECK(cudaGetLastError());
+  return 0;
+}
+
+int b200_momentum_from_gauss(const int lattice[4], const double* h, double* ip, void* stream) {
+  LexGeom g;
+  if (!geom_ok(lattice, &g) || !h || !ip) return fail_code(B200_EINVAL, "invalid argument");
+  const size_t n = 4 * g.vol;
+  momentum_from_gauss_kernel<<<(unsigned)((n + 127) / 128), 128, 0, (cudaStream_t)stream>>>(
+      h, ip, n, 1.0 / std::sqrt(3.0));
+  G_CHECK(cudaGetLastError());
   return 0;
 }
 
