@@ -78,6 +78,14 @@ def parse():
                     help="also time FP64 CG with the windowed multishift")
     ap.add_argument("--traj-lattice", type=int, nargs=4, default=[24, 24, 24, 48],
                     help="lattice of the 2+1-flavour trajectory timing")
+    ap.add_argument("--traj-ls", type=int, default=LS, help="Ls of the trajectory timing")
+    ap.add_argument("--traj-mass-l", type=float, default=MQ,
+                    help="light quark mass of the trajectory timing")
+    ap.add_argument("--traj-inner", default="f16", choices=["f32", "f16", "bf16"],
+                    help="storage of the mixed-precision Richardson's inner solve")
+    ap.add_argument("--traj-forms", nargs="+", default=["fp64_plain", "mixed_batched"],
+                    help="trajectory forms to time (add mixed_batched_learned for the learned "
+                         "light solves; about 5 minutes more at 24^3x48)")
     return ap.parse_args()
 
 
@@ -492,11 +500,14 @@ def trajectory_section(op, lattice, u_workload, args, lp=None):
     # (name, solver kinds, multishift window): the plain form is FP64 CG with
     # every shift updated every iteration; the optimised forms use the
     # mixed-precision solves and the windowed (batched) multishift
-    forms = [("fp64_plain", cg, 0)]
+    forms = []
+    if "fp64_plain" in args.traj_forms:
+        forms.append(("fp64_plain", cg, 0))
     if args.traj_all_forms:
         forms.append(("fp64_batched", cg, 16))
-    forms.append(("mixed_batched", mixed, 16))
-    if lp is not None:
+    if "mixed_batched" in args.traj_forms:
+        forms.append(("mixed_batched", mixed, 16))
+    if lp is not None and "mixed_batched_learned" in args.traj_forms:
         forms.append(("mixed_batched_learned",
                       dict({k: "mixed+" for k in ("h_md", "h_h", "pv_h")}, l_md="learned",
                            l_h="learned"), 16))
@@ -511,7 +522,8 @@ def trajectory_section(op, lattice, u_workload, args, lp=None):
     shutil.rmtree(table_dir, ignore_errors=True)
     gc.collect()
     torch.cuda.empty_cache()
-    out = {"lattice": lattice, "Ls": LS, "M0": M0, "masses": TRAJ_MASSES,
+    out = {"lattice": lattice, "Ls": args.traj_ls, "M0": M0,
+           "masses": dict(TRAJ_MASSES, l=args.traj_mass_l), "inner_storage": args.traj_inner,
            "actions": "rational ratio (strange / PV, 16|24 poles, FP64 multishift), "
                       "Hasenbusch ratios light/0.1 and 0.1/PV, Iwasaki beta 2.13, "
                       "2 stout rho 0.1 on the fermion links",
@@ -535,8 +547,13 @@ def _trajectory_form(lattice, u0, args, lp, kinds, window, tol2, table_dir=None)
     torch.cuda.empty_cache()
     # "mixed+": mixed-precision Richardson whose MD solves start from the
     # action's previous solution (use_initial_guess)
-    sv = {k: Solver(v.rstrip("+"), tol2, chrono=v.endswith("+")) for k, v in kinds.items()}
-    hmc = build_dwf_nf2p1(lattice, LS, M0, TRAJ_MASSES, 2.13, nstep=args.traj_nstep,
+    inner = {"f32": 1, "f16": 2, "bf16": 3}[args.traj_inner]
+    sv = {k: Solver(v.rstrip("+"), tol2, chrono=v.endswith("+"), inner_prec=inner)
+          for k, v in kinds.items()}
+    torch.cuda.reset_peak_memory_stats()
+    free0, total = torch.cuda.mem_get_info()
+    hmc = build_dwf_nf2p1(lattice, args.traj_ls, M0, dict(TRAJ_MASSES, l=args.traj_mass_l), 2.13,
+                          nstep=args.traj_nstep,
                           tau=args.traj_length, np_md=16, np_h=24, tol2_md=tol2, tol2_h=tol2,
                           solvers=sv, shift_window=window, rational_dir=table_dir)
     if "learned" in kinds.values():
@@ -560,8 +577,13 @@ def _trajectory_form(lattice, u0, args, lp, kinds, window, tol2, table_dir=None)
     t0 = time.perf_counter()
     r = hmc.trajectory(ud, noise)
     torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
     out = {"sec_per_trajectory": time.perf_counter() - t0, "dH": r["dH"],
-           "H0": r["H0"], "multishift_window": window, **hmc.stats()}
+           "H0": r["H0"], "multishift_window": window,
+           "device_memory_gb": {"in_use_after": (total - free1) / 1e9,
+                                "added_by_this_form": (free0 - free1) / 1e9,
+                                "torch_peak_allocated": torch.cuda.max_memory_allocated() / 1e9},
+           **hmc.stats()}
     del hmc, ud, r, sv
     gc.collect()
     torch.cuda.empty_cache()

@@ -588,6 +588,15 @@ class Leapfrog:
         self.p.evolve(0.5 * e, ip, u)
 
 
+def _momentum_from_gauss(h, ip, nvol):
+    """iP = i sum_a h_a lambda_a on the 4*nvol links (b200_momentum_from_gauss);
+    the kernel sees only the site count, so both buffers are checked here."""
+    if ip.numel() != 72 * nvol or h.numel() != 32 * nvol:
+        raise ValueError("momentum: %d and %d reals for %d sites (72 and 32 per site expected)"
+                         % (ip.numel(), h.numel(), nvol))
+    check(lib().b200_momentum_from_gauss((ctypes.c_int * 4)(nvol, 1, 1, 1), _p(h), _p(ip), None))
+
+
 class DeviceNoise:
     """Gaussian heatbath fields drawn on the device (torch's Philox stream):
     momenta iP = i sum_a h_a lambda_a with <h_a^2> = 1/2, so that
@@ -606,9 +615,7 @@ class DeviceNoise:
         import torch
         h = torch.empty(ip.numel() // 18, 8, dtype=torch.float64, device="cuda")
         h.normal_(0.0, 0.5 ** 0.5, generator=self.g)
-        nlink = ip.numel() // 18        # the kernel needs only the link count
-        check(lib().b200_momentum_from_gauss((ctypes.c_int * 4)(nlink // 4, 1, 1, 4), _p(h), _p(ip),
-                                             None))
+        _momentum_from_gauss(h, ip, ip.numel() // 72)
 
     def fermion(self, field):
         field.buf.view(dtype=__import__("torch").float64).normal_(0.0, 0.5 ** 0.5, generator=self.g)
@@ -638,13 +645,15 @@ class MseriesNoise:
         self.rng.reset(seed)
 
     def momentum(self, ip):
-        h = self.rng.gauss_lex_global(8, 4)
-        check(lib().b200_momentum_from_gauss((ctypes.c_int * 4)(*self.lattice), _p(h), _p(ip), None))
+        _momentum_from_gauss(self.rng.gauss_lex_global(8, 4), ip, self.nvol)
 
     def fermion(self, field):
-        lex = self.rng.gauss_lex_global(24, field.op.Ls)
-        check(lib().b200_field_convert_lex_device(field.op.handle, field.prec, field.ptr, _p(lex), 0,
-                                                  None))
+        op = field.op
+        if 2 * op.nvol != self.nvol:
+            raise ValueError("noise lattice (%d sites) differs from the operator's (%d)"
+                             % (self.nvol, 2 * op.nvol))
+        lex = self.rng.gauss_lex_global(24, op.Ls)
+        check(lib().b200_field_convert_lex_device(op.handle, field.prec, field.ptr, _p(lex), 0, None))
 
 
 class HostNoise:
