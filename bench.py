@@ -63,11 +63,6 @@ def parse():
     ap.add_argument("--lattice", type=int, nargs=4, default=LATTICE)
     ap.add_argument("--no-learned", action="store_true",
                     help="skip training and timing the learned preconditioner")
-    ap.add_argument("--learned-configs", type=int, default=4,
-                    help="gauge configurations the network is trained on")
-    ap.add_argument("--learned-pairs", type=int, default=16,
-                    help="(residual, error) pairs per configuration")
-    ap.add_argument("--learned-epochs", type=int, default=2)
     ap.add_argument("--no-trajectory", action="store_true",
                     help="skip the molecular-dynamics trajectory timing")
     ap.add_argument("--traj-nstep", type=int, nargs=3, default=[2, 1, 3],
@@ -83,6 +78,16 @@ def parse():
                     help="light quark mass of the trajectory timing")
     ap.add_argument("--traj-inner", default="f16", choices=["f32", "f16", "bf16"],
                     help="storage of the mixed-precision Richardson's inner solve")
+    ap.add_argument("--traj-np-h", type=int, default=24,
+                    help="poles of the heatbath and Hamiltonian rationals (16 or 24)")
+    ap.add_argument("--traj-window", type=int, default=16,
+                    help="residual window of the batched forms' multishift")
+    ap.add_argument("--traj-force-pool", default="paired", choices=["paired", "streamed"],
+                    help="the rational force's solution fields: two sets side by side, or "
+                         "one set at a time (np_md fewer fields, one more multishift)")
+    ap.add_argument("--traj-only", action="store_true",
+                    help="time only the trajectory forms (a fresh process holds only their "
+                         "fields) and print their JSON; not the benchmark line")
     ap.add_argument("--traj-forms", nargs="+", default=["fp64_plain", "mixed_batched"],
                     help="trajectory forms to time (add mixed_batched_learned for the learned "
                          "light solves; about 5 minutes more at 24^3x48)")
@@ -387,53 +392,59 @@ def reference_arm(args, rank, world):
 
 
 # ------------------------------------------------------------------ learned preconditioner
+LEARNED_WEIGHTS = os.path.join(REPO, "lqcd-dwf-hmc_b200", "b200dwf", "learned_weights",
+                               "hmc_16x16x16x32_Ls16.npz")
+
+
 def learned_section(args):
     """On the learned preconditioner's configuration (16^3x32, Ls=16,
-    m=0.01): train the gauge-covariant network on CG (residual, error) pairs
-    of seeded configurations (near-unit links + 2 stout steps, other seeds
-    than the evaluation's) and compare flexible CG with it against plain FP64
-    CG on the evaluation configuration and RHS, both to |r|/|b| < 1e-10."""
+    m=0.01): the network trained on the plain HMC's own configurations
+    (b200dwf.learned_train: 20 trajectories from conf_04040408.txt tiled,
+    100 CG (residual, error) pairs each; the committed weights and their
+    training record), evaluated on the tiled start after 2 stout steps --
+    a configuration it never saw -- with the workload's RHS: flexible CG with
+    it against plain FP64 CG, both to |r|/|b| < 1e-10.  One network
+    application is timed with CUDA events with both convolution kernels
+    (tensor cores, and packed FFMA2)."""
     import torch
     import b200dwf
-    from b200dwf import synth
+    from b200dwf import learned_train
+    from b200dwf.hopbench import learned_flops
     lattice = list(LEARN_LATTICE)
-    u_workload, b_host = workload_inputs(lattice, LS, device_smear=True)
+    z = np.load(LEARNED_WEIGHTS)
+    record = json.loads(str(z["record"]))
+    hidden = int(z["hidden"])
+    _, b_host = workload_inputs(lattice, LS)
     op = b200dwf.DomainWall(lattice, LS, MQ, M0, 1.0, 0.0, 1.0, (1, 1, 1, -1))
-    op.set_config(u_workload)
+    op.set_config(learned_train.smeared(learned_train.tiled_start(lattice), lattice))
     w = op.new_field(0)
     op.convert(w, b_host)
-    lp = b200dwf.LearnedPrecond(op, hidden=8, seed=11)
-    sm = b200dwf.StoutSmear(lattice, 0.1, 2)
-    losses = []
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    npairs = 0
-    for c in range(args.learned_configs):
-        sm.set_config(synth.gauge_field(lattice, SEED_U + 1000 + c, "near", 0.3))
-        op.set_config(sm.config(2))
-        b = op.new_field(0)
-        op.convert(b, synth.spinor_field(lattice, LS, SEED_B + 1000 + c))
-        n_ref, _, _ = op.cg(op.new_field(0), b, 1e-20, 20000)
-        iters = sorted(set(int(v) for v in np.linspace(2, max(3, n_ref - 2), args.learned_pairs)))
-        rs, es = b200dwf.cg_training_pairs(op, b, iters)
-        npairs += len(rs)
-        losses.append(lp.train(rs, es, args.learned_epochs, 3e-3, seed=c + 1))
-        del rs, es
-    torch.cuda.synchronize()
-    t_train = time.perf_counter() - t0
-    op.set_config(u_workload)
-    # network apply alone, CUDA events
+    lp = b200dwf.LearnedPrecond(op, hidden=hidden, seed=11)
+    lp.set_weights(z["weights"])
+    # one network application, CUDA events, each convolution kernel
     r32 = op.new_field(1)
     z32 = op.new_field(1)
     op.copy_convert(r32, w)
-    lp.apply(z32, r32)
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record()
-    for _ in range(10):
-        lp.apply(z32, r32)
-    ev1.record()
-    torch.cuda.synchronize()
-    t_apply = ev0.elapsed_time(ev1) / 10 / 1e3
+    apply_ms = {}
+    old = os.environ.get("B200_LP_CONV")
+    try:
+        for kernel in ("ffma2", "tc"):
+            os.environ["B200_LP_CONV"] = kernel
+            lp.apply(z32, r32)
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record()
+            for _ in range(10):
+                lp.apply(z32, r32)
+            ev1.record()
+            torch.cuda.synchronize()
+            apply_ms[kernel] = ev0.elapsed_time(ev1) / 10
+    finally:
+        if old is None:
+            os.environ.pop("B200_LP_CONV", None)
+        else:
+            os.environ["B200_LP_CONV"] = old
+    op.check_error()
+    flops = learned_flops(vh_of(lattice), LS, hidden)
     op.fcg(op.new_field(0), w, lp, 1.0, 20000, 8)     # untimed: flexible-CG buffers
     res = {}
     for name, fn in (("cg_f64", lambda x: op.cg(x, w, 1e-20, 20000)),
@@ -452,11 +463,17 @@ def learned_section(args):
             res[name] = {"iterations": out[0], "fallback_cg_iterations": out[1],
                          "true_rel_residual": out[2], "seconds": c1 - c0, "converged": out[3] == 0,
                          "orthogonalised_against": 8 if name == "fcg_learned" else 2}
-    return {"network": "3 layers, 4->8->4 channels per color, 11 paths, BF16 weights, FP32 accumulate",
-            "lattice": lattice, "train_configs": args.learned_configs, "train_pairs": npairs,
-            "epochs_per_config": args.learned_epochs,
-            "loss_first_last_per_config": losses, "train_seconds": t_train,
-            "apply_ms": t_apply * 1e3, "tol_rel_residual": 1e-10, **res,
+    train = record.get("train", [])
+    return {"network": "3 layers, 4->%d->4 channels per color, 11 paths, BF16 weights, "
+                       "channel mixing on tcgen05 (BF16 hi+lo inputs, FP32 accumulation)" % hidden,
+            "lattice": lattice, "evaluated_on": "conf_04040408.txt tiled, 2 stout rho 0.1",
+            "trained_on": "%d HMC configurations, %d CG pairs (b200dwf.learned_train)"
+                          % (len(train), record.get("pairs", 0)),
+            "train_loss_first_last_config": [train[0]["loss_first"], train[-1]["loss_last"]]
+                                            if train else None,
+            "apply_ms": apply_ms["tc"], "apply_ms_ffma2": apply_ms["ffma2"],
+            "apply_tflops": flops / (apply_ms["tc"] * 1e-3) / 1e12,
+            "tol_rel_residual": 1e-10, **res,
             "iteration_ratio": res["cg_f64"]["iterations"] / max(1, res["fcg_learned"]["iterations"]
                                                                  + res["fcg_learned"]["fallback_cg_iterations"]),
             "time_ratio": res["cg_f64"]["seconds"] / res["fcg_learned"]["seconds"]}, lp
@@ -506,11 +523,11 @@ def trajectory_section(op, lattice, u_workload, args, lp=None):
     if args.traj_all_forms:
         forms.append(("fp64_batched", cg, 16))
     if "mixed_batched" in args.traj_forms:
-        forms.append(("mixed_batched", mixed, 16))
+        forms.append(("mixed_batched", mixed, args.traj_window))
     if lp is not None and "mixed_batched_learned" in args.traj_forms:
         forms.append(("mixed_batched_learned",
                       dict({k: "mixed+" for k in ("h_md", "h_h", "pv_h")}, l_md="learned",
-                           l_h="learned"), 16))
+                           l_h="learned"), args.traj_window))
     tol2 = 1e-20
     res = {}
     for name, kinds, window in forms:
@@ -530,8 +547,9 @@ def trajectory_section(op, lattice, u_workload, args, lp=None):
            "integrator": "Omelyan %s, lambda 0.1931833275" % list(args.traj_nstep),
            "length": args.traj_length, "solver_tol_rel_residual": 1e-10,
            "links": "conf_04040408.txt tiled (the reference benchmark's start configuration)",
-           "rational_tables": "the reference's shipped 16-pole (MD) and 24-pole (heatbath, H) "
-                              "tables on [1e-4, 10]", **res}
+           "rational_tables": "the reference's shipped 16-pole (MD) and %d-pole (heatbath, H) "
+                              "tables on [1e-4, 10]" % args.traj_np_h,
+           "rational_force_pool": args.traj_force_pool, **res}
     for name in res:
         if "sec_per_trajectory" in res[name] and "sec_per_trajectory" in res.get("fp64_plain", {}):
             out["speedup_" + name] = (res["fp64_plain"]["sec_per_trajectory"]
@@ -554,11 +572,12 @@ def _trajectory_form(lattice, u0, args, lp, kinds, window, tol2, table_dir=None)
     free0, total = torch.cuda.mem_get_info()
     hmc = build_dwf_nf2p1(lattice, args.traj_ls, M0, dict(TRAJ_MASSES, l=args.traj_mass_l), 2.13,
                           nstep=args.traj_nstep,
-                          tau=args.traj_length, np_md=16, np_h=24, tol2_md=tol2, tol2_h=tol2,
-                          solvers=sv, shift_window=window, rational_dir=table_dir)
+                          tau=args.traj_length, np_md=16, np_h=args.traj_np_h, tol2_md=tol2,
+                          tol2_h=tol2, solvers=sv, shift_window=window, rational_dir=table_dir,
+                          rational_force_pool=args.traj_force_pool)
     if "learned" in kinds.values():
-        # the trained weights are volume independent; the network runs on
-        # the light operator's own (smeared) links
+        # the trained weights are independent of volume and Ls; the network
+        # runs on the light operator's own (smeared) links
         lp_form = b200dwf.LearnedPrecond(hmc.fermions["nf2"].f.op, hidden=lp.hidden, seed=1)
         lp_form.set_weights(lp.weights(deployed=False))
         for v in sv.values():
@@ -591,6 +610,45 @@ def _trajectory_form(lattice, u0, args, lp, kinds, window, tol2, table_dir=None)
 
 
 # ------------------------------------------------------------------ B200 arm
+class _Weights:
+    """The committed network weights in the shape _trajectory_form reads."""
+
+    def __init__(self, path):
+        z = np.load(path)
+        self.hidden = int(z["hidden"])
+        self._w = z["weights"]
+
+    def weights(self, deployed=False):
+        return self._w
+
+
+def trajectory_only(args):
+    """--traj-only: the trajectory forms alone, with the peak device memory
+    the process reached (torch's allocator and the library's own
+    allocations alike, from cudaMemGetInfo polled during the run)."""
+    import torch
+    torch.cuda.init()
+    lp = _Weights(LEARNED_WEIGHTS) if "mixed_batched_learned" in args.traj_forms else None
+    free_min = [torch.cuda.mem_get_info()[0]]
+    stop = threading.Event()
+
+    def poll():
+        while not stop.wait(0.5):
+            free_min[0] = min(free_min[0], torch.cuda.mem_get_info()[0])
+
+    total = torch.cuda.mem_get_info()[1]
+    thr = threading.Thread(target=poll, daemon=True)
+    thr.start()
+    try:
+        out = trajectory_section(None, args.traj_lattice, None, args, lp)
+    finally:
+        stop.set()
+        thr.join()
+    out["device_memory_high_water_gb"] = (total - free_min[0]) / 1e9
+    out["device_memory_total_gb"] = total / 1e9
+    print(json.dumps(out))
+
+
 def b200_arm(args, rank, world, local_rank):
     import torch
     import b200dwf
@@ -866,6 +924,13 @@ def b200_arm(args, rank, world, local_rank):
             if "speedup_" + form in trajectory:
                 line["speedup_" + form] = round(trajectory["speedup_" + form], 3)
         line["speedup_target"] = 3.0
+    if learned:
+        # one network application (tensor-core and FFMA2 convolutions), and
+        # CG / flexible-CG iterations and seconds on an unseen configuration
+        line["learned_apply_ms"] = round(learned["apply_ms"], 3)
+        line["learned_apply_ms_ffma2"] = round(learned["apply_ms_ffma2"], 3)
+        line["learned_iteration_ratio"] = round(learned["iteration_ratio"], 3)
+        line["learned_time_ratio"] = round(learned["time_ratio"], 3)
     if cpu_traj:
         line["sec_traj_cpu_reference_extrapolated"] = round(cpu_traj["sec_per_trajectory"], 1)
     if published and "device_sec" in published:
@@ -893,6 +958,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         reference_arm(args, rank, world)
+        return
+    if args.traj_only:
+        trajectory_only(args)
         return
     if world > 1:
         import datetime

@@ -407,12 +407,23 @@ class ActionFRationalRatio:
     det[(B^dag B)^(1/2) / (A^dag A)^(1/2)], A = fopr_numer (Pauli-Villars),
     B = fopr_denom.  rats: dict of Rational coefficient sets
     'md_numer' x^(1/4), 'md_denom' x^(-1/2), 'h_numer' x^(1/4),
-    'h_denom' x^(-1/2), 'psf_denom' x^(1/4), 'psf_numer' x^(-1/4)."""
+    'h_denom' x^(-1/2), 'psf_denom' x^(1/4), 'psf_numer' x^(-1/4).
 
-    def __init__(self, fopr_numer, fopr_denom, rats, tol2_md, tol2_h, label=""):
+    force_pool: 'paired' keeps the numerator's two sets of shifted solutions
+    (eta1_i, zeta_i) side by side, 2*np_md solution fields; 'streamed' takes
+    the numerator's cross terms from two further multishift solves of the
+    combined sources s*phi +- v/s (one balance factor s for all poles), one
+    set of np_md solution fields at a time: np_md fewer fields (39 GB at
+    32^3x64 Ls=12, FP64) for one more multishift per force evaluation."""
+
+    def __init__(self, fopr_numer, fopr_denom, rats, tol2_md, tol2_h, label="",
+                 force_pool="paired"):
         from . import Field
+        if force_pool not in ("paired", "streamed"):
+            raise ValueError("force_pool: 'paired' or 'streamed'")
         self.fa, self.fb = fopr_numer, fopr_denom
         self.label = label
+        self.force_pool = force_pool
         self.md_numer = FoprRational(fopr_numer, rats["md_numer"], tol2_md)
         self.md_denom = FoprRational(fopr_denom, rats["md_denom"], tol2_md)
         self.md_numer2 = FoprRational(fopr_numer, rats["md_numer"], tol2_md)
@@ -431,10 +442,17 @@ class ActionFRationalRatio:
         nmd, nh = len(rats["md_numer"].c), len(rats["h_numer"].c)
         if len(rats["md_denom"].c) != nmd:
             raise ValueError("numerator and denominator MD rationals need equal pole counts")
-        self.pool = [Field(op) for _ in range(max(2 * nmd, nh))]
-        self.md_numer.xs = self.pool[:nmd]
-        self.md_denom.xs = self.pool[nmd:2 * nmd]
-        self.md_numer2.xs = self.pool[nmd:2 * nmd]
+        if force_pool == "paired":
+            self.pool = [Field(op) for _ in range(max(2 * nmd, nh))]
+            self.md_numer.xs = self.pool[:nmd]
+            self.md_denom.xs = self.pool[nmd:2 * nmd]
+            self.md_numer2.xs = self.pool[nmd:2 * nmd]
+        else:
+            # eta1_i only make v1, eta2_i only the denominator's forces, and
+            # the combined sources' solutions are used one set at a time
+            self.pool = [Field(op) for _ in range(max(nmd, nh))]
+            for r in (self.md_numer, self.md_denom, self.md_numer2):
+                r.xs = self.pool[:nmd]
         for r in (self.h_numer, self.h_denom, self.psf_denom, self.psf_numer):
             r.xs = self.pool[:len(r.r.c)]
 
@@ -472,6 +490,21 @@ class ActionFRationalRatio:
         self.md_denom.mult(self.v2, self.v1)           # xi, eta2_i in md_denom.xs
         for bi, e2 in zip(rd.b, self.md_denom.xs):
             check(L.b200_dwf_force_acc(fb.handle, b"DdagD", _p(acc), e2.ptr, None, bi, None))
+        if self.force_pool == "streamed":
+            # sum_i b_i cross(eta1_i, zeta_i) = sum_i b_i/4 [F(x+_i) - F(x-_i)],
+            # x+-_i = (A^dag A + c_i)^-1 (s psf +- v2/s): F is quadratic and
+            # the shifted solve linear in its source
+            npsf, nv2 = fa.norm2(self.psf), fa.norm2(self.v2)
+            if npsf == 0.0 or nv2 == 0.0:
+                return
+            s = (nv2 / npsf) ** 0.25
+            for sign in (1.0, -1.0):
+                fa.axpby(self.t1, s, self.psf, 0.0)
+                fa.axpby(self.t1, sign / s, self.v2, 1.0)
+                for bi, x in zip(rn.b, self.md_numer2.shifts(self.t1)):
+                    check(L.b200_dwf_force_acc(fa.handle, b"DdagD", _p(acc), x.ptr, None,
+                                               0.5 * sign * bi, None))
+            return
         zetas = self.md_numer2.shifts(self.v2)         # zeta_i, over the eta2_i slots
         for bi, e1, z in zip(rn.b, self.md_numer.xs, zetas):
             ne, nz = fa.norm2(e1), fa.norm2(z)
@@ -848,7 +881,8 @@ def build_dwf_nf2p1(lattice, Ls, M0, masses, beta, c_plaq=3.648, c_rect=-0.331, 
                     lam=0.1931833275, nprec=8, np_md=16, np_h=24, rat_bounds=(1e-2, 3.16227766),
                     tol2_md=1e-20, tol2_h=1e-20, solvers=None, b=1.0, c=0.0,
                     bc=(1, 1, 1, -1), integrator="Omelyan", shift_window=None,
-                    rational_dir=None, tol2_rat_md=None, tol2_rat_h=None):
+                    rational_dir=None, tol2_rat_md=None, tol2_rat_h=None,
+                    rational_force_pool="paired"):
     """The benchmark driver's action set (hmc_dwf_eo.cpp:155-352) on the
     device.  masses: dict l (light), h (Hasenbusch), s (strange), pv.
     solvers: dict of Solver objects 'l_md', 'l_h', 'h_md', 'h_h', 'pv_h'
@@ -859,7 +893,9 @@ def build_dwf_nf2p1(lattice, Ls, M0, masses, beta, c_plaq=3.648, c_rect=-0.331, 
     the reference reads them from its run directory.  tol2_rat_md /
     tol2_rat_h: the multishift tolerances of the rational operators
     (Fopr_Nf1_Rational_MD / _calcH convergence_criterion_squared; default
-    tol2_md / tol2_h)."""
+    tol2_md / tol2_h).  rational_force_pool: ActionFRationalRatio's
+    force_pool ('streamed' for lattices whose 2*np_md solution fields do not
+    fit beside the rest)."""
     from . import DomainWall
     from .rational import Rational, TABLE_DIR
     tdir = rational_dir or TABLE_DIR
@@ -887,7 +923,8 @@ def build_dwf_nf2p1(lattice, Ls, M0, masses, beta, c_plaq=3.648, c_rect=-0.331, 
     for k, t in (("l_md", tol2_md), ("h_md", tol2_md), ("l_h", tol2_h), ("h_h", tol2_h),
                  ("pv_h", tol2_h)):
         sv.setdefault(k, Solver("cg", t))
-    nf1 = ActionFRationalRatio(f_pv1, f_s, rats, tol2_rat_md, tol2_rat_h, "Nf1")
+    nf1 = ActionFRationalRatio(f_pv1, f_s, rats, tol2_rat_md, tol2_rat_h, "Nf1",
+                               force_pool=rational_force_pool)
     nf2 = ActionFRatio(f_h, f_l, sv["l_md"], sv["l_h"], sv["h_h"], "Nf2")
     nf2p = ActionFRatio(f_pv, f_h, sv["h_md"], sv["h_h"], sv["pv_h"], "Nf2_prec")
     gauge = ActionGRectangle(lattice, beta, c_plaq, c_rect)

@@ -13,7 +13,16 @@ call and GB/s,
 with s_spinor the stored bytes of one (site, s) spinor (f64 192, f32 96,
 f16/bf16 48 + a 4-byte scale) and s_link the bytes of one link record (f64
 144, f32 80, f16/bf16 48).  --variant pins the hop kernel variant
-(B200_HOP_VARIANT) instead of the autotuner's choice."""
+(B200_HOP_VARIANT) instead of the autotuner's choice.
+
+    python -m b200dwf.hopbench --learned [--hidden 8] [--lp-conv ffma2] ...
+
+times one application of the learned preconditioner instead (five
+convolution launches on FP32 fields) and reports its FP32 work: per
+(site, s, color) row and path, 8 flops per complex multiply-add of the
+channel mixing, and per row and hop path 72 flops per channel of the SU(3)
+transport.  --lp-conv ffma2 selects the packed-FFMA2 convolution kernel
+(B200_LP_CONV) instead of the tensor-core one."""
 import argparse
 import json
 import os
@@ -36,9 +45,16 @@ def main(argv=None):
     ap.add_argument("--variant", type=int, default=None)
     ap.add_argument("--mq", type=float, default=0.01)
     ap.add_argument("--m0", type=float, default=1.8)
+    ap.add_argument("--learned", action="store_true")
+    ap.add_argument("--hidden", type=int, default=8)
+    ap.add_argument("--lp-conv", default=None, choices=["tc", "ffma2"])
     a = ap.parse_args(argv)
     if a.variant is not None:
         os.environ["B200_HOP_VARIANT"] = str(a.variant)
+    if a.lp_conv is not None:
+        os.environ["B200_LP_CONV"] = a.lp_conv
+    if a.learned:
+        return learned(a)
     import torch
     import b200dwf
     from b200dwf import synth
@@ -68,6 +84,45 @@ def main(argv=None):
         nbytes = vh * (a.ls * 2 * SPINOR_BYTES[prec] + 8 * LINK_BYTES[prec])
         out.update(bytes_per_call=nbytes, gbs=nbytes / (us * 1e-6) / 1e9)
     print(json.dumps(out))
+
+
+def learned_flops(vh, ls, hidden):
+    """FP32 flops of one network application (five launches)."""
+    rows = vh * ls
+    f = 0
+    for npath, nhop, cin, cout in ((3, 0, 4, hidden), (8, 8, 4, hidden), (11, 8, hidden, hidden),
+                                   (11, 8, hidden, hidden), (11, 8, hidden, 4)):
+        f += rows * (3 * npath * cin * cout * 8 + nhop * cin * 72)
+    return f
+
+
+def learned(a):
+    import torch
+    import b200dwf
+    from b200dwf import synth
+    op = b200dwf.DomainWall(a.lattice, a.ls, a.mq, a.m0)
+    op.set_config(synth.gauge_field(a.lattice, 1234567, "near", eps=0.3))
+    lp = b200dwf.LearnedPrecond(op, hidden=a.hidden, seed=3, init_noise=0.1)
+    f64 = op.new_field(0)
+    op.convert(f64, synth.spinor_field(a.lattice, a.ls, 7654321))
+    r, z = op.new_field(1), op.new_field(1)
+    op.copy_convert(r, f64)
+    for _ in range(a.warmup):
+        lp.apply(z, r)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.reps):
+        lp.apply(z, r)
+    e1.record()
+    torch.cuda.synchronize()
+    op.check_error()
+    us = e0.elapsed_time(e1) * 1e3 / a.reps
+    vh = int(np.prod(a.lattice)) // 2
+    fl = learned_flops(vh, a.ls, a.hidden)
+    print(json.dumps({"lattice": a.lattice, "Ls": a.ls, "learned": True, "hidden": a.hidden,
+                      "lp_conv": os.environ.get("B200_LP_CONV", "tc"), "us_per_apply": us,
+                      "flops_per_apply": fl, "tflops": fl / (us * 1e-6) / 1e12}))
 
 
 if __name__ == "__main__":

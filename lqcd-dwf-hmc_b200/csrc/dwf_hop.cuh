@@ -507,10 +507,17 @@ __device__ __forceinline__ void hop_epilogue_rows(const HopParams& p,
       for (int w = 0; w < WARPS; ++w) b += red_warp[w];
       if (NR == 1) {
         p.red[blockIdx.x] = b;
-      } else {
+      } else if (32 % LS == 0) {
         const int nb1 = (p.vh + WARPS * (32 / LS) - 1) / (WARPS * (32 / LS));
         p.red[2 * blockIdx.x] = b;
         if (2 * (int)blockIdx.x + 1 < nb1) p.red[2 * blockIdx.x + 1] = 0.0;
+      } else {
+        // Ls not dividing 32 (6, 12): the host reduces the one-slice kernel's
+        // block count of partials, more than this grid has blocks; each block
+        // writes its own and clears its share of the rest
+        const int nb1 = (p.vh + WARPS * (32 / LS) - 1) / (WARPS * (32 / LS));
+        p.red[blockIdx.x] = b;
+        for (int j = (int)(gridDim.x + blockIdx.x); j < nb1; j += (int)gridDim.x) p.red[j] = 0.0;
       }
     }
   }
@@ -718,7 +725,7 @@ dwf_hop_pair_kernel(const HopParams p, const __grid_constant__ ChainCoef<typenam
   using St = Store<P>;
   using R = typename St::R;
   static_assert(sizeof(R) == 4, "packed kernel is for FP32 arithmetic");
-  static_assert(32 % LS == 0 && LS % 2 == 0, "packed kernel needs Ls | 32");
+  static_assert(LS % 2 == 0 && LS / 2 <= 32, "packed kernel: even Ls, at most 64");
   constexpr bool kDagHop = EpiIsDag<EPI>::v;
   constexpr bool kPh = LinkLoad<LF>::kFolded;
   constexpr int H = LS / 2;               // lanes per site
@@ -856,23 +863,87 @@ __device__ __forceinline__ void pair_decode(const uint4 (&c)[3], float* v) {
   }
 }
 
+// The Dirac-basis projection (1 - sign*gamma_mu) of project(), applied to the
+// stored (re, im) half-precision pairs before any conversion to FP32: each
+// projected colour is one paired multiply-add, h = w_a + f * w_b or
+// w_a + f * swap(w_b) with f = (+-1, +-1), so a slice converts 6 pairs instead
+// of 12 and issues 6 paired operations instead of 12 FP32 adds.  The rounding
+// this adds is that of the storage format itself.  w[c + 3*spin],
+// h[c + 3*a]; t projection without its factor 2 (folded into the links).
+template <typename H2> struct Half2Ops;
+template <> struct Half2Ops<__half2> {
+  __device__ static __half2 k(float a, float b) { return __floats2half2_rn(a, b); }
+  __device__ static float2 f2(__half2 h) { return __half22float2(h); }
+};
+template <> struct Half2Ops<__nv_bfloat162> {
+  __device__ static __nv_bfloat162 k(float a, float b) { return __floats2bfloat162_rn(a, b); }
+  __device__ static float2 f2(__nv_bfloat162 h) { return __bfloat1622float2(h); }
+};
+
+template <typename H2, int MU, int SIGN>
+__device__ __forceinline__ void project_half2(const H2* w, H2* h) {
+  using O = Half2Ops<H2>;
+  constexpr float S = SIGN > 0 ? 1.f : -1.f;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const H2 w0 = w[c], w1 = w[c + 3], w2 = w[c + 6], w3 = w[c + 9];
+    H2 h0, h1;
+    if (MU == 0) {        // h0 = w0 -+ i w3, h1 = w1 -+ i w2 (as project)
+      h0 = __hfma2(__lowhigh2highlow(w3), O::k(-S, S), w0);
+      h1 = __hfma2(__lowhigh2highlow(w2), O::k(-S, S), w1);
+    } else if (MU == 1) { // h0 = w0 +- w3, h1 = w1 -+ w2
+      h0 = __hfma2(w3, O::k(S, S), w0);
+      h1 = __hfma2(w2, O::k(-S, -S), w1);
+    } else if (MU == 2) { // h0 = w0 -+ i w2, h1 = w1 +- i w3
+      h0 = __hfma2(__lowhigh2highlow(w2), O::k(-S, S), w0);
+      h1 = __hfma2(__lowhigh2highlow(w3), O::k(S, -S), w1);
+    } else {              // (1 - g4) keeps the lower spins, (1 + g4) the upper
+      h0 = SIGN > 0 ? w2 : w0;
+      h1 = SIGN > 0 ? w3 : w1;
+    }
+    h[c] = h0;
+    h[c + 3] = h1;
+  }
+}
+
+template <int P> struct Half2Of;
+template <> struct Half2Of<PREC_F16> { using T = __half2; };
+template <> struct Half2Of<PREC_BF16> { using T = __nv_bfloat162; };
+
+// the 12 stored pairs of one slice (three 16-byte chunks), spins swapped for
+// the gamma5-sandwiched dagger hop
+template <int P, bool kDagHop>
+__device__ __forceinline__ void pair_unpack(const uint4 (&c)[3], typename Half2Of<P>::T* w) {
+  using H2 = typename Half2Of<P>::T;
+  unsigned int u[12];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    u[4 * k] = c[k].x; u[4 * k + 1] = c[k].y; u[4 * k + 2] = c[k].z; u[4 * k + 3] = c[k].w;
+  }
+#pragma unroll
+  for (int q = 0; q < 12; ++q) {
+    const unsigned int v = kDagHop ? u[(q + 6) % 12] : u[q];
+    w[q] = *reinterpret_cast<const H2*>(&v);
+  }
+}
+
 template <int P, int MU, int SIGN, bool kDagHop>
 __device__ __forceinline__ void pair_compute(const PairRaw<P>& r, float ph, float2* acc) {
-  float w0[24], w1[24], h0[12], h1[12], u[18];
-  pair_decode<P>(r.c0, w0);
-  pair_decode<P>(r.c1, w1);
-  if (kDagHop) {
-#pragma unroll
-    for (int q = 0; q < 12; ++q) {
-      float t0 = w0[q]; w0[q] = w0[q + 12]; w0[q + 12] = t0;
-      float t1 = w1[q]; w1[q] = w1[q + 12]; w1[q + 12] = t1;
-    }
-  }
-  project<float, MU, SIGN, false>(w0, h0);   // LINK_F16_18: t factor in the links
-  project<float, MU, SIGN, false>(w1, h1);
+  using H2 = typename Half2Of<P>::T;
+  using O = Half2Ops<H2>;
+  float u[18];
+  H2 w0[12], w1[12], p0[6], p1[6];
+  pair_unpack<P, kDagHop>(r.c0, w0);
+  pair_unpack<P, kDagHop>(r.c1, w1);
+  project_half2<H2, MU, SIGN>(w0, p0);
+  project_half2<H2, MU, SIGN>(w1, p1);
   float2 h[12], o[12];
 #pragma unroll
-  for (int q = 0; q < 12; ++q) h[q] = make_float2(h0[q], h1[q]);
+  for (int q = 0; q < 6; ++q) {
+    const float2 a = O::f2(p0[q]), b = O::f2(p1[q]);
+    h[2 * q] = make_float2(a.x, b.x);
+    h[2 * q + 1] = make_float2(a.y, b.y);
+  }
   LinkLoad<LINK_F16_18>::decode(r.l0, r.l1, r.l2, u);
   su3_mult_half2<(SIGN < 0)>(u, h, o);
   reconstruct_acc2<MU, SIGN>(acc, o, make_float2(r.sc0 * ph, r.sc1 * ph));
@@ -885,7 +956,7 @@ dwf_hop_pair_pf_kernel(const HopParams p, const __grid_constant__ ChainCoef<type
   using St = Store<P>;
   using R = typename St::R;
   static_assert(St::kScaled, "prefetching packed kernel is for f16/bf16 storage");
-  static_assert(32 % LS == 0 && LS % 2 == 0, "packed kernel needs Ls | 32");
+  static_assert(LS % 2 == 0 && LS / 2 <= 32, "packed kernel: even Ls, at most 64");
   constexpr bool kDagHop = EpiIsDag<EPI>::v;
   constexpr int H = LS / 2;
   constexpr int G = 32 / H;
@@ -1185,7 +1256,7 @@ dwf_hop_tma_pair_kernel(const HopParams p, const __grid_constant__ ChainCoef<typ
   using St = Store<P>;
   using R = typename St::R;
   static_assert(sizeof(R) == 4, "packed kernel is for FP32 arithmetic");
-  static_assert(32 % LS == 0 && LS % 2 == 0, "packed kernel needs Ls | 32");
+  static_assert(LS % 2 == 0 && LS / 2 <= 32, "packed kernel: even Ls, at most 64");
   constexpr int H = LS / 2;
   constexpr int G = 32 / H;
   using TG = TmaGeom<LS, P, LF, G>;

@@ -271,7 +271,9 @@ bool variant_supported(int prec, int ls, int v) {
   // 8 stages of 16 sites x (f32 column + 80-byte link record) per warp would
   // need 232 KB of shared memory per block, above the 227 KB limit
   if (v == 8 && ls == 4 && prec == PREC_F32) return false;
-  return prec != PREC_F64 && 32 % ls == 0;
+  // packed two-slice kernels: every supported Ls (all even); Ls/2 lanes per
+  // site, 32/(Ls/2) sites per warp, the remaining lanes idle (Ls 6, 12)
+  return prec != PREC_F64;
 }
 std::map<TuneKey, std::pair<int, float> > g_tune;
 std::mutex g_tune_mu;
@@ -480,8 +482,8 @@ int report_err(b200_dwf* op, cudaStream_t st) {
   B200_CHECK_CUDA(cudaMemsetAsync(op->err, 0, sizeof(int), st));
   B200_CHECK_CUDA(cudaStreamSynchronize(st));
   return fail(B200_ECUDA,
-              "a hop kernel gave up waiting for its bulk copies (device error word %d); "
-              "its outputs were not written",
+              "a kernel gave up waiting for its bulk copies or tensor-core work "
+              "(device error word %d); its outputs were not written",
               code);
 }
 
@@ -1548,6 +1550,8 @@ int plan_geometry(b200_dwf* op, Geom* g, float bc[4]) {
 int plan_apply_ddagd(b200_dwf* op, void* v, const void* w, cudaStream_t st) {
   return apply_mode(op, PREC_F32, v, w, "DdagD", 0, st);
 }
+int* plan_error_word(b200_dwf* op) { return op->err; }
+int plan_check_error(b200_dwf* op, cudaStream_t st) { return check_err(op, st); }
 int plan_links_f32(b200_dwf* op, const void** links, cudaStream_t st) {
   const int rc = ensure_link_format(op, LINK_F32_12, st);
   if (rc) return rc;

@@ -113,14 +113,14 @@ cudaError_t run_tma_pair(const HopParams& p, const ChainCoefs& c, cudaStream_t s
 // arithmetic: the packed kernel) at 2 resident blocks; 8: the packed kernel
 // with all 8 directions in flight at once; 9: the packed kernel for f16/bf16
 // storage fetching the next direction into registers while computing the
-// current one (5-9 packed: FP32 arithmetic and Ls dividing 32 only).
+// current one (5-9 packed: FP32 arithmetic only).
 template <int LS, int P, int EPI, int FK>
 cudaError_t run(const HopParams& p, const ChainCoefs& c, cudaStream_t st) {
   if (p.variant == 1) return run_tma<LS, P, EPI, FK, 2, 1>(p, c, st);
   if (p.variant == 2) return run_tma<LS, P, EPI, FK, 3, 1>(p, c, st);
   if (p.variant == 3) return run_tma<LS, P, EPI, FK, 2, HopMinBlocks<P>::v1>(p, c, st);
   if (p.variant == 4) return run_mb<LS, P, EPI, FK, HopMinBlocks<P>::v1>(p, c, st);
-  if constexpr (P != PREC_F64 && 32 % LS == 0) {
+  if constexpr (P != PREC_F64) {
     if (p.variant == 5) return run_pair<LS, P, EPI, FK>(p, c, st);
     if (p.variant == 6) return run_tma_pair<LS, P, EPI, FK, 2, HopMinBlocks<P>::v0>(p, c, st);
     if (p.variant == 7) return run_tma_pair<LS, P, EPI, FK, 4, 2>(p, c, st);

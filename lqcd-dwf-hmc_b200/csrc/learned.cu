@@ -26,12 +26,14 @@
 
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
 #include "../../include/b200dwf.h"
 #include "dwf_hop.cuh"
 #include "learned.h"
+#include "umma.cuh"
 
 namespace b200 {
 
@@ -217,6 +219,199 @@ __global__ void __launch_bounds__(128) lp_conv_kernel(const __grid_constant__ Lp
       acc[2 * a + 1][c] = make_float2(accr[a][c].y, acci[a][c].y);
     }
   lp_store<COUT>(p.out, p.ls, site, s, acc);
+}
+
+// ------------------------------------------------------------ forward layer on the tensor cores
+// The same layer as a GEMM on the fifth-generation tensor cores (tcgen05).
+// A CTA owns tiles of 128 (site, s) rows; for each color c the layer is
+//   out_c[row][n] = sum_k A_c[row][k] B[n][k],
+// k running over (path, input channel b, re/im) of the transported inputs and
+// n over (output channel a, re/im).  B is the real form of the complex
+// weights: row 2a holds (Re W[a][b], -Im W[a][b]) and row 2a+1
+// (Im W[a][b], Re W[a][b]) against the (re, im) columns of input b; rows past
+// 2*COUT are zero (N = 16 is the smallest MMA width at M = 128).  K is walked
+// in steps of 16, one MMA deep: 8/CIN paths per step, the three paths on the
+// output parity (identity, s+-1) first, then the eight hops.
+//
+// The threads gather and transport a step's inputs (the CUDA-core part: the
+// SU(3) products), split each FP32 value into BF16 hi + lo (hi + lo carries
+// 16 significant bits), and write them as the step's A operand into one of
+// two shared-memory stages; one thread then issues 6 MMAs (M = 128, N = 16,
+// K = 16: 3 colors x hi/lo) accumulating into three FP32 tiles in tensor
+// memory and commits them to the stage's mbarrier, so the tensor core
+// multiplies step j while the threads build step j+1.  The weights are BF16
+// values, so B is exact and the result differs from FP32 arithmetic only by
+// the rounding of lo (2^-17 relative) and the accumulation order.  The
+// epilogue reads the accumulators back (warp w: tensor-memory lanes 32w..,
+// one row per thread) and stores the output column.
+//
+// Every mbarrier wait is bounded; a wait that gives up sets the plan's error
+// word (1), skips its row's store, and the CTA drains the MMAs it issued
+// (longer bound) before it frees its tensor memory.
+constexpr int kTcRows = 128;
+constexpr uint32_t kTcTile = kTcRows * 16 * 2;   // one 128 x 16 BF16 operand tile
+constexpr uint32_t kTcStage = 6 * kTcTile;       // 3 colors x (hi, lo)
+constexpr uint32_t kTcCols = 64;                 // tensor-memory columns (3 x 16 used)
+
+template <int CIN> struct TcShape {
+  static constexpr int PPS = 8 / CIN;                   // paths per K step
+  static constexpr int NS_SAME = (3 + PPS - 1) / PPS;   // steps of paths 0-2
+  static constexpr int NS = NS_SAME + 8 / PPS;          // + steps of the 8 hops
+  static constexpr uint32_t B_BYTES = 16u * 16u * 2u * NS;
+  static constexpr uint32_t SBO_B = 2u * NS * 128u;     // between the two 8-row groups of B
+};
+
+template <int CIN>
+constexpr size_t lp_conv_tc_smem() {
+  return 2 * (size_t)kTcStage + TcShape<CIN>::B_BYTES;
+}
+
+__device__ __forceinline__ uint32_t bf16x2_bits(__nv_bfloat162 h) {
+  return *reinterpret_cast<uint32_t*>(&h);
+}
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(128) lp_conv_tc_kernel(const __grid_constant__ LpConvParams p) {
+  using TS = TcShape<CIN>;
+  constexpr int PPS = TS::PPS, NS_SAME = TS::NS_SAME, NS = TS::NS;
+  constexpr uint32_t IDESC = umma_idesc_bf16_f32(kTcRows, 16);
+  static_assert(CIN == 4 || CIN == 8, "input channels: 4 or 8");
+  static_assert(2 * COUT <= 16, "output channels: at most 8");
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bars[3];    // stage 0, stage 1, tile done
+  __shared__ uint32_t tmem_base;
+
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const uint32_t sbase = smem_u32(smem);
+  const uint32_t bbase = sbase + 2 * kTcStage;
+
+  if (warp == 0) {
+    tmem_alloc(smem_u32(&tmem_base), kTcCols);
+    tmem_relinquish();
+  }
+  if (tid == 0) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) mbar_init(smem_u32(&bars[i]), 1);
+    mbar_fence_init();
+  }
+  // B, K-major without swizzle: element (n, k) at (n%8)*16 + (n/8)*SBO_B +
+  // (k/8)*128 + (k%8)*2 bytes.
+  for (int e = tid; e < 16 * NS * 16; e += blockDim.x) {
+    const int n = e / (NS * 16), k = e - n * (NS * 16);
+    const int j = k >> 4, kk = k & 15;
+    const int q = kk / (2 * CIN), b = (kk >> 1) % CIN, ri = kk & 1;
+    const int path = (j < NS_SAME) ? j * PPS + q : 3 + (j - NS_SAME) * PPS + q;
+    const int a = n >> 1;
+    float val = 0.f;
+    if ((j >= NS_SAME || path < 3) && a < COUT) {
+      const float2 w = p.w[(path * COUT + a) * CIN + b];
+      val = (n & 1) ? (ri ? w.x : w.y) : (ri ? -w.y : w.x);
+    }
+    const uint32_t off = (n & 7) * 16 + (n >> 3) * TS::SBO_B + (k >> 3) * 128 + (k & 7) * 2;
+    *reinterpret_cast<__nv_bfloat16*>(smem + 2 * kTcStage + off) = __float2bfloat16_rn(val);
+  }
+  fence_proxy_async_smem();
+  tc_fence_before_sync();
+  __syncthreads();
+  tc_fence_after_sync();
+  const uint32_t taddr = tmem_base;
+
+  const int rows = p.vh * p.ls;
+  const int ntiles = (rows + kTcRows - 1) / kTcRows;
+  const int j0 = p.in_same ? 0 : NS_SAME;
+  const int j1 = p.in_other ? NS : NS_SAME;
+  const uint32_t row_off = (uint32_t)(tid & 7) * 16 + (uint32_t)(tid >> 3) * 256;
+  int g = 0;        // K steps this CTA has issued; stage g & 1
+  int ndone = 0;    // tile-done commits
+  bool bad = false;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int idx = tile * kTcRows + tid;
+    const bool active = idx < rows;
+    const int site = active ? idx / p.ls : 0;
+    const int s = active ? idx - site * p.ls : 0;
+    for (int j = j0; j < j1; ++j, ++g) {
+      float v[3][16];
+#pragma unroll
+      for (int q = 0; q < PPS; ++q) {
+        const int path = (j < NS_SAME) ? j * PPS + q : 3 + (j - NS_SAME) * PPS + q;
+        float2 u[CIN][3];
+        if (active && (j >= NS_SAME || path < 3))
+          lp_path_input<CIN>(p, p.in_same, p.in_other, path, site, s, u);
+        else
+          lp_zero<CIN>(u);
+#pragma unroll
+        for (int b = 0; b < CIN; ++b)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            v[c][q * 2 * CIN + 2 * b] = u[b][c].x;
+            v[c][q * 2 * CIN + 2 * b + 1] = u[b][c].y;
+          }
+      }
+      const int st = g & 1;
+      // the stage's previous MMAs (step g - 2) must have read it
+      if (g >= 2 && !mbar_wait_bounded(smem_u32(&bars[st]), ((g - 2) >> 1) & 1)) bad = true;
+      unsigned char* stage = smem + st * kTcStage;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        uint32_t hi[8], lo[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const float x0 = v[c][2 * i], x1 = v[c][2 * i + 1];
+          const __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
+          const __nv_bfloat162 l = __floats2bfloat162_rn(x0 - __low2float(h), x1 - __high2float(h));
+          hi[i] = bf16x2_bits(h);
+          lo[i] = bf16x2_bits(l);
+        }
+        uint4* th = reinterpret_cast<uint4*>(stage + (2 * c) * kTcTile + row_off);
+        uint4* tl = reinterpret_cast<uint4*>(stage + (2 * c + 1) * kTcTile + row_off);
+        th[0] = make_uint4(hi[0], hi[1], hi[2], hi[3]);   // K 0-7
+        th[8] = make_uint4(hi[4], hi[5], hi[6], hi[7]);   // K 8-15, 128 bytes on
+        tl[0] = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+        tl[8] = make_uint4(lo[4], lo[5], lo[6], lo[7]);
+      }
+      fence_proxy_async_smem();
+      __syncthreads();
+      if (tid == 0) {
+        tc_fence_after_sync();
+        const uint64_t bdesc = umma_smem_desc(bbase + (uint32_t)j * 256, 128, TS::SBO_B);
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const uint64_t adesc = umma_smem_desc(sbase + st * kTcStage + (2 * c + h) * kTcTile, 128, 256);
+            umma_bf16_ss(taddr + (uint32_t)(c * 16), adesc, bdesc, IDESC, j > j0 || h > 0);
+          }
+        umma_commit(smem_u32(&bars[st]));
+      }
+    }
+    if (tid == 0) umma_commit(smem_u32(&bars[2]));
+    if (!mbar_wait_bounded(smem_u32(&bars[2]), ndone & 1)) bad = true;
+    ++ndone;
+    tc_fence_after_sync();
+    float2 acc[COUT][3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      float d[16];
+      tmem_ld16(taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)(c * 16), d);
+#pragma unroll
+      for (int a = 0; a < COUT; ++a) acc[a][c] = make_float2(d[2 * a], d[2 * a + 1]);
+    }
+    if (active && !bad) lp_store<COUT>(p.out, p.ls, site, s, acc);
+    tc_fence_before_sync();
+  }
+  if (__syncthreads_or(bad)) {
+    if (tid == 0) {
+      if (p.err) atomicExch(p.err, 1);
+      umma_commit(smem_u32(&bars[2]));
+    }
+    mbar_wait_drain(smem_u32(&bars[2]), ndone & 1);
+    tc_fence_before_sync();
+    __syncthreads();
+  }
+  if (warp == 0) {
+    tc_fence_after_sync();
+    tmem_dealloc(taddr, kTcCols);
+  }
 }
 
 // ------------------------------------------------------------ weight gradient
@@ -433,8 +628,39 @@ __global__ void lp_adam_kernel(float2* w, float2* m, float2* v, const float2* g,
   m[i] = mm; v[i] = vv; w[i] = ww;
 }
 
+// The convolution kernel: the tensor-core form unless B200_LP_CONV=ffma2
+// selects the packed-FFMA2 form (both compute the same layer; the first
+// rounds the transported inputs to 16 significant bits before the product).
+bool lp_use_ffma2() {
+  const char* e = getenv("B200_LP_CONV");
+  return e && strcmp(e, "ffma2") == 0;
+}
+
+template <int CIN, int COUT>
+cudaError_t run_conv_tc(const LpConvParams& p, cudaStream_t st) {
+  constexpr size_t smem = lp_conv_tc_smem<CIN>();
+  auto k = lp_conv_tc_kernel<CIN, COUT>;
+  static int grid_cap = 0;
+  if (!grid_cap) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0, dev = 0, nsm = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kTcRows, smem)) != cudaSuccess) return e;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    // resident CTAs share the SM's 512 tensor-memory columns: never more than
+    // 512 / kTcCols of them, so no allocation has to wait
+    per_sm = per_sm < 1 ? 1 : (per_sm > (int)(512 / kTcCols) ? (int)(512 / kTcCols) : per_sm);
+    grid_cap = per_sm * nsm;
+  }
+  const int ntiles = (p.vh * p.ls + kTcRows - 1) / kTcRows;
+  k<<<ntiles < grid_cap ? ntiles : grid_cap, kTcRows, smem, st>>>(p);
+  return cudaGetLastError();
+}
+
 template <int CIN, int COUT>
 cudaError_t run_conv(const LpConvParams& p, cudaStream_t st) {
+  if (!lp_use_ffma2()) return run_conv_tc<CIN, COUT>(p, st);
   const int n = p.vh * p.ls;
   lp_conv_kernel<CIN, COUT><<<(n + 127) / 128, 128, 0, st>>>(p);
   return cudaGetLastError();
@@ -545,6 +771,7 @@ LpConvParams conv_base(const b200_lp* lp, const void* links, int ieo) {
   LpConvParams p;
   memset(&p, 0, sizeof(p));
   p.links = links;
+  p.err = plan_error_word(lp->op);
   p.vh = lp->g.vh; p.nx2 = lp->g.nx2; p.ny = lp->g.ny; p.nz = lp->g.nz; p.nt = lp->g.nt;
   p.ls = lp->g.ls;
   p.ieo = ieo;
@@ -597,6 +824,26 @@ int forward(b200_lp* lp, const void* links, const float4* r, float4* y3, cudaStr
   if ((rc = conv(lp, links, 1, false, 0, a[Y1E], a[Y1O], a[Y2E], st))) return rc;
   if ((rc = conv(lp, links, 1, false, 1, a[Y1O], a[Y1E], a[Y2O], st))) return rc;
   if ((rc = conv(lp, links, 2, false, 0, a[Y2E], a[Y2O], y3, st))) return rc;
+  return 0;
+}
+
+// Activations of the backward pass, the loss temporaries and the gradient
+// partials, allocated by the first training call.
+int ensure_train_buffers(b200_lp* lp) {
+  for (int i = Y3; i < NACT; ++i) {
+    if (lp->act[i]) continue;
+    const int ch = (i == Y3 || i == D3 || i == T4 || i == AD4) ? kLpIn : lp->hidden;
+    if (cudaMalloc(&lp->act[i], act_bytes(lp, ch)) != cudaSuccess) {
+      lp->act[i] = nullptr;
+      return lp_fail(B200_ENOMEM, "allocation of the training buffers failed");
+    }
+  }
+  if (!lp->partial &&
+      cudaMalloc(&lp->partial, sizeof(float2) * (size_t)lp->max_blocks * kLpPaths * lp->hidden * lp->hidden) !=
+          cudaSuccess) {
+    lp->partial = nullptr;
+    return lp_fail(B200_ENOMEM, "allocation of the gradient partials failed");
+  }
   return 0;
 }
 
@@ -660,12 +907,10 @@ int b200_lp_create(b200_lp_t** out, b200_dwf_t* op, int hidden, unsigned long lo
   bool ok = cudaMalloc(&lp->master, pb) == cudaSuccess && cudaMalloc(&lp->adam_m, pb) == cudaSuccess &&
             cudaMalloc(&lp->adam_v, pb) == cudaSuccess && cudaMalloc(&lp->grad, pb) == cudaSuccess &&
             cudaMalloc(&lp->wf, pb) == cudaSuccess && cudaMalloc(&lp->wadj, pb) == cudaSuccess;
-  for (int i = 0; ok && i < NACT; ++i) {
-    const int ch = (i == Y3 || i == D3 || i == T4 || i == AD4) ? kLpIn : hidden;
-    ok = cudaMalloc(&lp->act[i], act_bytes(lp, ch)) == cudaSuccess;
-  }
+  // the forward pass needs the hidden layers' activations only; the
+  // training buffers come with the first training call
+  for (int i = Y1E; ok && i <= Y2O; ++i) ok = cudaMalloc(&lp->act[i], act_bytes(lp, hidden)) == cudaSuccess;
   lp->max_blocks = 148 * 3;
-  ok = ok && cudaMalloc(&lp->partial, sizeof(float2) * (size_t)lp->max_blocks * kLpPaths * hidden * hidden) == cudaSuccess;
   ok = ok && cudaMalloc(&lp->red, sizeof(double) * kRedBlocks) == cudaSuccess;
   ok = ok && cudaMalloc(&lp->sc, sizeof(double) * 4) == cudaSuccess;
   ok = ok && cudaMallocHost(&lp->sc_host, sizeof(double) * 4) == cudaSuccess;
@@ -733,6 +978,7 @@ int b200_lp_loss_grad(b200_lp_t* lp, const void* r_f32, const void* e_f32, doubl
   cudaStream_t st = (cudaStream_t)stream;
   const void* links = nullptr;
   int rc;
+  if ((rc = ensure_train_buffers(lp))) return rc;
   if ((rc = plan_links_f32(lp->op, &links, st))) return rc;
   const float4* r = reinterpret_cast<const float4*>(r_f32);
   const float4* e = reinterpret_cast<const float4*>(e_f32);
@@ -762,7 +1008,7 @@ int b200_lp_loss_grad(b200_lp_t* lp, const void* r_f32, const void* e_f32, doubl
   if ((rc = gradw(lp, links, 0, 0, a[D1E], r, nullptr, false, st))) return rc;
   if ((rc = gradw(lp, links, 0, 1, a[D1O], nullptr, r, true, st))) return rc;
   LP_CHECK(cudaMemcpyAsync(lp->sc_host, lp->sc, sizeof(double) * 2, cudaMemcpyDeviceToHost, st));
-  LP_CHECK(cudaStreamSynchronize(st));
+  if ((rc = plan_check_error(lp->op, st))) return rc;      // synchronises the stream
   if (!(lp->sc_host[0] > 0.0)) return lp_fail(B200_EINVAL, "residual field r is zero");
   if (loss) *loss = lp->sc_host[1] / lp->sc_host[0];
   return 0;
@@ -804,6 +1050,7 @@ int b200_lp_train(b200_lp_t* lp, int npairs, const void* const* r_f32, const voi
     cudaStream_t st = (cudaStream_t)stream;
     const void* links = nullptr;
     int rc;
+    if ((rc = ensure_train_buffers(lp))) return rc;
     if ((rc = plan_links_f32(lp->op, &links, st))) return rc;
     float4** a = lp->act;
     const size_t n4 = act_bytes(lp, kLpIn) / sizeof(float4);

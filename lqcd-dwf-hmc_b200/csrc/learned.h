@@ -27,6 +27,7 @@ struct LpConvParams {
   float4* out;
   const void* links;       // plan links, f32 two-row records
   const float2* w;         // [kLpPaths][COUT][CIN] complex weights (BF16 values)
+  int* err;                // plan's device error word (bounded waits), or null
   int vh, nx2, ny, nz, nt, ls, ieo;
   float bc[4];
 };
@@ -51,6 +52,10 @@ int lp_apply_internal(b200_lp* lp, void* z_f32, const void* r_f32, cudaStream_t 
 
 // Accessors into the operator plan for learned.cu.
 int plan_geometry(b200_dwf* op, Geom* g, float bc[4]);
+// The plan's device error word, and its synchronising check (B200_ECUDA and
+// cleared when a kernel gave up a bounded wait).
+int* plan_error_word(b200_dwf* op);
+int plan_check_error(b200_dwf* op, cudaStream_t st);
 int plan_links_f32(b200_dwf* op, const void** links, cudaStream_t st);
 // v = DdagD w on FP32 fields of the plan (the operator's own kernels).
 int plan_apply_ddagd(b200_dwf* op, void* v, const void* w, cudaStream_t st);

@@ -135,11 +135,13 @@ def test_fp64_hop_variants_all_modes(variant, ci, monkeypatch):
 
 
 @pytest.mark.parametrize("variant", [5, 6, 7, 8, 9])
-@pytest.mark.parametrize("ci", [1, 4])
+@pytest.mark.parametrize("ci", range(len(CASES)))
 def test_packed_variants_reduced_precision(variant, ci):
     """The packed two-slice FP32x2 hop kernels (direct, and 2/4/8-deep TMA
     feeds) on every reduced storage precision, pinned with B200_HOP_VARIANT,
-    against the FP64 oracle; Ls = 8 and 16 (the packed kernels need Ls | 32)."""
+    against the FP64 oracle, at every Ls (6 and 12 leave 2 lanes of a warp
+    idle).  A mixed-precision solve with the pinned variant in the inner
+    solver covers the fused |out|^2 partials the solvers reduce."""
     import os
     case = CASES[ci]
     ora, dev = make(case, 5)
@@ -155,6 +157,12 @@ def test_packed_variants_reduced_precision(variant, ci):
                     (dev.mult_dag if dag else dev.mult)(fv, fw, mode)
                     ref = ora.mult(mode, w, dag)
                     assert rel(dev.reverse(fv), ref) < 4 * TOL[prec], (variant, prec, mode, dag)
+        fb, fx = dev.new_field(0), dev.new_field(0)
+        dev.convert(fb, w)
+        nout, nin, diff, rc = dev.richardson(fx, fb, 1, 1e-20, 60, 1e-8, 5000)
+        assert rc == 0 and diff < 1e-10, (variant, nout, nin, diff)
+        xr, _, _, _ = ora.cg(w, 1e-24, 5000)
+        assert rel(dev.reverse(fx), xr) < 1e-8
     finally:
         if old is None:
             del os.environ["B200_HOP_VARIANT"]

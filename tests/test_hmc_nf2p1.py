@@ -177,6 +177,25 @@ def test_smeared_fermion_force_is_minus_gradient(name):
 
 
 @pytest.mark.gpu
+def test_streamed_rational_force_matches_paired():
+    """The rational ratio's force with one pool of np_md solution fields
+    (numerator cross terms from the combined sources s*phi +- v/s) equals
+    the paired form (eta1_i and zeta_i side by side, balanced per pole) to
+    the multishift tolerance, and holds np_md fewer fields."""
+    import torch
+    F = {}
+    for pool in ("paired", "streamed"):
+        hmc, u, ud, _ = _small_hmc(151, rational_force_pool=pool)
+        act = hmc.fermions["nf1"]
+        out = torch.zeros_like(ud)
+        hmc.level_force([act], ud, out)
+        F[pool] = (out.cpu().numpy(), len(act.pool))
+    err = np.linalg.norm(F["streamed"][0] - F["paired"][0]) / np.linalg.norm(F["paired"][0])
+    assert err < 1e-9, err
+    assert F["paired"][1] == 32 and F["streamed"][1] == 16
+
+
+@pytest.mark.gpu
 def test_nested_omelyan_energy_violation_falls_as_step_squared():
     """The full action set under the nested Omelyan integrator: |dH| falls
     ~4x per doubling of the outer step count (inner levels nested inside),

@@ -50,12 +50,19 @@ def random_weights(lp, rng, scale=0.3):
     lp.set_weights(w)
 
 
+@pytest.mark.parametrize("kernel", ["tc", "ffma2"])
 @pytest.mark.parametrize("lat,ls,hidden,bc", [
     ([4, 4, 4, 4], 4, 8, (1, 1, 1, -1)),
     ([4, 4, 2, 8], 8, 4, (1, -1, 1, -1)),
+    ([6, 4, 2, 6], 12, 8, (1, 1, -1, -1)),
 ])
-def test_forward_and_gradient_match_oracle(lat, ls, hidden, bc):
+def test_forward_and_gradient_match_oracle(lat, ls, hidden, bc, kernel, monkeypatch):
+    """Both convolution kernels: the tensor-core form (tcgen05, BF16 hi + lo
+    split of the transported inputs, FP32 accumulation in tensor memory; the
+    default) and the packed-FFMA2 form (B200_LP_CONV=ffma2).  The 6x4x2x6
+    Ls=12 case has 1728 rows: 13 full 128-row tiles and a ragged 14th."""
     from oracle import learned_oracle as lo
+    monkeypatch.setenv("B200_LP_CONV", kernel)
     u, dev, lp = setup(lat, ls, hidden=hidden, bc=bc)
     rng = np.random.default_rng(4)
     random_weights(lp, rng)
