@@ -85,6 +85,9 @@ def parse():
     ap.add_argument("--traj-force-pool", default="paired", choices=["paired", "streamed"],
                     help="the rational force's solution fields: two sets side by side, or "
                          "one set at a time (np_md fewer fields, one more multishift)")
+    ap.add_argument("--traj-seed", type=int, default=SEED_U + 11,
+                    help="seed of the driver's generator (Mseries_parallel) for the trajectory; "
+                         "(seed + 1) * Lz * Lt must stay below 2^31")
     ap.add_argument("--traj-only", action="store_true",
                     help="time only the trajectory forms (a fresh process holds only their "
                          "fields) and print their JSON; not the benchmark line")
@@ -428,7 +431,7 @@ def learned_section(args):
     apply_ms = {}
     old = os.environ.get("B200_LP_CONV")
     try:
-        for kernel in ("ffma2", "tc"):
+        for kernel in ("ffma2", "tc1", "tc"):
             os.environ["B200_LP_CONV"] = kernel
             lp.apply(z32, r32)
             ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -471,7 +474,8 @@ def learned_section(args):
                           % (len(train), record.get("pairs", 0)),
             "train_loss_first_last_config": [train[0]["loss_first"], train[-1]["loss_last"]]
                                             if train else None,
-            "apply_ms": apply_ms["tc"], "apply_ms_ffma2": apply_ms["ffma2"],
+            "apply_ms": apply_ms["tc"], "apply_ms_tc1": apply_ms["tc1"],
+            "apply_ms_ffma2": apply_ms["ffma2"],
             "apply_tflops": flops / (apply_ms["tc"] * 1e-3) / 1e12,
             "tol_rel_residual": 1e-10, **res,
             "iteration_ratio": res["cg_f64"]["iterations"] / max(1, res["fcg_learned"]["iterations"]
@@ -591,7 +595,7 @@ def _trajectory_form(lattice, u0, args, lp, kinds, window, tol2, table_dir=None)
         r.iterations, r.seconds, r.calls = 0, 0.0, 0
     # the benchmark driver's generator (Mseries_parallel) on the device; its
     # streams are seeded here, outside the timed trajectory
-    noise = MseriesNoise(lattice, SEED_U + 11)
+    noise = MseriesNoise(lattice, args.traj_seed)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     r = hmc.trajectory(ud, noise)
@@ -626,7 +630,9 @@ def trajectory_only(args):
     """--traj-only: the trajectory forms alone, with the peak device memory
     the process reached (torch's allocator and the library's own
     allocations alike, from cudaMemGetInfo polled during the run)."""
+    import faulthandler
     import torch
+    faulthandler.enable()        # a native crash prints every thread's Python stack
     torch.cuda.init()
     lp = _Weights(LEARNED_WEIGHTS) if "mixed_batched_learned" in args.traj_forms else None
     free_min = [torch.cuda.mem_get_info()[0]]
@@ -928,6 +934,7 @@ def b200_arm(args, rank, world, local_rank):
         # one network application (tensor-core and FFMA2 convolutions), and
         # CG / flexible-CG iterations and seconds on an unseen configuration
         line["learned_apply_ms"] = round(learned["apply_ms"], 3)
+        line["learned_apply_ms_tc1"] = round(learned["apply_ms_tc1"], 3)
         line["learned_apply_ms_ffma2"] = round(learned["apply_ms_ffma2"], 3)
         line["learned_iteration_ratio"] = round(learned["iteration_ratio"], 3)
         line["learned_time_ratio"] = round(learned["time_ratio"], 3)

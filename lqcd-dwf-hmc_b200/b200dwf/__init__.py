@@ -100,6 +100,7 @@ def lib():
     L.b200_momentum_energy.argtypes = [ip, vp, dp, vp]
     L.b200_momentum_from_gauss.argtypes = [ip, vp, vp, vp]
     L.b200_links_axpby.argtypes = [ip, d_, vp, d_, vp, vp]
+    L.b200_blas_fill.argtypes = [ctypes.c_int, ctypes.c_size_t, d_, vp, vp]
     L.b200_field_convert_lex_device.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_int, vp]
     fp = ctypes.POINTER(ctypes.c_float)
     L.b200_lp_create.argtypes = [ctypes.POINTER(vp), vp, ctypes.c_int, ctypes.c_ulonglong,
@@ -157,6 +158,11 @@ class Field:
     @property
     def ptr(self):
         return ctypes.c_void_p(self.buf.data_ptr())
+
+    def zero(self):
+        """Every value 0, by the library's fill kernel (zero bits are a zero
+        value in every storage precision, scales included)."""
+        check(lib().b200_blas_fill(1, self.buf.numel() // 4, 0.0, self.ptr, None))
 
 
 class DomainWall:

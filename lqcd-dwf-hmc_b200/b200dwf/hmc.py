@@ -64,10 +64,13 @@ class TwoFlavour:
         self.solve()
         return self.op.dot(self.psi, self.eta)
 
-    def force_udiv(self, md, u, out):
+    def force_udiv(self, md, u, out, accumulate=False):
+        """out (+)= force_udiv(eta) (accumulate: add to out, else overwrite)."""
         md.set_links(self.op, u)
         self.solve()
-        check(lib().b200_dwf_force_udiv(self.op.handle, _p(out), self.eta.ptr, None))
+        check(lib().b200_dwf_force_acc(self.op.handle, b"DdagD", _p(out), self.eta.ptr, None, 1.0,
+                                       None) if accumulate else
+              lib().b200_dwf_force_udiv(self.op.handle, _p(out), self.eta.ptr, None))
 
 
 class Rational:
@@ -96,15 +99,20 @@ class Rational:
             s += bi * self.op.dot(self.phi, x)
         return s
 
-    def force_udiv(self, md, u, out):
-        import torch
+    def force_udiv(self, md, u, out, accumulate=False):
+        """out (+)= sum_i b_i force_udiv(x_i), accumulated in place by the
+        library's force kernels (the first pole overwrites unless
+        accumulate)."""
         md.set_links(self.op, u)
         self.solve()
-        tmp = torch.empty_like(out)
-        out.zero_()
-        for bi, x in zip(self.b, self.xs):
-            check(lib().b200_dwf_force_udiv(self.op.handle, _p(tmp), x.ptr, None))
-            out.add_(tmp, alpha=bi)
+        L = lib()
+        for i, (bi, x) in enumerate(zip(self.b, self.xs)):
+            if i == 0 and not accumulate:
+                check(L.b200_dwf_force_udiv(self.op.handle, _p(out), x.ptr, None))
+                if bi != 1.0:       # out = bi * out (x = y = out, finite here)
+                    check(L.b200_links_axpby(md._L, 0.0, _p(out), bi, _p(out), None))
+            else:
+                check(L.b200_dwf_force_acc(self.op.handle, b"DdagD", _p(out), x.ptr, None, bi, None))
 
 
 class GaugeMD:
@@ -137,12 +145,10 @@ class GaugeMD:
 
     def fermion_force(self, u, action=None):
         """Sum of the fermion forces (or one action's), lexical Field_G layout."""
-        import torch
         acts = self.fermions if action is None else [action]
-        total = torch.zeros_like(self.fbuf)
-        for a in acts:
-            a.force_udiv(self, u, self.fbuf)
-            total.add_(self.fbuf)
+        total = self.fbuf
+        for k, a in enumerate(acts):
+            a.force_udiv(self, u, total, accumulate=k > 0)
         # mult_generator is linear: applied once to the summed force_udiv
         check(lib().b200_force_mult_generator(self._L, _p(total), _p(u), None))
         return total
@@ -292,7 +298,7 @@ class Solver:
         if use:
             op.set_initial_guess(True)
         else:
-            x.buf.zero_()
+            x.zero()
         try:
             n = self._solve(op, x, b)
         finally:
@@ -433,7 +439,10 @@ class ActionFRationalRatio:
         self.psf_numer = FoprRational(fopr_numer, rats["psf_numer"], tol2_h)
         op = fopr_denom.op
         self.psf, self.v1, self.v2 = Field(op), Field(op), Field(op)
-        self.t1, self.t2 = Field(op), Field(op)
+        # the combined source of the streamed force; the paired force's two
+        # polarised vectors
+        self.t1 = Field(op)
+        self.t2 = Field(op) if force_pool == "paired" else None
         self.fermion = True
         # one pool of solution vectors: eta1_i in the first np_md slots, eta2_i
         # and later zeta_i in the next np_md (the denominator's forces are
@@ -783,9 +792,11 @@ class HMCGeneral:
         parts = [self.momentum_energy(ip)]
         for a in self.actions:
             if a.fermion:
-                xi = getattr(a, "_xi", None)
+                # one noise field for every action: each consumes its xi in
+                # its own langevin (all operators share the geometry)
+                xi = getattr(self, "_xi", None)
                 if xi is None:
-                    xi = a._xi = Field(a.f.op if hasattr(a, "f") else a.fb.op)
+                    xi = self._xi = Field(a.f.op if hasattr(a, "f") else a.fb.op)
                 noise.fermion(xi)
                 parts.append(a.langevin(xi))
             else:

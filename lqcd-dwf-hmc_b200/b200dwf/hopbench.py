@@ -21,8 +21,9 @@ times one application of the learned preconditioner instead (five
 convolution launches on FP32 fields) and reports its FP32 work: per
 (site, s, color) row and path, 8 flops per complex multiply-add of the
 channel mixing, and per row and hop path 72 flops per channel of the SU(3)
-transport.  --lp-conv ffma2 selects the packed-FFMA2 convolution kernel
-(B200_LP_CONV) instead of the tensor-core one."""
+transport.  --lp-conv selects the convolution kernel (B200_LP_CONV): tc,
+the tensor-core form on BF16 hi + lo inputs (default); tc1, the
+tensor-core form on BF16 inputs; ffma2, the packed-FFMA2 form."""
 import argparse
 import json
 import os
@@ -47,7 +48,7 @@ def main(argv=None):
     ap.add_argument("--m0", type=float, default=1.8)
     ap.add_argument("--learned", action="store_true")
     ap.add_argument("--hidden", type=int, default=8)
-    ap.add_argument("--lp-conv", default=None, choices=["tc", "ffma2"])
+    ap.add_argument("--lp-conv", default=None, choices=["tc", "tc1", "ffma2"])
     a = ap.parse_args(argv)
     if a.variant is not None:
         os.environ["B200_HOP_VARIANT"] = str(a.variant)

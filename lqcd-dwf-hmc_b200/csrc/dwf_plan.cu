@@ -104,6 +104,7 @@ void set_precond(DwfCoef& k) {
 // geometry must not run calls concurrently on different streams.
 struct Workspace {
   void* work[12][4] = {};       // work fields per slot and storage precision
+  void* tune_out[2][4] = {};    // autotuner scratch outputs per precision (trials run inside one call)
   std::vector<void*> p;         // multishift directions p_1..p_(n-1)
   std::vector<void*> win;       // multishift residual window slots
   int users = 0;
@@ -127,6 +128,8 @@ static void workspace_release(Workspace* ws) {
   if (--ws->users > 0) return;
   for (int i = 0; i < 12; ++i)
     for (int p = 0; p < 4; ++p) cudaFree(ws->work[i][p]);
+  for (int i = 0; i < 2; ++i)
+    for (int p = 0; p < 4; ++p) cudaFree(ws->tune_out[i][p]);
   for (void* q : ws->p) cudaFree(q);
   for (void* q : ws->win) cudaFree(q);
   for (auto it = g_workspaces.begin(); it != g_workspaces.end(); ++it)
@@ -167,7 +170,6 @@ struct b200_dwf {
   int ring_next[2] = {0, 0};
   Workspace* ws = nullptr;      // shared per-call workspace of this geometry
   void* (*work)[4] = nullptr;   // = ws->work: work fields per slot and precision
-  void* tune_out[2][4] = {};    // autotuner scratch outputs per precision
   ChainCoefs coefs;             // fifth-dimension chain coefficients
   bool m5pre_id = false;        // D_eo pre-factor is the identity (b = 1, c = 0, alpha = 1)
   double* ms_state = nullptr;   // multishift scalar state (device)
@@ -284,16 +286,22 @@ bool tuning_enabled() {
 }
 
 int tune_hop(b200_dwf* op, int prec, const HopParams& p0, cudaStream_t st, int* best) {
-  for (int i = 0; i < 2; ++i)
-    if (!op->tune_out[i][prec]) {
-      const size_t bytes = field_bytes(prec, op->g.vh, op->g.ls);
-      if (cudaMalloc(&op->tune_out[i][prec], bytes) != cudaSuccess)
-        return fail(B200_ENOMEM, "cudaMalloc for autotuner scratch failed");
-    }
+  {
+    // scratch outputs shared by the plans of this geometry
+    std::lock_guard<std::mutex> lock(g_ws_mu);
+    for (int i = 0; i < 2; ++i)
+      if (!op->ws->tune_out[i][prec]) {
+        const size_t bytes = field_bytes(prec, op->g.vh, op->g.ls);
+        if (cudaMalloc(&op->ws->tune_out[i][prec], bytes) != cudaSuccess) {
+          op->ws->tune_out[i][prec] = nullptr;
+          return fail(B200_ENOMEM, "cudaMalloc for autotuner scratch failed");
+        }
+      }
+  }
   HopParams p = p0;
   p.fail_dir = -1;   // the trials time real launches
-  if (p.out1) p.out1 = op->tune_out[0][prec];
-  if (p.out2) p.out2 = op->tune_out[1][prec];
+  if (p.out1) p.out1 = op->ws->tune_out[0][prec];
+  if (p.out2) p.out2 = op->ws->tune_out[1][prec];
   cudaEvent_t a, b;
   B200_CHECK_CUDA(cudaEventCreate(&a));
   B200_CHECK_CUDA(cudaEventCreate(&b));
@@ -649,8 +657,6 @@ int b200_dwf_destroy(b200_dwf_t* op) {
   cudaFree(op->fcg_part);
   cudaFree(op->fcg_sc);
   if (op->gst) cudaStreamDestroy(op->gst);
-  for (int i = 0; i < 2; ++i)
-    for (int p = 0; p < 4; ++p) cudaFree(op->tune_out[i][p]);
   delete op;
   return 0;
 }

@@ -234,23 +234,25 @@ __global__ void __launch_bounds__(128) lp_conv_kernel(const __grid_constant__ Lp
 // output parity (identity, s+-1) first, then the eight hops.
 //
 // The threads gather and transport a step's inputs (the CUDA-core part: the
-// SU(3) products), split each FP32 value into BF16 hi + lo (hi + lo carries
-// 16 significant bits), and write them as the step's A operand into one of
-// two shared-memory stages; one thread then issues 6 MMAs (M = 128, N = 16,
-// K = 16: 3 colors x hi/lo) accumulating into three FP32 tiles in tensor
-// memory and commits them to the stage's mbarrier, so the tensor core
-// multiplies step j while the threads build step j+1.  The weights are BF16
-// values, so B is exact and the result differs from FP32 arithmetic only by
-// the rounding of lo (2^-17 relative) and the accumulation order.  The
-// epilogue reads the accumulators back (warp w: tensor-memory lanes 32w..,
-// one row per thread) and stores the output column.
+// SU(3) products), round each FP32 value to NSPLIT BF16 parts (NSPLIT = 2:
+// hi + lo, 16 significant bits; NSPLIT = 1: BF16 activations, 8 bits, half
+// the shared memory and twice the resident CTAs), and write them as the
+// step's A operand into one of two shared-memory stages; one thread then
+// issues 3 x NSPLIT MMAs (M = 128, N = 16, K = 16: 3 colors x parts)
+// accumulating into three FP32 tiles in tensor memory and commits them to
+// the stage's mbarrier, so the tensor core multiplies step j while the
+// threads build step j+1.  The weights are BF16 values, so B is exact and,
+// with NSPLIT = 2, the result differs from FP32 arithmetic only by the
+// rounding of lo (2^-17 relative) and the accumulation order.  The epilogue
+// reads the accumulators back (warp w: tensor-memory lanes 32w.., one row
+// per thread) and stores the output column.
 //
 // Every mbarrier wait is bounded; a wait that gives up sets the plan's error
 // word (1), skips its row's store, and the CTA drains the MMAs it issued
 // (longer bound) before it frees its tensor memory.
 constexpr int kTcRows = 128;
 constexpr uint32_t kTcTile = kTcRows * 16 * 2;   // one 128 x 16 BF16 operand tile
-constexpr uint32_t kTcStage = 6 * kTcTile;       // 3 colors x (hi, lo)
+template <int NSPLIT> constexpr uint32_t tc_stage() { return 3u * NSPLIT * kTcTile; }  // 3 colors x parts
 constexpr uint32_t kTcCols = 64;                 // tensor-memory columns (3 x 16 used)
 
 template <int CIN> struct TcShape {
@@ -261,19 +263,22 @@ template <int CIN> struct TcShape {
   static constexpr uint32_t SBO_B = 2u * NS * 128u;     // between the two 8-row groups of B
 };
 
-template <int CIN>
+template <int CIN, int NSPLIT>
 constexpr size_t lp_conv_tc_smem() {
-  return 2 * (size_t)kTcStage + TcShape<CIN>::B_BYTES;
+  return 2 * (size_t)tc_stage<NSPLIT>() + TcShape<CIN>::B_BYTES;
 }
 
 __device__ __forceinline__ uint32_t bf16x2_bits(__nv_bfloat162 h) {
   return *reinterpret_cast<uint32_t*>(&h);
 }
 
-template <int CIN, int COUT>
-__global__ void __launch_bounds__(128) lp_conv_tc_kernel(const __grid_constant__ LpConvParams p) {
+template <int CIN, int COUT, int NSPLIT>
+__global__ void __launch_bounds__(128, NSPLIT == 1 ? 5 : 4)
+lp_conv_tc_kernel(const __grid_constant__ LpConvParams p) {
   using TS = TcShape<CIN>;
   constexpr int PPS = TS::PPS, NS_SAME = TS::NS_SAME, NS = TS::NS;
+  constexpr uint32_t kTcStage = tc_stage<NSPLIT>();
+  static_assert(NSPLIT == 1 || NSPLIT == 2, "BF16 parts per value: 1 or 2");
   constexpr uint32_t IDESC = umma_idesc_bf16_f32(kTcRows, 16);
   static_assert(CIN == 4 || CIN == 8, "input channels: 4 or 8");
   static_assert(2 * COUT <= 16, "output channels: at most 8");
@@ -358,16 +363,18 @@ __global__ void __launch_bounds__(128) lp_conv_tc_kernel(const __grid_constant__
         for (int i = 0; i < 8; ++i) {
           const float x0 = v[c][2 * i], x1 = v[c][2 * i + 1];
           const __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
-          const __nv_bfloat162 l = __floats2bfloat162_rn(x0 - __low2float(h), x1 - __high2float(h));
           hi[i] = bf16x2_bits(h);
-          lo[i] = bf16x2_bits(l);
+          if (NSPLIT == 2)
+            lo[i] = bf16x2_bits(__floats2bfloat162_rn(x0 - __low2float(h), x1 - __high2float(h)));
         }
-        uint4* th = reinterpret_cast<uint4*>(stage + (2 * c) * kTcTile + row_off);
-        uint4* tl = reinterpret_cast<uint4*>(stage + (2 * c + 1) * kTcTile + row_off);
+        uint4* th = reinterpret_cast<uint4*>(stage + (NSPLIT * c) * kTcTile + row_off);
         th[0] = make_uint4(hi[0], hi[1], hi[2], hi[3]);   // K 0-7
         th[8] = make_uint4(hi[4], hi[5], hi[6], hi[7]);   // K 8-15, 128 bytes on
-        tl[0] = make_uint4(lo[0], lo[1], lo[2], lo[3]);
-        tl[8] = make_uint4(lo[4], lo[5], lo[6], lo[7]);
+        if (NSPLIT == 2) {
+          uint4* tl = reinterpret_cast<uint4*>(stage + (2 * c + 1) * kTcTile + row_off);
+          tl[0] = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+          tl[8] = make_uint4(lo[4], lo[5], lo[6], lo[7]);
+        }
       }
       fence_proxy_async_smem();
       __syncthreads();
@@ -377,8 +384,8 @@ __global__ void __launch_bounds__(128) lp_conv_tc_kernel(const __grid_constant__
 #pragma unroll
         for (int c = 0; c < 3; ++c)
 #pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const uint64_t adesc = umma_smem_desc(sbase + st * kTcStage + (2 * c + h) * kTcTile, 128, 256);
+          for (int h = 0; h < NSPLIT; ++h) {
+            const uint64_t adesc = umma_smem_desc(sbase + st * kTcStage + (NSPLIT * c + h) * kTcTile, 128, 256);
             umma_bf16_ss(taddr + (uint32_t)(c * 16), adesc, bdesc, IDESC, j > j0 || h > 0);
           }
         umma_commit(smem_u32(&bars[st]));
@@ -628,26 +635,49 @@ __global__ void lp_adam_kernel(float2* w, float2* m, float2* v, const float2* g,
   m[i] = mm; v[i] = vv; w[i] = ww;
 }
 
-// The convolution kernel: the tensor-core form unless B200_LP_CONV=ffma2
-// selects the packed-FFMA2 form (both compute the same layer; the first
-// rounds the transported inputs to 16 significant bits before the product).
-bool lp_use_ffma2() {
+// The convolution kernel, by B200_LP_CONV: "tc" (default) the tensor-core
+// form with BF16 hi + lo inputs, "tc1" the tensor-core form with BF16
+// inputs, "ffma2" the packed-FFMA2 form.  All compute the same layer; the
+// tensor-core forms round the transported inputs to 16 (tc) or 8 (tc1)
+// significant bits before the product.
+enum LpConvKind { LP_TC2 = 0, LP_TC1 = 1, LP_FFMA2 = 2 };
+LpConvKind lp_conv_kind() {
   const char* e = getenv("B200_LP_CONV");
-  return e && strcmp(e, "ffma2") == 0;
+  if (e && strcmp(e, "ffma2") == 0) return LP_FFMA2;
+  if (e && strcmp(e, "tc1") == 0) return LP_TC1;
+  return LP_TC2;
 }
 
-template <int CIN, int COUT>
+template <int CIN, int COUT, int NSPLIT>
 cudaError_t run_conv_tc(const LpConvParams& p, cudaStream_t st) {
-  constexpr size_t smem = lp_conv_tc_smem<CIN>();
-  auto k = lp_conv_tc_kernel<CIN, COUT>;
+  constexpr size_t smem = lp_conv_tc_smem<CIN, NSPLIT>();
+  auto k = lp_conv_tc_kernel<CIN, COUT, NSPLIT>;
   static int grid_cap = 0;
   if (!grid_cap) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    int per_sm = 0, dev = 0, nsm = 0;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kTcRows, smem)) != cudaSuccess) return e;
+    // the whole unified L1 as shared memory, so that the most CTAs fit an SM
+    e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0, dev = 0, nsm = 0, smem_sm = 0, regs_sm = 0;
+    cudaFuncAttributes fa;
+    if ((e = cudaFuncGetAttributes(&fa, k)) != cudaSuccess) return e;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev)) != cudaSuccess)
+      return e;
+    if ((e = cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev)) != cudaSuccess)
+      return e;
+    // resident CTAs per SM from the kernel's own footprint (shared memory
+    // with the 1 KB the system reserves per CTA, registers); a grid sized
+    // from the occupancy query alone came out at one CTA per SM (148), so
+    // the larger of the two counts is used
+    const int by_smem = smem_sm / (int)(smem + fa.sharedSizeBytes + 1024);
+    const int by_regs = regs_sm / (fa.numRegs * kTcRows);
+    per_sm = by_smem < by_regs ? by_smem : by_regs;
+    int api = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&api, k, kTcRows, smem) == cudaSuccess && api > per_sm)
+      per_sm = api;
     // resident CTAs share the SM's 512 tensor-memory columns: never more than
     // 512 / kTcCols of them, so no allocation has to wait
     per_sm = per_sm < 1 ? 1 : (per_sm > (int)(512 / kTcCols) ? (int)(512 / kTcCols) : per_sm);
@@ -660,7 +690,9 @@ cudaError_t run_conv_tc(const LpConvParams& p, cudaStream_t st) {
 
 template <int CIN, int COUT>
 cudaError_t run_conv(const LpConvParams& p, cudaStream_t st) {
-  if (!lp_use_ffma2()) return run_conv_tc<CIN, COUT>(p, st);
+  const LpConvKind kind = lp_conv_kind();
+  if (kind == LP_TC2) return run_conv_tc<CIN, COUT, 2>(p, st);
+  if (kind == LP_TC1) return run_conv_tc<CIN, COUT, 1>(p, st);
   const int n = p.vh * p.ls;
   lp_conv_kernel<CIN, COUT><<<(n + 127) / 128, 128, 0, st>>>(p);
   return cudaGetLastError();

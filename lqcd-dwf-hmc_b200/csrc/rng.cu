@@ -198,10 +198,20 @@ int rng_fail(int code, const char* msg) {
 }
 
 int seed_planes(b200_rng* g, unsigned long seed) {
+  const int lz = g->L[2], lt = g->L[3];
+  // The generator of plane zt starts from the delay (seed + 1) Lz Lt + zt,
+  // which the reference hands to RandomNumbers_Mseries as an int
+  // (randomNumbers_parallel_Mseries.cpp:52-55); past INT_MAX that int is
+  // negative and the jump-ahead (delay3, randomNumbers_Mseries.cpp:79-140)
+  // indexes its polynomial below zero.  Such seeds are refused.
+  const unsigned long long planes = (unsigned long long)lz * (unsigned long long)lt;
+  if ((unsigned long long)seed + 1ull > (2147483647ull - (planes - 1ull)) / planes)
+    return rng_fail(B200_EINVAL,
+                    "seed too large for this lattice: (seed + 1) * Lz * Lt + plane must fit the "
+                    "M-series generator's int delay");
   // draws still running on any stream finish before the state is replaced
   const cudaError_t es = cudaDeviceSynchronize();
   if (es != cudaSuccess) return rng_fail(B200_ECUDA, cudaGetErrorString(es));
-  const int lz = g->L[2], lt = g->L[3];
   std::vector<int> h((size_t)g->nplanes * kStride, 0);
   for (int t = 0; t < lt; ++t)
     for (int z = 0; z < lz; ++z) {

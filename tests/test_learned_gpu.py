@@ -50,16 +50,23 @@ def random_weights(lp, rng, scale=0.3):
     lp.set_weights(w)
 
 
-@pytest.mark.parametrize("kernel", ["tc", "ffma2"])
+# tc1 rounds the transported inputs to BF16 (8 significant bits) before the
+# tensor-core product: its bound is that rounding, not FP32's
+KERNEL_TOL = {"tc": (TOL_FWD, 1e-4, TOL_GRAD), "ffma2": (TOL_FWD, 1e-4, TOL_GRAD),
+              "tc1": (6e-3, 2e-2, 3e-2)}
+
+
+@pytest.mark.parametrize("kernel", ["tc", "tc1", "ffma2"])
 @pytest.mark.parametrize("lat,ls,hidden,bc", [
     ([4, 4, 4, 4], 4, 8, (1, 1, 1, -1)),
     ([4, 4, 2, 8], 8, 4, (1, -1, 1, -1)),
     ([6, 4, 2, 6], 12, 8, (1, 1, -1, -1)),
 ])
 def test_forward_and_gradient_match_oracle(lat, ls, hidden, bc, kernel, monkeypatch):
-    """Both convolution kernels: the tensor-core form (tcgen05, BF16 hi + lo
+    """Every convolution kernel: the tensor-core form (tcgen05, BF16 hi + lo
     split of the transported inputs, FP32 accumulation in tensor memory; the
-    default) and the packed-FFMA2 form (B200_LP_CONV=ffma2).  The 6x4x2x6
+    default), the tensor-core form on BF16 inputs (B200_LP_CONV=tc1) and the
+    packed-FFMA2 form (B200_LP_CONV=ffma2).  The 6x4x2x6
     Ls=12 case has 1728 rows: 13 full 128-row tiles and a ragged 14th."""
     from oracle import learned_oracle as lo
     monkeypatch.setenv("B200_LP_CONV", kernel)
@@ -88,13 +95,14 @@ def test_forward_and_gradient_match_oracle(lat, ls, hidden, bc, kernel, monkeypa
         return lo.spinor_to_act(ora.mult("DdagD", lo.act_to_spinor(v)), vh, ls)
 
     loss_ref, G_ref, y_ref = lo.loss_and_grad(geo, Ws, ra, ea, A)
-    assert rel(z_dev, y_ref) < TOL_FWD
+    tol_fwd, tol_loss, tol_grad = KERNEL_TOL[kernel]
+    assert rel(z_dev, y_ref) < tol_fwd
     loss = lp.loss_grad(r, e)
-    assert abs(loss - loss_ref) < 1e-4 * loss_ref
+    assert abs(loss - loss_ref) < tol_loss * loss_ref
     g = lp.grad()
-    assert rel(g, lo.join_weights(G_ref)) < TOL_GRAD
+    assert rel(g, lo.join_weights(G_ref)) < tol_grad
     for layer, (a, b) in enumerate(zip(lo.split_weights(g, hidden), G_ref)):
-        assert rel(a, b) < TOL_GRAD, layer
+        assert rel(a, b) < tol_grad, layer
 
 
 def test_deployed_weights_are_bf16():

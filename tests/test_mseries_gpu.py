@@ -57,6 +57,19 @@ def test_rejects_odd_gaussian_blocks():
         r.gauss_lex_global(3, 1)
 
 
+def test_refuses_seeds_past_the_int_delay():
+    """Plane zt starts from the delay (seed + 1) Lz Lt + zt, an int in the
+    reference (randomNumbers_parallel_Mseries.cpp:52-55); seeds that push it
+    past INT_MAX are refused at create and reset, the largest one that fits
+    is taken (Lz Lt = 2048: seed <= 1048574)."""
+    import b200dwf
+    with pytest.raises(b200dwf.B200Error, match="seed too large"):
+        b200dwf.MseriesParallel([2, 2, 32, 64], 1234578)
+    r = b200dwf.MseriesParallel([2, 2, 32, 64], 1048574)
+    with pytest.raises(b200dwf.B200Error, match="seed too large"):
+        r.reset(1048575)
+
+
 def _set_ip_su3(h, nvol):
     """Langevin_Momentum::set_iP_SU3 (src/lib/HMC/langevin_Momentum.cpp:171-209)
     on Field(8, Nvol, 4) Gaussians -> lexical Field_G iP."""
