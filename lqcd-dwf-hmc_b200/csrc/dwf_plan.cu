@@ -1564,4 +1564,10 @@ int plan_links_f32(b200_dwf* op, const void** links, cudaStream_t st) {
   *links = op->links[LINK_F32_12];
   return 0;
 }
+int plan_links_f32_folded(b200_dwf* op, const void** links, cudaStream_t st) {
+  const int rc = ensure_link_format(op, LINK_F32_18, st);
+  if (rc) return rc;
+  *links = op->links[LINK_F32_18];
+  return 0;
+}
 }  // namespace b200

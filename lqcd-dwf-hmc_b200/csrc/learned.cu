@@ -221,6 +221,91 @@ __global__ void __launch_bounds__(128) lp_conv_kernel(const __grid_constant__ Lp
   lp_store<COUT>(p.out, p.ls, site, s, acc);
 }
 
+// ------------------------------------------------------------ gathers of the tensor-core layer
+// o[b] = U v[b] (DAG = false) or U^+ v[b] on every channel, two channels per
+// packed FP32x2 instruction.
+template <int C, bool DAG>
+__device__ __forceinline__ void lp_transport2(const float* u, const float2 (&v)[C][3],
+                                              float2 (&o)[C][3]) {
+  static_assert(C % 2 == 0, "channels in pairs");
+#pragma unroll
+  for (int b2 = 0; b2 < C / 2; ++b2)
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      float2 re = make_float2(0.f, 0.f), im = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const float ur = DAG ? u[2 * (i + 3 * j)] : u[2 * (j + 3 * i)];
+        const float ui = DAG ? -u[2 * (i + 3 * j) + 1] : u[2 * (j + 3 * i) + 1];
+        const float2 vx = make_float2(v[2 * b2][j].x, v[2 * b2 + 1][j].x);
+        const float2 vy = make_float2(v[2 * b2][j].y, v[2 * b2 + 1][j].y);
+        re = __ffma2_rn(make_float2(ur, ur), vx, re);
+        re = __ffma2_rn(make_float2(-ui, -ui), vy, re);
+        im = __ffma2_rn(make_float2(ur, ur), vy, im);
+        im = __ffma2_rn(make_float2(ui, ui), vx, im);
+      }
+      o[2 * b2][i] = make_float2(re.x, im.x);
+      o[2 * b2 + 1][i] = make_float2(re.y, im.y);
+    }
+}
+
+// Coordinates of a site of parity ieo, computed once per tile row.
+struct LpSite {
+  int site, ix2, iyzt, y, z, t, keo;
+};
+
+template <typename PP>
+__device__ __forceinline__ LpSite lp_site(const PP& p, int site) {
+  LpSite c;
+  c.site = site;
+  c.ix2 = site % p.nx2;
+  c.iyzt = site / p.nx2;
+  c.y = c.iyzt % p.ny;
+  const int izt = c.iyzt / p.ny;
+  c.z = izt % p.nz;
+  c.t = izt / p.nz;
+  c.keo = (p.ieo + c.y + c.z + c.t) & 1;
+  return c;
+}
+
+// Input of one path at (site, s) for the tensor-core layer: the same-parity
+// paths read in_same at s, s+1, s-1 (zero past the walls); the hops read
+// in_other at the neighbour and transport it with the folded full-record
+// links (boundary phase inside; the t links carry the hop's factor 2, which
+// the layer's t-path weights undo).
+template <int C, typename PP>
+__device__ __forceinline__ void lp_tc_path_input(const PP& p, int path, const LpSite& c, int s,
+                                                 float2 (&u)[C][3]) {
+  if (path < 3) {
+    const int ss = (path == 0) ? s : (path == 1 ? s + 1 : s - 1);
+    if (ss >= 0 && ss < p.ls) lp_load<C>(p.in_same, p.ls, c.site, ss, u);
+    else lp_zero<C>(u);
+    return;
+  }
+  const int d = path - 3;
+  const int mu = d >> 1;
+  const bool fwd = (d & 1) == 0;
+  int nb;
+  if (mu == 0) {
+    const int row = p.nx2 * c.iyzt;
+    nb = fwd ? row + ((c.ix2 + c.keo == p.nx2) ? 0 : c.ix2 + c.keo)
+             : row + ((c.ix2 - 1 + c.keo < 0) ? p.nx2 - 1 : c.ix2 - 1 + c.keo);
+  } else {
+    const int coord = (mu == 1) ? c.y : (mu == 2 ? c.z : c.t);
+    const int ext = (mu == 1) ? p.ny : (mu == 2 ? p.nz : p.nt);
+    const int stride = (mu == 1) ? p.nx2 : (mu == 2 ? p.nx2 * p.ny : p.nx2 * p.ny * p.nz);
+    nb = fwd ? ((coord == ext - 1) ? c.site - (ext - 1) * stride : c.site + stride)
+             : ((coord == 0) ? c.site + (ext - 1) * stride : c.site - stride);
+  }
+  const size_t lidx = fwd ? (size_t)(p.ieo + 2 * mu) * p.vh + c.site : (size_t)(1 - p.ieo + 2 * mu) * p.vh + nb;
+  float2 v[C][3];
+  lp_load<C>(p.in_other, p.ls, nb, s, v);
+  float U[18];
+  LinkLoad<LINK_F32_18>::load(p.links_folded, lidx, U);
+  if (fwd) lp_transport2<C, false>(U, v, u);
+  else lp_transport2<C, true>(U, v, u);
+}
+
 // ------------------------------------------------------------ forward layer on the tensor cores
 // The same layer as a GEMM on the fifth-generation tensor cores (tcgen05).
 // A CTA owns tiles of 128 (site, s) rows; for each color c the layer is
@@ -311,6 +396,7 @@ lp_conv_tc_kernel(const __grid_constant__ LpConvParams p) {
     if ((j >= NS_SAME || path < 3) && a < COUT) {
       const float2 w = p.w[(path * COUT + a) * CIN + b];
       val = (n & 1) ? (ri ? w.x : w.y) : (ri ? -w.y : w.x);
+      if (path >= 9) val *= 0.5f;   // the folded t links carry a factor 2 (exact)
     }
     const uint32_t off = (n & 7) * 16 + (n >> 3) * TS::SBO_B + (k >> 3) * 128 + (k & 7) * 2;
     *reinterpret_cast<__nv_bfloat16*>(smem + 2 * kTcStage + off) = __float2bfloat16_rn(val);
@@ -334,6 +420,7 @@ lp_conv_tc_kernel(const __grid_constant__ LpConvParams p) {
     const bool active = idx < rows;
     const int site = active ? idx / p.ls : 0;
     const int s = active ? idx - site * p.ls : 0;
+    const LpSite cs = lp_site(p, site);
     for (int j = j0; j < j1; ++j, ++g) {
       float v[3][16];
 #pragma unroll
@@ -341,7 +428,7 @@ lp_conv_tc_kernel(const __grid_constant__ LpConvParams p) {
         const int path = (j < NS_SAME) ? j * PPS + q : 3 + (j - NS_SAME) * PPS + q;
         float2 u[CIN][3];
         if (active && (j >= NS_SAME || path < 3))
-          lp_path_input<CIN>(p, p.in_same, p.in_other, path, site, s, u);
+          lp_tc_path_input<CIN>(p, path, cs, s, u);
         else
           lp_zero<CIN>(u);
 #pragma unroll
@@ -814,6 +901,8 @@ LpConvParams conv_base(const b200_lp* lp, const void* links, int ieo) {
 int conv(b200_lp* lp, const void* links, int layer, bool adjoint, int ieo, const float4* in_same,
          const float4* in_other, float4* out, cudaStream_t st) {
   LpConvParams p = conv_base(lp, links, ieo);
+  int rc;
+  if ((rc = plan_links_f32_folded(lp->op, &p.links_folded, st))) return rc;
   p.in_same = in_same;
   p.in_other = in_other;
   p.out = out;

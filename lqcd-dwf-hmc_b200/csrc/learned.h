@@ -26,6 +26,8 @@ struct LpConvParams {
   const float4* in_other;  // input on the other parity (the 8 hop paths)
   float4* out;
   const void* links;       // plan links, f32 two-row records
+  const void* links_folded;  // plan links, f32 full records with the boundary phases and
+                             // the hop's factor 2 on t links folded in (tensor-core kernel)
   const float2* w;         // [kLpPaths][COUT][CIN] complex weights (BF16 values)
   int* err;                // plan's device error word (bounded waits), or null
   int vh, nx2, ny, nz, nt, ls, ieo;
@@ -57,6 +59,7 @@ int plan_geometry(b200_dwf* op, Geom* g, float bc[4]);
 int* plan_error_word(b200_dwf* op);
 int plan_check_error(b200_dwf* op, cudaStream_t st);
 int plan_links_f32(b200_dwf* op, const void** links, cudaStream_t st);
+int plan_links_f32_folded(b200_dwf* op, const void** links, cudaStream_t st);
 // v = DdagD w on FP32 fields of the plan (the operator's own kernels).
 int plan_apply_ddagd(b200_dwf* op, void* v, const void* w, cudaStream_t st);
 
