@@ -252,6 +252,38 @@ def run_reference_cpu(lattice, ls, steps, warmup, budget_s=60.0, threads=None, i
     return out
 
 
+QXS_HARNESS = os.path.join(REPO, "oracle", "_ref", "qxs", "qxs_harness")
+
+
+def run_reference_qxs_mixed(lattice, ls, inputs, threads=None):
+    """The reference's own mixed-precision solver on this host's cores:
+    Fprop_alt_Standard_eo_Richardson<AField<double,QXS>, AField<float,QXS>>
+    (the QXS backend, compiled from the reference's sources by
+    oracle/Makefile.qxs; FP64 Richardson, FP32 CG inner solves on DdagD) on
+    the workload: one FP64 and one FP32 DdagD of its operators, and one
+    bounded solve (1 outer x 1 inner iteration).  Returns the harness's
+    figures."""
+    if not os.path.exists(QXS_HARNESS):
+        raise RuntimeError("oracle/_ref/qxs/qxs_harness not built")
+    threads = threads or os.cpu_count() or 1
+    u, b = inputs
+    with tempfile.TemporaryDirectory() as d:
+        u.tofile(os.path.join(d, "gauge.bin"))
+        b.tofile(os.path.join(d, "src.bin"))
+        with open(os.path.join(d, "params.txt"), "w") as f:
+            f.write("lattice %s\nLs %d\nmq %r\nM0 %r\nb 1.0\nc 0.0\nbc 1 1 1 -1\nthreads %d\n"
+                    "reps 1\n" % (" ".join(map(str, lattice)), ls, MQ, M0, threads))
+        r = subprocess.run([QXS_HARNESS, os.path.join(d, "params.txt"), d],
+                           capture_output=True, text=True, check=True)
+    out = {}
+    for line in r.stdout.splitlines():
+        p = line.split()
+        if len(p) == 2 and p[0] in ("ddagd_f64_seconds", "ddagd_f32_seconds", "solve_1x1_seconds",
+                                    "threads"):
+            out[p[0]] = float(p[1])
+    return out
+
+
 # The configuration the reference runs on its CPU path (4^3x8, Ls=8 Shamir
 # M0=1.8, hot start, light 0.01 / Hasenbusch 0.1 / strange 0.04 / PV 1.0,
 # Iwasaki beta 2.13, 2 stout rho 0.1, Omelyan [2,1,3], length 1, 10-pole
@@ -895,6 +927,32 @@ def b200_arm(args, rank, world, local_rank):
         except Exception as e:  # noqa: BLE001
             cpu = {"value": None, "unit": "GB/s", "cores": 0, "kind": "reference",
                    "sample": "unavailable: %s" % e}
+    # the reference's own mixed-precision solver (QXS backend) on the host
+    # cores, a bounded sample, extrapolated with the device solve's
+    # iteration counts (same algorithm: FP64 Richardson, FP32 CG inner)
+    cpu_mixed = None
+    if world == 1 and not args.no_cpu and solvers and "f32" in solvers["richardson"]:
+        try:
+            q = run_reference_qxs_mixed(lattice, LS, (u, b))
+            rf = solvers["richardson"]["f32"]
+            est = (rf["outer_iterations"] * q["ddagd_f64_seconds"]
+                   + rf["inner_iterations"] * q["ddagd_f32_seconds"])
+            cpu_mixed = {"kind": "reference", "cores": int(q.get("threads", 0)),
+                         "what": "Fprop_alt_Standard_eo_Richardson<AField<double,QXS>, "
+                                 "AField<float,QXS>>::invert_DdagD_even (QXS general backend, "
+                                 "oracle/Makefile.qxs), FP64 Richardson with FP32 CG inner solves",
+                         "sample": "one FP64 and one FP32 DdagD, and one 1 x 1 (outer x inner) "
+                                   "bounded solve, on the full %s Ls=16 workload"
+                                   % "x".join(map(str, lattice)),
+                         **q,
+                         "extrapolated_solve_seconds": est,
+                         "device_solve_seconds": rf["seconds"],
+                         "how": "a lower bound: the device's f32-inner Richardson iteration "
+                                "counts (%d outer, %d inner) x the reference's measured seconds per "
+                                "FP64 and per FP32 DdagD (vector updates, conversions and solver "
+                                "setup left out)" % (rf["outer_iterations"], rf["inner_iterations"])}
+        except Exception as e:  # noqa: BLE001
+            cpu_mixed = {"unavailable": str(e)}
     line = {
         "metric": METRIC, "value_is": VALUE_IS, "value": value, "unit": "GB/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_total * 1e3 / args.steps,
@@ -940,6 +998,9 @@ def b200_arm(args, rank, world, local_rank):
         line["learned_time_ratio"] = round(learned["time_ratio"], 3)
     if cpu_traj:
         line["sec_traj_cpu_reference_extrapolated"] = round(cpu_traj["sec_per_trajectory"], 1)
+    if cpu_mixed and "extrapolated_solve_seconds" in cpu_mixed:
+        line["sec_mixed_solve_cpu_reference_extrapolated"] = round(cpu_mixed["extrapolated_solve_seconds"], 1)
+        line["sec_mixed_solve_device"] = round(cpu_mixed["device_solve_seconds"], 3)
     if published and "device_sec" in published:
         line["sec_traj_published_8x8x8x8_device"] = round(published["device_sec"], 3)
         line["sec_traj_published_8x8x8x8_reference_gpu"] = published["published_sec"]
@@ -947,6 +1008,7 @@ def b200_arm(args, rank, world, local_rank):
     line.update({
         "cpu_baseline": cpu,
         "cpu_trajectory": cpu_traj,
+        "cpu_mixed_precision": cpu_mixed,
         "cg_f64": cg,
         "solvers": solvers,
         "learned_preconditioner": learned,
