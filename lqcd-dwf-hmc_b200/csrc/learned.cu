@@ -368,7 +368,10 @@ lp_conv_tc_kernel(const __grid_constant__ LpConvParams p) {
   static_assert(CIN == 4 || CIN == 8, "input channels: 4 or 8");
   static_assert(2 * COUT <= 16, "output channels: at most 8");
   extern __shared__ __align__(1024) unsigned char smem[];
-  __shared__ __align__(8) uint64_t bars[3];    // stage 0, stage 1, tile done
+  // stage s free again (MMAs of its last use complete: tcgen05.commit), tile
+  // done (every MMA of the tile complete), stage s written (every thread
+  // arrived)
+  __shared__ __align__(8) uint64_t bars[5];    // empty 0, empty 1, done, full 0, full 1
   __shared__ uint32_t tmem_base;
 
   const int tid = threadIdx.x, warp = tid >> 5;
@@ -382,6 +385,8 @@ lp_conv_tc_kernel(const __grid_constant__ LpConvParams p) {
   if (tid == 0) {
 #pragma unroll
     for (int i = 0; i < 3; ++i) mbar_init(smem_u32(&bars[i]), 1);
+    mbar_init(smem_u32(&bars[3]), kTcRows);
+    mbar_init(smem_u32(&bars[4]), kTcRows);
     mbar_fence_init();
   }
   // B, K-major without swizzle: element (n, k) at (n%8)*16 + (n/8)*SBO_B +
@@ -412,9 +417,29 @@ lp_conv_tc_kernel(const __grid_constant__ LpConvParams p) {
   const int j0 = p.in_same ? 0 : NS_SAME;
   const int j1 = p.in_other ? NS : NS_SAME;
   const uint32_t row_off = (uint32_t)(tid & 7) * 16 + (uint32_t)(tid >> 3) * 256;
-  int g = 0;        // K steps this CTA has issued; stage g & 1
+  int g = 0;        // K steps this CTA has built; stage g & 1
   int ndone = 0;    // tile-done commits
   bool bad = false;
+  // One thread issues step h's MMAs once every thread has written its stage
+  // (full barrier of the stage, phase h / 2), then frees the stage by a
+  // commit to its empty barrier.  Issued one step late, so that the wait is
+  // for writes that are normally done already and no CTA-wide barrier
+  // holds the gathers back.
+  auto issue = [&](int h, int jj) {
+    const int sh = h & 1;
+    if (!mbar_wait_bounded(smem_u32(&bars[3 + sh]), (h >> 1) & 1)) bad = true;
+    tc_fence_after_sync();
+    const uint64_t bdesc = umma_smem_desc(bbase + (uint32_t)jj * 256, 128, TS::SBO_B);
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int part = 0; part < NSPLIT; ++part) {
+        const uint64_t adesc =
+            umma_smem_desc(sbase + sh * kTcStage + (NSPLIT * c + part) * kTcTile, 128, 256);
+        umma_bf16_ss(taddr + (uint32_t)(c * 16), adesc, bdesc, IDESC, jj > j0 || part > 0);
+      }
+    umma_commit(smem_u32(&bars[sh]));
+  };
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int idx = tile * kTcRows + tid;
     const bool active = idx < rows;
@@ -464,21 +489,14 @@ lp_conv_tc_kernel(const __grid_constant__ LpConvParams p) {
         }
       }
       fence_proxy_async_smem();
-      __syncthreads();
-      if (tid == 0) {
-        tc_fence_after_sync();
-        const uint64_t bdesc = umma_smem_desc(bbase + (uint32_t)j * 256, 128, TS::SBO_B);
-#pragma unroll
-        for (int c = 0; c < 3; ++c)
-#pragma unroll
-          for (int h = 0; h < NSPLIT; ++h) {
-            const uint64_t adesc = umma_smem_desc(sbase + st * kTcStage + (NSPLIT * c + h) * kTcTile, 128, 256);
-            umma_bf16_ss(taddr + (uint32_t)(c * 16), adesc, bdesc, IDESC, j > j0 || h > 0);
-          }
-        umma_commit(smem_u32(&bars[st]));
-      }
+      tc_fence_before_sync();
+      mbar_arrive(smem_u32(&bars[3 + st]));
+      if (tid == 0 && j > j0) issue(g - 1, j - 1);
     }
-    if (tid == 0) umma_commit(smem_u32(&bars[2]));
+    if (tid == 0) {
+      issue(g - 1, j1 - 1);
+      umma_commit(smem_u32(&bars[2]));
+    }
     if (!mbar_wait_bounded(smem_u32(&bars[2]), ndone & 1)) bad = true;
     ++ndone;
     tc_fence_after_sync();
