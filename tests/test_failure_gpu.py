@@ -14,7 +14,7 @@ no copy is abandoned: the copies complete normally.  Checked here:
 * the solvers and the force report it too.
 
 The reference has no fault handling on this path (its OpenACC runtime aborts;
-SURVEY-level behaviour: solvers log and continue), so the oracle only checks
+its solvers log a non-convergence and continue), so the oracle only checks
 the recovered results."""
 import numpy as np
 import pytest
