@@ -210,8 +210,7 @@ int b200_solver_set_initial_guess(b200_dwf_t *op, int use);
  *   - Scratch is a fixed 512 KiB device array inside the library, held by
  *     every GPU that loads it until the process exits; fields larger than
  *     8,388,608 (site, s) pairs are rejected with B200_EINVAL.
- *   - The first call on each device looks the array up (once per device);
- *     make that first call before any stream capture.
+ *   - The first call on each device looks the array up (once per device).
  *   - All calls on a device share the array: calls that overlap on the GPU
  *     (different streams, no ordering between them) race and give wrong sums.
  *   - Calls no cudaMalloc/cudaFree; synchronous on `stream`. */
