@@ -138,6 +138,27 @@ int b200_dwf_check_error(b200_dwf_t *op, void *stream);
  * -1 switches it off (the default). */
 int b200_dwf_inject_wait_failure(b200_dwf_t *op, int direction);
 
+/* Halo exchange for a lattice split along t over several ranks (replaces the
+ * reference's per-hop face exchange, afopr_Domainwall_5din_eo-tmpl.h:998-1101
+ * and 1126-1228 over the MPI channels of src/lib/Communicator/MPI/
+ * channel.cpp:36-150).  A rank owning nt_loc slices (even) creates its plan
+ * on the lattice {Lx, Ly, Lz, nt_loc + 2}, periodic in t, whose slices are its
+ * own nt_loc slices, then the next rank's first slice, then the previous
+ * rank's last slice; the global t boundary phase is folded into the global
+ * last slice's t links by the caller.  The stencils then read the previous
+ * rank's slice through the t wrap, and every site keeps its global parity.
+ * Before each hop, and before the force kernels, the plan calls
+ * fn(ctx, field, prec, stream) for every field they read at neighbouring
+ * sites; fn must fill that field's two ghost slices (the t slowest index, so
+ * each slice is one contiguous range of (Lx Ly Lz / 2) site columns) from the
+ * neighbours' interior edge slices, ordered after the work already queued on
+ * `stream`, and return 0.  Outputs on the ghost slices are not meaningful.
+ * With a hook set, the solvers and the learned preconditioner refuse the
+ * plan (B200_EINVAL), and b200_field_norm2/dot cover the whole extended
+ * lattice.  fn = NULL removes the hook. */
+typedef int (*b200_halo_fn)(void *ctx, void *field, int prec, void *stream);
+int b200_dwf_set_halo_exchange(b200_dwf_t *op, b200_halo_fn fn, void *ctx);
+
 /* ---------------------------------------------------------------- fields
  * AField<REAL, ACCEL> BLAS (src/lib_alt_Accel/Field/afield-tmpl.h:637-720 ->
  * BridgeOpenACC/src/afield_openacc-inc.h:130-355).  norm2/dot accumulate in
@@ -224,7 +245,9 @@ int b200_field_norm2_noalloc(int prec, const void *x, long nsite, int ls,
  * BridgeACC vector functions (src/lib_alt_Accel/BridgeOpenACC/src/
  * afield_openacc-inc.h:14-446).  Element-wise work does not depend on the
  * layout; complex forms act on adjacent (re, im) pairs (n even).
- * Reductions accumulate in double and return synchronously on `stream`. */
+ * Reductions accumulate in double and return synchronously on `stream`;
+ * reductions from several host threads on one device take turns (they share
+ * the device's scratch). */
 int b200_blas_axpby(int prec, size_t n, double a, const void *x, double b, void *y,
                     void *stream);                         /* y = a x + b y (b = 0: y not read) */
 int b200_blas_caxpby(int prec, size_t n, double ar, double ai, const void *x, double br,

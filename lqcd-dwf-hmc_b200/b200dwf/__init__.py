@@ -31,6 +31,11 @@ class B200Error(RuntimeError):
     pass
 
 
+# int (*b200_halo_fn)(void* ctx, void* field, int prec, void* stream)
+HALO_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                           ctypes.c_void_p)
+
+
 def lib():
     """Load libb200dwf.so (raises if it was not built)."""
     global _lib
@@ -62,6 +67,7 @@ def lib():
     L.b200_dwf_set_async.argtypes = [vp, ctypes.c_int]
     L.b200_dwf_check_error.argtypes = [vp, vp]
     L.b200_dwf_inject_wait_failure.argtypes = [vp, ctypes.c_int]
+    L.b200_dwf_set_halo_exchange.argtypes = [vp, HALO_FN, vp]
     L.b200_field_axpby.argtypes = [vp, ctypes.c_int, vp, ctypes.c_double, vp, ctypes.c_double, vp]
     L.b200_field_norm2.argtypes = [vp, ctypes.c_int, vp, dp, vp]
     L.b200_field_dot.argtypes = [vp, ctypes.c_int, vp, vp, dp, vp]
@@ -101,6 +107,8 @@ def lib():
     L.b200_momentum_from_gauss.argtypes = [ip, vp, vp, vp]
     L.b200_links_axpby.argtypes = [ip, d_, vp, d_, vp, vp]
     L.b200_blas_fill.argtypes = [ctypes.c_int, ctypes.c_size_t, d_, vp, vp]
+    L.b200_blas_axpby.argtypes = [ctypes.c_int, ctypes.c_size_t, d_, vp, d_, vp, vp]
+    L.b200_blas_dot.argtypes = [ctypes.c_int, ctypes.c_size_t, vp, vp, dp, vp]
     L.b200_field_convert_lex_device.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_int, vp]
     fp = ctypes.POINTER(ctypes.c_float)
     L.b200_lp_create.argtypes = [ctypes.POINTER(vp), vp, ctypes.c_int, ctypes.c_ulonglong,

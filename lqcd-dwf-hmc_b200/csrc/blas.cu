@@ -112,16 +112,21 @@ __global__ void sum_partials_kernel(const double* partial, int nblocks, int ncom
 }
 
 // Reduction scratch of the calling device (2 * kBlocks partials + 2 results),
-// allocated on the first reduction on that device and kept.
+// allocated on the first reduction on that device and kept.  A reduction
+// holds its device's lock from the first launch until its result is back,
+// so host threads reducing on one device take turns instead of overwriting
+// each other's partials.
 std::mutex g_mu;
 double* g_scratch[kMaxDevices] = {};
+std::mutex g_reduce_mu[kMaxDevices];
 
-int scratch(double** out) {
+int scratch(double** out, int* dev_out) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
     b200::set_last_error(B200_ECUDA, "blas: no usable current device");
     return B200_ECUDA;
   }
+  *dev_out = dev;
   std::lock_guard<std::mutex> lk(g_mu);
   if (!g_scratch[dev] && cudaMalloc(&g_scratch[dev], (2 * kBlocks + 2) * sizeof(double)) != cudaSuccess) {
     g_scratch[dev] = nullptr;
@@ -152,8 +157,10 @@ int blocks_for(size_t n) {
 template <typename T, bool kConj>
 int reduce(size_t n, const void* x, const void* y, double* res, int ncomp, cudaStream_t st) {
   double* s = nullptr;
-  int rc = scratch(&s);
+  int dev = 0;
+  int rc = scratch(&s, &dev);
   if (rc) return rc;
+  std::lock_guard<std::mutex> lk(g_reduce_mu[dev]);
   const int nb = blocks_for(kConj ? n / 2 : n);
   dot_partial_kernel<T, kConj><<<nb, kThreads, 0, st>>>(n, (const T*)x, (const T*)y, s);
   sum_partials_kernel<<<1, kThreads, 0, st>>>(s, nb, ncomp, s + 2 * kBlocks);

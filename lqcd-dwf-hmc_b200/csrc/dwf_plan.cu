@@ -161,6 +161,8 @@ struct b200_dwf {
   double* sc_host = nullptr;    // pinned mirror (also of the multishift scalars)
   int* err_host = nullptr;      // pinned mirror of err
   bool async_calls = false;     // mult / force return without synchronising (b200_dwf_set_async)
+  b200_halo_fn halo_fn = nullptr;   // fills a field's ghost t-slices before a stencil reads it
+  void* halo_ctx = nullptr;
   int inject_dir = -1;          // hop direction whose bulk-copy wait reports failure (-1: none)
   double* stage = nullptr;      // device f64 staging for convert/reverse
   // staging rings of the asynchronous host transfers (upload, download): a
@@ -334,8 +336,32 @@ int forced_variant() {
   return (v >= 0 && v < kHopVariants) ? v : -1;
 }
 
+// A rank's share of a lattice split along t is run as its own periodic
+// lattice with two ghost t-slices after its interior (the next rank's first
+// slice, then the previous rank's last); a stencil reads the previous rank's
+// slice through the t wrap.  Before a kernel reads a field at neighbouring
+// sites, the host's exchange hook fills that field's ghost slices.
+static int halo(b200_dwf* op, const void* f, int prec, cudaStream_t st) {
+  if (!op->halo_fn || !f) return 0;
+  const int rc = op->halo_fn(op->halo_ctx, const_cast<void*>(f), prec, (void*)st);
+  if (rc) return fail(B200_EINVAL, "the halo exchange hook failed (%d)", rc);
+  return 0;
+}
+
+static int no_halo(const b200_dwf* op, const char* what) {
+  if (!op->halo_fn) return 0;
+  return fail(B200_EINVAL,
+              "%s: not available on a plan with a halo exchange hook (its reductions would "
+              "cover only this rank's extended lattice)",
+              what);
+}
+
 int run_hop(b200_dwf* op, int prec, HopParams& p, cudaStream_t st) {
   int variant = 0;
+  if (op->halo_fn) {
+    const int hrc = halo(op, p.in, prec, st);
+    if (hrc) return hrc;
+  }
   const int fv = forced_variant();
   if (fv >= 0 && variant_supported(prec, op->g.ls, fv)) {
     variant = fv;
@@ -798,6 +824,13 @@ int b200_dwf_mult(b200_dwf_t* op, int prec, void* v, const void* w, const char* 
   return finish_call(op, apply_mode(op, prec, v, w, mode, dag, st), st);
 }
 
+int b200_dwf_set_halo_exchange(b200_dwf_t* op, b200_halo_fn fn, void* ctx) {
+  if (!op) return fail(B200_EINVAL, "null argument");
+  op->halo_fn = fn;
+  op->halo_ctx = fn ? ctx : nullptr;
+  return 0;
+}
+
 int b200_dwf_set_async(b200_dwf_t* op, int async_calls) {
   if (!op) return fail(B200_EINVAL, "null operator");
   op->async_calls = async_calls != 0;
@@ -961,6 +994,7 @@ int b200_cg_solve(b200_dwf_t* op, int prec, void* x, const void* b, int maxiter,
                   int* nconv, double* diff, void* stream) {
   if (!op || !x || !b || prec < 0 || prec > 3 || maxiter < 0) return fail(B200_EINVAL, "invalid argument");
   if (misaligned(x) || misaligned(b)) return fail(B200_EINVAL, "field pointers must be 16-byte aligned");
+  if (no_halo(op, "CG")) return B200_EINVAL;
   cudaStream_t st = (cudaStream_t)stream;
   int n = 0;
   double rel2 = 0.0;
@@ -1017,6 +1051,7 @@ int b200_shiftcg_solve(b200_dwf_t* op, void* const* x, const double* sigma, int 
   if (!op || !x || !sigma || !b || nshift < 1 || maxiter < 0)
     return fail(B200_EINVAL, "invalid argument");
   if (nshift > kMaxShift) return fail(B200_EINVAL, "at most %d shifts (got %d)", kMaxShift, nshift);
+  if (no_halo(op, "multishift CG")) return B200_EINVAL;
   for (int i = 0; i < nshift; ++i)
     if (!x[i] || misaligned(x[i])) return fail(B200_EINVAL, "solution field %d null or not 16-byte aligned", i);
   if (misaligned(b)) return fail(B200_EINVAL, "field pointers must be 16-byte aligned");
@@ -1228,6 +1263,7 @@ int b200_richardson_solve(b200_dwf_t* op, int inner_prec, void* x, const void* b
                           int* nconv_inner, double* diff, void* stream) {
   if (!op || !x || !b || inner_prec < 0 || inner_prec > 3 || maxiter < 0 || maxiter_inner < 1)
     return fail(B200_EINVAL, "invalid argument");
+  if (no_halo(op, "Richardson")) return B200_EINVAL;
   if (misaligned(x) || misaligned(b)) return fail(B200_EINVAL, "field pointers must be 16-byte aligned");
   cudaStream_t st = (cudaStream_t)stream;
   const int P64 = PREC_F64;
@@ -1301,6 +1337,7 @@ int b200_cg_snapshots(b200_dwf_t* op, int prec, void* x, const void* b, int maxi
   if (misaligned(x) || misaligned(b)) return fail(B200_EINVAL, "field pointers must be 16-byte aligned");
   for (int j = 0; j < nsnap; ++j)
     if (!snaps[j] || misaligned(snaps[j])) return fail(B200_EINVAL, "snapshot %d is not a valid field", j);
+  if (no_halo(op, "CG")) return B200_EINVAL;
   const CgSnap sn = {nsnap, iters, snaps};
   int n = 0;
   double rel2 = 0.0;
@@ -1323,6 +1360,7 @@ int b200_fcg_solve(b200_dwf_t* op, b200_lp_t* lp, void* x, const void* b, int ma
   constexpr int kFallbackMaxiter = 100000;
   if (!op || !lp || !x || !b || maxiter < 0 || mtrunc < 1 || mtrunc > 8)
     return fail(B200_EINVAL, "invalid argument");
+  if (no_halo(op, "flexible CG")) return B200_EINVAL;
   if (misaligned(x) || misaligned(b)) return fail(B200_EINVAL, "field pointers must be 16-byte aligned");
   cudaStream_t st = (cudaStream_t)stream;
   const int P64 = PREC_F64, P32 = PREC_F32;
@@ -1503,6 +1541,9 @@ static int force_impl(b200_dwf_t* op, const char* mode, double* force, const voi
   fe.beta = beta; fo.beta = beta;
   if (udiv || !hdag) { fe.y1 = yo; fe.z1 = ae; fo.y1 = ye; fo.z1 = ao; }
   if (udiv || hdag) { fe.y2 = ao; fe.z2 = ye; fo.y2 = ae; fo.z2 = yo; }
+  const void* read[4] = {ye, yo, ae, ao};
+  for (const void* f : read)
+    if ((rc = halo(op, f, PREC_F64, st))) return rc;
   B200_CHECK_CUDA(launch_force(fe, st));
   B200_CHECK_CUDA(launch_force(fo, st));
   return 0;
@@ -1558,6 +1599,7 @@ int plan_apply_ddagd(b200_dwf* op, void* v, const void* w, cudaStream_t st) {
 }
 int* plan_error_word(b200_dwf* op) { return op->err; }
 int plan_check_error(b200_dwf* op, cudaStream_t st) { return check_err(op, st); }
+bool plan_has_halo(const b200_dwf* op) { return op->halo_fn != nullptr; }
 int plan_links_f32(b200_dwf* op, const void** links, cudaStream_t st) {
   const int rc = ensure_link_format(op, LINK_F32_12, st);
   if (rc) return rc;

@@ -1018,6 +1018,8 @@ int b200_lp_create(b200_lp_t** out, b200_dwf_t* op, int hidden, unsigned long lo
                    double init_noise) {
   if (!out || !op) return lp_fail(B200_EINVAL, "invalid argument");
   if (hidden != 4 && hidden != 8) return lp_fail(B200_EINVAL, "hidden channels must be 4 or 8");
+  if (plan_has_halo(op))
+    return lp_fail(B200_EINVAL, "the learned preconditioner needs a plan without a halo exchange hook");
   *out = nullptr;
   b200_lp* lp = new b200_lp();
   lp->op = op;

@@ -58,6 +58,8 @@ int plan_geometry(b200_dwf* op, Geom* g, float bc[4]);
 // cleared when a kernel gave up a bounded wait).
 int* plan_error_word(b200_dwf* op);
 int plan_check_error(b200_dwf* op, cudaStream_t st);
+// true when the plan has a halo exchange hook (a rank of a lattice split along t)
+bool plan_has_halo(const b200_dwf* op);
 int plan_links_f32(b200_dwf* op, const void** links, cudaStream_t st);
 int plan_links_f32_folded(b200_dwf* op, const void** links, cudaStream_t st);
 // v = DdagD w on FP32 fields of the plan (the operator's own kernels).
