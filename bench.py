@@ -82,6 +82,10 @@ def parse():
                     help="poles of the heatbath and Hamiltonian rationals (16 or 24)")
     ap.add_argument("--traj-window", type=int, default=16,
                     help="residual window of the batched forms' multishift")
+    ap.add_argument("--traj-chrono", type=int, default=4,
+                    help="MD solves of the mixed forms start from the minimal residual "
+                         "extrapolation of this many previous solutions (1: the previous one; "
+                         "each more costs one FP64 field per solver)")
     ap.add_argument("--traj-force-pool", default="paired", choices=["paired", "streamed"],
                     help="the rational force's solution fields: two sets side by side, or "
                          "one set at a time (np_md fewer fields, one more multishift)")
@@ -602,7 +606,8 @@ def _trajectory_form(lattice, u0, args, lp, kinds, window, tol2, table_dir=None)
     # "mixed+": mixed-precision Richardson whose MD solves start from the
     # action's previous solution (use_initial_guess)
     inner = {"f32": 1, "f16": 2, "bf16": 3}[args.traj_inner]
-    sv = {k: Solver(v.rstrip("+"), tol2, chrono=v.endswith("+"), inner_prec=inner)
+    sv = {k: Solver(v.rstrip("+"), tol2, chrono=v.endswith("+"), inner_prec=inner,
+                    chrono_depth=args.traj_chrono)
           for k, v in kinds.items()}
     torch.cuda.reset_peak_memory_stats()
     free0, total = torch.cuda.mem_get_info()

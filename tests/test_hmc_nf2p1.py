@@ -254,3 +254,49 @@ def test_chronological_guess_keeps_the_trajectory_and_saves_iterations():
         assert abs(a[0] - b[0]) < 1e-8, kind
         assert np.max(np.abs(a[1] - b[1])) < 1e-10, kind
         assert b[2] < a[2], (kind, a[2], b[2])
+
+
+@pytest.mark.gpu
+def test_minimal_residual_guess_keeps_the_trajectory():
+    """MD solves starting from the minimal residual extrapolation of the last
+    4 solutions (chrono_depth 4) against the previous solution alone
+    (chrono_depth 1): the same dH and end links to the solver tolerance, and
+    no more iterations (the extrapolation's error is minimal in the DdagD
+    norm over a span that holds the previous solution)."""
+    from b200dwf.hmc import Solver
+    out = {}
+    for depth in (1, 4):
+        sv = {k: Solver("mixed", 1e-24, chrono=True, chrono_depth=depth)
+              for k in ("l_md", "h_md", "l_h", "h_h", "pv_h")}
+        hmc, u, ud, ip = _small_hmc(161, solvers=sv, nstep=(4, 1, 3))
+        h0, _ = hmc.calc_hamiltonian(ip)
+        hmc.integrator.evolve(0.2, ip, ud)
+        h1, _ = hmc.calc_hamiltonian(ip)
+        out[depth] = (h1 - h0, ud.cpu().numpy(), sum(sv[k].iterations for k in ("l_md", "h_md")))
+    assert abs(out[4][0] - out[1][0]) < 1e-8
+    assert np.max(np.abs(out[4][1] - out[1][1])) < 1e-10
+    assert out[4][2] <= out[1][2], (out[1][2], out[4][2])
+
+
+@pytest.mark.gpu
+def test_minimal_residual_guess_reproduces_a_repeated_solve():
+    """Two solutions of one system in the history: the extrapolation alone
+    is the solution (the degenerate direction of the nearly singular 2x2
+    system is dropped), so the third solve, from a zeroed x, needs only the
+    iterations of the second."""
+    import b200dwf
+    from b200dwf.hmc import Solver
+    lat, ls = [4, 4, 4, 8], 8
+    op = b200dwf.DomainWall(lat, ls, 0.05, 1.8)
+    op.set_config(synth.gauge_field(lat, 171, "near", 0.3))
+    b = op.new_field()
+    op.convert(b, synth.spinor_field(lat, ls, 172))
+    x = op.new_field()
+    s = Solver("cg", 1e-24, chrono=True, chrono_depth=3)
+    n1 = s.solve(op, x, b)
+    n2 = s.solve(op, x, b, guess=True)
+    x.zero()                                   # the guess must come from the history
+    n3 = s.solve(op, x, b, guess=True)
+    # a solution to |r| < 1e-12 recursively can sit a little above it in the
+    # true residual the restarted solve checks: a few iterations at most
+    assert n1 > 50 and n2 <= 5 and n3 <= 5, (n1, n2, n3)
