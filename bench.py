@@ -854,7 +854,9 @@ def b200_arm(args, rank, world, local_rank):
     solvers = None
     if not args.no_solvers and world == 1:
         solvers = {"richardson": {}, "multishift": None}
-        for name, prec, tin in (("f32", 1, 1e-8), ("f16", 2, 1e-4), ("bf16", 3, 1e-4)):
+        from b200dwf.hmc import INNER_TOL2
+        for name, prec in (("f32", 1), ("f16", 2), ("bf16", 3)):
+            tin = INNER_TOL2[prec]
             x = op.new_field(0)
             op.richardson(x, w, prec, 1e-20, 1, tin, 3)   # untimed warm-up (buffers, autotuning)
             torch.cuda.synchronize()

@@ -31,6 +31,16 @@ def _p(t):
     return ctypes.c_void_p(t.data_ptr())
 
 
+# |r|^2 / |b|^2 at which the mixed-precision Richardson's inner CG stops, per
+# inner storage precision (1 f32, 2 f16, 3 bf16).  The half-precision values
+# are the fastest of a sweep of one light solve to 1e-10 at 24^3x48 Ls=16,
+# mass 0.01, on the tiled conf_04040408 with 2 stout steps: f16 1e-2 / 3e-3 /
+# 1e-3 / 1e-4 / 1e-5 took 5.93 / 5.22 / 5.09 / 5.44 / 6.77 s, bf16 1e-2 /
+# 3e-3 / 1e-3 / 1e-4 6.05 / 6.03 / 7.41 / 6.84 s (a looser inner solve
+# restarts more often, a tighter one runs into the storage's rounding).
+INNER_TOL2 = {1: 1e-8, 2: 1e-3, 3: 3e-3}
+
+
 class TwoFlavour:
     """Two-flavour even/odd domain-wall pseudofermion action."""
 
@@ -49,7 +59,7 @@ class TwoFlavour:
             n, _, rc = self.op.cg(self.eta, self.psi, self.tol2, 100000)
         elif self.solver == "mixed":
             _, n, _, rc = self.op.richardson(self.eta, self.psi, self.inner_prec, self.tol2, 200,
-                                             1e-4 if self.inner_prec != 1 else 1e-8, 100000)
+                                             INNER_TOL2[self.inner_prec], 100000)
         elif self.solver == "learned":
             n0, n1, _, rc = self.op.fcg(self.eta, self.psi, self.lp, self.tol2, 100000, 2)
             n = n0 + n1
@@ -375,7 +385,7 @@ class Solver:
             n, _, rc = op.cg(x, b, self.tol2, self.maxiter)
         elif self.kind == "mixed":
             _, n, _, rc = op.richardson(x, b, self.inner_prec, self.tol2, 200,
-                                        1e-4 if self.inner_prec != 1 else 1e-8, self.maxiter)
+                                        INNER_TOL2[self.inner_prec], self.maxiter)
         elif self.kind == "learned":
             n0, n1, _, rc = op.fcg(x, b, self.lp, self.tol2, self.maxiter, 2)
             n = n0 + n1
