@@ -23,7 +23,15 @@ convolution launches on FP32 fields) and reports its FP32 work: per
 channel mixing, and per row and hop path 72 flops per channel of the SU(3)
 transport.  --lp-conv selects the convolution kernel (B200_LP_CONV): tc,
 the tensor-core form on BF16 hi + lo inputs (default); tc1, the
-tensor-core form on BF16 inputs; ffma2, the packed-FFMA2 form."""
+tensor-core form on BF16 inputs; ffma2, the packed-FFMA2 form.
+
+    python -m b200dwf.hopbench --richardson f16 --inner-iters 20 ...
+
+runs one bounded mixed-precision Richardson solve instead (one outer
+iteration of at most --inner-iters inner CG iterations in the given
+storage, inner tolerance b200dwf.hmc.INNER_TOL2, after one untimed solve
+for the autotuner) and reports its iterations and seconds: the command
+whose launch list shows what one inner iteration launches."""
 import argparse
 import json
 import os
@@ -49,6 +57,8 @@ def main(argv=None):
     ap.add_argument("--learned", action="store_true")
     ap.add_argument("--hidden", type=int, default=8)
     ap.add_argument("--lp-conv", default=None, choices=["tc", "tc1", "ffma2"])
+    ap.add_argument("--richardson", default=None, choices=["f32", "f16", "bf16"])
+    ap.add_argument("--inner-iters", type=int, default=20)
     a = ap.parse_args(argv)
     if a.variant is not None:
         os.environ["B200_HOP_VARIANT"] = str(a.variant)
@@ -56,6 +66,8 @@ def main(argv=None):
         os.environ["B200_LP_CONV"] = a.lp_conv
     if a.learned:
         return learned(a)
+    if a.richardson:
+        return richardson(a)
     import torch
     import b200dwf
     from b200dwf import synth
@@ -85,6 +97,28 @@ def main(argv=None):
         nbytes = vh * (a.ls * 2 * SPINOR_BYTES[prec] + 8 * LINK_BYTES[prec])
         out.update(bytes_per_call=nbytes, gbs=nbytes / (us * 1e-6) / 1e9)
     print(json.dumps(out))
+
+
+def richardson(a):
+    import time
+    import torch
+    import b200dwf
+    from b200dwf import synth
+    from b200dwf.hmc import INNER_TOL2
+    prec = b200dwf.PREC_NAMES[a.richardson]
+    op = b200dwf.DomainWall(a.lattice, a.ls, a.mq, a.m0)
+    op.set_config(synth.gauge_field(a.lattice, 1234567, "near", eps=0.3))
+    b, x = op.new_field(0), op.new_field(0)
+    op.convert(b, synth.spinor_field(a.lattice, a.ls, 7654321))
+    op.richardson(x, b, prec, 1e-20, 1, INNER_TOL2[prec], 30)    # untimed: buffers, autotuner
+    x.zero()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    nout, nin, diff, rc = op.richardson(x, b, prec, 1e-20, 1, INNER_TOL2[prec], a.inner_iters)
+    sec = time.perf_counter() - t0
+    print(json.dumps({"lattice": a.lattice, "Ls": a.ls, "richardson": a.richardson,
+                      "inner_tol2": INNER_TOL2[prec], "outer": nout, "inner": nin,
+                      "seconds": sec, "ms_per_inner": sec * 1e3 / max(nin, 1)}))
 
 
 def learned_flops(vh, ls, hidden):
