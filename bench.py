@@ -124,6 +124,25 @@ def vh_of(lattice):
     return int(np.prod(lattice)) // 2
 
 
+# kernel template of each FP64 hop variant (the autotuner's variant numbers)
+HOP_KERNEL_OF_VARIANT = {0: "dwf_hop_kernel", 4: "dwf_hop_kernel", 1: "dwf_hop_tma_kernel",
+                         2: "dwf_hop_tma_kernel", 3: "dwf_hop_tma_kernel", 7: "dwf_hop_tma_kernel"}
+
+
+def dagger_hop_kernel(vh):
+    """Name of the FP64 dagger-hop kernel the autotuner kept at this Vh
+    (epilogue EPI_DDAGEO), from the library's tuning table."""
+    import b200dwf
+    for ln in b200dwf.tuning_table().splitlines():
+        f = dict(kv.split("=", 1) for kv in ln.split())
+        if (f.get("vh") == str(vh) and f.get("ls") == str(LS) and f.get("prec") == "f64"
+                and f.get("epi") == "1" and f.get("fk") == "0"):
+            v = int(f["variant"])
+            return "%s<16,f64,EPI_DDAGEO> (mult_dag Deo, autotuned variant %d)" % (
+                HOP_KERNEL_OF_VARIANT.get(v, "hop variant"), v)
+    return "fused FP64 dagger hop (mult_dag Deo, EPI_DDAGEO)"
+
+
 def read_peaks():
     path = os.path.join(REPO, "MEASURED_PEAKS.json")
     try:
@@ -972,7 +991,7 @@ def b200_arm(args, rank, world, local_rank):
         # Shamir b=1, c=0, alpha=1: the D_eo pre-factor is the identity, so a
         # step is two hop launches (mult Deo, mult_dag Deo)
         "gpu_launches": 2 * args.steps,
-        "roofline": {"kernel": "dwf_hop_tma_kernel<16,f64,EPI_DDAGEO> (mult_dag Deo, autotuned variant)",
+        "roofline": {"kernel": dagger_hop_kernel(vh),
                      "bound": "hbm",
                      "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
