@@ -152,12 +152,25 @@ int b200_dwf_inject_wait_failure(b200_dwf_t *op, int direction);
  * sites; fn must fill that field's two ghost slices (the t slowest index, so
  * each slice is one contiguous range of (Lx Ly Lz / 2) site columns) from the
  * neighbours' interior edge slices, ordered after the work already queued on
- * `stream`, and return 0.  Outputs on the ghost slices are not meaningful.
+ * `stream`, and return 0.  The hops leave the output's ghost slices
+ * unwritten (or, where they also reduce |out|^2, not meaningful).
  * With a hook set, the solvers and the learned preconditioner refuse the
  * plan (B200_EINVAL), and b200_field_norm2/dot cover the whole extended
  * lattice.  fn = NULL removes the hook. */
 typedef int (*b200_halo_fn)(void *ctx, void *field, int prec, void *stream);
 int b200_dwf_set_halo_exchange(b200_dwf_t *op, b200_halo_fn fn, void *ctx);
+/* The same exchange in two halves, overlapped with the interior as the
+ * reference overlaps its bulk hop with the face transfer
+ * (afopr_Domainwall_5din_eo-tmpl.h:998-1101): start(ctx, field, prec, stream)
+ * begins filling the ghost slices, ordered after the work on `stream`, and
+ * returns; finish(...) makes `stream` wait until they are filled.  A hop
+ * then launches the sites whose t neighbours are the rank's own (t = 1 ..
+ * nt-2) between the two calls and the two edge slices after finish; the
+ * force kernels call both before they run.  Needs nt >= 2 own slices.
+ * Replaces a hook set by b200_dwf_set_halo_exchange; (NULL, NULL) removes
+ * both. */
+int b200_dwf_set_halo_exchange_split(b200_dwf_t *op, b200_halo_fn start, b200_halo_fn finish,
+                                     void *ctx);
 
 /* ---------------------------------------------------------------- fields
  * AField<REAL, ACCEL> BLAS (src/lib_alt_Accel/Field/afield-tmpl.h:637-720 ->

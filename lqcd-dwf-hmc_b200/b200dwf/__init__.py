@@ -68,6 +68,7 @@ def lib():
     L.b200_dwf_check_error.argtypes = [vp, vp]
     L.b200_dwf_inject_wait_failure.argtypes = [vp, ctypes.c_int]
     L.b200_dwf_set_halo_exchange.argtypes = [vp, HALO_FN, vp]
+    L.b200_dwf_set_halo_exchange_split.argtypes = [vp, HALO_FN, HALO_FN, vp]
     L.b200_field_axpby.argtypes = [vp, ctypes.c_int, vp, ctypes.c_double, vp, ctypes.c_double, vp]
     L.b200_field_norm2.argtypes = [vp, ctypes.c_int, vp, dp, vp]
     L.b200_field_dot.argtypes = [vp, ctypes.c_int, vp, vp, dp, vp]

@@ -13,8 +13,9 @@ first global t is even and every site keeps its global parity).  Its plan
 is an ordinary DomainWall on the periodic lattice {Lx, Ly, Lz, nt + 2}
 whose slices are its own nt slices, then the next rank's first slice (the
 back ghost), then the previous rank's last slice (the front ghost).  The
-kernels then read the previous rank's slice through their t wrap and need
-no change; outputs on the two ghost slices are not meaningful.  The global t
+kernels then read the previous rank's slice through their t wrap; a hop
+launch covers only the rank's own slices (the two ghost slices of its
+output stay unwritten).  The global t
 boundary phase is folded into the global last slice's t links (the force
 kernels apply the phase themselves to their link-free outer products, so
 the rank owning that slice applies it to those links' forces).  Before each
@@ -24,10 +25,14 @@ sites.  Since t is the slowest site index, each ghost slice is one
 contiguous range of (Lx Ly Lz / 2) site columns: the hook sends the field's
 first and last interior slices as they lie, with no pack kernel, through
 torch.distributed point-to-point calls (NCCL between GPUs, ordered on the
-plan's stream).  A face carries full 24 Ls-real columns, twice the
-reference's spin-projected half spinors, and the exchange is not overlapped
-with the interior; at 24^3 x 48 x 16 one FP64 face is 21 MB (about 27 us
-over NVLink beside a 700 us hop).
+plan's stream).  With overlap=True the hook comes in two halves
+(b200_dwf_set_halo_exchange_split): the transfer starts, the hop runs the
+sites whose t neighbours are the rank's own (t = 1 .. nt-2), the plan's
+stream waits for the transfer, and the two edge slices run last, as the
+reference overlaps its bulk hop with the face exchange.  A face carries full
+24 Ls-real columns, twice the reference's spin-projected half spinors; at
+24^3 x 48 x 16 one FP64 face is 21 MB (about 27 us over NVLink beside a
+700 us hop).
 
 The solvers and reductions of the plan would cover only the rank's
 extended lattice, so the plan refuses them; HaloDomainWall supplies the
@@ -143,23 +148,31 @@ class TorchComm:
         self.size = dist.get_world_size(group)
         self.nccl = dist.get_backend(group) == "nccl"
 
-    def exchange(self, split, first, last, back, front):
-        """front <- previous rank's last slice, back <- next rank's first
-        slice (every rank calls this with tensors of its own extended
-        field)."""
+    def start(self, split, first, last, back, front):
+        """Begin: front <- previous rank's last slice, back <- next rank's
+        first slice (every rank calls this with tensors of its own extended
+        field), ordered after the work on the current stream; returns what
+        finish() waits for."""
         if split.nranks != self.size or split.rank != self.rank:
             raise B200Error("the split's ranks are not this group's ranks")
         if self.size == 1:
             front.copy_(last)
             back.copy_(first)
-            return
+            return []
         d = self.dist
         ops = [d.P2POp(d.isend, last, split.next, self.group, 0),
                d.P2POp(d.irecv, front, split.prev, self.group, 0),
                d.P2POp(d.isend, first, split.prev, self.group, 1),
                d.P2POp(d.irecv, back, split.next, self.group, 1)]
-        for req in d.batch_isend_irecv(ops):
+        return d.batch_isend_irecv(ops)
+
+    def finish(self, reqs):
+        """The current stream (NCCL) or the host (gloo) waits for start()'s transfers."""
+        for req in reqs:
             req.wait()
+
+    def exchange(self, split, first, last, back, front):
+        self.finish(self.start(split, first, last, back, front))
 
     def sum(self, x):
         import torch
@@ -196,6 +209,14 @@ class ThreadComm:
         if first.is_cuda:
             torch.cuda.synchronize()
         hub.barrier.wait()                    # nobody overwrites a slice still being read
+
+    # the host-synchronised exchange cannot overlap anything: start does it all
+    def start(self, split, first, last, back, front):
+        self.exchange(split, first, last, back, front)
+        return []
+
+    def finish(self, reqs):
+        pass
 
     def sum(self, x):
         hub = self.hub
@@ -241,39 +262,77 @@ class HaloDomainWall:
     mult / mult_dag take every mode of DomainWall and the force entry points
     return this rank's interior link forces; fields live on the extended
     lattice (new_field), their ghost slices filled by the plan's exchange
-    hook when a stencil reads them.  norm2, dot and cg are global over the
+    hook when a stencil reads them.  overlap=True splits each exchange
+    around the hop's interior sites.  norm2, dot and cg are global over the
     ranks."""
 
-    def __init__(self, split, comm, Ls, mq, M0, b=1.0, c=0.0, alpha=1.0, bc=(1, 1, 1, -1)):
+    def __init__(self, split, comm, Ls, mq, M0, b=1.0, c=0.0, alpha=1.0, bc=(1, 1, 1, -1),
+                 overlap=False):
         self.split = split
         self.comm = comm
         self.Ls = Ls
         self.bc_t = bc[3]
+        self.overlap = bool(overlap)
         self.op = DomainWall(split.ext, Ls, mq, M0, b, c, alpha, bc=(bc[0], bc[1], bc[2], 1))
         self._err = None
-        self._hook = HALO_FN(self._exchange)          # kept alive with the plan
-        check(lib().b200_dwf_set_halo_exchange(self.op.handle, self._hook, None))
+        self._pending = {}
+        # the hooks are kept alive with the plan
+        if self.overlap:
+            self._hooks = (HALO_FN(self._start), HALO_FN(self._finish))
+            check(lib().b200_dwf_set_halo_exchange_split(self.op.handle, *self._hooks, None))
+        else:
+            self._hooks = (HALO_FN(self._exchange),)
+            check(lib().b200_dwf_set_halo_exchange(self.op.handle, self._hooks[0], None))
         self.n_interior = 24 * Ls * split.nvol_half   # reals of one parity's interior
 
     def close(self):
         if self.op is not None:
-            check(lib().b200_dwf_set_halo_exchange(self.op.handle, HALO_FN(), None))
+            if self.overlap:
+                check(lib().b200_dwf_set_halo_exchange_split(self.op.handle, HALO_FN(), HALO_FN(),
+                                                             None))
+            else:
+                check(lib().b200_dwf_set_halo_exchange(self.op.handle, HALO_FN(), None))
             self.op = None
 
-    # the hook ---------------------------------------------------------
+    # the hooks --------------------------------------------------------
+    def _views(self, field, prec):
+        import torch
+        nbytes = lib().b200_dwf_field_bytes(self.op.handle, prec)
+        buf = torch.as_tensor(_CudaBytes(field, nbytes), device="cuda")
+        return _slices(buf, self.split.nt)
+
+    def _on_stream(self, stream, fn):
+        import torch
+        if stream:
+            with torch.cuda.stream(torch.cuda.ExternalStream(stream)):
+                return fn()
+        return fn()
+
     def _exchange(self, ctx, field, prec, stream):
         try:
-            import torch
-            nbytes = lib().b200_dwf_field_bytes(self.op.handle, prec)
-            buf = torch.as_tensor(_CudaBytes(field, nbytes), device="cuda")
-            views = _slices(buf, self.split.nt)
-            if stream:
-                with torch.cuda.stream(torch.cuda.ExternalStream(stream)):
-                    self.comm.exchange(self.split, *views)
-            else:
-                self.comm.exchange(self.split, *views)
+            views = self._views(field, prec)
+            self._on_stream(stream, lambda: self.comm.exchange(self.split, *views))
             return 0
         except BaseException as e:                     # reported by _call
+            self._err = e
+            return 1
+
+    def _start(self, ctx, field, prec, stream):
+        try:
+            views = self._views(field, prec)
+            reqs = self._on_stream(stream, lambda: self.comm.start(self.split, *views))
+            self._pending[field] = (views, reqs)       # the views live until finish
+            return 0
+        except BaseException as e:
+            self._err = e
+            return 1
+
+    def _finish(self, ctx, field, prec, stream):
+        try:
+            _, reqs = self._pending.pop(field)
+            self._on_stream(stream, lambda: self.comm.finish(reqs))
+            return 0
+        except BaseException as e:
             self._err = e
             return 1
 

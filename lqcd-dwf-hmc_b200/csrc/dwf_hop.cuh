@@ -359,6 +359,7 @@ struct HopParams {
   const double* skip;    // when non-null and *skip != 0 the launch does nothing
                          // (lets a captured solver iteration replay as a no-op)
   int vh, nx2, ny, nz, nt, ls;
+  int site0, site_end;   // output sites [site0, site_end) of this launch (the plan: 0, vh)
   int ieo;               // output parity (0 even, 1 odd)
   double bc[4];
 };
@@ -564,8 +565,8 @@ dwf_hop_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename Sto
   const int warp = tid >> 5;
   const int g = lane / LS;
   const int s = lane - g * LS;
-  const int site = (blockIdx.x * WARPS + warp) * G + g;
-  const bool active = (g < G) && (site < p.vh);
+  const int site = p.site0 + (blockIdx.x * WARPS + warp) * G + g;
+  const bool active = (g < G) && (site < p.site_end);
   const size_t vh = p.vh;
 
   R acc[24];
@@ -741,8 +742,8 @@ dwf_hop_pair_kernel(const HopParams p, const __grid_constant__ ChainCoef<typenam
   const int warp = tid >> 5;
   const int g = lane / H;
   const int j = lane - g * H;
-  const int site = (blockIdx.x * WARPS + warp) * G + g;
-  const bool active = (g < G) && (site < p.vh);
+  const int site = p.site0 + (blockIdx.x * WARPS + warp) * G + g;
+  const bool active = (g < G) && (site < p.site_end);
   const size_t vh = p.vh;
   const int s0 = j, s1 = j + H;
 
@@ -971,8 +972,8 @@ dwf_hop_pair_pf_kernel(const HopParams p, const __grid_constant__ ChainCoef<type
   const int warp = tid >> 5;
   const int g = lane / H;
   const int j = lane - g * H;
-  const int site = (blockIdx.x * WARPS + warp) * G + g;
-  const bool active = (g < G) && (site < p.vh);
+  const int site = p.site0 + (blockIdx.x * WARPS + warp) * G + g;
+  const bool active = (g < G) && (site < p.site_end);
   const size_t vh = p.vh;
   const int s0 = j, s1 = j + H;
 
@@ -1109,8 +1110,8 @@ dwf_hop_tma_kernel(const HopParams p, const __grid_constant__ ChainCoef<typename
   const int warp = tid >> 5;
   const int g = lane / LS;
   const int s = lane - g * LS;
-  const int site = (blockIdx.x * WARPS + warp) * G + g;
-  const bool active = (g < G) && (site < p.vh);
+  const int site = p.site0 + (blockIdx.x * WARPS + warp) * G + g;
+  const bool active = (g < G) && (site < p.site_end);
   const bool issuer = (g < G) && (s == 0);
   unsigned char* wbase = smem_raw + (size_t)warp * WBA;
   const size_t vh = p.vh;
@@ -1275,8 +1276,8 @@ dwf_hop_tma_pair_kernel(const HopParams p, const __grid_constant__ ChainCoef<typ
   const int warp = tid >> 5;
   const int g = lane / H;
   const int j = lane - g * H;
-  const int site = (blockIdx.x * WARPS + warp) * G + g;
-  const bool active = (g < G) && (site < p.vh);
+  const int site = p.site0 + (blockIdx.x * WARPS + warp) * G + g;
+  const bool active = (g < G) && (site < p.site_end);
   const bool issuer = (g < G) && (j == 0);
   unsigned char* wbase = smem_raw + (size_t)warp * WBA;
   const size_t vh = p.vh;

@@ -161,7 +161,8 @@ struct b200_dwf {
   double* sc_host = nullptr;    // pinned mirror (also of the multishift scalars)
   int* err_host = nullptr;      // pinned mirror of err
   bool async_calls = false;     // mult / force return without synchronising (b200_dwf_set_async)
-  b200_halo_fn halo_fn = nullptr;   // fills a field's ghost t-slices before a stencil reads it
+  b200_halo_fn halo_fn = nullptr;   // fills (or starts filling) a field's ghost t-slices
+  b200_halo_fn halo_finish = nullptr;  // with the split hooks: waits for that filling
   void* halo_ctx = nullptr;
   int inject_dir = -1;          // hop direction whose bulk-copy wait reports failure (-1: none)
   double* stage = nullptr;      // device f64 staging for convert/reverse
@@ -238,6 +239,8 @@ HopParams hop_base(const b200_dwf* op, int prec, int ieo, int epi, int fk = F_NO
   p.links = op->links[link_format_for(prec)];
   p.vh = op->g.vh; p.nx2 = op->g.nx2; p.ny = op->g.ny; p.nz = op->g.nz; p.nt = op->g.nt;
   p.ls = op->g.ls;
+  p.site0 = 0;
+  p.site_end = op->g.vh;
   p.ieo = ieo;
   p.ce = 1.0;
   p.err = op->err;
@@ -357,11 +360,17 @@ int forced_variant() {
 // slice, then the previous rank's last); a stencil reads the previous rank's
 // slice through the t wrap.  Before a kernel reads a field at neighbouring
 // sites, the host's exchange hook fills that field's ghost slices.
-static int halo(b200_dwf* op, const void* f, int prec, cudaStream_t st) {
-  if (!op->halo_fn || !f) return 0;
-  const int rc = op->halo_fn(op->halo_ctx, const_cast<void*>(f), prec, (void*)st);
+static int halo_call(b200_dwf* op, b200_halo_fn fn, const void* f, int prec, cudaStream_t st) {
+  if (!fn || !f) return 0;
+  const int rc = fn(op->halo_ctx, const_cast<void*>(f), prec, (void*)st);
   if (rc) return fail(B200_EINVAL, "the halo exchange hook failed (%d)", rc);
   return 0;
+}
+
+// the whole exchange: start, and finish where the hooks are split
+static int halo(b200_dwf* op, const void* f, int prec, cudaStream_t st) {
+  const int rc = halo_call(op, op->halo_fn, f, prec, st);
+  return rc ? rc : halo_call(op, op->halo_finish, f, prec, st);
 }
 
 static int no_halo(const b200_dwf* op, const char* what) {
@@ -372,12 +381,9 @@ static int no_halo(const b200_dwf* op, const char* what) {
               what);
 }
 
-int run_hop(b200_dwf* op, int prec, HopParams& p, cudaStream_t st) {
+// The hop variant for p (pinned, tuned earlier, or tuned now on p's sites).
+static int select_variant(b200_dwf* op, int prec, HopParams& p, cudaStream_t st) {
   int variant = 0;
-  if (op->halo_fn) {
-    const int hrc = halo(op, p.in, prec, st);
-    if (hrc) return hrc;
-  }
   const int fv = forced_variant();
   if (fv >= 0 && variant_supported(prec, op->g.ls, fv)) {
     variant = fv;
@@ -395,6 +401,47 @@ int run_hop(b200_dwf* op, int prec, HopParams& p, cudaStream_t st) {
     }
   }
   p.variant = variant;
+  return 0;
+}
+
+int run_hop(b200_dwf* op, int prec, HopParams& p, cudaStream_t st) {
+  int rc;
+  if (op->halo_fn && !p.red) {
+    // The two ghost t-slices come last and their outputs are not meaningful:
+    // a launch that writes no block partials skips them.  With split hooks
+    // the sites whose t neighbours are this rank's own (t = 1 .. nt-2) run
+    // while the edge slices travel, the two edge slices after.
+    const int slice = op->g.nx2 * op->g.ny * op->g.nz;
+    const int nt = op->g.nt - 2;
+    if (op->halo_finish) {
+      if ((rc = halo_call(op, op->halo_fn, p.in, prec, st))) return rc;
+      HopParams pi = p;
+      pi.site0 = slice;
+      pi.site_end = (nt - 1) * slice;
+      const bool interior = pi.site_end > pi.site0;
+      if (interior) {
+        if ((rc = select_variant(op, prec, pi, st))) return rc;
+        B200_CHECK_CUDA(launch_hop(prec, pi, op->coefs, st));
+      }
+      if ((rc = halo_call(op, op->halo_finish, p.in, prec, st))) return rc;
+      HopParams pb = p;
+      pb.site0 = 0;
+      pb.site_end = slice;
+      if (interior) pb.variant = pi.variant;
+      else if ((rc = select_variant(op, prec, pb, st))) return rc;
+      B200_CHECK_CUDA(launch_hop(prec, pb, op->coefs, st));
+      pb.site0 = (nt - 1) * slice;
+      pb.site_end = nt * slice;
+      B200_CHECK_CUDA(launch_hop(prec, pb, op->coefs, st));
+      p.variant = pb.variant;
+      return 0;
+    }
+    if ((rc = halo(op, p.in, prec, st))) return rc;
+    p.site_end = nt * slice;
+  } else if (op->halo_fn) {
+    if ((rc = halo(op, p.in, prec, st))) return rc;
+  }
+  if ((rc = select_variant(op, prec, p, st))) return rc;
   B200_CHECK_CUDA(launch_hop(prec, p, op->coefs, st));
   return 0;
 }
@@ -843,7 +890,18 @@ int b200_dwf_mult(b200_dwf_t* op, int prec, void* v, const void* w, const char* 
 int b200_dwf_set_halo_exchange(b200_dwf_t* op, b200_halo_fn fn, void* ctx) {
   if (!op) return fail(B200_EINVAL, "null argument");
   op->halo_fn = fn;
+  op->halo_finish = nullptr;
   op->halo_ctx = fn ? ctx : nullptr;
+  return 0;
+}
+
+int b200_dwf_set_halo_exchange_split(b200_dwf_t* op, b200_halo_fn start, b200_halo_fn finish,
+                                     void* ctx) {
+  if (!op || (!start) != (!finish)) return fail(B200_EINVAL, "start and finish go together");
+  if (start && op->g.nt < 4) return fail(B200_EINVAL, "a rank needs at least 2 t slices of its own");
+  op->halo_fn = start;
+  op->halo_finish = finish;
+  op->halo_ctx = start ? ctx : nullptr;
   return 0;
 }
 

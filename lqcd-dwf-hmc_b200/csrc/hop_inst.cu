@@ -33,7 +33,7 @@ cudaError_t run_mb(const HopParams& p, const ChainCoefs& c, cudaStream_t st) {
   }
   const ChainCoef<R>& kc = *reinterpret_cast<const ChainCoef<R>*>(
       std::is_same<R, double>::value ? (const void*)&c.d : (const void*)&c.f);
-  k<<<hop_grid(LS, p.vh), 128, smem, st>>>(p, kc);
+  k<<<hop_grid(LS, p.site_end - p.site0), 128, smem, st>>>(p, kc);
   return cudaGetLastError();
 }
 
@@ -51,7 +51,7 @@ cudaError_t run_tma(const HopParams& p, const ChainCoefs& c, cudaStream_t st) {
   }
   const ChainCoef<R>& kc = *reinterpret_cast<const ChainCoef<R>*>(
       std::is_same<R, double>::value ? (const void*)&c.d : (const void*)&c.f);
-  k<<<hop_grid(LS, p.vh), 128, smem, st>>>(p, kc);
+  k<<<hop_grid(LS, p.site_end - p.site0), 128, smem, st>>>(p, kc);
   return cudaGetLastError();
 }
 
@@ -68,7 +68,7 @@ cudaError_t run_pair(const HopParams& p, const ChainCoefs& c, cudaStream_t st) {
     attr_done = true;
   }
   const ChainCoef<R>& kc = *reinterpret_cast<const ChainCoef<R>*>(&c.f);
-  k<<<hop_pair_grid(LS, p.vh), 128, smem, st>>>(p, kc);
+  k<<<hop_pair_grid(LS, p.site_end - p.site0), 128, smem, st>>>(p, kc);
   return cudaGetLastError();
 }
 
@@ -84,7 +84,7 @@ cudaError_t run_pair_pf(const HopParams& p, const ChainCoefs& c, cudaStream_t st
     attr_done = true;
   }
   const ChainCoef<R>& kc = *reinterpret_cast<const ChainCoef<R>*>(&c.f);
-  k<<<hop_pair_grid(LS, p.vh), 128, smem, st>>>(p, kc);
+  k<<<hop_pair_grid(LS, p.site_end - p.site0), 128, smem, st>>>(p, kc);
   return cudaGetLastError();
 }
 
@@ -101,7 +101,7 @@ cudaError_t run_tma_pair(const HopParams& p, const ChainCoefs& c, cudaStream_t s
     attr_done = true;
   }
   const ChainCoef<R>& kc = *reinterpret_cast<const ChainCoef<R>*>(&c.f);
-  k<<<hop_pair_grid(LS, p.vh), 128, smem, st>>>(p, kc);
+  k<<<hop_pair_grid(LS, p.site_end - p.site0), 128, smem, st>>>(p, kc);
   return cudaGetLastError();
 }
 

@@ -8,8 +8,9 @@ no kernel waits for another.  The slabs have different t extents, so no two
 plans share a geometry (plans of one geometry share their work fields).
 The inputs' ghost slices are filled with garbage first: every neighbour
 value a rank uses must come through the hook.  Checked: all 13 modes x dag,
-the force (force_udiv, force_udiv1 H / Hdag), reduced-precision storage,
-and the distributed CG against the plan's CG on the whole lattice."""
+the force (force_udiv, force_udiv1 H / Hdag), with the exchange whole before
+each hop and split around the interior sites (overlap), reduced-precision
+storage, and the distributed CG against the plan's CG on the whole lattice."""
 import threading
 
 import numpy as np
@@ -30,7 +31,7 @@ def rel(a, b):
     return np.linalg.norm(a - b) / np.linalg.norm(b)
 
 
-def run_ranks(nts, b, c, u, work, ls=LS, bc=(1, 1, 1, -1)):
+def run_ranks(nts, b, c, u, work, ls=LS, bc=(1, 1, 1, -1), overlap=False):
     """work(rank, split, hop) in one thread per rank; returns the results in
     rank order (re-raises the first failure)."""
     from b200dwf.halo import HaloDomainWall, ThreadComm, ThreadHub, TSplit
@@ -40,7 +41,8 @@ def run_ranks(nts, b, c, u, work, ls=LS, bc=(1, 1, 1, -1)):
     def body(rank):
         try:
             split = TSplit(LAT, nts, rank)
-            hop = HaloDomainWall(split, ThreadComm(hub, rank), ls, MQ, M0, b, c, bc=bc)
+            hop = HaloDomainWall(split, ThreadComm(hub, rank), ls, MQ, M0, b, c, bc=bc,
+                                 overlap=overlap)
             hop.set_config(split.gauge(u, bc[3]))
             res[rank] = work(rank, split, hop)
             hop.close()
@@ -74,8 +76,9 @@ def whole(b, c, u):
     return op
 
 
+@pytest.mark.parametrize("overlap", [False, True])
 @pytest.mark.parametrize("nts,b,c", SPLITS)
-def test_all_modes_match_the_whole_lattice(nts, b, c, monkeypatch):
+def test_all_modes_match_the_whole_lattice(nts, b, c, overlap, monkeypatch):
     from b200dwf.halo import assemble_spinor
     monkeypatch.setenv("B200_HOP_VARIANT", "0")
     u = synth.gauge_field(LAT, 41, "hot")
@@ -99,14 +102,15 @@ def test_all_modes_match_the_whole_lattice(nts, b, c, monkeypatch):
                 out[(mode, dag)] = hop.reverse(gv)
         return out
 
-    parts = run_ranks(nts, b, c, u, work)
+    parts = run_ranks(nts, b, c, u, work, overlap=overlap)
     for key, r in ref.items():
         got = assemble_spinor([p[key] for p in parts], LS)
         assert rel(got, r) < 1e-14, (key, rel(got, r))
 
 
+@pytest.mark.parametrize("overlap", [False, True])
 @pytest.mark.parametrize("nts,b,c", SPLITS)
-def test_force_matches_the_whole_lattice(nts, b, c):
+def test_force_matches_the_whole_lattice(nts, b, c, overlap):
     from b200dwf.halo import assemble_links
     u = synth.gauge_field(LAT, 43, "hot")
     eta = synth.spinor_field(LAT, LS, 44)
@@ -123,7 +127,7 @@ def test_force_matches_the_whole_lattice(nts, b, c):
         hop.convert(gz, spoiled(split, zeta))
         return [hop.force_udiv(ge), hop.force_udiv1("H", gz, ge), hop.force_udiv1("Hdag", ge, gz)]
 
-    parts = run_ranks(nts, b, c, u, work)
+    parts = run_ranks(nts, b, c, u, work, overlap=overlap)
     for k in range(3):
         got = assemble_links([p[k] for p in parts])
         assert rel(got, ref[k]) < 1e-13, (k, rel(got, ref[k]))
