@@ -17,7 +17,7 @@ import torch.multiprocessing as mp
 
 from b200dwf import synth
 from b200dwf.halo import (TSplit, ThreadComm, ThreadHub, TorchComm, _slices, assemble_links,
-                          assemble_spinor, extend_links)
+                          assemble_spinor)
 
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LAT = [4, 2, 2, 12]
