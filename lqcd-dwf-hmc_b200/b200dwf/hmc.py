@@ -344,13 +344,12 @@ class Solver:
         return n
 
     def _remember(self, op, x):
-        from . import Field
         if len(self._hist) == self.chrono_depth:
             f = self._hist.pop(0)
         elif self._spare:
             f = self._spare.pop()
         else:
-            f = Field(op)
+            f = op.new_field()
         op.axpby(f, 1.0, x, 0.0)
         self._hist.append(f)
 
@@ -359,11 +358,10 @@ class Solver:
         G c = f with G_ij = Re<v_i, A v_j>, f_i = Re<v_i, b>, solved on the
         eigenvectors of G above 1e-13 of its largest eigenvalue (successive
         solutions are nearly parallel)."""
-        from . import Field
         v = self._hist
         k = len(v)
         if self._tmp is None:
-            self._tmp = Field(op)
+            self._tmp = op.new_field()
         t = self._tmp
         g = np.empty((k, k))
         f = np.empty(k)
