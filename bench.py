@@ -852,6 +852,44 @@ def b200_arm(args, rank, world, local_rank):
     torch.cuda.synchronize()
     t_sync = replicas.max_over_ranks(q2.elapsed_time(q3) / 1e3, dist, "cuda")
     e2e_sync_value = replicas.whole_job_rate(step_bytes * ne, t_sync, world) / 1e9
+
+    # The host link the end-to-end step runs on: pinned copies of one field
+    # each way alone and both ways at once (CUDA events), and the step's
+    # lower bound on it (its download beside its upload).
+    d_scr = torch.empty(h_in.numel(), dtype=torch.float64, device="cuda")
+    d_scr2 = torch.empty_like(d_scr)
+    h_dn = h_outs[0][0]
+
+    def timed_copies(pairs, reps=3):
+        starts, ends = [], []
+        for st, fn in pairs:
+            with torch.cuda.stream(st):
+                fn()                                   # warm
+        torch.cuda.synchronize()
+        for st, _ in pairs:
+            a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            starts.append(a)
+            ends.append(z)
+        for st, fn in pairs:
+            with torch.cuda.stream(st):
+                for _ in range(reps):
+                    fn()
+        for (st, _), z in zip(pairs, ends):
+            z.record(st)
+        torch.cuda.synchronize()
+        return [reps * nbytes / (a.elapsed_time(z) * 1e-3) / 1e9 for a, z in zip(starts, ends)]
+
+    up = (s_in, lambda: d_scr.copy_(h_in, non_blocking=True))
+    dn = (s_out, lambda: h_dn.copy_(d_scr2, non_blocking=True))
+    h2d_alone = timed_copies([up])[0]
+    d2h_alone = timed_copies([dn])[0]
+    h2d_both, d2h_both = timed_copies([up, dn])
+    step_bound_s = max(nbytes / (h2d_both * 1e9), 2 * nbytes / (d2h_both * 1e9))
+    host_link = {"h2d_gbs": h2d_alone, "d2h_gbs": d2h_alone, "h2d_gbs_both_ways": h2d_both,
+                 "d2h_gbs_both_ways": d2h_both, "step_bound_ms": step_bound_s * 1e3,
+                 "step_ms": t_e2e * 1e3 / ne, "frac_of_link_bound": step_bound_s / (t_e2e / ne)}
+    del d_scr, d_scr2, h_dn
     del h_in, h_outs, h_in_np, h_out_np, ws, v1s, v2s
 
     # FP64 CG time to solution, |r|/|b| < 1e-10
@@ -1002,7 +1040,7 @@ def b200_arm(args, rank, world, local_rank):
                 "d2h_bytes_per_step": 2 * nbytes, "steps": ne,
                 "how": "pipelined: convert_async / 2 hops / 2 reverse_async on three streams, "
                        "double-buffered, step k+1's upload overlapping step k's download",
-                "synchronous_calls_value": e2e_sync_value},
+                "synchronous_calls_value": e2e_sync_value, "host_link": host_link},
     }
     # the trajectory's headline numbers as short top-level keys
     if trajectory:
