@@ -44,6 +44,10 @@ MQ, M0 = 0.01, 1.8
 MS = 0.04                   # strange-quark mass of the 2+1-flavour trajectory
 SEED_U, SEED_B = 1234567, 7654321
 BYTES_PER_HALF_SITE = LS * 24 * (8 + 8) + 8 * 18 * 8
+# flops of one fused D_eo per 4D half-site: the reference's count for the
+# Wilson hop and the M5 pre-factor on every slice, halved for one parity
+# (afopr_Domainwall_5din_eo-tmpl.h:1445-1448, 1476, 1492)
+FLOPS_PER_HALF_SITE = 1488 * LS
 REF_HARNESS = os.path.join(REPO, "oracle", "_ref", "ref_harness")
 WORKLOAD = "dwf_eo_dslash_24x24x24x48_Ls16_f64"
 METRIC = "sec/trajectory 24^3x48 Ls=16: mixed+learned vs plain FP64 on B200; Dslash GB/s"
@@ -439,6 +443,7 @@ def reference_arm(args, rank, world):
         "n_gpus": args.gpus,
         "steps": reps, "warmup": max(1, args.warmup), "ms_per_step": t_step * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "dslash_gflops": 2 * FLOPS_PER_HALF_SITE * vh_of(args.lattice) / t_step / 1e9,
         "config": {"workload": WORKLOAD, "lattice": args.lattice, "Ls": LS, "M0": M0, "mq": MQ,
                    "links": "near-unit exp(i*0.3*H) + 2 stout rho=0.1", "parallelism": "replicas"},
         "cpu_baseline": {"value": gbs, "unit": "GB/s", "cores": threads, "kind": "reference",
@@ -1022,6 +1027,8 @@ def b200_arm(args, rank, world, local_rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_total * 1e3 / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
+        "dslash_gflops": replicas.whole_job_rate(2 * FLOPS_PER_HALF_SITE * vh * args.steps, t_total,
+                                                 world) / 1e9,
         "config": {"workload": WORKLOAD, "lattice": lattice, "Ls": LS, "M0": M0, "mq": MQ,
                    "links": "near-unit exp(i*0.3*H) + 2 stout rho=0.1", "parallelism": "replicas",
                    "l2": "inputs larger than L2 (%.0f MB per field)" % (nbytes / 1e6)},
@@ -1035,6 +1042,7 @@ def b200_arm(args, rank, world, local_rank):
                      "frac": achieved / peak, "traffic": traffic,
                      "traffic_note": "ncu DRAM bytes of a 16^3x32 launch scaled by sites",
                      "algorithmic_bytes_per_launch": BYTES_PER_HALF_SITE * vh,
+                     "gflops": FLOPS_PER_HALF_SITE * vh / t_hop / 1e9,
                      "launch_us": t_hop * 1e6, "target_frac": 0.7},
         "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": nbytes,
                 "d2h_bytes_per_step": 2 * nbytes, "steps": ne,
