@@ -96,6 +96,8 @@ struct MsUpdParams {
   int nblocks;
   Geom g;
   void* const* win;      // windowed mode: device array [kMaxWin] of residual slots (else null)
+  void* p0s;             // windowed mode with x_0 deferred to the flush: p_0 at the window's
+                         // start (else null; x_0 is then updated every iteration)
 };
 cudaError_t launch_ms_update(int prec, const MsUpdParams& p, const ChainCoefs& c, cudaStream_t st);
 // Windowed mode: once the window is full (or the solve is over) apply the

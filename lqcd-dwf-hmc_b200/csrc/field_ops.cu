@@ -338,18 +338,20 @@ ms_update_kernel(MsUpdParams p, const __grid_constant__ ChainCoef<typename Store
 #pragma unroll
   for (int i = 0; i < 24; ++i) { rv[i] = 0; pv[i] = 0; }
   double nrm = 0.0;
+  // with p0s set, x_0 is left to the window flush like the other shifts
+  const bool defer_x0 = p.p0s != nullptr;
   if (active) {
     R xv[24];
     St::load(p.r, vh, LS, site, s, rv);
-    St::load(p.xs[0], vh, LS, site, s, xv);
+    if (!defer_x0) St::load(p.xs[0], vh, LS, site, s, xv);
     St::load(p.ps[0], vh, LS, site, s, pv);
 #pragma unroll
     for (int i = 0; i < 24; ++i) {
-      xv[i] = fma(-beta, pv[i], xv[i]);
+      if (!defer_x0) xv[i] = fma(-beta, pv[i], xv[i]);
       pv[i] = fma(alpha, pv[i], rv[i]);
       nrm += (double)pv[i] * (double)pv[i];
     }
-    St::store(p.xs[0], vh, LS, site, s, xv);
+    if (!defer_x0) St::store(p.xs[0], vh, LS, site, s, xv);
     St::store(p.ps[0], vh, LS, site, s, pv);
   }
   if (p.y0) {         // null: identity pre-factor, the next hop reads p_0
@@ -494,16 +496,18 @@ __global__ void ms_scalar_kernel(int step, const double* partials, int n, double
         // every earlier direction): pp_i = zeta_i^2 |r|^2 + alpha_i^2 pp_i
         const int w = (int)st[MS_WIN];
         const double rrn = rr * st[MS_SNORM];
-        for (int i = 1; i < nact; ++i) {
+        // shift 0 too (beta, alpha, zeta = 1): its p_0 is updated every
+        // iteration, its x_0 by the flush where that is deferred
+        for (int i = 0; i < nact; ++i) {
           double* pc = st + kMsCoef + i * (kMaxWin + 1);
           double* xc = st + kMsXCoef + i * (kMaxWin + 1);
-          const double bs = betas[i], as = alphas[i], zt = zeta[i];
+          const double bs = i ? betas[i] : beta, as = i ? alphas[i] : alpha, zt = i ? zeta[i] : 1.0;
           for (int j = 0; j <= w; ++j) {
             xc[j] -= bs * pc[j];
             pc[j] *= as;
           }
           pc[1 + w] = zt;
-          pp[i] = zt * zt * rrn + as * as * pp[i];
+          if (i) pp[i] = zt * zt * rrn + as * as * pp[i];
         }
       }
       st[MS_ALPHA_P] = alpha;
@@ -567,6 +571,23 @@ __global__ void __launch_bounds__(256) ms_flush_kernel(MsUpdParams p, long n2) {
 #pragma unroll
     for (int l = 0; l < kMaxWin; ++l)
       if (l < w) rv[l] = __ldcs(reinterpret_cast<const double2*>(p.win[l]) + e);
+    if (p.p0s) {
+      // x_0 += XC0 p_0(window start) + sum_l XC_l r_l; p_0 itself is current,
+      // and becomes the next window's start
+      const double* xc = cs + kMaxShift * (kMaxWin + 1);
+      double2* x0p = reinterpret_cast<double2*>(p.xs[0]) + e;
+      double2* s0p = reinterpret_cast<double2*>(p.p0s) + e;
+      const double2 ps0 = __ldcs(s0p);
+      const double2 pc0 = __ldcs(reinterpret_cast<const double2*>(p.ps[0]) + e);
+      double2 x = __ldcs(x0p);
+      x.x = fma(xc[0], ps0.x, x.x); x.y = fma(xc[0], ps0.y, x.y);
+#pragma unroll
+      for (int l = 0; l < kMaxWin; ++l) {
+        if (l < w) { x.x = fma(xc[1 + l], rv[l].x, x.x); x.y = fma(xc[1 + l], rv[l].y, x.y); }
+      }
+      __stcs(x0p, x);
+      __stcs(s0p, pc0);
+    }
     // the next shift's p_i, x_i are loaded while this shift is combined, so
     // every thread keeps two shifts' loads in flight
     double2 pn = make_double2(0.0, 0.0), xn = pn;
